@@ -1,0 +1,177 @@
+/*
+ * libpgx: C ABI of the B200 (sm_100a) engine behind pomerol's G2 / G / chi path.
+ *
+ * One context = one GPU, one CUDA stream, and every device buffer of one
+ * exact-diagonalisation problem (symmetry blocks, eigensystem, Boltzmann
+ * weights, rotated monomial operators).  Callers pass host pointers with
+ * explicit sizes; every entry point returns a PGX_* status and never throws.
+ * Complex numbers are interleaved (re, im) doubles.  Matrices are row-major.
+ *
+ * Each entry point names the reference code it replaces (pomerol 2.3 paths,
+ * relative to the reference project root).
+ */
+#ifndef PGX_H
+#define PGX_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PGX_OK 0
+#define PGX_ERR_ARG 1       /* invalid argument or size */
+#define PGX_ERR_OOM 2       /* device allocation failed */
+#define PGX_ERR_CUDA 3      /* CUDA runtime error */
+#define PGX_ERR_TIMEOUT 4   /* bounded device wait expired */
+#define PGX_ERR_NUMERIC 5   /* eigensolver did not converge / non-finite input */
+#define PGX_ERR_STATE 6     /* call order violated (e.g. rotate before eigh) */
+#define PGX_ERR_NODEV 7     /* no CUDA device */
+
+/* G2 evaluation flags */
+#define PGX_G2_EXACT 0           /* no coefficient filters */
+#define PGX_G2_REFERENCE_RULE 1  /* apply the reference's weight filter at block level */
+
+typedef struct pgx_ctx pgx_ctx;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int pgx_version(void);
+
+/* Create a context on `device` (one CUDA stream, no device memory yet). */
+int pgx_create(int device, pgx_ctx** out);
+/* Destroy a context and free all of its device memory. */
+int pgx_destroy(pgx_ctx* ctx);
+/* Message of the last failed call on this context ("" if none). */
+const char* pgx_last_error(const pgx_ctx* ctx);
+
+/* ------------------------------------------------------------------------
+ * Symmetry blocks and K1 eigensolve.
+ * Replaces: StatesClassification block sizes (StatesClassification.hpp:59-70)
+ * and HamiltonianPart::computeImpl / Hamiltonian::compute
+ * (HamiltonianPart.cpp:90-102, Hamiltonian.cpp:69-113).
+ * ------------------------------------------------------------------------ */
+
+/* Declare nblocks blocks of sizes dims[b] (real symmetric: is_complex = 0;
+ * complex Hermitian: 1).  Resets every per-problem device buffer. */
+int pgx_set_blocks(pgx_ctx* ctx, int32_t nblocks, const int32_t* dims, int32_t is_complex);
+
+/* Upload the block Hamiltonians: block b is dims[b]^2 consecutive (row-major)
+ * elements, blocks in order.  Host -> device copy only. */
+int pgx_set_hamiltonian(pgx_ctx* ctx, const double* H);
+
+/* Diagonalise every block in one launch (FP64).  Eigenvalues ascending per
+ * block; eigenvectors are the columns of each block's U.  The uploaded
+ * Hamiltonian is kept, so this can be re-run. */
+int pgx_eigh(pgx_ctx* ctx);
+
+/* Copy the eigensystem to the host: E (sum of dims), U (packed like H).
+ * Either pointer may be NULL. */
+int pgx_get_eigensystem(pgx_ctx* ctx, double* E, double* U);
+
+/* Ground energy min_b min E (Hamiltonian::computeGroundEnergy,
+ * Hamiltonian.cpp:125-130). */
+int pgx_ground_energy(pgx_ctx* ctx, double* E0);
+
+/* ------------------------------------------------------------------------
+ * K5 Boltzmann weights.
+ * Replaces: DensityMatrixPart::computeUnnormalized/normalize/truncate and
+ * DensityMatrix::compute/truncateBlocks (DensityMatrixPart.cpp:23-50,
+ * DensityMatrix.cpp:38-92).
+ * ------------------------------------------------------------------------ */
+
+/* w_s = exp(-beta (E_s - E0)) / Z for every state; w (sum of dims) and Z are
+ * copied out when non-NULL. */
+int pgx_weights(pgx_ctx* ctx, double beta, double* w, double* Z);
+
+/* Retained flag per block: any weight > tol (all blocks retained if never
+ * called). */
+int pgx_truncate_blocks(pgx_ctx* ctx, double tol, int32_t* retained);
+
+/* ------------------------------------------------------------------------
+ * K2 monomial-operator rotation.
+ * Replaces: MonomialOperator::prepare/compute (MonomialOperator.hpp:160-195,
+ * MonomialOperator.cpp:33-46), MonomialOperatorPart::computeImpl and
+ * setFromAdjoint (MonomialOperatorPart.cpp:48-111), FieldOperatorContainer::
+ * computeAll (FieldOperatorContainer.cpp:22-37).
+ * ------------------------------------------------------------------------ */
+
+/* Define a monomial operator by its Fock action.  Part p maps right block
+ * right_block[p] into left block left_block[p]; for state k (inner index) of
+ * the right block, target[k] is the inner index of O|k> in the left block (-1
+ * if O|k> = 0) and coef[k] its coefficient (Jordan-Wigner sign times the
+ * monomial's coefficient; real).  target/coef are concatenated over parts in
+ * order, dims[right_block[p]] entries per part.  Returns an operator id. */
+int pgx_op_define(pgx_ctx* ctx, int32_t nparts, const int32_t* right_block, const int32_t* left_block,
+                  const int32_t* target, const double* coef, int32_t* op_id);
+
+/* O'_p = U_L^dagger (O U_R) for every part of the operator, in one launch. */
+int pgx_op_rotate(pgx_ctx* ctx, int32_t op_id);
+
+/* New operator whose parts are the adjoints of `src`'s rotated parts
+ * (c from c^+).  Returns its id. */
+int pgx_op_adjoint(pgx_ctx* ctx, int32_t src, int32_t* op_id);
+
+/* Number of parts, and per part (right block, left block). */
+int pgx_op_info(pgx_ctx* ctx, int32_t op_id, int32_t* nparts, int32_t* right_block, int32_t* left_block);
+
+/* Copy part `part` of a rotated operator (d_left x d_right, row-major). */
+int pgx_op_read(pgx_ctx* ctx, int32_t op_id, int32_t part, double* out);
+
+/* ------------------------------------------------------------------------
+ * K3 pair-Lehmann sums: G and chi, plus <A>.
+ * Replaces: GreensFunction(Part) compute/operator() (GreensFunction.cpp:41-100,
+ * GreensFunctionPart.cpp:24-110, GreensFunction.hpp:123-136) and
+ * Susceptibility(Part) (Susceptibility.cpp:42-119, SusceptibilityPart.cpp:27-127,
+ * SusceptibilityPart.hpp:212-220), EnsembleAverage (EnsembleAverage.cpp:27-67).
+ * ------------------------------------------------------------------------ */
+
+/* G(z_n) = sum over parts (outer block o, inner block i) of
+ * sum_{a in o, b in i} F1_ab F2_ba (w_a + w_b) / (z_n - (E_b - E_a)),
+ * dropping residues with |R| <= coef_tol.  F1 is the part of op1 whose left
+ * block is o; F2 the part of op2 whose right block is o.  z: nz complex;
+ * out: nz complex. */
+int pgx_gf(pgx_ctx* ctx, int32_t op1, int32_t op2, int32_t nparts, const int32_t* outer, const int32_t* inner,
+           int32_t nz, const double* z, double coef_tol, double* out);
+
+/* chi(z_n) = -sum R/(z_n - P) + (|z_n| <= eps ? beta * W0 : 0), where pairs
+ * with |P| < pole_res go to the zero-pole weight W0 = sum A_ab B_ba w_a and the
+ * rest carry R = A_ab B_ba (w_a - w_b) (dropped if |R| <= coef_tol).  The
+ * zero-pole weight is also returned (complex) when zero_pole is non-NULL. */
+int pgx_susc(pgx_ctx* ctx, int32_t opA, int32_t opB, int32_t nparts, const int32_t* outer, const int32_t* inner,
+             int32_t nz, const double* z, double pole_res, double coef_tol, double beta, double* out,
+             double* zero_pole);
+
+/* <A> = sum over diagonal, retained parts of sum_a A_aa w_a (complex out). */
+int pgx_ensemble_average(pgx_ctx* ctx, int32_t op, double* out);
+
+/* ------------------------------------------------------------------------
+ * K4 two-particle Green's function.
+ * Replaces: TwoParticleGFPart::computeImpl/addMultiterm/operator()
+ * (TwoParticleGFPart.cpp:189-322, TwoParticleGFPart.hpp:475-495) and the
+ * frequency loop of TwoParticleGF::compute (TwoParticleGF.cpp:123-204).
+ * ------------------------------------------------------------------------ */
+
+/* One block chain <S1|O1|S2><S2|O2|S3><S3|O3|S4><S4|CX4|S1>: the operator ids
+ * in chain order (O1, O2, O3, CX4), the blocks S1..S4, the permutation of the
+ * frequencies {z1, z2, -z3} that the chain uses and its sign. */
+typedef struct pgx_g2_part {
+    int32_t op[4];
+    int32_t block[4];
+    int32_t perm[3];
+    int32_t sign;
+} pgx_g2_part;
+
+/* out[t] = sum over parts of the Lehmann sum at triple t = (z1, z2, z3)
+ * (z: 3*nfreq complex; out: nfreq complex).  Resonant terms use the delta
+ * rule |D| <= pole_res.  flags: PGX_G2_EXACT or PGX_G2_REFERENCE_RULE. */
+int pgx_g2(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, int32_t nfreq, const double* z,
+           double pole_res, double coef_tol, int32_t flags, double* out);
+
+/* Device time (ms) of the last pgx_g2 call and its dominant GEMM stage. */
+int pgx_g2_last_timing(pgx_ctx* ctx, double* total_ms, double* gemm_ms, double* gemm_flops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PGX_H */

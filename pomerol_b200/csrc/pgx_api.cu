@@ -1,0 +1,373 @@
+// extern "C" entry points of libpgx (declared in include/pgx.h).
+// Every call translates pgx::Error into a status code and a message; no
+// exception crosses the ABI.
+
+#include <algorithm>
+#include <numeric>
+
+#include "pgx_common.cuh"
+#include "pgx_internal.h"
+
+namespace pgx {
+void launch_retained(Problem& P, double tol, int* d_flags, cudaStream_t st);
+}
+
+using pgx::Error;
+
+namespace {
+
+template <typename F> int guarded(pgx_ctx* c, F&& f) {
+    if (!c) return PGX_ERR_ARG;
+    try {
+        PGX_CUDA(cudaSetDevice(c->device));
+        f();
+        c->last_error.clear();
+        return PGX_OK;
+    } catch (const Error& e) {
+        c->last_error = e.msg;
+        return e.code;
+    } catch (const std::bad_alloc&) {
+        c->last_error = "host allocation failed";
+        return PGX_ERR_OOM;
+    } catch (...) {
+        c->last_error = "unexpected host exception";
+        return PGX_ERR_ARG;
+    }
+}
+
+void reset_problem(pgx::Problem& P) {
+    for (auto* b : {&P.H, &P.work, &P.work2, &P.U, &P.E, &P.w, &P.dims_d, &P.moff_d, &P.eoff_d, &P.order_d, &P.status})
+        b->release();
+    for (auto& op : P.ops) {
+        op.mat.release();
+        op.target.release();
+        op.coef.release();
+    }
+    P = pgx::Problem();
+}
+
+}  // namespace
+
+extern "C" {
+
+int pgx_version(void) { return 10000; }
+
+int pgx_create(int device, pgx_ctx** out) {
+    if (!out) return PGX_ERR_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return PGX_ERR_NODEV;
+    }
+    if (device < 0 || device >= n) return PGX_ERR_ARG;
+    pgx_ctx* c = new (std::nothrow) pgx_ctx();
+    if (!c) return PGX_ERR_OOM;
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete c;
+        return PGX_ERR_CUDA;
+    }
+    *out = c;
+    return PGX_OK;
+}
+
+int pgx_destroy(pgx_ctx* c) {
+    if (!c) return PGX_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    reset_problem(c->P);
+    for (auto& b : c->scratch) b.release();
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return PGX_OK;
+}
+
+const char* pgx_last_error(const pgx_ctx* c) { return c ? c->last_error.c_str() : "null context"; }
+
+int pgx_set_blocks(pgx_ctx* c, int32_t nblocks, const int32_t* dims, int32_t is_complex) {
+    return guarded(c, [&] {
+        PGX_CHECK(nblocks > 0 && dims, PGX_ERR_ARG, "need at least one block");
+        for (int b = 0; b < nblocks; ++b) PGX_CHECK(dims[b] > 0, PGX_ERR_ARG, "block sizes must be positive");
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+        reset_problem(c->P);
+        pgx::Problem& P = c->P;
+        P.nblocks = nblocks;
+        P.is_complex = is_complex != 0;
+        P.dims.assign(dims, dims + nblocks);
+        P.moff.resize(nblocks);
+        P.eoff.resize(nblocks);
+        long m = 0, e = 0;
+        for (int b = 0; b < nblocks; ++b) {
+            P.moff[b] = m;
+            P.eoff[b] = e;
+            m += (long)dims[b] * dims[b];
+            e += dims[b];
+            P.dmax = std::max(P.dmax, (int)dims[b]);
+        }
+        P.msize = m;
+        P.esize = e;
+        const size_t sc = P.is_complex ? 2 : 1;
+        P.H.reserve(m * sc * sizeof(double));
+        P.U.reserve(m * sc * sizeof(double));
+        P.work.reserve(m * sc * sizeof(double));
+        P.work2.reserve(m * sc * sizeof(double));
+        P.E.reserve(e * sizeof(double));
+        P.w.reserve(e * sizeof(double));
+        P.dims_d.reserve(nblocks * sizeof(int));
+        P.moff_d.reserve(nblocks * sizeof(long));
+        P.eoff_d.reserve(nblocks * sizeof(long));
+        P.order_d.reserve(nblocks * sizeof(int));
+        P.status.reserve(64);
+        P.d_H = P.H.as<double>();
+        P.d_U = P.U.as<double>();
+        P.d_work = P.work.as<double>();
+        P.d_work2 = P.work2.as<double>();
+        P.d_E = P.E.as<double>();
+        P.d_w = P.w.as<double>();
+        P.d_dims = P.dims_d.as<int>();
+        P.d_moff = P.moff_d.as<long>();
+        P.d_eoff = P.eoff_d.as<long>();
+        P.d_order = P.order_d.as<int>();
+        P.d_status = P.status.as<int>();
+        std::vector<int> order(nblocks);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return dims[a] > dims[b]; });
+        PGX_CUDA(cudaMemcpy(P.d_dims, dims, nblocks * sizeof(int), cudaMemcpyHostToDevice));
+        PGX_CUDA(cudaMemcpy(P.d_moff, P.moff.data(), nblocks * sizeof(long), cudaMemcpyHostToDevice));
+        PGX_CUDA(cudaMemcpy(P.d_eoff, P.eoff.data(), nblocks * sizeof(long), cudaMemcpyHostToDevice));
+        PGX_CUDA(cudaMemcpy(P.d_order, order.data(), nblocks * sizeof(int), cudaMemcpyHostToDevice));
+        PGX_CUDA(cudaMemset(P.d_status, 0, 64));
+    });
+}
+
+int pgx_set_hamiltonian(pgx_ctx* c, const double* H) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.nblocks > 0, PGX_ERR_STATE, "pgx_set_blocks first");
+        PGX_CHECK(H, PGX_ERR_ARG, "null Hamiltonian");
+        const size_t sc = P.is_complex ? 2 : 1;
+        PGX_CUDA(cudaMemcpyAsync(P.d_H, H, P.msize * sc * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+        P.have_H = true;
+        P.have_eig = P.have_w = false;
+        for (auto& op : P.ops) op.rotated = false;
+    });
+}
+
+int pgx_eigh(pgx_ctx* c) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.have_H, PGX_ERR_STATE, "pgx_set_hamiltonian first");
+        PGX_CHECK(!P.is_complex, PGX_ERR_ARG, "complex Hermitian blocks are not supported by this build");
+        PGX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int), c->stream));
+        pgx::launch_eigh(P, c->stream);
+        int st = 0;
+        PGX_CUDA(cudaMemcpyAsync(&st, P.d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+        PGX_CHECK(st == 0, PGX_ERR_NUMERIC, "eigensolver did not converge");
+        P.have_eig = true;
+        P.have_w = false;
+        for (auto& op : P.ops) op.rotated = false;
+    });
+}
+
+int pgx_get_eigensystem(pgx_ctx* c, double* E, double* U) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.have_eig, PGX_ERR_STATE, "pgx_eigh first");
+        const size_t sc = P.is_complex ? 2 : 1;
+        if (E) PGX_CUDA(cudaMemcpyAsync(E, P.d_E, P.esize * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (U) PGX_CUDA(cudaMemcpyAsync(U, P.d_U, P.msize * sc * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int pgx_ground_energy(pgx_ctx* c, double* E0) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.have_eig && E0, PGX_ERR_STATE, "pgx_eigh first");
+        std::vector<double> e(P.esize);
+        PGX_CUDA(cudaMemcpyAsync(e.data(), P.d_E, P.esize * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+        *E0 = *std::min_element(e.begin(), e.end());
+    });
+}
+
+int pgx_weights(pgx_ctx* c, double beta, double* w, double* Z) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.have_eig, PGX_ERR_STATE, "pgx_eigh first");
+        PGX_CHECK(beta > 0, PGX_ERR_ARG, "beta must be positive");
+        pgx::launch_weights(P, beta, c->stream);
+        P.beta = beta;
+        P.have_w = true;
+        P.retained.assign(P.nblocks, 1);
+        if (w) {
+            PGX_CUDA(cudaMemcpyAsync(w, P.d_w, P.esize * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+            PGX_CUDA(cudaStreamSynchronize(c->stream));
+        }
+        if (Z) *Z = P.Z;
+    });
+}
+
+int pgx_truncate_blocks(pgx_ctx* c, double tol, int32_t* retained) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.have_w, PGX_ERR_STATE, "pgx_weights first");
+        pgx::DevBuf flags;
+        flags.reserve(P.nblocks * sizeof(int));
+        pgx::launch_retained(P, tol, flags.as<int>(), c->stream);
+        P.retained.resize(P.nblocks);
+        PGX_CUDA(cudaMemcpyAsync(P.retained.data(), flags.p, P.nblocks * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+        flags.release();
+        if (retained) std::copy(P.retained.begin(), P.retained.end(), retained);
+    });
+}
+
+int pgx_op_define(pgx_ctx* c, int32_t nparts, const int32_t* right_block, const int32_t* left_block,
+                  const int32_t* target, const double* coef, int32_t* op_id) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.nblocks > 0, PGX_ERR_STATE, "pgx_set_blocks first");
+        PGX_CHECK(nparts >= 0 && op_id && (nparts == 0 || (right_block && left_block && target && coef)),
+                  PGX_ERR_ARG, "bad operator description");
+        pgx::Operator op;
+        op.by_left.assign(P.nblocks, -1);
+        op.by_right.assign(P.nblocks, -1);
+        std::vector<int> kA, kB;
+        std::vector<double> ks;
+        op.act_off.push_back(0);
+        long in = 0, off = 0;
+        for (int q = 0; q < nparts; ++q) {
+            const int R = right_block[q], L = left_block[q];
+            PGX_CHECK(R >= 0 && R < P.nblocks && L >= 0 && L < P.nblocks, PGX_ERR_ARG, "bad block in operator");
+            PGX_CHECK(op.by_right[R] < 0 && op.by_left[L] < 0, PGX_ERR_ARG,
+                      "an operator may connect a block to at most one block");
+            const int dr = P.dims[R], dl = P.dims[L];
+            for (int k = 0; k < dr; ++k) {
+                const int t = target[in + k];
+                PGX_CHECK(t >= -1 && t < dl, PGX_ERR_ARG, "operator target out of range");
+                if (t >= 0 && coef[in + k] != 0.0) {
+                    kA.push_back(t);
+                    kB.push_back(k);
+                    ks.push_back(coef[in + k]);
+                }
+            }
+            in += dr;
+            op.act_off.push_back((long)kA.size());
+            op.by_right[R] = q;
+            op.by_left[L] = q;
+            op.parts.push_back(pgx::OpPart{R, L, dl, dr, off});
+            off += (long)dl * dr;
+        }
+        op.total = off;
+        const long K = (long)kA.size();
+        op.target.reserve(std::max<long>(2 * K, 1) * sizeof(int));
+        op.coef.reserve(std::max<long>(K, 1) * sizeof(double));
+        if (K > 0) {
+            PGX_CUDA(cudaMemcpy(op.target.as<int>(), kA.data(), K * sizeof(int), cudaMemcpyHostToDevice));
+            PGX_CUDA(cudaMemcpy(op.target.as<int>() + K, kB.data(), K * sizeof(int), cudaMemcpyHostToDevice));
+            PGX_CUDA(cudaMemcpy(op.coef.as<double>(), ks.data(), K * sizeof(double), cudaMemcpyHostToDevice));
+        }
+        P.ops.push_back(std::move(op));
+        *op_id = (int32_t)P.ops.size() - 1;
+    });
+}
+
+int pgx_op_rotate(pgx_ctx* c, int32_t op_id) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(op_id >= 0 && op_id < (int)P.ops.size(), PGX_ERR_ARG, "bad operator id");
+        PGX_CHECK(P.have_eig, PGX_ERR_STATE, "pgx_eigh first");
+        PGX_CHECK(!P.ops[op_id].act_off.empty(), PGX_ERR_ARG, "operator has no Fock action (adjoint?)");
+        pgx::rotate_operator(P, P.ops[op_id], c->stream);
+    });
+}
+
+int pgx_op_adjoint(pgx_ctx* c, int32_t src, int32_t* op_id) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(src >= 0 && src < (int)P.ops.size() && op_id, PGX_ERR_ARG, "bad operator id");
+        PGX_CHECK(P.ops[src].rotated, PGX_ERR_STATE, "rotate the source operator first");
+        pgx::Operator dst;
+        pgx::adjoint_operator(P, P.ops[src], dst, c->stream);
+        P.ops.push_back(std::move(dst));
+        *op_id = (int32_t)P.ops.size() - 1;
+    });
+}
+
+int pgx_op_info(pgx_ctx* c, int32_t op_id, int32_t* nparts, int32_t* right_block, int32_t* left_block) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(op_id >= 0 && op_id < (int)P.ops.size(), PGX_ERR_ARG, "bad operator id");
+        const auto& op = P.ops[op_id];
+        if (nparts) *nparts = (int32_t)op.parts.size();
+        for (size_t q = 0; q < op.parts.size(); ++q) {
+            if (right_block) right_block[q] = op.parts[q].right;
+            if (left_block) left_block[q] = op.parts[q].left;
+        }
+    });
+}
+
+int pgx_op_read(pgx_ctx* c, int32_t op_id, int32_t part, double* out) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(op_id >= 0 && op_id < (int)P.ops.size() && out, PGX_ERR_ARG, "bad operator id");
+        const auto& op = P.ops[op_id];
+        PGX_CHECK(op.rotated, PGX_ERR_STATE, "operator not rotated");
+        PGX_CHECK(part >= 0 && part < (int)op.parts.size(), PGX_ERR_ARG, "bad part index");
+        const auto& pt = op.parts[part];
+        const size_t sc = P.is_complex ? 2 : 1;
+        PGX_CUDA(cudaMemcpyAsync(out, op.mat.as<double>() + pt.off * sc, (size_t)pt.dl * pt.dr * sc * sizeof(double),
+                                 cudaMemcpyDeviceToHost, c->stream));
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
+int pgx_gf(pgx_ctx* c, int32_t op1, int32_t op2, int32_t nparts, const int32_t* outer, const int32_t* inner,
+           int32_t nz, const double* z, double coef_tol, double* out) {
+    return guarded(c, [&] {
+        PGX_CHECK(nparts >= 0 && nz >= 0 && (nz == 0 || (z && out)) && (nparts == 0 || (outer && inner)), PGX_ERR_ARG,
+                  "bad arguments");
+        pgx::run_gf(c, op1, op2, nparts, outer, inner, nz, z, coef_tol, out);
+    });
+}
+
+int pgx_susc(pgx_ctx* c, int32_t opA, int32_t opB, int32_t nparts, const int32_t* outer, const int32_t* inner,
+             int32_t nz, const double* z, double pole_res, double coef_tol, double beta, double* out,
+             double* zero_pole) {
+    return guarded(c, [&] {
+        PGX_CHECK(nparts >= 0 && nz >= 0 && (nz == 0 || (z && out)) && (nparts == 0 || (outer && inner)), PGX_ERR_ARG,
+                  "bad arguments");
+        pgx::run_susc(c, opA, opB, nparts, outer, inner, nz, z, pole_res, coef_tol, beta, out, zero_pole);
+    });
+}
+
+int pgx_ensemble_average(pgx_ctx* c, int32_t op, double* out) {
+    return guarded(c, [&] {
+        PGX_CHECK(out, PGX_ERR_ARG, "null output");
+        pgx::run_ensemble_average(c, op, out);
+    });
+}
+
+int pgx_g2(pgx_ctx* c, int32_t nparts, const pgx_g2_part* parts, int32_t nfreq, const double* z, double pole_res,
+           double coef_tol, int32_t flags, double* out) {
+    return guarded(c, [&] {
+        PGX_CHECK(nparts >= 0 && nfreq >= 0 && (nparts == 0 || parts) && (nfreq == 0 || (z && out)), PGX_ERR_ARG,
+                  "bad arguments");
+        pgx::run_g2(c, nparts, parts, nfreq, z, pole_res, coef_tol, flags, out);
+    });
+}
+
+int pgx_g2_last_timing(pgx_ctx* c, double* total_ms, double* gemm_ms, double* gemm_flops) {
+    return guarded(c, [&] {
+        if (total_ms) *total_ms = c->g2t.total_ms;
+        if (gemm_ms) *gemm_ms = c->g2t.gemm_ms;
+        if (gemm_flops) *gemm_flops = c->g2t.gemm_flops;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,504 @@
+// K4: two-particle Green's function, factorised Lehmann sum on the GPU.
+//
+// Reference: TwoParticleGFPart::computeImpl / addMultiterm (TwoParticleGFPart.cpp:189-298)
+// enumerate every state quadruple (1,2,3,4) of a block chain with
+// M = sign * O1_12 O2_23 O3_34 CX4_41 and four sub-terms; TwoParticleGFPart::operator()
+// (TwoParticleGFPart.cpp:309-322, .hpp:475-495) sums them at a frequency triple.
+//
+// With A(z1)_12 = O1_12 / (z1 - (E2 - E1)) and C(z3)_34 = O3_34 / (z3 - (E4 - E3))
+// the four sub-terms of the Lehmann sum become
+//   T1 = -sign sum_23 X_32 O2_23 (w2 + w3) / (z2 - (E3 - E2)),    X = C(z3) CX4 A(z1)
+//   T2 =  sign sum_14 Y_14 CX4_41 (w1 + w4) / (z1+z2+z3 - (E4 - E1)), Y = A(z1) O2 C(z3)
+//   T3 =  sign sum_13 P_13 Q_31 F13(z1 + z2),   P = A(z1) O2, Q = C(z3) CX4
+//   T4 =  sign sum_24 R_24 L_42 F24(z2 + z3),   R = O2 C(z3), L = CX4 A(z1)
+// with the resonant rule of ResonantTerm::operator():
+//   F13(s) = |s - (E3 - E1)| <= tol ? beta w1 : (w3 - w1) / (s - (E3 - E1))
+//   F24(s) = |s - (E4 - E2)| <= tol ? -beta w2 : (w2 - w4) / (s - (E4 - E2)).
+// Per chain: dressed operators per distinct z1 / z3, four batched GEMMs per
+// distinct frequency, two batched GEMMs per distinct (z1, z3) pair (the
+// dominant FP64 work), and four contractions over the triples of each pair.
+// Everything stays FP64; the delta test is made per element in FP64.
+
+#include <chrono>
+#include <cstring>
+#include <map>
+#include <tuple>
+
+#include "pgx_common.cuh"
+#include "pgx_gemm.cuh"
+#include "pgx_internal.h"
+
+namespace pgx {
+
+namespace {
+
+// out[iz][a][b] = O[a][b] / (z[iz] - (Eb[b] - Ea[a]))
+template <typename T>
+__global__ void dress_kernel(const T* O, int da, int db, const double* Ea, const double* Eb, const cd* z, int nz,
+                             cd* out) {
+    const long n = (long)da * db;
+    const int iz = blockIdx.y;
+    if (iz >= nz) return;
+    const cd zz = z[iz];
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
+        const int a = (int)(e / db), b = (int)(e % db);
+        const cd den{zz.x - (Eb[b] - Ea[a]), zz.y};
+        out[(long)iz * n + e] = tocd(O[e]) * inv(den);
+    }
+}
+
+struct ContractArgs {
+    const cd* Lm;
+    long L_stride;
+    const int* L_idx;
+    long L_sa, L_sb;
+    const void* Rm;
+    long R_stride;
+    const int* R_idx;
+    long R_sa, R_sb;
+    const double *Ea, *Eb, *wa, *wb;
+    int da, db;
+    const int* pair_ptr;
+    const int* slot_out;
+    const cd* s;
+    double beta, tol, coef;
+    cd* out;
+    int pair0;  // pairs of this launch start here; unindexed matrices are chunk-local
+};
+
+constexpr int CT_THREADS = 256, CT_CHUNK = 4096, CT_GROUP = 16;
+
+__device__ __forceinline__ double wsum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// MODE 1/2: K = (wa + wb) / (s - (Eb - Ea))
+// MODE 3:   K = delta ? beta wa : (wb - wa) / (s - (Eb - Ea))
+// MODE 4:   K = delta ? -beta wa : (wa - wb) / (s - (Eb - Ea))
+template <typename TR, int MODE>
+__global__ void __launch_bounds__(CT_THREADS) contract_kernel(ContractArgs g) {
+    __shared__ cd s_s[CT_GROUP];
+    __shared__ double s_acc[CT_GROUP][2];
+    const int pl = blockIdx.y, p = g.pair0 + pl;
+    const int t0 = g.pair_ptr[p], t1 = g.pair_ptr[p + 1];
+    const long n = (long)g.da * g.db;
+    const long e0 = (long)blockIdx.x * CT_CHUNK;
+    const cd* L = g.Lm + (long)(g.L_idx ? g.L_idx[p] : pl) * g.L_stride;
+    const TR* R = static_cast<const TR*>(g.Rm) + (long)(g.R_idx ? g.R_idx[p] : pl) * g.R_stride;
+    for (int tg = t0; tg < t1; tg += CT_GROUP) {
+        const int nt = min(CT_GROUP, t1 - tg);
+        __syncthreads();
+        if (threadIdx.x < nt) {
+            s_s[threadIdx.x] = g.s[tg + threadIdx.x];
+            s_acc[threadIdx.x][0] = 0.0;
+            s_acc[threadIdx.x][1] = 0.0;
+        }
+        __syncthreads();
+        cd acc[CT_GROUP];
+#pragma unroll
+        for (int j = 0; j < CT_GROUP; ++j) acc[j] = cd{0.0, 0.0};
+        for (long e = e0 + threadIdx.x; e < min(n, e0 + CT_CHUNK); e += CT_THREADS) {
+            const int a = (int)(e / g.db), b = (int)(e % g.db);
+            const cd lr = L[a * g.L_sa + b * g.L_sb] * tocd(R[a * g.R_sa + b * g.R_sb]);
+            if (lr.x == 0.0 && lr.y == 0.0) continue;
+            const double dE = g.Eb[b] - g.Ea[a];
+            const double wa = g.wa[a], wb = g.wb[b];
+            double num;
+            if (MODE <= 2) num = wa + wb;
+            else if (MODE == 3) num = wb - wa;
+            else num = wa - wb;
+#pragma unroll
+            for (int j = 0; j < CT_GROUP; ++j) {
+                if (j < nt) {
+                    const cd d{s_s[j].x - dE, s_s[j].y};
+                    cd K;
+                    if (MODE >= 3 && sqrt(abs2(d)) <= g.tol) {
+                        K = cd{(MODE == 3 ? 1.0 : -1.0) * g.beta * wa, 0.0};
+                    } else {
+                        const double r = num / abs2(d);
+                        K = cd{d.x * r, -d.y * r};
+                    }
+                    const cd v = lr * K;
+                    acc[j].x += v.x;
+                    acc[j].y += v.y;
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < CT_GROUP; ++j) {
+            if (j < nt) {
+                const double x = wsum(acc[j].x), y = wsum(acc[j].y);
+                if ((threadIdx.x & 31) == 0 && (x != 0.0 || y != 0.0)) {
+                    atomicAdd(&s_acc[j][0], x);
+                    atomicAdd(&s_acc[j][1], y);
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x < nt) {
+            const double x = s_acc[threadIdx.x][0], y = s_acc[threadIdx.x][1];
+            if (x != 0.0 || y != 0.0) {
+                cd* o = g.out + g.slot_out[tg + threadIdx.x];
+                atomicAdd(&o->x, g.coef * x);
+                atomicAdd(&o->y, g.coef * y);
+            }
+        }
+    }
+}
+
+// Frequency plan of one permutation: distinct z1, z3, distinct (z1, z3)
+// pairs, and the triples of each pair in CSR order with the four s values.
+struct Plan {
+    std::vector<cd> Z1, Z3;
+    std::vector<int> pi1, pi3, ptr, slot;
+    std::vector<cd> s1, s2, s3, s4;
+    // device
+    DevBuf buf;
+    cd *dZ1, *dZ3, *ds1, *ds2, *ds3, *ds4;
+    int *dpi1, *dpi3, *dptr, *dslot;
+};
+
+struct Key {
+    double a, b;
+    bool operator<(const Key& o) const { return std::tie(a, b) < std::tie(o.a, o.b); }
+};
+
+void build_plan(Plan& pl, const int perm[3], int nfreq, const double* z) {
+    std::map<Key, int> m1, m3;
+    std::map<std::pair<int, int>, int> mp;
+    std::vector<int> tp(nfreq);
+    std::vector<cd> zz1(nfreq), zz2(nfreq), zz3(nfreq);
+    for (int t = 0; t < nfreq; ++t) {
+        const cd F[3] = {cd{z[6 * t], z[6 * t + 1]}, cd{z[6 * t + 2], z[6 * t + 3]}, cd{-z[6 * t + 4], -z[6 * t + 5]}};
+        const cd a = F[perm[0]], b = F[perm[1]], c3 = F[perm[2]];
+        zz1[t] = a;
+        zz2[t] = b;
+        zz3[t] = c3;
+        auto i1 = m1.emplace(Key{a.x, a.y}, (int)pl.Z1.size());
+        if (i1.second) pl.Z1.push_back(a);
+        auto i3 = m3.emplace(Key{c3.x, c3.y}, (int)pl.Z3.size());
+        if (i3.second) pl.Z3.push_back(c3);
+        auto ip = mp.emplace(std::make_pair(i1.first->second, i3.first->second), (int)pl.pi1.size());
+        if (ip.second) {
+            pl.pi1.push_back(i1.first->second);
+            pl.pi3.push_back(i3.first->second);
+        }
+        tp[t] = ip.first->second;
+    }
+    const int np = (int)pl.pi1.size();
+    pl.ptr.assign(np + 1, 0);
+    for (int t = 0; t < nfreq; ++t) pl.ptr[tp[t] + 1]++;
+    for (int q = 0; q < np; ++q) pl.ptr[q + 1] += pl.ptr[q];
+    std::vector<int> fill(pl.ptr.begin(), pl.ptr.end() - 1);
+    pl.slot.resize(nfreq);
+    pl.s1.resize(nfreq);
+    pl.s2.resize(nfreq);
+    pl.s3.resize(nfreq);
+    pl.s4.resize(nfreq);
+    for (int t = 0; t < nfreq; ++t) {
+        const int k = fill[tp[t]]++;
+        pl.slot[k] = t;
+        pl.s1[k] = zz2[t];
+        pl.s2[k] = zz1[t] + zz2[t] + zz3[t];
+        pl.s3[k] = zz1[t] + zz2[t];
+        pl.s4[k] = zz2[t] + zz3[t];
+    }
+}
+
+void upload_plan(Plan& pl, cudaStream_t st) {
+    const size_t n1 = pl.Z1.size(), n3 = pl.Z3.size(), np = pl.pi1.size(), nf = pl.slot.size();
+    const size_t bytes = (n1 + n3 + 4 * nf) * sizeof(cd) + (2 * np + np + 1 + nf) * sizeof(int) + 256;
+    pl.buf.reserve(bytes);
+    char* p = pl.buf.as<char>();
+    auto take = [&](size_t b) {
+        char* r = p;
+        p += (b + 15) & ~size_t(15);
+        return r;
+    };
+    pl.dZ1 = reinterpret_cast<cd*>(take(n1 * sizeof(cd)));
+    pl.dZ3 = reinterpret_cast<cd*>(take(n3 * sizeof(cd)));
+    pl.ds1 = reinterpret_cast<cd*>(take(nf * sizeof(cd)));
+    pl.ds2 = reinterpret_cast<cd*>(take(nf * sizeof(cd)));
+    pl.ds3 = reinterpret_cast<cd*>(take(nf * sizeof(cd)));
+    pl.ds4 = reinterpret_cast<cd*>(take(nf * sizeof(cd)));
+    pl.dpi1 = reinterpret_cast<int*>(take(np * sizeof(int)));
+    pl.dpi3 = reinterpret_cast<int*>(take(np * sizeof(int)));
+    pl.dptr = reinterpret_cast<int*>(take((np + 1) * sizeof(int)));
+    pl.dslot = reinterpret_cast<int*>(take(nf * sizeof(int)));
+    auto up = [&](void* d, const void* h, size_t b) {
+        if (b) PGX_CUDA(cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, st));
+    };
+    up(pl.dZ1, pl.Z1.data(), n1 * sizeof(cd));
+    up(pl.dZ3, pl.Z3.data(), n3 * sizeof(cd));
+    up(pl.ds1, pl.s1.data(), nf * sizeof(cd));
+    up(pl.ds2, pl.s2.data(), nf * sizeof(cd));
+    up(pl.ds3, pl.s3.data(), nf * sizeof(cd));
+    up(pl.ds4, pl.s4.data(), nf * sizeof(cd));
+    up(pl.dpi1, pl.pi1.data(), np * sizeof(int));
+    up(pl.dpi3, pl.pi3.data(), np * sizeof(int));
+    up(pl.dptr, pl.ptr.data(), (np + 1) * sizeof(int));
+    up(pl.dslot, pl.slot.data(), nf * sizeof(int));
+}
+
+template <typename TA, typename TB>
+GemmProblem<TA, TB, cd> prob(const TA* A, const TB* B, cd* C, int M, int N, int K) {
+    GemmProblem<TA, TB, cd> g{};
+    g.A = A;
+    g.B = B;
+    g.C = C;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.sa_i = K;
+    g.sa_k = 1;
+    g.sb_k = N;
+    g.sb_j = 1;
+    g.sc_i = N;
+    g.sc_j = 1;
+    return g;
+}
+
+struct Workspace {
+    cd *A1, *C3, *L, *Pm, *Q, *R, *X;
+    long pair_cap;  // complex elements available at X for X and Y of one pair chunk
+    void* probs;
+    size_t probs_cap;
+    void* tiles;
+    size_t tiles_cap;
+};
+
+template <typename T>
+void g2_part(pgx_ctx* c, const pgx_g2_part& gp, const Plan& pl, Workspace& ws, double pole_res, cd* d_out,
+             cudaEvent_t ev0, cudaEvent_t ev1, double& gemm_ms, double& gemm_flops) {
+    Problem& P = c->P;
+    cudaStream_t st = c->stream;
+    const int S1 = gp.block[0], S2 = gp.block[1], S3 = gp.block[2], S4 = gp.block[3];
+    const int d1 = P.dims[S1], d2 = P.dims[S2], d3 = P.dims[S3], d4 = P.dims[S4];
+    const Operator &o1 = P.ops[gp.op[0]], &o2 = P.ops[gp.op[1]], &o3 = P.ops[gp.op[2]], &o4 = P.ops[gp.op[3]];
+    const T* O1 = o1.mat.as<T>() + o1.parts[o1.by_left[S1]].off;
+    const T* O2 = o2.mat.as<T>() + o2.parts[o2.by_left[S2]].off;
+    const T* O3 = o3.mat.as<T>() + o3.parts[o3.by_left[S3]].off;
+    const T* X4 = o4.mat.as<T>() + o4.parts[o4.by_left[S4]].off;
+    const double *E1 = P.d_E + P.eoff[S1], *E2 = P.d_E + P.eoff[S2], *E3 = P.d_E + P.eoff[S3], *E4 = P.d_E + P.eoff[S4];
+    const double *w1 = P.d_w + P.eoff[S1], *w2 = P.d_w + P.eoff[S2], *w3 = P.d_w + P.eoff[S3], *w4 = P.d_w + P.eoff[S4];
+    const int N1 = (int)pl.Z1.size(), N3 = (int)pl.Z3.size(), NP = (int)pl.pi1.size();
+    const double sign = gp.sign;
+
+    // dressed operators
+    {
+        dim3 g1(std::min(ceil_div((long)d1 * d2, 256), 256), N1);
+        dress_kernel<T><<<g1, 256, 0, st>>>(O1, d1, d2, E1, E2, pl.dZ1, N1, ws.A1);
+        dim3 g3(std::min(ceil_div((long)d3 * d4, 256), 256), N3);
+        dress_kernel<T><<<g3, 256, 0, st>>>(O3, d3, d4, E3, E4, pl.dZ3, N3, ws.C3);
+        check_launch("dress_kernel");
+    }
+    const long s12 = (long)d1 * d2, s34 = (long)d3 * d4, s42 = (long)d4 * d2, s13 = (long)d1 * d3,
+               s31 = (long)d3 * d1, s24 = (long)d2 * d4, s32 = (long)d3 * d2, s14 = (long)d1 * d4;
+    // per-frequency GEMMs
+    {
+        std::vector<GemmProblem<T, cd, cd>> pa;   // T x cd
+        std::vector<GemmProblem<cd, T, cd>> pb;   // cd x T
+        for (int i = 0; i < N1; ++i) {
+            pa.push_back(prob<T, cd>(X4, ws.A1 + i * s12, ws.L + i * s42, d4, d2, d1));      // L = CX4 A1
+            pb.push_back(prob<cd, T>(ws.A1 + i * s12, O2, ws.Pm + i * s13, d1, d3, d2));     // P = A1 O2
+        }
+        for (int i = 0; i < N3; ++i) {
+            pb.push_back(prob<cd, T>(ws.C3 + i * s34, X4, ws.Q + i * s31, d3, d1, d4));      // Q = C3 CX4
+            pa.push_back(prob<T, cd>(O2, ws.C3 + i * s34, ws.R + i * s24, d2, d4, d3));      // R = O2 C3
+        }
+        launch_gemm_batch(pa, ws.probs, ws.probs_cap, ws.tiles, ws.tiles_cap, st);
+        launch_gemm_batch(pb, ws.probs, ws.probs_cap, ws.tiles, ws.tiles_cap, st);
+    }
+    // contractions that need no per-pair product: T3 and T4 over all pairs
+    ContractArgs a{};
+    a.pair_ptr = pl.dptr;
+    a.slot_out = pl.dslot;
+    a.beta = P.beta;
+    a.tol = pole_res;
+    a.out = d_out;
+    auto launch = [&](auto kern, int da, int db, int npairs) {
+        if (npairs <= 0 || da <= 0 || db <= 0) return;
+        dim3 grid(ceil_div((long)da * db, CT_CHUNK), npairs);
+        kern<<<grid, CT_THREADS, 0, st>>>(a);
+        check_launch("contract_kernel");
+    };
+    a.pair0 = 0;
+    // T3: a in S1, b in S3, L = P[z1] (a,b), R = Q[z3] (b,a)
+    a.Lm = ws.Pm; a.L_stride = s13; a.L_idx = pl.dpi1; a.L_sa = d3; a.L_sb = 1;
+    a.Rm = ws.Q; a.R_stride = s31; a.R_idx = pl.dpi3; a.R_sa = 1; a.R_sb = d1;
+    a.Ea = E1; a.Eb = E3; a.wa = w1; a.wb = w3; a.da = d1; a.db = d3; a.s = pl.ds3; a.coef = sign;
+    launch(contract_kernel<cd, 3>, d1, d3, NP);
+    // T4: a in S2, b in S4, L = R[z3] (a,b), R = L[z1] (b,a)
+    a.Lm = ws.R; a.L_stride = s24; a.L_idx = pl.dpi3; a.L_sa = d4; a.L_sb = 1;
+    a.Rm = ws.L; a.R_stride = s42; a.R_idx = pl.dpi1; a.R_sa = 1; a.R_sb = d2;
+    a.Ea = E2; a.Eb = E4; a.wa = w2; a.wb = w4; a.da = d2; a.db = d4; a.s = pl.ds4; a.coef = sign;
+    launch(contract_kernel<cd, 4>, d2, d4, NP);
+
+    // per-pair GEMMs (dominant), in chunks of pairs that fit the workspace
+    const long per_pair = s32 + s14;
+    const int chunk = (int)std::max<long>(1, std::min<long>(NP, ws.pair_cap / std::max<long>(per_pair, 1)));
+    for (int q0 = 0; q0 < NP; q0 += chunk) {
+        const int nq = std::min(chunk, NP - q0);
+        std::vector<GemmProblem<cd, cd, cd>> pc;
+        cd* X = ws.X;
+        cd* Y = ws.X + (long)nq * s32;
+        for (int q = 0; q < nq; ++q) {
+            const int i1 = pl.pi1[q0 + q], i3 = pl.pi3[q0 + q];
+            pc.push_back(prob<cd, cd>(ws.C3 + i3 * s34, ws.L + i1 * s42, X + q * s32, d3, d2, d4));   // X
+            pc.push_back(prob<cd, cd>(ws.Pm + i1 * s13, ws.C3 + i3 * s34, Y + q * s14, d1, d4, d3));  // Y
+        }
+        PGX_CUDA(cudaEventRecord(ev0, st));
+        launch_gemm_batch(pc, ws.probs, ws.probs_cap, ws.tiles, ws.tiles_cap, st);
+        PGX_CUDA(cudaEventRecord(ev1, st));
+        PGX_CUDA(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        PGX_CUDA(cudaEventElapsedTime(&ms, ev0, ev1));
+        gemm_ms += ms;
+        gemm_flops += 8.0 * nq * ((double)d3 * d2 * d4 + (double)d1 * d4 * d3);
+        a.pair0 = q0;
+        // T1: a in S2, b in S3, L = X[pair] (X_ba), R = O2 (a,b)
+        a.Lm = X; a.L_stride = s32; a.L_idx = nullptr; a.L_sa = 1; a.L_sb = d2;
+        a.Rm = O2; a.R_stride = 0; a.R_idx = nullptr; a.R_sa = d3; a.R_sb = 1;
+        a.Ea = E2; a.Eb = E3; a.wa = w2; a.wb = w3; a.da = d2; a.db = d3; a.s = pl.ds1; a.coef = -sign;
+        launch(contract_kernel<T, 1>, d2, d3, nq);
+        // T2: a in S1, b in S4, L = Y[pair] (a,b), R = CX4 (b,a)
+        a.Lm = Y; a.L_stride = s14; a.L_idx = nullptr; a.L_sa = d4; a.L_sb = 1;
+        a.Rm = X4; a.R_stride = 0; a.R_idx = nullptr; a.R_sa = 1; a.R_sb = d1;
+        a.Ea = E1; a.Eb = E4; a.wa = w1; a.wb = w4; a.da = d1; a.db = d4; a.s = pl.ds2; a.coef = sign;
+        launch(contract_kernel<T, 2>, d1, d4, nq);
+    }
+}
+
+}  // namespace
+
+
+void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
+            double coef_tol, int flags, double* out) {
+    (void)coef_tol;
+    (void)flags;
+    Problem& P = c->P;
+    cudaStream_t st = c->stream;
+    PGX_CHECK(P.have_w, PGX_ERR_STATE, "weights must be computed before pgx_g2");
+    PGX_CHECK(nfreq >= 0 && nparts >= 0, PGX_ERR_ARG, "negative size");
+    for (int q = 0; q < nparts; ++q) {
+        const pgx_g2_part& gp = parts[q];
+        for (int k = 0; k < 4; ++k) {
+            PGX_CHECK(gp.op[k] >= 0 && gp.op[k] < (int)P.ops.size(), PGX_ERR_ARG, "bad operator id in G2 part");
+            PGX_CHECK(gp.block[k] >= 0 && gp.block[k] < P.nblocks, PGX_ERR_ARG, "bad block in G2 part");
+            PGX_CHECK(P.ops[gp.op[k]].rotated, PGX_ERR_STATE, "G2 operator not rotated");
+        }
+        for (int k = 0; k < 4; ++k) {
+            const Operator& o = P.ops[gp.op[k]];
+            const int left = gp.block[k], right = gp.block[(k + 1) % 4];
+            const int pi = o.by_left[left];
+            PGX_CHECK(pi >= 0 && o.parts[pi].right == right, PGX_ERR_ARG, "G2 part is not a block chain");
+        }
+        bool okp = true;
+        for (int k = 0; k < 3; ++k) okp = okp && gp.perm[k] >= 0 && gp.perm[k] < 3;
+        PGX_CHECK(okp && gp.perm[0] != gp.perm[1] && gp.perm[1] != gp.perm[2] && gp.perm[0] != gp.perm[2],
+                  PGX_ERR_ARG, "bad permutation");
+        PGX_CHECK(gp.sign == 1 || gp.sign == -1, PGX_ERR_ARG, "bad permutation sign");
+    }
+    cudaEvent_t e0, e1, ea, eb;
+    PGX_CUDA(cudaEventCreate(&e0));
+    PGX_CUDA(cudaEventCreate(&e1));
+    PGX_CUDA(cudaEventCreate(&ea));
+    PGX_CUDA(cudaEventCreate(&eb));
+    PGX_CUDA(cudaEventRecord(ea, st));
+    // one frequency plan per distinct permutation
+    std::map<std::tuple<int, int, int>, int> perm_id;
+    std::vector<Plan> plans;
+    plans.reserve(6);
+    std::vector<int> part_plan(nparts);
+    for (int q = 0; q < nparts; ++q) {
+        auto key = std::make_tuple(parts[q].perm[0], parts[q].perm[1], parts[q].perm[2]);
+        auto it = perm_id.find(key);
+        if (it == perm_id.end()) {
+            it = perm_id.emplace(key, (int)plans.size()).first;
+            plans.emplace_back();
+        }
+        part_plan[q] = it->second;
+    }
+    for (auto& kv : perm_id) {
+        const int perm[3] = {std::get<0>(kv.first), std::get<1>(kv.first), std::get<2>(kv.first)};
+        build_plan(plans[kv.second], perm, nfreq, z);
+        upload_plan(plans[kv.second], st);
+    }
+    // workspace: the largest part decides
+    long nA1 = 1, nC3 = 1, nL = 1, nPm = 1, nQ = 1, nR = 1, max_pair = 1, nprob = 1, ntile = 1;
+    for (int q = 0; q < nparts; ++q) {
+        const Plan& pl = plans[part_plan[q]];
+        const long d1 = P.dims[parts[q].block[0]], d2 = P.dims[parts[q].block[1]], d3 = P.dims[parts[q].block[2]],
+                   d4 = P.dims[parts[q].block[3]];
+        const long N1 = pl.Z1.size(), N3 = pl.Z3.size(), NP = pl.pi1.size();
+        nA1 = std::max(nA1, N1 * d1 * d2);
+        nC3 = std::max(nC3, N3 * d3 * d4);
+        nL = std::max(nL, N1 * d4 * d2);
+        nPm = std::max(nPm, N1 * d1 * d3);
+        nQ = std::max(nQ, N3 * d3 * d1);
+        nR = std::max(nR, N3 * d2 * d4);
+        max_pair = std::max(max_pair, d3 * d2 + d1 * d4);
+        nprob = std::max(nprob, std::max(2 * NP, 2 * (N1 + N3)));
+        const long tz = (N1 + N3) * ((long)ceil_div(d4, GEMM_BM) * ceil_div(d2, GEMM_BN) +
+                                     (long)ceil_div(d1, GEMM_BM) * ceil_div(d3, GEMM_BN) +
+                                     (long)ceil_div(d3, GEMM_BM) * ceil_div(d1, GEMM_BN) +
+                                     (long)ceil_div(d2, GEMM_BM) * ceil_div(d4, GEMM_BN));
+        const long tp = NP * ((long)ceil_div(d3, GEMM_BM) * ceil_div(d2, GEMM_BN) +
+                              (long)ceil_div(d1, GEMM_BM) * ceil_div(d4, GEMM_BN));
+        ntile = std::max(ntile, std::max(tz, tp));
+    }
+    long np_max = 1;
+    for (auto& pl : plans) np_max = std::max<long>(np_max, (long)pl.pi1.size());
+    // pair workspace: at most 16 GiB of complex doubles, at least one pair
+    const long pair_budget = std::max<long>(max_pair, std::min<long>(np_max * max_pair, (16L << 30) / (long)sizeof(cd)));
+    Workspace ws{};
+    DevBuf* S = c->scratch;
+    S[0].reserve(nA1 * sizeof(cd));
+    S[1].reserve(nC3 * sizeof(cd));
+    S[2].reserve(nL * sizeof(cd));
+    S[3].reserve(nPm * sizeof(cd));
+    S[4].reserve(nQ * sizeof(cd));
+    S[5].reserve(nR * sizeof(cd));
+    S[6].reserve(pair_budget * sizeof(cd));
+    S[7].reserve(nprob * sizeof(GemmProblem<cd, cd, cd>));
+    S[8].reserve(ntile * sizeof(GemmTile));
+    S[9].reserve(std::max(nfreq, 1) * sizeof(cd));
+    ws.A1 = S[0].as<cd>();
+    ws.C3 = S[1].as<cd>();
+    ws.L = S[2].as<cd>();
+    ws.Pm = S[3].as<cd>();
+    ws.Q = S[4].as<cd>();
+    ws.R = S[5].as<cd>();
+    ws.X = S[6].as<cd>();
+    ws.pair_cap = pair_budget;
+    ws.probs = S[7].p;
+    ws.probs_cap = S[7].bytes;
+    ws.tiles = S[8].p;
+    ws.tiles_cap = S[8].bytes;
+    cd* d_out = S[9].as<cd>();
+    PGX_CUDA(cudaMemsetAsync(d_out, 0, std::max(nfreq, 1) * sizeof(cd), st));
+    double gemm_ms = 0.0, gemm_flops = 0.0;
+    if (nfreq > 0) {
+        for (int q = 0; q < nparts; ++q) {
+            if (P.is_complex)
+                g2_part<cd>(c, parts[q], plans[part_plan[q]], ws, pole_res, d_out, e0, e1, gemm_ms, gemm_flops);
+            else
+                g2_part<double>(c, parts[q], plans[part_plan[q]], ws, pole_res, d_out, e0, e1, gemm_ms, gemm_flops);
+        }
+    }
+    if (nfreq > 0) PGX_CUDA(cudaMemcpyAsync(out, d_out, nfreq * sizeof(cd), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaEventRecord(eb, st));
+    PGX_CUDA(cudaEventSynchronize(eb));
+    float tot = 0.f;
+    PGX_CUDA(cudaEventElapsedTime(&tot, ea, eb));
+    c->g2t.total_ms = tot;
+    c->g2t.gemm_ms = gemm_ms;
+    c->g2t.gemm_flops = gemm_flops;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(ea);
+    cudaEventDestroy(eb);
+}
+
+}  // namespace pgx

@@ -1,0 +1,170 @@
+// Batched FP64 (real / complex) GEMM over a flat tile list.
+//
+// One launch covers many independent products of uneven shapes (symmetry
+// blocks of different sizes, frequency batches): the host builds a list of
+// (problem, tile_m, tile_n) entries and the grid walks it, so no CTA idles
+// on an empty tile of a small block.  Operands are addressed through
+// arbitrary (row, column) strides, so transposes cost nothing, and the
+// reduction index k may be gathered through index arrays with a per-k scale
+// (the signed row gather of a fermionic operator).
+#pragma once
+
+#include <type_traits>
+#include <vector>
+
+#include "pgx_common.cuh"
+
+namespace pgx {
+
+template <typename TA, typename TB, typename TC> struct GemmProblem {
+    const TA* A;
+    const TB* B;
+    TC* C;
+    int M, N, K;
+    long sa_i, sa_k;   // A(i,k) = A[i*sa_i + k'*sa_k], k' = a_kidx ? a_kidx[k] : k
+    long sb_k, sb_j;   // B(k,j) = B[k''*sb_k + j*sb_j], k'' = b_kidx ? b_kidx[k] : k
+    long sc_i, sc_j;
+    const int* a_kidx;
+    const int* b_kidx;
+    const double* kscale;  // multiplies B(k, :) when non-null
+    int accumulate;        // C += A B instead of C = A B
+    int conj_a;            // use conj(A) (complex A only)
+};
+
+struct GemmTile {
+    int prob, tm, tn, pad;
+};
+
+__device__ __forceinline__ void mac(double& c, double a, double b) { c = fma(a, b, c); }
+__device__ __forceinline__ void mac(cd& c, cd a, double b) {
+    c.x = fma(a.x, b, c.x);
+    c.y = fma(a.y, b, c.y);
+}
+__device__ __forceinline__ void mac(cd& c, double a, cd b) {
+    c.x = fma(a, b.x, c.x);
+    c.y = fma(a, b.y, c.y);
+}
+__device__ __forceinline__ void mac(cd& c, cd a, cd b) {
+    c.x = fma(a.x, b.x, c.x);
+    c.x = fma(-a.y, b.y, c.x);
+    c.y = fma(a.x, b.y, c.y);
+    c.y = fma(a.y, b.x, c.y);
+}
+__device__ __forceinline__ double scale_by(double a, double s) { return a * s; }
+__device__ __forceinline__ cd scale_by(cd a, double s) { return cd{a.x * s, a.y * s}; }
+__device__ __forceinline__ double maybe_conj(double a, int) { return a; }
+__device__ __forceinline__ cd maybe_conj(cd a, int c) { return c ? cd{a.x, -a.y} : a; }
+__device__ __forceinline__ void store_c(double& dst, double v, int acc) { dst = acc ? dst + v : v; }
+__device__ __forceinline__ void store_c(cd& dst, double v, int acc) {
+    dst = acc ? cd{dst.x + v, dst.y} : cd{v, 0.0};
+}
+__device__ __forceinline__ void store_c(cd& dst, cd v, int acc) { dst = acc ? dst + v : v; }
+template <typename T> __device__ __forceinline__ T zero_of();
+template <> __device__ __forceinline__ double zero_of<double>() { return 0.0; }
+template <> __device__ __forceinline__ cd zero_of<cd>() { return cd{0.0, 0.0}; }
+
+constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_THREADS = 256;
+
+template <typename TA, typename TB, typename TC>
+__global__ void __launch_bounds__(GEMM_THREADS)
+    gemm_tiles_kernel(const GemmProblem<TA, TB, TC>* __restrict__ probs, const GemmTile* __restrict__ tiles) {
+    using TAcc = typename std::conditional<is_cd<TA>::value || is_cd<TB>::value, cd, double>::type;
+    constexpr int BK = (is_cd<TA>::value || is_cd<TB>::value) ? 8 : 16;
+    __shared__ TA As[BK][GEMM_BM + 1];
+    __shared__ TB Bs[BK][GEMM_BN + 1];
+
+    const GemmTile t = tiles[blockIdx.x];
+    const GemmProblem<TA, TB, TC> p = probs[t.prob];
+    const int i0 = t.tm * GEMM_BM, j0 = t.tn * GEMM_BN;
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+
+    TAcc acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = zero_of<TAcc>();
+
+    const bool a_i_fast = (p.sa_i == 1);
+    const bool b_j_fast = (p.sb_j == 1);
+
+    for (int k0 = 0; k0 < p.K; k0 += BK) {
+        // ---- A tile: BM x BK
+        for (int l = tid; l < GEMM_BM * BK; l += GEMM_THREADS) {
+            int ii, kk;
+            if (a_i_fast) { ii = l % GEMM_BM; kk = l / GEMM_BM; }
+            else { ii = l / BK; kk = l % BK; }
+            const int gi = i0 + ii, gk = k0 + kk;
+            TA v = zero_of<TA>();
+            if (gi < p.M && gk < p.K) {
+                const long kq = p.a_kidx ? p.a_kidx[gk] : gk;
+                v = maybe_conj(p.A[gi * p.sa_i + kq * p.sa_k], p.conj_a);
+            }
+            As[kk][ii] = v;
+        }
+        // ---- B tile: BK x BN
+        for (int l = tid; l < GEMM_BN * BK; l += GEMM_THREADS) {
+            int jj, kk;
+            if (b_j_fast) { jj = l % GEMM_BN; kk = l / GEMM_BN; }
+            else { jj = l / BK; kk = l % BK; }
+            const int gj = j0 + jj, gk = k0 + kk;
+            TB v = zero_of<TB>();
+            if (gj < p.N && gk < p.K) {
+                const long kq = p.b_kidx ? p.b_kidx[gk] : gk;
+                v = p.B[kq * p.sb_k + gj * p.sb_j];
+                if (p.kscale) v = scale_by(v, p.kscale[gk]);
+            }
+            Bs[kk][jj] = v;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < BK; ++kk) {
+            TA a[4];
+            TB b[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                a[q] = As[kk][ty + 16 * q];
+                b[q] = Bs[kk][tx + 16 * q];
+            }
+#pragma unroll
+            for (int qa = 0; qa < 4; ++qa)
+#pragma unroll
+                for (int qb = 0; qb < 4; ++qb) mac(acc[qa][qb], a[qa], b[qb]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int qa = 0; qa < 4; ++qa) {
+        const int gi = i0 + ty + 16 * qa;
+        if (gi >= p.M) continue;
+#pragma unroll
+        for (int qb = 0; qb < 4; ++qb) {
+            const int gj = j0 + tx + 16 * qb;
+            if (gj >= p.N) continue;
+            store_c(p.C[gi * p.sc_i + gj * p.sc_j], acc[qa][qb], p.accumulate);
+        }
+    }
+}
+
+// Host helper: upload problems + tile list into scratch buffers and launch.
+template <typename TA, typename TB, typename TC>
+void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* d_probs, size_t probs_cap,
+                       void* d_tiles, size_t tiles_cap, cudaStream_t st) {
+    if (probs.empty()) return;
+    std::vector<GemmTile> tiles;
+    for (size_t q = 0; q < probs.size(); ++q) {
+        const int tm = ceil_div(probs[q].M, GEMM_BM), tn = ceil_div(probs[q].N, GEMM_BN);
+        if (probs[q].M <= 0 || probs[q].N <= 0) continue;
+        for (int a = 0; a < tm; ++a)
+            for (int b = 0; b < tn; ++b) tiles.push_back(GemmTile{(int)q, a, b, 0});
+    }
+    if (tiles.empty()) return;
+    PGX_CHECK(probs.size() * sizeof(probs[0]) <= probs_cap, PGX_ERR_ARG, "gemm problem list overflow");
+    PGX_CHECK(tiles.size() * sizeof(GemmTile) <= tiles_cap, PGX_ERR_ARG, "gemm tile list overflow");
+    PGX_CUDA(cudaMemcpyAsync(d_probs, probs.data(), probs.size() * sizeof(probs[0]), cudaMemcpyHostToDevice, st));
+    PGX_CUDA(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(GemmTile), cudaMemcpyHostToDevice, st));
+    gemm_tiles_kernel<TA, TB, TC><<<(unsigned)tiles.size(), GEMM_THREADS, 0, st>>>(
+        static_cast<const GemmProblem<TA, TB, TC>*>(d_probs), static_cast<const GemmTile*>(d_tiles));
+    check_launch("gemm_tiles_kernel");
+}
+
+}  // namespace pgx

@@ -1,0 +1,116 @@
+// Internal state of a libpgx context (host side of the device runtime).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "pgx_common.cuh"
+
+namespace pgx {
+
+// Device allocation owned by a context.
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t n) {
+        if (n <= bytes) return;
+        release();
+        if (n == 0) return;
+        cudaError_t e = cudaMalloc(&p, n);
+        if (e != cudaSuccess) {
+            p = nullptr;
+            bytes = 0;
+            cudaGetLastError();
+            throw Error{PGX_ERR_OOM, "cudaMalloc(" + std::to_string(n) + " bytes) failed"};
+        }
+        bytes = n;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// One rotated monomial operator.
+struct OpPart {
+    int right, left;     // blocks
+    int dl, dr;          // sizes
+    long off;            // element offset of the rotated matrix in Operator::mat
+};
+
+struct Operator {
+    std::vector<OpPart> parts;
+    std::vector<int> by_left, by_right;  // block -> part index or -1
+    DevBuf mat;                           // rotated parts (double or cd), row-major dl x dr
+    DevBuf target, coef;                  // Fock action (int per right state, double per right state)
+    std::vector<long> act_off;            // offset into target/coef per part
+    bool rotated = false;
+    bool is_complex = false;
+    long total = 0;                       // elements in mat
+};
+
+// One exact-diagonalisation problem: blocks, eigensystem, weights, operators.
+struct Problem {
+    int nblocks = 0;
+    int dmax = 0;
+    bool is_complex = false;
+    std::vector<int> dims;
+    std::vector<long> moff, eoff;  // matrix / vector offsets
+    long msize = 0, esize = 0;
+    bool have_H = false, have_eig = false, have_w = false;
+    double beta = 0.0, E0 = 0.0, Z = 0.0;
+    std::vector<int> retained;
+
+    DevBuf H, work, work2, U, E, w, dims_d, moff_d, eoff_d, order_d, status;
+    int* d_dims = nullptr;
+    long* d_moff = nullptr;
+    long* d_eoff = nullptr;
+    int* d_order = nullptr;
+    int* d_status = nullptr;
+    double* d_H = nullptr;
+    double* d_work = nullptr;
+    double* d_work2 = nullptr;
+    double* d_U = nullptr;
+    double* d_E = nullptr;
+    double* d_w = nullptr;
+
+    std::vector<Operator> ops;
+};
+
+struct G2Timing {
+    double total_ms = 0, gemm_ms = 0, gemm_flops = 0;
+};
+
+}  // namespace pgx
+
+struct pgx_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    pgx::Problem P;
+    pgx::G2Timing g2t;
+    // scratch for G2 and Lehmann kernels
+    pgx::DevBuf scratch[12];
+};
+
+namespace pgx {
+
+void launch_eigh(Problem& P, cudaStream_t st);
+void launch_weights(Problem& P, double beta, cudaStream_t st);
+void rotate_operator(Problem& P, Operator& op, cudaStream_t st);
+void adjoint_operator(Problem& P, const Operator& src, Operator& dst, cudaStream_t st);
+void run_gf(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,
+            const double* z, double coef_tol, double* out);
+void run_susc(pgx_ctx* c, int opA, int opB, int nparts, const int32_t* outer, const int32_t* inner, int nz,
+              const double* z, double pole_res, double coef_tol, double beta, double* out, double* zero_pole);
+void run_ensemble_average(pgx_ctx* c, int op, double* out);
+void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
+            double coef_tol, int flags, double* out);
+
+}  // namespace pgx

@@ -1,0 +1,225 @@
+"""ctypes binding of libpgx's C ABI (include/pgx.h).
+
+This is the Python face of the CUDA engine: plain numpy arrays in and out,
+no torch types.  Loading fails loudly when the library is missing; there is
+no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libpgx.so"
+
+PGX_OK, PGX_ERR_ARG, PGX_ERR_OOM, PGX_ERR_CUDA, PGX_ERR_TIMEOUT, PGX_ERR_NUMERIC, PGX_ERR_STATE, PGX_ERR_NODEV = range(8)
+PGX_G2_EXACT, PGX_G2_REFERENCE_RULE = 0, 1
+
+EXPORTS = [
+    "pgx_version", "pgx_create", "pgx_destroy", "pgx_last_error", "pgx_set_blocks", "pgx_set_hamiltonian",
+    "pgx_eigh", "pgx_get_eigensystem", "pgx_ground_energy", "pgx_weights", "pgx_truncate_blocks",
+    "pgx_op_define", "pgx_op_rotate", "pgx_op_adjoint", "pgx_op_info", "pgx_op_read", "pgx_gf", "pgx_susc",
+    "pgx_ensemble_average", "pgx_g2", "pgx_g2_last_timing",
+]
+
+
+class PgxError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"pgx error {code}: {msg}")
+        self.code = code
+
+
+class G2Part(C.Structure):
+    _fields_ = [("op", C.c_int32 * 4), ("block", C.c_int32 * 4), ("perm", C.c_int32 * 3), ("sign", C.c_int32)]
+
+
+_lib = None
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            raise ImportError(f"libpgx not built: {LIB_PATH} missing (run python -m pomerol_b200.build)")
+        lib = C.CDLL(str(LIB_PATH))
+        P, I32, D = C.c_void_p, C.c_int32, C.c_double
+        lib.pgx_last_error.restype = C.c_char_p
+        lib.pgx_last_error.argtypes = [P]
+        lib.pgx_create.argtypes = [C.c_int, C.POINTER(P)]
+        lib.pgx_destroy.argtypes = [P]
+        lib.pgx_set_blocks.argtypes = [P, I32, P, I32]
+        lib.pgx_set_hamiltonian.argtypes = [P, P]
+        lib.pgx_eigh.argtypes = [P]
+        lib.pgx_get_eigensystem.argtypes = [P, P, P]
+        lib.pgx_ground_energy.argtypes = [P, P]
+        lib.pgx_weights.argtypes = [P, D, P, P]
+        lib.pgx_truncate_blocks.argtypes = [P, D, P]
+        lib.pgx_op_define.argtypes = [P, I32, P, P, P, P, P]
+        lib.pgx_op_rotate.argtypes = [P, I32]
+        lib.pgx_op_adjoint.argtypes = [P, I32, P]
+        lib.pgx_op_info.argtypes = [P, I32, P, P, P]
+        lib.pgx_op_read.argtypes = [P, I32, I32, P]
+        lib.pgx_gf.argtypes = [P, I32, I32, I32, P, P, I32, P, D, P]
+        lib.pgx_susc.argtypes = [P, I32, I32, I32, P, P, I32, P, D, D, D, P, P]
+        lib.pgx_ensemble_average.argtypes = [P, I32, P]
+        lib.pgx_g2.argtypes = [P, I32, P, I32, P, D, D, I32, P]
+        lib.pgx_g2_last_timing.argtypes = [P, P, P, P]
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+class Engine:
+    """One libpgx context (one GPU, one stream, one ED problem)."""
+
+    def __init__(self, device: int = 0):
+        self.lib = load()
+        h = C.c_void_p()
+        rc = self.lib.pgx_create(int(device), C.byref(h))
+        if rc != PGX_OK:
+            raise PgxError(rc, "pgx_create failed (no CUDA device?)")
+        self.h = h
+        self.dims = None
+        self.is_complex = False
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pgx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _ck(self, rc):
+        if rc != PGX_OK:
+            raise PgxError(rc, self.lib.pgx_last_error(self.h).decode())
+
+    # ---- blocks / eigensystem
+    def set_blocks(self, dims, is_complex=False):
+        self.dims = np.ascontiguousarray(dims, dtype=np.int32)
+        self.is_complex = bool(is_complex)
+        self._ck(self.lib.pgx_set_blocks(self.h, len(self.dims), _p(self.dims), int(is_complex)))
+        self.eoff = np.concatenate([[0], np.cumsum(self.dims)]).astype(np.int64)
+        self.moff = np.concatenate([[0], np.cumsum(self.dims.astype(np.int64) ** 2)]).astype(np.int64)
+
+    def set_hamiltonian(self, blocks):
+        packed = np.concatenate([np.ascontiguousarray(b, dtype=complex if self.is_complex else float).ravel()
+                                 for b in blocks])
+        if self.is_complex:
+            packed = packed.view(np.float64)
+        packed = np.ascontiguousarray(packed)
+        self._ck(self.lib.pgx_set_hamiltonian(self.h, _p(packed)))
+
+    def eigh(self):
+        self._ck(self.lib.pgx_eigh(self.h))
+
+    def eigensystem(self):
+        E = np.empty(int(self.eoff[-1]))
+        U = np.empty(int(self.moff[-1]) * (2 if self.is_complex else 1))
+        self._ck(self.lib.pgx_get_eigensystem(self.h, _p(E), _p(U)))
+        if self.is_complex:
+            U = U.view(complex)
+        Es = [E[self.eoff[b]:self.eoff[b + 1]] for b in range(len(self.dims))]
+        Us = [U[self.moff[b]:self.moff[b + 1]].reshape(d, d) for b, d in enumerate(self.dims)]
+        return Es, Us
+
+    def weights(self, beta):
+        w = np.empty(int(self.eoff[-1]))
+        Z = np.zeros(1)
+        self._ck(self.lib.pgx_weights(self.h, float(beta), _p(w), _p(Z)))
+        return [w[self.eoff[b]:self.eoff[b + 1]] for b in range(len(self.dims))], float(Z[0])
+
+    def truncate_blocks(self, tol):
+        r = np.zeros(len(self.dims), dtype=np.int32)
+        self._ck(self.lib.pgx_truncate_blocks(self.h, float(tol), _p(r)))
+        return r.astype(bool)
+
+    # ---- operators
+    def op_define(self, parts):
+        """parts: list of (right_block, left_block, target[int], coef[float])."""
+        rb = np.array([p[0] for p in parts], dtype=np.int32)
+        lb = np.array([p[1] for p in parts], dtype=np.int32)
+        tg = np.ascontiguousarray(np.concatenate([np.asarray(p[2]) for p in parts]) if parts else np.zeros(0),
+                                  dtype=np.int32)
+        cf = np.ascontiguousarray(np.concatenate([np.asarray(p[3]) for p in parts]) if parts else np.zeros(0),
+                                  dtype=np.float64)
+        out = np.zeros(1, dtype=np.int32)
+        self._ck(self.lib.pgx_op_define(self.h, len(parts), _p(rb), _p(lb), _p(tg), _p(cf), _p(out)))
+        return int(out[0])
+
+    def op_rotate(self, op):
+        self._ck(self.lib.pgx_op_rotate(self.h, int(op)))
+
+    def op_adjoint(self, op):
+        out = np.zeros(1, dtype=np.int32)
+        self._ck(self.lib.pgx_op_adjoint(self.h, int(op), _p(out)))
+        return int(out[0])
+
+    def op_info(self, op):
+        n = np.zeros(1, dtype=np.int32)
+        self._ck(self.lib.pgx_op_info(self.h, int(op), _p(n), None, None))
+        r = np.zeros(max(int(n[0]), 1), dtype=np.int32)
+        l = np.zeros(max(int(n[0]), 1), dtype=np.int32)
+        self._ck(self.lib.pgx_op_info(self.h, int(op), _p(n), _p(r), _p(l)))
+        return [(int(r[i]), int(l[i])) for i in range(int(n[0]))]
+
+    def op_read(self, op, part):
+        R, L = self.op_info(op)[part]
+        out = np.empty(int(self.dims[L]) * int(self.dims[R]) * (2 if self.is_complex else 1))
+        self._ck(self.lib.pgx_op_read(self.h, int(op), int(part), _p(out)))
+        if self.is_complex:
+            out = out.view(complex)
+        return out.reshape(int(self.dims[L]), int(self.dims[R]))
+
+    # ---- Lehmann sums
+    def gf(self, op1, op2, outer, inner, z, coef_tol=1e-8):
+        z = np.ascontiguousarray(np.asarray(z, dtype=complex))
+        o = np.ascontiguousarray(outer, dtype=np.int32)
+        i = np.ascontiguousarray(inner, dtype=np.int32)
+        out = np.zeros(len(z), dtype=complex)
+        self._ck(self.lib.pgx_gf(self.h, op1, op2, len(o), _p(o), _p(i), len(z), _p(z.view(np.float64)),
+                                 float(coef_tol), _p(out.view(np.float64))))
+        return out
+
+    def susc(self, opA, opB, outer, inner, z, beta, pole_res=1e-8, coef_tol=1e-8):
+        z = np.ascontiguousarray(np.asarray(z, dtype=complex))
+        o = np.ascontiguousarray(outer, dtype=np.int32)
+        i = np.ascontiguousarray(inner, dtype=np.int32)
+        out = np.zeros(len(z), dtype=complex)
+        zp = np.zeros(1, dtype=complex)
+        self._ck(self.lib.pgx_susc(self.h, opA, opB, len(o), _p(o), _p(i), len(z), _p(z.view(np.float64)),
+                                   float(pole_res), float(coef_tol), float(beta), _p(out.view(np.float64)),
+                                   _p(zp.view(np.float64))))
+        return out, complex(zp[0])
+
+    def ensemble_average(self, op):
+        out = np.zeros(1, dtype=complex)
+        self._ck(self.lib.pgx_ensemble_average(self.h, int(op), _p(out.view(np.float64))))
+        return complex(out[0])
+
+    def g2(self, parts, triples, pole_res=1e-8, coef_tol=1e-16, flags=PGX_G2_EXACT):
+        """parts: list of (ops[4], blocks[4], perm[3], sign); triples: (n,3) complex."""
+        arr = (G2Part * max(len(parts), 1))()
+        for k, (ops, blocks, perm, sign) in enumerate(parts):
+            arr[k].op[:] = list(ops)
+            arr[k].block[:] = list(blocks)
+            arr[k].perm[:] = list(perm)
+            arr[k].sign = int(sign)
+        z = np.ascontiguousarray(np.asarray(triples, dtype=complex).reshape(-1, 3))
+        out = np.zeros(len(z), dtype=complex)
+        self._ck(self.lib.pgx_g2(self.h, len(parts), C.cast(arr, C.c_void_p), len(z), _p(z.view(np.float64)),
+                                 float(pole_res), float(coef_tol), int(flags), _p(out.view(np.float64))))
+        return out
+
+    def g2_timing(self):
+        t = np.zeros(3)
+        self._ck(self.lib.pgx_g2_last_timing(self.h, _p(t[0:1]), _p(t[1:2]), _p(t[2:3])))
+        return {"total_ms": t[0], "gemm_ms": t[1], "gemm_flops": t[2]}

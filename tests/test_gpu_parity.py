@@ -1,0 +1,224 @@
+"""GPU parity through the C ABI (libpgx) against the CPU oracle and the
+reference's known-answer tests.  Tolerances: eigen-residuals 1e-10 (as
+HamiltonianTest.cpp:80-89), golden vectors at the reference tests' own
+tolerances, and GPU-vs-oracle on the same inputs at 1e-10 relative (FP64)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from oracle import ed as EDm
+from oracle import lehmann as L
+from oracle import model as M
+
+pytestmark = pytest.mark.gpu
+
+KATS = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "reference_kats.json")))
+
+
+@pytest.fixture(scope="module")
+def harness():
+    from tests.pgx_harness import GpuED
+    return GpuED
+
+
+def cplx(a):
+    return np.array([complex(x, y) for x, y in a])
+
+
+def plaquette_expr():
+    k = KATS["gf4site"]
+    e = M.Expr()
+    for lab, U, eps in k["coulomb"]:
+        e += M.CoulombS(lab, U, eps)
+    for a, b, t in k["hopping"]:
+        e += M.Hopping(a, b, t)
+    return e
+
+
+def test_eigh_residual_and_order(harness):
+    m = M.make_model(plaquette_expr())
+    g = harness(m, 10.0)
+    for b in range(len(m.blocks)):
+        h = m.h_block(b)
+        E, U = g.E[b], g.U[b]
+        assert np.all(np.diff(E) >= -1e-14)
+        assert np.abs(h @ U - U * E[None, :]).max() < 1e-10
+        assert np.abs(U.T @ U - np.eye(len(E))).max() < 1e-12
+        assert np.abs(E - np.linalg.eigvalsh(h)).max() < 1e-11
+
+
+def test_eigh_larger_blocks(harness):
+    """Random symmetric blocks up to 300 with a degenerate spectrum."""
+    rng = np.random.default_rng(7)
+    dims = [1, 2, 3, 17, 64, 129, 300]
+    blocks = []
+    for d in dims:
+        a = rng.standard_normal((d, d))
+        h = (a + a.T) / 2
+        if d == 129:   # exact degeneracies
+            q, _ = np.linalg.qr(rng.standard_normal((d, d)))
+            ev = np.repeat(np.arange(43.0), 3)
+            h = (q * ev) @ q.T
+        blocks.append(h)
+    from pomerol_b200.pgx import Engine
+    eng = Engine()
+    eng.set_blocks(dims)
+    eng.set_hamiltonian(blocks)
+    eng.eigh()
+    E, U = eng.eigensystem()
+    for h, e, u in zip(blocks, E, U):
+        scale = max(1.0, np.abs(e).max())
+        assert np.abs(h @ u - u * e[None, :]).max() < 1e-10 * scale
+        assert np.abs(u.T @ u - np.eye(len(e))).max() < 1e-11
+        assert np.abs(e - np.linalg.eigvalsh(h)).max() < 1e-11 * scale
+
+
+def test_hamiltonian_ground_energy(harness):
+    e = M.CoulombS("A", 1.0, -0.5) + M.CoulombS("B", 2.0, -1.0) + M.Hopping("A", "B", -1.0)
+    g = harness(M.make_model(e), 10.0)
+    assert abs(min(x.min() for x in g.E) - KATS["hamiltonian"]["E0"]) < 1e-7
+
+
+def test_weights_and_rotation_match_oracle(harness):
+    m = M.make_model(plaquette_expr())
+    g = harness(m, 10.0)
+    ed = EDm.ED(m, 10.0)
+    for b in range(len(m.blocks)):
+        assert np.abs(g.w[b] - ed.w[b]).max() < 1e-13
+    # rotation with the GPU's own eigenvectors (gauge fixed by the same U)
+    ix = m.info.getIndex("A", 0, 0)
+    op = g.cdag(ix)
+    for k, (R, Lb) in enumerate(g.eng.op_info(op)):
+        Lb2, tgt, sg = m.monomial_parts(((True, m.info.tuples[ix]),))[R]
+        assert Lb2 == Lb
+        G = np.zeros((len(m.blocks[Lb]), len(m.blocks[R])))
+        ok = tgt >= 0
+        np.add.at(G, tgt[ok], sg[ok, None] * g.U[R][ok, :])
+        ref = g.U[Lb].T @ G
+        assert np.abs(g.eng.op_read(op, k) - ref).max() < 1e-12
+    c = g.c(ix)
+    for k, (R, Lb) in enumerate(g.eng.op_info(c)):
+        kk = [i for i, (r2, l2) in enumerate(g.eng.op_info(op)) if r2 == Lb][0]
+        assert np.abs(g.eng.op_read(c, k) - g.eng.op_read(op, kk).T).max() == 0.0
+
+
+def test_gf1site_closed_form(harness):
+    U, mu, beta = 1.0, 0.4, 10.0
+    m = M.make_model(M.CoulombS("A", U, -mu))
+    g = harness(m, beta)
+    dn = m.info.getIndex("A", 0, 0)
+    n = np.arange(-100, 100)
+    om = np.pi * (2 * n + 1) / beta
+    w0, w1, w2 = 1.0, np.exp(beta * mu), np.exp(-beta * (-2 * mu + U))
+    Z = w0 + 2 * w1 + w2
+    ref = (w0 + w1) / Z / (1j * om + mu) + (w1 + w2) / Z / (1j * om + mu - U)
+    v = g.gf(g.c(dn), g.cdag(dn), 1j * om)
+    assert np.abs(v - ref).max() < 1e-14
+
+
+def test_gf4site_golden(harness):
+    k = KATS["gf4site"]
+    m = M.make_model(plaquette_expr())
+    g = harness(m, k["beta"])
+    dn = m.info.getIndex("A", 0, 0)
+    v = g.gf(g.c(dn), g.cdag(dn), L.fermionic(np.arange(10), k["beta"]))
+    assert np.abs(v - cplx(k["G_A_down"])).max() < k["tol"]
+    ed = EDm.ED(m, k["beta"])
+    ref = L.gf_eval(L.gf_terms(ed, ed.c(dn), ed.cdag(dn), rule=False), L.fermionic(np.arange(256), k["beta"]))
+    v = g.gf(g.c(dn), g.cdag(dn), L.fermionic(np.arange(256), k["beta"]), coef_tol=0.0)
+    assert np.abs(v - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+def test_anderson_golden(harness):
+    k = KATS["anderson"]
+    U = k["U"]
+    e = (M.CoulombS("C", U, -k["mu_over_U"] * U) + M.Magnetization("C", k["h"])
+         + M.Level("0", -k["epsilon"]) + M.Level("1", k["epsilon"])
+         + M.Hopping("C", "0", k["V"]) + M.Hopping("C", "1", k["V"]))
+    m = M.make_model(e)
+    g = harness(m, k["beta"])
+    z = L.fermionic(np.arange(10), k["beta"])
+    for s, key in ((1, "G_up"), (0, "G_down")):
+        i = m.info.getIndex("C", 0, s)
+        assert np.abs(g.gf(g.c(i), g.cdag(i), z) - cplx(k[key])).max() < k["tol"]
+
+
+def test_susceptibility_closed_form(harness):
+    U, mu, h, beta = 1.0, 0.4, 0.01, 10.0
+    m = M.make_model(M.CoulombS("A", U, -mu) + M.Magnetization("A", -h))
+    g = harness(m, beta)
+    up, dn = m.info.getIndex("A", 0, 1), m.info.getIndex("A", 0, 0)
+    sp, sm = g.quadratic(up, dn), g.quadratic(dn, up)
+    nu, nd = g.quadratic(up, up), g.quadratic(dn, dn)
+    wr = np.array([1.0, np.exp(-beta * (-mu - h)), np.exp(-beta * (-mu + h)), np.exp(-beta * (-2 * mu + U))])
+    wr /= wr.sum()
+    wu, wd, w2 = wr[1:]
+    ea = g.eng.ensemble_average
+    assert abs(ea(sp)) < 1e-14 and abs(ea(nu) - (wu + w2)) < 1e-14 and abs(ea(nd) - (wd + w2)) < 1e-14
+    n = np.arange(20)
+    z = L.bosonic(n, beta)
+    om = 2 * np.pi * n / beta
+    v, _ = g.susc(sp, sm, z)
+    v = v - np.where(n == 0, ea(sp) * ea(sm) * beta, 0)
+    assert np.abs(v - (-(wu - wd) / (1j * om - 2 * h))).max() < 1e-14
+    v, _ = g.susc(nu, nu, z)
+    v = v - np.where(n == 0, ea(nu) * ea(nu) * beta, 0)
+    assert np.abs(v - np.where(n == 0, (wu + w2) * (1 - wu - w2) * beta, 0)).max() < 1e-14
+    v, _ = g.susc(nu, nd, z)
+    v = v - np.where(n == 0, ea(nu) * ea(nd) * beta, 0)
+    assert np.abs(v - np.where(n == 0, (w2 - (wu + w2) * (wd + w2)) * beta, 0)).max() < 1e-14
+
+
+def test_vertex4_closed_form(harness):
+    from tests.test_oracle_golden import _vertex4_refs
+    U, beta, n_iw = 1.0, 40.0, 4
+    m = M.make_model(M.CoulombS("A", U, -U / 2))
+    g = harness(m, beta)
+    up, dn = m.info.getIndex("A", 0, 1), m.info.getIndex("A", 0, 0)
+    GFv = {i: g.gf(g.c(i), g.cdag(i), L.fermionic(np.arange(-3 * n_iw, 3 * n_iw), beta)) for i in (up, dn)}
+    GF = lambda i, n: GFv[i][n + 3 * n_iw]
+    g_uuuu, g_udud, delta = _vertex4_refs(U, beta)
+    trip = [(a, b, x) for a in range(-n_iw, n_iw) for b in range(-n_iw, n_iw) for x in range(-n_iw, n_iw)]
+    fz = np.array([L.fermionic(np.array(t), beta) for t in trip])
+    for (i, j, k, l), tol in (((up, up, up, up), 1e-6), ((up, dn, up, dn), 1e-10)):
+        v, _ = g.g2(g.c(i), g.c(j), g.cdag(k), g.cdag(l), fz, pole_res=1e-4)
+        for t, (n1, n2, n3) in enumerate(trip):
+            n4 = n1 + n2 - n3
+            if j == up:
+                ref = (g_uuuu(n1, n2, n3) * GF(up, n1) * GF(up, n2) * GF(up, n3) * GF(up, n4)
+                       + beta * GF(up, n1) * GF(up, n2) * delta(n1, n4) - beta * GF(up, n1) * GF(up, n2) * delta(n1, n3))
+            else:
+                ref = (g_udud(n1, n2, n3) * GF(up, n1) * GF(dn, n2) * GF(up, n3) * GF(dn, n4)
+                       - beta * GF(up, n1) * GF(dn, n2) * delta(n1, n3))
+            assert abs(v[t] - ref) < tol, (n1, n2, n3)
+
+
+def test_anderson2pgf_golden(harness):
+    from tests.test_oracle_golden import anderson2pgf_freqs, anderson2pgf_model
+    k, e = anderson2pgf_model()
+    m = M.make_model(e)
+    g = harness(m, k["beta"])
+    fz = np.array(anderson2pgf_freqs(k["beta"]))
+    for s in (M.UP, M.DOWN):
+        i = m.info.getIndex("C", 0, s)
+        v, _ = g.g2(g.c(i), g.c(i), g.cdag(i), g.cdag(i), fz, pole_res=k["pole_resolution"])
+        assert np.abs(v - np.array(k["chi_uuuu"])).max() < k["tol"]
+
+
+def test_plaquette_g2_matches_oracle(harness):
+    """Plaquette (t=1, U=4, mu=2, beta=10), chi_(u0,d0,u0,d0) on n in [-4,3]^3."""
+    beta = 10.0
+    m = M.make_model(M.plaquette())
+    g = harness(m, beta)
+    ed = EDm.ED(m, beta)
+    u, d = m.info.getIndex("A", 0, 1), m.info.getIndex("A", 0, 0)
+    trip = [(a, b, x) for a in range(-4, 4) for b in range(-4, 4) for x in range(-4, 4)]
+    fz = np.array([L.fermionic(np.array(t), beta) for t in trip])
+    v, parts = g.g2(g.c(u), g.c(d), g.cdag(u), g.cdag(d), fz)
+    oparts = L.g2_parts(ed, ed.c(u), ed.c(d), ed.cdag(u), ed.cdag(d))
+    assert len(parts) == len(oparts)
+    sel = list(range(0, len(trip), 37))
+    ref = L.g2_exact(ed, oparts, [tuple(fz[t]) for t in sel])
+    assert np.abs(v[sel] - ref).max() < 1e-10 * np.abs(ref).max()
