@@ -167,6 +167,20 @@ typedef struct pgx_g2_part {
 int pgx_g2(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, int32_t nfreq, const double* z,
            double pole_res, double coef_tol, int32_t flags, double* out);
 
+/* Number of state quadruples the reference enumerates for these parts
+ * (TwoParticleGFPart.cpp:210-250): all four rotated elements |x| > nz_tol and
+ * w1 + w2 + w3 + w4 > coef_tol.  The work unit of the G2 throughput metric. */
+int pgx_g2_count(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, double coef_tol, double nz_tol,
+                 long long* count);
+
+/* Device-side timing of everything the context issues between the two
+ * calls (CUDA events on the context's stream). */
+int pgx_timer_begin(pgx_ctx* ctx);
+int pgx_timer_end(pgx_ctx* ctx, double* ms);
+
+/* Number of kernels this library has launched in this process. */
+long long pgx_launch_count(void);
+
 /* Device time (ms) of the last pgx_g2 call and its dominant GEMM stage. */
 int pgx_g2_last_timing(pgx_ctx* ctx, double* total_ms, double* gemm_ms, double* gemm_flops);
 

@@ -25,6 +25,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdint>
+#include <algorithm>
 #include <cstring>
 #include <unordered_map>
 #include <vector>
@@ -123,14 +124,14 @@ long long g2o_part(int d1, int d2, int d3, int d4, const double* O1, const doubl
                    const double* X4, const double* E1, const double* E2, const double* E3, const double* E4,
                    const double* w1, const double* w2, const double* w3, const double* w4, const int* perm, int sign,
                    double beta, double pole_res, double coef_tol, double nz_tol, int rule, int nfreq, const double* z,
-                   int row_begin, int row_end, double* out, long long* terms_out, int nthreads) {
+                   int row_begin, int row_end, int row_step, double* out, long long* terms_out, int nthreads) {
     TermList NR{pole_res, coef_tol, {}}, RS{pole_res, coef_tol, {}};
     std::vector<Term> nr_plain, rs_plain;  // exact mode keeps every term
     std::vector<int> flags_nr, flags_rs;
     long long nq = 0;
     std::vector<int> l4;
     const double ctol = rule ? coef_tol : -1.0;
-    for (int i1 = row_begin; i1 < row_end; ++i1) {
+    for (int i1 = row_begin; i1 < row_end; i1 += std::max(row_step, 1)) {
         for (int i3 = 0; i3 < d3; ++i3) {
             l4.clear();
             for (int i4 = 0; i4 < d4; ++i4)

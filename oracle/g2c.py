@@ -21,7 +21,7 @@ def lib():
         L.g2o_count.restype = C.c_longlong
         L.g2o_count.argtypes = [I, I, I, I] + [P] * 8 + [D, D]
         L.g2o_part.restype = C.c_longlong
-        L.g2o_part.argtypes = [I, I, I, I] + [P] * 12 + [P, I, D, D, D, D, I, I, P, I, I, P, P, I]
+        L.g2o_part.argtypes = [I, I, I, I] + [P] * 12 + [P, I, D, D, D, D, I, I, P, I, I, I, P, P, I]
         _LIB = L
     return _LIB
 
@@ -60,12 +60,12 @@ def evaluate(ed, parts, freqs, pole_res=1e-8, coef_tol=1e-16, rule=True, nz_tol=
     for k in sel:
         p = parts[k]
         dims, mats, E, w = _part_arrays(ed, p)
-        r0, r1 = (0, dims[0]) if rows is None else (rows[1], rows[2])
+        r0, r1, rs = (0, dims[0], 1) if rows is None else (rows[1], rows[2], rows[3] if len(rows) > 3 else 1)
         perm = np.ascontiguousarray(p["perm"], dtype=np.int32)
         t = np.zeros(2, dtype=np.int64)
         nq += lib().g2o_part(*dims, *[m.ctypes.data for m in mats], *[x.ctypes.data for x in E],
                              *[x.ctypes.data for x in w], perm.ctypes.data, int(p["sign"]), ed.beta, pole_res,
-                             coef_tol, nz_tol, int(rule), out.size // 2, z.ctypes.data, r0, r1, out.ctypes.data,
-                             t.ctypes.data, int(nthreads))
+                             coef_tol, nz_tol, int(rule), out.size // 2, z.ctypes.data, r0, r1, rs,
+                             out.ctypes.data, t.ctypes.data, int(nthreads))
         terms += t
     return out.view(complex), nq, terms

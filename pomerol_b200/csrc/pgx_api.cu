@@ -10,6 +10,10 @@
 
 namespace pgx {
 void launch_retained(Problem& P, double tol, int* d_flags, cudaStream_t st);
+long long& launch_counter() {
+    static long long n = 0;
+    return n;
+}
 }
 
 using pgx::Error;
@@ -79,6 +83,8 @@ int pgx_destroy(pgx_ctx* c) {
     cudaStreamSynchronize(c->stream);
     reset_problem(c->P);
     for (auto& b : c->scratch) b.release();
+    if (c->ev_begin) cudaEventDestroy(c->ev_begin);
+    if (c->ev_end) cudaEventDestroy(c->ev_end);
     cudaStreamDestroy(c->stream);
     delete c;
     return PGX_OK;
@@ -361,6 +367,35 @@ int pgx_g2(pgx_ctx* c, int32_t nparts, const pgx_g2_part* parts, int32_t nfreq, 
         pgx::run_g2(c, nparts, parts, nfreq, z, pole_res, coef_tol, flags, out);
     });
 }
+
+int pgx_g2_count(pgx_ctx* c, int32_t nparts, const pgx_g2_part* parts, double coef_tol, double nz_tol,
+                 long long* count) {
+    return guarded(c, [&] {
+        PGX_CHECK(nparts >= 0 && (nparts == 0 || parts) && count, PGX_ERR_ARG, "bad arguments");
+        pgx::run_g2_count(c, nparts, parts, coef_tol, nz_tol, count);
+    });
+}
+
+int pgx_timer_begin(pgx_ctx* c) {
+    return guarded(c, [&] {
+        if (!c->ev_begin) PGX_CUDA(cudaEventCreate(&c->ev_begin));
+        if (!c->ev_end) PGX_CUDA(cudaEventCreate(&c->ev_end));
+        PGX_CUDA(cudaEventRecord(c->ev_begin, c->stream));
+    });
+}
+
+int pgx_timer_end(pgx_ctx* c, double* ms) {
+    return guarded(c, [&] {
+        PGX_CHECK(c->ev_begin && ms, PGX_ERR_STATE, "pgx_timer_begin first");
+        PGX_CUDA(cudaEventRecord(c->ev_end, c->stream));
+        PGX_CUDA(cudaEventSynchronize(c->ev_end));
+        float t = 0.f;
+        PGX_CUDA(cudaEventElapsedTime(&t, c->ev_begin, c->ev_end));
+        *ms = t;
+    });
+}
+
+long long pgx_launch_count(void) { return pgx::launch_counter(); }
 
 int pgx_g2_last_timing(pgx_ctx* c, double* total_ms, double* gemm_ms, double* gemm_flops) {
     return guarded(c, [&] {

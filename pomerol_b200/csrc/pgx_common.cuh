@@ -57,7 +57,11 @@ struct Error {
         if (!(cond)) throw ::pgx::Error{(code), std::string(text)}; \
     } while (0)
 
+// Kernel launches issued by this library (process-wide).
+long long& launch_counter();
+
 inline void check_launch(const char* what) {
+    ++launch_counter();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) throw Error{PGX_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e)};
 }

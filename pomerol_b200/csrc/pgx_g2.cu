@@ -147,6 +147,53 @@ __global__ void __launch_bounds__(CT_THREADS) contract_kernel(ContractArgs g) {
     }
 }
 
+// Number of state quadruples of one chain that the reference enumerates
+// (TwoParticleGFPart.cpp:210-250): all four rotated elements non-zero
+// (|x| > nz) and w1 + w2 + w3 + w4 > tol.  One thread per (i1, i3).  When
+// w1 + w3 > tol every (i2, i4) of the pair counts; otherwise a pair only
+// fails when all four weights are below tol, and the cold (i2, i4) pairs are
+// enumerated only for i2 close enough to the threshold to matter.
+template <typename T>
+__global__ void count_kernel(const T* O1, const T* O2, const T* O3, const T* X4, int d1, int d2, int d3, int d4,
+                             const double* w1, const double* w2, const double* w3, const double* w4, double tol,
+                             double nz, double cold_max4, unsigned long long* out) {
+    const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    unsigned long long cnt = 0;
+    if (idx < (long)d1 * d3) {
+        const int i1 = (int)(idx / d3), i3 = (int)(idx % d3);
+        const double a = w1[i1] + w3[i3];
+        long n2 = 0, n4 = 0, n2c = 0, n4c = 0;
+        for (int i2 = 0; i2 < d2; ++i2) {
+            const bool v = sqrt(abs2(tocd(O1[(long)i1 * d2 + i2]))) > nz && sqrt(abs2(tocd(O2[(long)i2 * d3 + i3]))) > nz;
+            n2 += v;
+            n2c += v && !(w2[i2] > tol);
+        }
+        for (int i4 = 0; i4 < d4; ++i4) {
+            const bool v = sqrt(abs2(tocd(O3[(long)i3 * d4 + i4]))) > nz && sqrt(abs2(tocd(X4[(long)i4 * d1 + i1]))) > nz;
+            n4 += v;
+            n4c += v && !(w4[i4] > tol);
+        }
+        if (a > tol) {
+            cnt = (unsigned long long)(n2 * n4);
+        } else {
+            cnt = (unsigned long long)(n2 * n4 - n2c * n4c);
+            const double t = tol - a;
+            for (int i2 = 0; i2 < d2; ++i2) {
+                if (w2[i2] > tol || !(w2[i2] + cold_max4 > t)) continue;
+                if (!(sqrt(abs2(tocd(O1[(long)i1 * d2 + i2]))) > nz && sqrt(abs2(tocd(O2[(long)i2 * d3 + i3]))) > nz)) continue;
+                for (int i4 = 0; i4 < d4; ++i4) {
+                    if (w4[i4] > tol) continue;
+                    const bool v =
+                        sqrt(abs2(tocd(O3[(long)i3 * d4 + i4]))) > nz && sqrt(abs2(tocd(X4[(long)i4 * d1 + i1]))) > nz;
+                    cnt += v && (w2[i2] + w4[i4] > t);
+                }
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
 // Frequency plan of one permutation: distinct z1, z3, distinct (z1, z3)
 // pairs, and the triples of each pair in CSR order with the four s values.
 struct Plan {
@@ -499,6 +546,60 @@ void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const d
     cudaEventDestroy(e1);
     cudaEventDestroy(ea);
     cudaEventDestroy(eb);
+}
+
+}  // namespace pgx
+
+namespace pgx {
+
+void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_tol, double nz_tol,
+                  long long* count) {
+    Problem& P = c->P;
+    cudaStream_t st = c->stream;
+    PGX_CHECK(P.have_w, PGX_ERR_STATE, "weights must be computed before counting");
+    DevBuf& b = c->scratch[10];
+    b.reserve(sizeof(unsigned long long));
+    PGX_CUDA(cudaMemsetAsync(b.p, 0, sizeof(unsigned long long), st));
+    std::vector<double> w(P.esize);
+    PGX_CUDA(cudaMemcpyAsync(w.data(), P.d_w, P.esize * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaStreamSynchronize(st));
+    for (int q = 0; q < nparts; ++q) {
+        const pgx_g2_part& gp = parts[q];
+        for (int k = 0; k < 4; ++k) {
+            PGX_CHECK(gp.op[k] >= 0 && gp.op[k] < (int)P.ops.size() && gp.block[k] >= 0 && gp.block[k] < P.nblocks,
+                      PGX_ERR_ARG, "bad G2 part");
+            const Operator& o = P.ops[gp.op[k]];
+            const int pi = o.by_left[gp.block[k]];
+            PGX_CHECK(o.rotated && pi >= 0 && o.parts[pi].right == gp.block[(k + 1) % 4], PGX_ERR_ARG,
+                      "G2 part is not a block chain of rotated operators");
+        }
+        const int S1 = gp.block[0], S2 = gp.block[1], S3 = gp.block[2], S4 = gp.block[3];
+        const int d1 = P.dims[S1], d2 = P.dims[S2], d3 = P.dims[S3], d4 = P.dims[S4];
+        double cold4 = 0.0;
+        for (int i = 0; i < d4; ++i) {
+            const double x = w[P.eoff[S4] + i];
+            if (!(x > coef_tol)) cold4 = std::max(cold4, x);
+        }
+        const Operator &o1 = P.ops[gp.op[0]], &o2 = P.ops[gp.op[1]], &o3 = P.ops[gp.op[2]], &o4 = P.ops[gp.op[3]];
+        const long n = (long)d1 * d3;
+        const double *w1 = P.d_w + P.eoff[S1], *w2 = P.d_w + P.eoff[S2], *w3 = P.d_w + P.eoff[S3], *w4 = P.d_w + P.eoff[S4];
+        if (P.is_complex) {
+            count_kernel<cd><<<ceil_div(n, 256), 256, 0, st>>>(
+                o1.mat.as<cd>() + o1.parts[o1.by_left[S1]].off, o2.mat.as<cd>() + o2.parts[o2.by_left[S2]].off,
+                o3.mat.as<cd>() + o3.parts[o3.by_left[S3]].off, o4.mat.as<cd>() + o4.parts[o4.by_left[S4]].off, d1, d2,
+                d3, d4, w1, w2, w3, w4, coef_tol, nz_tol, cold4, b.as<unsigned long long>());
+        } else {
+            count_kernel<double><<<ceil_div(n, 256), 256, 0, st>>>(
+                o1.mat.as<double>() + o1.parts[o1.by_left[S1]].off, o2.mat.as<double>() + o2.parts[o2.by_left[S2]].off,
+                o3.mat.as<double>() + o3.parts[o3.by_left[S3]].off, o4.mat.as<double>() + o4.parts[o4.by_left[S4]].off,
+                d1, d2, d3, d4, w1, w2, w3, w4, coef_tol, nz_tol, cold4, b.as<unsigned long long>());
+        }
+        check_launch("count_kernel");
+    }
+    unsigned long long h = 0;
+    PGX_CUDA(cudaMemcpyAsync(&h, b.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaStreamSynchronize(st));
+    *count = (long long)h;
 }
 
 }  // namespace pgx

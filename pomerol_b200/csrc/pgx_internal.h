@@ -95,6 +95,7 @@ struct pgx_ctx {
     std::string last_error;
     pgx::Problem P;
     pgx::G2Timing g2t;
+    cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
     // scratch for G2 and Lehmann kernels
     pgx::DevBuf scratch[12];
 };
@@ -112,5 +113,6 @@ void run_susc(pgx_ctx* c, int opA, int opB, int nparts, const int32_t* outer, co
 void run_ensemble_average(pgx_ctx* c, int op, double* out);
 void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
             double coef_tol, int flags, double* out);
+void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_tol, double nz_tol, long long* count);
 
 }  // namespace pgx

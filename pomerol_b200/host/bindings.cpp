@@ -169,7 +169,12 @@ PYBIND11_MODULE(_pomerol, m) {
         .def("getBlockMapping", [](MonomialOperator const& o) { return o.getBlockMapping().right; })
         .def("getPartFromRightIndex", &MonomialOperator::getPartFromRightIndex, py::return_value_policy::reference_internal)
         .def("getPartFromLeftIndex", &MonomialOperator::getPartFromLeftIndex, py::return_value_policy::reference_internal)
-        .def("isComplex", &MonomialOperator::isComplex);
+        .def("isComplex", &MonomialOperator::isComplex)
+        .def("fockAction", [](MonomialOperator const& o) {
+            std::vector<std::tuple<int, int, std::vector<int32_t>, std::vector<double>>> r;
+            for (auto& a : o.fockAction()) r.emplace_back(a.right, a.left, a.target, a.coef);
+            return r;
+        });
     py::class_<FieldOperator, MonomialOperator>(m, "FieldOperator").def("getIndex", &FieldOperator::getIndex);
     py::class_<CreationOperator, FieldOperator>(m, "CreationOperator")
         .def(py::init<IndexClassification const&, HilbertSpace const&, StatesClassification const&, Hamiltonian const&,

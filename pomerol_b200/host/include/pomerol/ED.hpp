@@ -266,6 +266,14 @@ public:
 
     int deviceId() const { return OpId; }
     int devicePart(BlockNumber Right) const;
+    // Fock action per part (right block, left block, inner target per right
+    // state or -1, coefficient): the input of pgx_op_define.
+    struct Action {
+        BlockNumber right, left;
+        std::vector<int32_t> target;
+        std::vector<double> coef;
+    };
+    std::vector<Action> fockAction() const;
     Hamiltonian const& getHamiltonian() const { return H; }
 
 protected:

@@ -398,26 +398,38 @@ void MonomialOperator::prepare(HilbertSpace const& HS) {
     setStatus(Prepared);
 }
 
+std::vector<MonomialOperator::Action> MonomialOperator::fockAction() const {
+    checkPrepared();
+    std::vector<Action> out;
+    for (auto const& p : parts) {
+        Action a{p.getRightIndex(), p.getLeftIndex(), {}, {}};
+        for (QuantumState s : S.getFockStates(p.getRightIndex())) {
+            QuantumState o;
+            double sg;
+            if (Mono.apply(s, o, sg)) {
+                a.target.push_back((int32_t)S.getInnerState(o));
+                a.coef.push_back(sg * Coef.real());
+            } else {
+                a.target.push_back(-1);
+                a.coef.push_back(0.0);
+            }
+        }
+        out.push_back(std::move(a));
+    }
+    return out;
+}
+
 void MonomialOperator::compute(RealType, MPI_Comm const&) {
     checkPrepared();
     if (getStatus() >= Computed) return;
     Device& dev = H.device();
     std::vector<int32_t> rb, lb, tg;
     std::vector<double> cf;
-    for (auto const& p : parts) {
-        rb.push_back(p.getRightIndex());
-        lb.push_back(p.getLeftIndex());
-        for (QuantumState s : S.getFockStates(p.getRightIndex())) {
-            QuantumState o;
-            double sg;
-            if (Mono.apply(s, o, sg)) {
-                tg.push_back((int32_t)S.getInnerState(o));
-                cf.push_back(sg * Coef.real());
-            } else {
-                tg.push_back(-1);
-                cf.push_back(0.0);
-            }
-        }
+    for (auto const& a : fockAction()) {
+        rb.push_back(a.right);
+        lb.push_back(a.left);
+        tg.insert(tg.end(), a.target.begin(), a.target.end());
+        cf.insert(cf.end(), a.coef.begin(), a.coef.end());
     }
     int32_t id = -1;
     dev.check(pgx_op_define(dev.ctx(), (int32_t)parts.size(), rb.data(), lb.data(), tg.data(), cf.data(), &id),

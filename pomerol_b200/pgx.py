@@ -21,7 +21,8 @@ EXPORTS = [
     "pgx_version", "pgx_create", "pgx_destroy", "pgx_last_error", "pgx_set_blocks", "pgx_set_hamiltonian",
     "pgx_eigh", "pgx_get_eigensystem", "pgx_ground_energy", "pgx_weights", "pgx_truncate_blocks",
     "pgx_op_define", "pgx_op_rotate", "pgx_op_adjoint", "pgx_op_info", "pgx_op_read", "pgx_gf", "pgx_susc",
-    "pgx_ensemble_average", "pgx_g2", "pgx_g2_last_timing",
+    "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
+    "pgx_launch_count",
 ]
 
 
@@ -66,6 +67,10 @@ def load():
         lib.pgx_ensemble_average.argtypes = [P, I32, P]
         lib.pgx_g2.argtypes = [P, I32, P, I32, P, D, D, I32, P]
         lib.pgx_g2_last_timing.argtypes = [P, P, P, P]
+        lib.pgx_g2_count.argtypes = [P, I32, P, D, D, P]
+        lib.pgx_timer_begin.argtypes = [P]
+        lib.pgx_timer_end.argtypes = [P, P]
+        lib.pgx_launch_count.restype = C.c_longlong
         _lib = lib
     return _lib
 
@@ -219,7 +224,43 @@ class Engine:
                                  float(pole_res), float(coef_tol), int(flags), _p(out.view(np.float64))))
         return out
 
+    @staticmethod
+    def _parts_array(parts):
+        arr = (G2Part * max(len(parts), 1))()
+        for k, (ops, blocks, perm, sign) in enumerate(parts):
+            arr[k].op[:] = list(ops)
+            arr[k].block[:] = list(blocks)
+            arr[k].perm[:] = list(perm)
+            arr[k].sign = int(sign)
+        return arr
+
+    def g2_count(self, parts, coef_tol=1e-16, nz_tol=1e-12):
+        arr = self._parts_array(parts)
+        out = np.zeros(1, dtype=np.int64)
+        self._ck(self.lib.pgx_g2_count(self.h, len(parts), C.cast(arr, C.c_void_p), float(coef_tol), float(nz_tol),
+                                       _p(out)))
+        return int(out[0])
+
     def g2_timing(self):
         t = np.zeros(3)
         self._ck(self.lib.pgx_g2_last_timing(self.h, _p(t[0:1]), _p(t[1:2]), _p(t[2:3])))
         return {"total_ms": t[0], "gemm_ms": t[1], "gemm_flops": t[2]}
+
+
+def launch_count() -> int:
+    """Kernels launched by libpgx in this process."""
+    return int(load().pgx_launch_count())
+
+
+def _timer_begin(self):
+    self._ck(self.lib.pgx_timer_begin(self.h))
+
+
+def _timer_end(self):
+    ms = np.zeros(1)
+    self._ck(self.lib.pgx_timer_end(self.h, _p(ms)))
+    return float(ms[0])
+
+
+Engine.timer_begin = _timer_begin
+Engine.timer_end = _timer_end

@@ -1,0 +1,174 @@
+"""Synthetic workloads of the G2 path, built through the drop-in API.
+
+  plaquette  2x2 Hubbard plaquette: CoulombS(U=4, -mu=-2) on sites A..D,
+             nearest-neighbour Hopping(t=-1), beta=10, dim 256
+  a5         Anderson impurity + 5 bath sites: CoulombS(U=3, eps_d=-U/2) on
+             "C", Level(b_k, eps_k) + Hopping(C, b_k, V_k) with
+             rng = numpy.random.default_rng(0), eps = rng.uniform(-2,2,5) then
+             V = rng.uniform(0.2,0.8,5); beta=20, dim 4096
+  ring8      8-site Hubbard ring, PBC, t=1, U=4, mu=2, beta=5, dim 65536
+
+The G2 component is chi_(u0,d0,u0,d0) (c_up c_down c^+_up c^+_down at the
+first site) on the fermionic cube n_k in [-N/2, N/2).  No public dataset is
+involved: the inputs are fully specified by these parameters.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _pomerol as P
+
+L = P.LatticePresets
+
+
+def plaquette_expr(t=1.0, U=4.0, mu=2.0):
+    sites = ["A", "B", "C", "D"]
+    e = P.RealExpr()
+    for s in sites:
+        e += L.CoulombS(s, U, -mu)
+    for a, b in zip(sites, sites[1:] + sites[:1]):
+        e += L.Hopping(a, b, -t)
+    return e, "A"
+
+
+def anderson_expr(U, eps_d, eps, V, imp="C"):
+    e = L.CoulombS(imp, U, eps_d)
+    for k, (ek, vk) in enumerate(zip(eps, V)):
+        e += L.Level(f"b{k}", float(ek))
+        e += L.Hopping(imp, f"b{k}", float(vk))
+    return e, imp
+
+
+def a5_params(seed=0, nb=5):
+    rng = np.random.default_rng(seed)
+    eps = rng.uniform(-2, 2, nb)
+    V = rng.uniform(0.2, 0.8, nb)
+    return 3.0, -1.5, eps, V, 20.0
+
+
+def ring_expr(L_sites=8, t=1.0, U=4.0, mu=2.0):
+    sites = [f"S{i}" for i in range(L_sites)]
+    e = P.RealExpr()
+    for s in sites:
+        e += L.CoulombS(s, U, -mu)
+    for i in range(L_sites):
+        e += L.Hopping(sites[i], sites[(i + 1) % L_sites], -t)
+    return e, "S0"
+
+
+CONFIGS = {
+    "plaquette": dict(beta=10.0, nfreq=8, dm_trunc=None),
+    "a5": dict(beta=20.0, nfreq=16, dm_trunc=None),
+    "ring8": dict(beta=5.0, nfreq=24, dm_trunc=1e-12),
+}
+
+
+def expr_of(name):
+    if name == "plaquette":
+        return plaquette_expr()
+    if name == "a5":
+        U, epsd, eps, V, _ = a5_params(0)
+        return anderson_expr(U, epsd, eps, V)
+    if name == "ring8":
+        return ring_expr()
+    raise KeyError(name)
+
+
+def matsubara_cube(beta, nfreq, shift=0):
+    n = np.arange(-nfreq // 2, nfreq // 2) + shift
+    idx = np.array([(a, b, c) for a in n for b in n for c in n])
+    z = 1j * np.pi * (2 * idx + 1) / beta
+    return idx, z
+
+
+class Problem:
+    """One G2 problem set up through the drop-in API (prepare stage)."""
+
+    def __init__(self, name, device=0):
+        cfg = CONFIGS[name]
+        self.name, self.beta, self.nfreq, self.dm_trunc = name, cfg["beta"], cfg["nfreq"], cfg["dm_trunc"]
+        self.HExpr, site = expr_of(name)
+        self.ii = P.MakeIndexClassification(self.HExpr)
+        self.hs = P.MakeHilbertSpace(self.ii, self.HExpr)
+        self.hs.compute()
+        self.S = P.StatesClassification()
+        self.S.compute(self.hs)
+        self.u0 = self.ii.getIndex(site, 0, P.up)
+        self.d0 = self.ii.getIndex(site, 0, P.down)
+        self.dims = [self.S.getBlockSize(b) for b in range(self.S.getNumberOfBlocks())]
+        self.device = device
+
+    def run_api(self, freqs):
+        """Full drop-in sequence from the Hamiltonian expression: Hamiltonian
+        (eigensolve), DensityMatrix, FieldOperatorContainer (rotation),
+        TwoParticleGFContainer.computeAll on the triples.  Returns the values."""
+        H = P.Hamiltonian(self.S, self.device)
+        H.prepare(self.HExpr, self.hs)
+        H.compute()
+        rho = P.DensityMatrix(self.S, H, self.beta)
+        rho.prepare()
+        rho.compute()
+        if self.dm_trunc:
+            rho.truncateBlocks(self.dm_trunc)
+        ops = P.FieldOperatorContainer(self.ii, self.hs, self.S, H, {self.u0, self.d0})
+        ops.prepareAll(self.hs)
+        ops.computeAll()
+        chi = P.TwoParticleGFContainer(self.ii, self.S, H, rho, ops)
+        key = (self.u0, self.d0, self.u0, self.d0)
+        chi.prepareAll([key])
+        out = chi.computeAll(True, [tuple(t) for t in freqs])
+        self._last = (H, rho, ops, chi)
+        return np.asarray(out[key])
+
+    def engine_inputs(self):
+        """Inputs of the C-ABI leg: block Hamiltonians, Fock actions of c^+,
+        and the block chains of chi_(u0,d0,u0,d0) as found by TwoParticleGF."""
+        H = P.Hamiltonian(self.S, self.device)
+        H.prepare(self.HExpr, self.hs)
+        blocks = [np.array(H.getPart(b).getMatrix()) for b in range(len(self.dims))]
+        H.compute()
+        rho = P.DensityMatrix(self.S, H, self.beta)
+        rho.prepare()
+        rho.compute()
+        if self.dm_trunc:
+            rho.truncateBlocks(self.dm_trunc)
+        ops = P.FieldOperatorContainer(self.ii, self.hs, self.S, H, {self.u0, self.d0})
+        ops.prepareAll(self.hs)
+        ops.computeAll()
+        g2 = P.TwoParticleGF(self.S, H, ops.getAnnihilationOperator(self.u0), ops.getAnnihilationOperator(self.d0),
+                             ops.getCreationOperator(self.u0), ops.getCreationOperator(self.d0), rho)
+        g2.prepare()
+        actions = {i: ops.getCreationOperator(i).fockAction() for i in (self.u0, self.d0)}
+        return blocks, actions, g2.parts()
+
+
+class EngineRun:
+    """The G2 stage chain on one libpgx context with the Hamiltonian resident
+    in HBM: eigensolve, weights, rotation of c^+ and c, G2 on the triples."""
+
+    def __init__(self, prob: Problem, device=0):
+        from .pgx import Engine
+        self.prob = prob
+        blocks, self.actions, self.chains = prob.engine_inputs()
+        self.eng = Engine(device)
+        self.eng.set_blocks(prob.dims)
+        self.eng.set_hamiltonian(blocks)
+        self.h2d_bytes = sum(b.nbytes for b in blocks)
+        self.cdag = {i: self.eng.op_define([(r, l, np.asarray(t), np.asarray(c)) for r, l, t, c in a])
+                     for i, a in self.actions.items()}
+
+    def step(self, triples):
+        e = self.eng
+        e.eigh()
+        e.weights(self.prob.beta)
+        if self.prob.dm_trunc:
+            e.truncate_blocks(self.prob.dm_trunc)
+        u, d = self.prob.u0, self.prob.d0
+        for i in (u, d):
+            e.op_rotate(self.cdag[i])
+        c = {i: e.op_adjoint(self.cdag[i]) for i in (u, d)}
+        slots = (c[u], c[d], self.cdag[u])  # C1, C2, CX3 of chi_(u0,d0,u0,d0)
+        parts = [((slots[p[0]], slots[p[1]], slots[p[2]], self.cdag[d]), tuple(b), tuple(p), s)
+                 for b, p, s in self.chains]
+        self.parts = parts
+        return e.g2(parts, triples, pole_res=1e-8)

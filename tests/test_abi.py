@@ -11,7 +11,7 @@ ROOT = Path(__file__).resolve().parents[1]
 
 def declared_symbols():
     text = (ROOT / "include" / "pgx.h").read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|const char\*)\s+(pgx_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|long long|const char\*)\s+(pgx_\w+)\s*\(", text, re.M)))
 
 
 def test_header_lists_entry_points():
