@@ -31,6 +31,8 @@ extern "C" {
 /* G2 evaluation flags */
 #define PGX_G2_EXACT 0           /* no coefficient filters */
 #define PGX_G2_REFERENCE_RULE 1  /* apply the reference's weight filter at block level */
+#define PGX_G2_ANCHORED 2        /* weight-anchored sum: each sub-term is restricted to the
+                                    states of its weighted index with w > coef_tol */
 
 typedef struct pgx_ctx pgx_ctx;
 

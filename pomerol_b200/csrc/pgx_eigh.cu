@@ -115,12 +115,22 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
         __syncthreads();
         if (tid == 0) { v[0] = v0; ed[k] = alpha; }
         __syncthreads();
-        // p = tau * B v  (B symmetric: p_i = sum_j B(j,i) v_j, coalesced over i)
+        // p = tau * B v  (B symmetric: p_i = sum_j B(j,i) v_j, coalesced over i);
+        // four independent accumulators keep several loads in flight
         for (int i = tid; i < m; i += nt) {
-            double acc = 0.0;
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
             const double* col = A + base + i;
-            for (int j = 0; j < m; ++j) acc += col[(long)j * n] * v[j];
-            w[i] = tau * acc;
+            int j = 0;
+            for (; j + 3 < m; j += 4) {
+                const double b0 = col[(long)j * n], b1 = col[(long)(j + 1) * n], b2 = col[(long)(j + 2) * n],
+                             b3 = col[(long)(j + 3) * n];
+                a0 = fma(b0, v[j], a0);
+                a1 = fma(b1, v[j + 1], a1);
+                a2 = fma(b2, v[j + 2], a2);
+                a3 = fma(b3, v[j + 3], a3);
+            }
+            for (; j < m; ++j) a0 = fma(col[(long)j * n], v[j], a0);
+            w[i] = tau * ((a0 + a1) + (a2 + a3));
         }
         __syncthreads();
         part = 0.0;
@@ -129,11 +139,24 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
         __syncthreads();
         for (int i = tid; i < m; i += nt) w[i] -= K * v[i];
         __syncthreads();
-        // B -= v w^T + w v^T
-        for (int j = 0; j < m; ++j) {
-            const double vj = v[j], wj = w[j];
-            double* row = A + base + (long)j * n;
-            for (int i = tid; i < m; i += nt) row[i] -= vj * w[i] + wj * v[i];
+        // B -= v w^T + w v^T  (rows in groups of four: loads issued before stores)
+        for (int i = tid; i < m; i += nt) {
+            const double vi = v[i], wi = w[i];
+            double* colp = A + base + i;
+            int j = 0;
+            for (; j + 3 < m; j += 4) {
+                double b0 = colp[(long)j * n], b1 = colp[(long)(j + 1) * n], b2 = colp[(long)(j + 2) * n],
+                       b3 = colp[(long)(j + 3) * n];
+                b0 -= v[j] * wi + w[j] * vi;
+                b1 -= v[j + 1] * wi + w[j + 1] * vi;
+                b2 -= v[j + 2] * wi + w[j + 2] * vi;
+                b3 -= v[j + 3] * wi + w[j + 3] * vi;
+                colp[(long)j * n] = b0;
+                colp[(long)(j + 1) * n] = b1;
+                colp[(long)(j + 2) * n] = b2;
+                colp[(long)(j + 3) * n] = b3;
+            }
+            for (; j < m; ++j) colp[(long)j * n] -= v[j] * wi + w[j] * vi;
         }
         // keep v (scaled by sqrt(tau)) in column k below the diagonal
         const double st = sqrt(tau);
@@ -231,13 +254,23 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
             if (st == 1) break;
             const int m = s_m, nrot = s_nrot;
             // rotations at i = m-1, m-2, ..., m-nrot on columns (i, i+1)
+            // columns m-1-q are loaded eight at a time before the stores of
+            // the same group, so the loads overlap instead of waiting on them
             for (int r = tid; r < n; r += nt) {
                 double carry = Z[(long)m * n + r];
-                for (int q = 0; q < nrot; ++q) {
-                    const int i = m - 1 - q;
-                    const double zi = Z[(long)i * n + r];
-                    Z[(long)(i + 1) * n + r] = sn[q] * zi + cs[q] * carry;
-                    carry = cs[q] * zi - sn[q] * carry;
+                for (int q0 = 0; q0 < nrot; q0 += 8) {
+                    double zi[8];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u)
+                        if (q0 + u < nrot) zi[u] = Z[(long)(m - 1 - q0 - u) * n + r];
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) {
+                        if (q0 + u < nrot) {
+                            const double s = sn[q0 + u], c = cs[q0 + u];
+                            Z[(long)(m - q0 - u) * n + r] = s * zi[u] + c * carry;
+                            carry = c * zi[u] - s * carry;
+                        }
+                    }
                 }
                 if (nrot > 0) Z[(long)(m - nrot) * n + r] = carry;
             }

@@ -1,0 +1,524 @@
+// K4, weight-anchored form of the G2 Lehmann sum.
+//
+// Every sub-term of TwoParticleGFPart::addMultiterm (TwoParticleGFPart.cpp:277-297)
+// is a product of the matrix element M and ONE Boltzmann weight once the weight
+// sums are split: -M(w2+w3) -> w2 and w3 parts, M(w1+w4) -> w1 and w4 parts, the
+// resonant z1z2 term -> w1 (delta: beta w1, else -w1/D) and w3 (w3/D), the z2z3
+// term -> w2 (delta: -beta w2, else w2/D) and w4 (-w4/D).  Each part only needs
+// the states of its weighted ("anchor") index whose weight exceeds the anchor
+// threshold; the other three indices are summed completely.  The dropped
+// contribution is bounded by threshold * d * (beta/pi)^3 per chain, the same
+// order as the reference's own CoefficientTolerance filter (:241, :283-297).
+//
+// With A(z1) = O1 / (z1 - (E2 - E1)), C(z3) = O3 / (z3 - (E4 - E3)) and H_b the
+// anchor states of block b, the eight anchored sub-terms are
+//   T1a  -s  w2 sum_3 O2[h,3] / (z2 - (E3 - E2h)) [C(z3) X4 A(z1)[:,h]]_3
+//   T1b  -s  w3 sum_2 O2[2,h] / (z2 - (E3h - E2)) [C(z3)[h,:] X4 A(z1)]_2
+//   T2a   s  w1 sum_4 X4[4,h] / (Z - (E4 - E1h))  [A(z1)[h,:] O2 C(z3)]_4
+//   T2b   s  w4 sum_1 X4[h,1] / (Z - (E4h - E1))  [A(z1) O2 C(z3)[:,h]]_1
+//   T3a   s  sum_3 [A(z1)[h,:] O2]_3 [C(z3) X4[:,h]]_3 (delta ? beta w1 : -w1/D)
+//   T3b   s  sum_1 [A(z1) O2[:,h]]_1 [C(z3)[h,:] X4]_1 (delta ? 0 : w3/D)
+//   T4a   s  sum_4 [O2[h,:] C(z3)]_4 [X4 A(z1)[:,h]]_4 (delta ? -beta w2 : w2/D)
+//   T4b   s  sum_2 [O2 C(z3)[:,h]]_2 [X4[h,:] A(z1)]_2 (delta ? 0 : -w4/D)
+// (Z = z1+z2+z3, D = s - (E_b - E_a) with s = z1+z2 for T3 and z2+z3 for T4).
+// Stages, each one launch for a batch of chains: dressing of A(z1), C(z3);
+// anchored products per frequency (gather GEMMs); products per (z1, z3)
+// stacked into GEMMs over all anchors; contractions per triple (warp per
+// (sub-term, triple), resonant delta test in FP64).
+
+#include <array>
+#include <map>
+#include <tuple>
+
+#include "pgx_common.cuh"
+#include "pgx_gemm.cuh"
+#include "pgx_internal.h"
+
+namespace pgx {
+
+namespace {
+
+struct DressItem {
+    const void* O;  // d_a x d_b operator block (double or cd)
+    const double *Ea, *Eb;
+    const cd* z;
+    int nz, da, db;
+    cd* out;        // nz x da x db
+};
+
+template <typename T>
+__global__ void dress_list_kernel(const DressItem* items, int nitems) {
+    const DressItem it = items[blockIdx.y];
+    const long n = (long)it.da * it.db;
+    const long total = n * it.nz;
+    const T* O = static_cast<const T*>(it.O);
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
+        const int iz = (int)(e / n);
+        const long r = e % n;
+        const int a = (int)(r / it.db), b = (int)(r % it.db);
+        const cd zz = it.z[iz];
+        it.out[e] = tocd(O[r]) * inv(cd{zz.x - (it.Eb[b] - it.Ea[a]), zz.y});
+    }
+}
+
+struct DTerm {
+    const void* VA;
+    long a1, a3, ah, ak;
+    const void* VB;
+    long b1, b3, bh, bk;
+    const double *Ek, *Eh, *wh;
+    const int* hot;       // anchor states (inner indices) of the anchor block
+    const int* ti1;       // per triple: index of z1 in the plan
+    const int* ti3;       // per triple: index of z3 in the plan
+    const cd* ts;         // per triple: s of this sub-term
+    int nh, nk;
+    int va_cplx, vb_cplx; // operand element types
+    int va_hstate, vb_hstate;  // h stride applies to the anchor's state index instead of its position
+    int use_delta;
+    double sgn, cdelta, cnum, pref;
+};
+
+__device__ __forceinline__ cd load_v(const void* p, int cplx, long idx) {
+    return cplx ? static_cast<const cd*>(p)[idx] : cd{static_cast<const double*>(p)[idx], 0.0};
+}
+
+// One warp per (sub-term, triple): lanes over the summed index k.
+__global__ void __launch_bounds__(256) dterm_kernel(const DTerm* terms, int nterms, int nfreq, double beta,
+                                                    double tol, cd* out) {
+    const long nwork = (long)nterms * nfreq;
+    const int lane = threadIdx.x & 31;
+    for (long wk = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; wk < nwork;
+         wk += ((long)gridDim.x * blockDim.x) >> 5) {
+        const int q = (int)(wk / nfreq), t = (int)(wk % nfreq);
+        const DTerm& d = terms[q];
+        const int i1 = d.ti1[t], i3 = d.ti3[t];
+        const cd s = d.ts[t];
+        double ax = 0.0, ay = 0.0;
+        for (int h = 0; h < d.nh; ++h) {
+            const int hs = d.hot[h];
+            const double eh = d.Eh[hs], w = d.wh[hs];
+            const long oa = i1 * d.a1 + i3 * d.a3 + (long)(d.va_hstate ? hs : h) * d.ah;
+            const long ob = i1 * d.b1 + i3 * d.b3 + (long)(d.vb_hstate ? hs : h) * d.bh;
+            for (int k = lane; k < d.nk; k += 32) {
+                const cd ab = load_v(d.VA, d.va_cplx, oa + k * d.ak) * load_v(d.VB, d.vb_cplx, ob + k * d.bk);
+                const cd D{s.x - d.sgn * (d.Ek[k] - eh), s.y};
+                cd K;
+                if (d.use_delta && sqrt(abs2(D)) <= tol) {
+                    K = cd{d.cdelta * beta * w, 0.0};
+                } else {
+                    const double r = d.cnum * w / abs2(D);
+                    K = cd{D.x * r, -D.y * r};
+                }
+                const cd v = ab * K;
+                ax += v.x;
+                ay += v.y;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            ax += __shfl_xor_sync(0xffffffffu, ax, o);
+            ay += __shfl_xor_sync(0xffffffffu, ay, o);
+        }
+        if (lane == 0 && (ax != 0.0 || ay != 0.0)) {
+            atomicAdd(&out[t].x, d.pref * ax);
+            atomicAdd(&out[t].y, d.pref * ay);
+        }
+    }
+}
+
+struct APlan {
+    std::vector<cd> Z1, Z3;
+    std::vector<int> i1, i3;
+    std::vector<cd> s[4];
+    DevBuf buf;
+    cd *dZ1 = nullptr, *dZ3 = nullptr, *ds[4] = {nullptr, nullptr, nullptr, nullptr};
+    int *di1 = nullptr, *di3 = nullptr;
+};
+
+struct KeyC {
+    double a, b;
+    bool operator<(const KeyC& o) const { return std::tie(a, b) < std::tie(o.a, o.b); }
+};
+
+void build_aplan(APlan& pl, const int perm[3], int nfreq, const double* z, cudaStream_t st) {
+    std::map<KeyC, int> m1, m3;
+    pl.i1.resize(nfreq);
+    pl.i3.resize(nfreq);
+    for (auto& v : pl.s) v.resize(nfreq);
+    for (int t = 0; t < nfreq; ++t) {
+        const cd F[3] = {cd{z[6 * t], z[6 * t + 1]}, cd{z[6 * t + 2], z[6 * t + 3]}, cd{-z[6 * t + 4], -z[6 * t + 5]}};
+        const cd a = F[perm[0]], b = F[perm[1]], c = F[perm[2]];
+        auto x1 = m1.emplace(KeyC{a.x, a.y}, (int)pl.Z1.size());
+        if (x1.second) pl.Z1.push_back(a);
+        auto x3 = m3.emplace(KeyC{c.x, c.y}, (int)pl.Z3.size());
+        if (x3.second) pl.Z3.push_back(c);
+        pl.i1[t] = x1.first->second;
+        pl.i3[t] = x3.first->second;
+        pl.s[0][t] = b;
+        pl.s[1][t] = a + b + c;
+        pl.s[2][t] = a + b;
+        pl.s[3][t] = b + c;
+    }
+    const size_t n1 = pl.Z1.size(), n3 = pl.Z3.size(), nf = nfreq;
+    pl.buf.reserve((n1 + n3 + 4 * nf) * sizeof(cd) + 2 * nf * sizeof(int) + 256);
+    char* p = pl.buf.as<char>();
+    auto take = [&](size_t b) {
+        char* r = p;
+        p += (b + 15) & ~size_t(15);
+        return r;
+    };
+    pl.dZ1 = reinterpret_cast<cd*>(take(n1 * sizeof(cd)));
+    pl.dZ3 = reinterpret_cast<cd*>(take(n3 * sizeof(cd)));
+    for (int k = 0; k < 4; ++k) pl.ds[k] = reinterpret_cast<cd*>(take(nf * sizeof(cd)));
+    pl.di1 = reinterpret_cast<int*>(take(nf * sizeof(int)));
+    pl.di3 = reinterpret_cast<int*>(take(nf * sizeof(int)));
+    auto up = [&](void* d, const void* h, size_t b) {
+        if (b) PGX_CUDA(cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, st));
+    };
+    up(pl.dZ1, pl.Z1.data(), n1 * sizeof(cd));
+    up(pl.dZ3, pl.Z3.data(), n3 * sizeof(cd));
+    for (int k = 0; k < 4; ++k) up(pl.ds[k], pl.s[k].data(), nf * sizeof(cd));
+    up(pl.di1, pl.i1.data(), nf * sizeof(int));
+    up(pl.di3, pl.i3.data(), nf * sizeof(int));
+}
+
+// Workspace of one chain inside a batch (element offsets into one cd pool).
+struct ChainWs {
+    long A1, C3, Lc, Lr, Pr, Pc, Rho, Qc, Rr, Rc, V1a, V1b, V2a, V2b, end;
+};
+
+template <typename TA, typename TB>
+GemmProblem<TA, TB, cd> gp(const TA* A, long sai, long sak, const TB* B, long sbk, long sbj, cd* C, long sci, int M, int N,
+                           int K, const int* aii = nullptr, const int* bjj = nullptr) {
+    GemmProblem<TA, TB, cd> g{};
+    g.A = A;
+    g.B = B;
+    g.C = C;
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.sa_i = sai;
+    g.sa_k = sak;
+    g.sb_k = sbk;
+    g.sb_j = sbj;
+    g.sc_i = sci;
+    g.sc_j = 1;
+    g.a_iidx = aii;
+    g.b_jidx = bjj;
+    return g;
+}
+
+}  // namespace
+
+template <typename T>
+static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part* parts, const std::vector<int>& part_plan,
+                      std::vector<APlan>& plans, const std::vector<std::array<int, 4>>& rs,
+                      const std::vector<ChainWs>& wsl, cd* pool, const int* d_hot, const std::vector<long>& hot_off,
+                      double pole_res, int nfreq, cd* d_out) {
+    Problem& P = c->P;
+    cudaStream_t st = c->stream;
+    constexpr bool TC = is_cd<T>::value;
+    // ---- dressing
+    std::vector<DressItem> di;
+    for (int q : idx) {
+        const pgx_g2_part& g = parts[q];
+        const APlan& pl = plans[part_plan[q]];
+        const ChainWs& w = wsl[q];
+        const int S1 = g.block[0], S2 = g.block[1], S3 = g.block[2], S4 = g.block[3];
+        const Operator &o1 = P.ops[g.op[0]], &o3 = P.ops[g.op[2]];
+        di.push_back(DressItem{o1.mat.as<T>() + o1.parts[o1.by_left[S1]].off, P.d_E + P.eoff[S1], P.d_E + P.eoff[S2],
+                               pl.dZ1, (int)pl.Z1.size(), P.dims[S1], P.dims[S2], pool + w.A1});
+        di.push_back(DressItem{o3.mat.as<T>() + o3.parts[o3.by_left[S3]].off, P.d_E + P.eoff[S3], P.d_E + P.eoff[S4],
+                               pl.dZ3, (int)pl.Z3.size(), P.dims[S3], P.dims[S4], pool + w.C3});
+    }
+    DevBuf& bi = c->scratch[2];
+    bi.reserve(di.size() * sizeof(DressItem));
+    PGX_CUDA(cudaMemcpyAsync(bi.p, di.data(), di.size() * sizeof(DressItem), cudaMemcpyHostToDevice, st));
+    {
+        long maxe = 1;
+        for (auto& x : di) maxe = std::max(maxe, (long)x.nz * x.da * x.db);
+        dim3 grid(std::min(ceil_div(maxe, 256), 1024), (unsigned)di.size());
+        dress_list_kernel<T><<<grid, 256, 0, st>>>(bi.as<DressItem>(), (int)di.size());
+        check_launch("dress_list_kernel");
+    }
+    // ---- anchored products per frequency
+    std::vector<GemmProblem<T, cd, cd>> pa;  // operator x dressed
+    std::vector<GemmProblem<cd, T, cd>> pb;  // dressed x operator
+    std::vector<GemmProblem<cd, cd, cd>> pc;  // per (z1, z3), all anchors stacked
+    for (int q : idx) {
+        const pgx_g2_part& g = parts[q];
+        const APlan& pl = plans[part_plan[q]];
+        const ChainWs& w = wsl[q];
+        const int S1 = g.block[0], S2 = g.block[1], S3 = g.block[2], S4 = g.block[3];
+        const int d1 = P.dims[S1], d2 = P.dims[S2], d3 = P.dims[S3], d4 = P.dims[S4];
+        const int r1 = rs[q][0], r2 = rs[q][1], r3 = rs[q][2], r4 = rs[q][3];
+        const int N1 = (int)pl.Z1.size(), N3 = (int)pl.Z3.size();
+        const Operator &o2 = P.ops[g.op[1]], &o4 = P.ops[g.op[3]];
+        const T* O2 = o2.mat.as<T>() + o2.parts[o2.by_left[S2]].off;
+        const T* X4 = o4.mat.as<T>() + o4.parts[o4.by_left[S4]].off;
+        const int *H1 = d_hot + hot_off[S1], *H2 = d_hot + hot_off[S2], *H3 = d_hot + hot_off[S3], *H4 = d_hot + hot_off[S4];
+        const long s12 = (long)d1 * d2, s34 = (long)d3 * d4;
+        for (int i = 0; i < N1; ++i) {
+            const cd* A1 = pool + w.A1 + i * s12;
+            if (r2) pa.push_back(gp<T, cd>(X4, d1, 1, A1, d2, 1, pool + w.Lc + (long)i * r2, (long)N1 * r2, d4, r2, d1,
+                                           nullptr, H2));                                     // Lc = X4 A1[:,H2]
+            if (r4) pa.push_back(gp<T, cd>(X4, d1, 1, A1, d2, 1, pool + w.Lr + (long)i * r4 * d2, d2, r4, d2, d1, H4));  // Lr
+            if (r1) pb.push_back(gp<cd, T>(A1, d2, 1, O2, d3, 1, pool + w.Pr + (long)i * r1 * d3, d3, r1, d3, d2, H1));  // Pr
+            if (r3) pb.push_back(gp<cd, T>(A1, d2, 1, O2, d3, 1, pool + w.Pc + (long)i * d1 * r3, r3, d1, r3, d2,
+                                           nullptr, H3));                                     // Pc = A1 O2[:,H3]
+        }
+        for (int i = 0; i < N3; ++i) {
+            const cd* C3 = pool + w.C3 + i * s34;
+            if (r3) pb.push_back(gp<cd, T>(C3, d4, 1, X4, d1, 1, pool + w.Rho + (long)i * r3 * d1, d1, r3, d1, d4, H3));  // rho
+            if (r1) pb.push_back(gp<cd, T>(C3, d4, 1, X4, d1, 1, pool + w.Qc + (long)i * d3 * r1, r1, d3, r1, d4,
+                                           nullptr, H1));                                     // Qc = C3 X4[:,H1]
+            if (r2) pa.push_back(gp<T, cd>(O2, d3, 1, C3, d4, 1, pool + w.Rr + (long)i * r2 * d4, d4, r2, d4, d3, H2));  // Rr
+            if (r4) pa.push_back(gp<T, cd>(O2, d3, 1, C3, d4, 1, pool + w.Rc + (long)i * r4, (long)N3 * r4, d2, r4, d3,
+                                           nullptr, H4));                                     // Rc = O2 C3[:,H4]
+        }
+        // products over (z1, z3): anchors of all frequencies stacked as columns / rows
+        for (int i = 0; i < N3; ++i) {
+            const cd* C3 = pool + w.C3 + i * s34;
+            if (r2) pc.push_back(gp<cd, cd>(C3, d4, 1, pool + w.Lc, (long)N1 * r2, 1, pool + w.V1a + (long)i * d3 * N1 * r2,
+                                            (long)N1 * r2, d3, N1 * r2, d4));                 // V1a = C3 LcAll
+            if (r1) pc.push_back(gp<cd, cd>(pool + w.Pr, d3, 1, C3, d4, 1, pool + w.V2a + (long)i * N1 * r1 * d4, d4,
+                                            N1 * r1, d4, d3));                                // V2a = PrAll C3
+        }
+        for (int i = 0; i < N1; ++i) {
+            const cd* A1 = pool + w.A1 + i * s12;
+            if (r3) pc.push_back(gp<cd, cd>(pool + w.Rho, d1, 1, A1, d2, 1, pool + w.V1b + (long)i * N3 * r3 * d2, d2,
+                                            N3 * r3, d2, d1));                                // V1b = rhoAll A1
+            if (r4) pc.push_back(gp<cd, cd>(A1, d2, 1, pool + w.Rc, (long)N3 * r4, 1, pool + w.V2b + (long)i * d1 * N3 * r4,
+                                            (long)N3 * r4, d1, N3 * r4, d2));                 // V2b = A1 RcAll
+        }
+    }
+    // descriptor buffers sized once for the largest list, before any launch
+    {
+        auto tiles = [](auto& probs) {
+            long nt = 0;
+            for (auto& g : probs) nt += (long)ceil_div(g.M, GEMM_BM) * ceil_div(g.N, GEMM_BN);
+            return nt;
+        };
+        const long nprob = (long)(pa.size() + pb.size() + pc.size());
+        const long nt = tiles(pa) + tiles(pb) + tiles(pc);
+        c->scratch[7].reserve(std::max<long>(nprob, 1) * sizeof(GemmProblem<cd, cd, cd>));
+        c->scratch[8].reserve(std::max<long>(nt, 1) * sizeof(GemmTile));
+    }
+    auto launch = [&](auto& probs) {
+        if (probs.empty()) return;
+        launch_gemm_batch(probs, c->scratch[7].p, c->scratch[7].bytes, c->scratch[8].p, c->scratch[8].bytes, st);
+    };
+    if constexpr (TC) {
+        // complex operators: all products are complex x complex
+        std::vector<GemmProblem<cd, cd, cd>> all;
+        for (auto& g : pa) all.push_back(g);
+        for (auto& g : pb) all.push_back(g);
+        launch(all);
+    } else {
+        launch(pa);
+        launch(pb);
+    }
+    launch(pc);
+    // ---- contractions per triple
+    std::vector<DTerm> dt;
+    for (int q : idx) {
+        const pgx_g2_part& g = parts[q];
+        const APlan& pl = plans[part_plan[q]];
+        const ChainWs& w = wsl[q];
+        const int S[4] = {g.block[0], g.block[1], g.block[2], g.block[3]};
+        const int d1 = P.dims[S[0]], d2 = P.dims[S[1]], d3 = P.dims[S[2]], d4 = P.dims[S[3]];
+        const int r1 = rs[q][0], r2 = rs[q][1], r3 = rs[q][2], r4 = rs[q][3];
+        const long N1 = (long)pl.Z1.size(), N3 = (long)pl.Z3.size();
+        const Operator &o2 = P.ops[g.op[1]], &o4 = P.ops[g.op[3]];
+        const T* O2 = o2.mat.as<T>() + o2.parts[o2.by_left[S[1]]].off;
+        const T* X4 = o4.mat.as<T>() + o4.parts[o4.by_left[S[3]]].off;
+        const double* E[4];
+        const double* W[4];
+        for (int k = 0; k < 4; ++k) {
+            E[k] = P.d_E + P.eoff[S[k]];
+            W[k] = P.d_w + P.eoff[S[k]];
+        }
+        const double sign = g.sign;
+        auto base = [&](int anchor, int nh, int nk, int kb, double sgn, int sidx, int use_delta, double cd_, double cn,
+                        double pref) {
+            DTerm d{};
+            d.Ek = E[kb];
+            d.Eh = E[anchor];
+            d.wh = W[anchor];
+            d.hot = d_hot + hot_off[S[anchor]];
+            d.nh = nh;
+            d.nk = nk;
+            d.ti1 = pl.di1;
+            d.ti3 = pl.di3;
+            d.ts = pl.ds[sidx];
+            d.sgn = sgn;
+            d.use_delta = use_delta;
+            d.cdelta = cd_;
+            d.cnum = cn;
+            d.pref = pref;
+            return d;
+        };
+        const int opc = TC ? 1 : 0;
+        if (r2) {  // T1a: va = O2[h,k] (state h), vb = V1a[i3][k][(i1,h)]
+            DTerm d = base(1, r2, d3, 2, +1.0, 0, 0, 0.0, 1.0, -sign);
+            d.VA = O2; d.va_cplx = opc; d.va_hstate = 1; d.ah = d3; d.ak = 1;
+            d.VB = pool + w.V1a; d.vb_cplx = 1; d.b3 = (long)d3 * N1 * r2; d.bk = N1 * r2; d.b1 = r2; d.bh = 1;
+            dt.push_back(d);
+            // T4a: va = Rr[i3][h][k], vb = LcAll[k][(i1,h)]
+            DTerm e = base(1, r2, d4, 3, +1.0, 3, 1, -1.0, 1.0, sign);
+            e.VA = pool + w.Rr; e.va_cplx = 1; e.a3 = (long)r2 * d4; e.ah = d4; e.ak = 1;
+            e.VB = pool + w.Lc; e.vb_cplx = 1; e.bk = N1 * r2; e.b1 = r2; e.bh = 1;
+            dt.push_back(e);
+        }
+        if (r3) {  // T1b: va = O2[k,h] (state h), vb = V1b[i1][(i3,h)][k]
+            DTerm d = base(2, r3, d2, 1, -1.0, 0, 0, 0.0, 1.0, -sign);
+            d.VA = O2; d.va_cplx = opc; d.va_hstate = 1; d.ah = 1; d.ak = d3;
+            d.VB = pool + w.V1b; d.vb_cplx = 1; d.b1 = N3 * r3 * d2; d.b3 = (long)r3 * d2; d.bh = d2; d.bk = 1;
+            dt.push_back(d);
+            // T3b: va = Pc[i1][k][h], vb = rho[(i3,h)][k]
+            DTerm e = base(2, r3, d1, 0, -1.0, 2, 1, 0.0, 1.0, sign);
+            e.VA = pool + w.Pc; e.va_cplx = 1; e.a1 = (long)d1 * r3; e.ak = r3; e.ah = 1;
+            e.VB = pool + w.Rho; e.vb_cplx = 1; e.b3 = (long)r3 * d1; e.bh = d1; e.bk = 1;
+            dt.push_back(e);
+        }
+        if (r1) {  // T2a: va = X4[k,h] (state h), vb = V2a[i3][(i1,h)][k]
+            DTerm d = base(0, r1, d4, 3, +1.0, 1, 0, 0.0, 1.0, sign);
+            d.VA = X4; d.va_cplx = opc; d.va_hstate = 1; d.ah = 1; d.ak = d1;
+            d.VB = pool + w.V2a; d.vb_cplx = 1; d.b3 = N1 * r1 * d4; d.b1 = (long)r1 * d4; d.bh = d4; d.bk = 1;
+            dt.push_back(d);
+            // T3a: va = PrAll[(i1,h)][k], vb = Qc[i3][k][h]
+            DTerm e = base(0, r1, d3, 2, +1.0, 2, 1, 1.0, -1.0, sign);
+            e.VA = pool + w.Pr; e.va_cplx = 1; e.a1 = (long)r1 * d3; e.ah = d3; e.ak = 1;
+            e.VB = pool + w.Qc; e.vb_cplx = 1; e.b3 = (long)d3 * r1; e.bk = r1; e.bh = 1;
+            dt.push_back(e);
+        }
+        if (r4) {  // T2b: va = X4[h,k] (state h), vb = V2b[i1][k][(i3,h)]
+            DTerm d = base(3, r4, d1, 0, -1.0, 1, 0, 0.0, 1.0, sign);
+            d.VA = X4; d.va_cplx = opc; d.va_hstate = 1; d.ah = d1; d.ak = 1;
+            d.VB = pool + w.V2b; d.vb_cplx = 1; d.b1 = (long)d1 * N3 * r4; d.bk = N3 * r4; d.b3 = r4; d.bh = 1;
+            dt.push_back(d);
+            // T4b: va = RcAll[k][(i3,h)], vb = Lr[i1][h][k]
+            DTerm e = base(3, r4, d2, 1, -1.0, 3, 1, 0.0, -1.0, sign);
+            e.VA = pool + w.Rc; e.va_cplx = 1; e.ak = N3 * r4; e.a3 = r4; e.ah = 1;
+            e.VB = pool + w.Lr; e.vb_cplx = 1; e.b1 = (long)r4 * d2; e.bh = d2; e.bk = 1;
+            dt.push_back(e);
+        }
+    }
+    if (!dt.empty()) {
+        DevBuf& bd = c->scratch[3];
+        bd.reserve(dt.size() * sizeof(DTerm));
+        PGX_CUDA(cudaMemcpyAsync(bd.p, dt.data(), dt.size() * sizeof(DTerm), cudaMemcpyHostToDevice, st));
+        const long warps = (long)dt.size() * nfreq;
+        const int blocks = (int)std::min<long>(ceil_div(warps * 32, 256), 148L * 16);
+        dterm_kernel<<<blocks, 256, 0, st>>>(bd.as<DTerm>(), (int)dt.size(), nfreq, P.beta, pole_res, d_out);
+        check_launch("dterm_kernel");
+    }
+    // the scratch descriptor buffers are reused by the next batch
+    PGX_CUDA(cudaStreamSynchronize(st));
+}
+
+void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
+                     double anchor_tol, double* out) {
+    Problem& P = c->P;
+    cudaStream_t st = c->stream;
+    // anchor states per block (weights above the threshold)
+    std::vector<double> w(P.esize);
+    PGX_CUDA(cudaMemcpyAsync(w.data(), P.d_w, P.esize * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaStreamSynchronize(st));
+    std::vector<int> hot;
+    std::vector<long> hot_off(P.nblocks + 1, 0);
+    std::vector<int> nhot(P.nblocks, 0);
+    for (int b = 0; b < P.nblocks; ++b) {
+        hot_off[b] = (long)hot.size();
+        for (int i = 0; i < P.dims[b]; ++i)
+            if (w[P.eoff[b] + i] > anchor_tol) hot.push_back(i);
+        nhot[b] = (int)(hot.size() - hot_off[b]);
+    }
+    hot_off[P.nblocks] = (long)hot.size();
+    DevBuf& bh = c->scratch[11];
+    bh.reserve(std::max<size_t>(hot.size(), 1) * sizeof(int));
+    if (!hot.empty()) PGX_CUDA(cudaMemcpyAsync(bh.p, hot.data(), hot.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    // frequency plans per permutation
+    std::map<std::tuple<int, int, int>, int> perm_id;
+    std::vector<APlan> plans;
+    plans.reserve(6);
+    std::vector<int> part_plan(nparts);
+    for (int q = 0; q < nparts; ++q) {
+        auto key = std::make_tuple(parts[q].perm[0], parts[q].perm[1], parts[q].perm[2]);
+        auto it = perm_id.find(key);
+        if (it == perm_id.end()) {
+            it = perm_id.emplace(key, (int)plans.size()).first;
+            plans.emplace_back();
+            const int perm[3] = {parts[q].perm[0], parts[q].perm[1], parts[q].perm[2]};
+            build_aplan(plans.back(), perm, nfreq, z, st);
+        }
+        part_plan[q] = it->second;
+    }
+    // workspace per chain and batching under a memory budget
+    std::vector<std::array<int, 4>> rs(nparts);
+    std::vector<ChainWs> wsl(nparts);
+    const long budget = (long)(3L << 30) / (long)sizeof(cd);
+    DevBuf& pool_b = c->scratch[6];
+    DevBuf& out_b = c->scratch[9];
+    out_b.reserve(std::max(nfreq, 1) * sizeof(cd));
+    PGX_CUDA(cudaMemsetAsync(out_b.p, 0, std::max(nfreq, 1) * sizeof(cd), st));
+    std::vector<int> batch;
+    long used = 0;
+    auto flush = [&]() {
+        if (batch.empty()) return;
+        pool_b.reserve(std::max<long>(used, 1) * sizeof(cd));
+        if (P.is_complex)
+            run_batch<cd>(c, batch, parts, part_plan, plans, rs, wsl, pool_b.as<cd>(), bh.as<int>(), hot_off, pole_res,
+                          nfreq, out_b.as<cd>());
+        else
+            run_batch<double>(c, batch, parts, part_plan, plans, rs, wsl, pool_b.as<cd>(), bh.as<int>(), hot_off,
+                              pole_res, nfreq, out_b.as<cd>());
+        batch.clear();
+        used = 0;
+    };
+    for (int q = 0; q < nparts; ++q) {
+        const pgx_g2_part& g = parts[q];
+        int r[4], d[4];
+        for (int k = 0; k < 4; ++k) {
+            r[k] = nhot[g.block[k]];
+            d[k] = P.dims[g.block[k]];
+        }
+        rs[q] = {r[0], r[1], r[2], r[3]};
+        if (r[0] + r[1] + r[2] + r[3] == 0) continue;
+        const APlan& pl = plans[part_plan[q]];
+        const long N1 = (long)pl.Z1.size(), N3 = (long)pl.Z3.size();
+        ChainWs x{};
+        long o = 0;
+        auto take = [&](long n) {
+            long r0 = o;
+            o += (n + 1) & ~1L;  // keep 32-byte alignment of complex doubles
+            return r0;
+        };
+        x.A1 = take(N1 * d[0] * d[1]);
+        x.C3 = take(N3 * d[2] * d[3]);
+        x.Lc = take((long)d[3] * N1 * r[1]);
+        x.Lr = take(N1 * r[3] * d[1]);
+        x.Pr = take(N1 * r[0] * d[2]);
+        x.Pc = take(N1 * d[0] * r[2]);
+        x.Rho = take(N3 * r[2] * d[0]);
+        x.Qc = take(N3 * d[2] * r[0]);
+        x.Rr = take(N3 * r[1] * d[3]);
+        x.Rc = take((long)d[1] * N3 * r[3]);
+        x.V1a = take(N3 * d[2] * N1 * r[1]);
+        x.V1b = take(N1 * N3 * r[2] * d[1]);
+        x.V2a = take(N3 * N1 * r[0] * d[3]);
+        x.V2b = take(N1 * d[0] * N3 * r[3]);
+        x.end = o;
+        if (used > 0 && used + x.end > budget) flush();
+        for (long* f : {&x.A1, &x.C3, &x.Lc, &x.Lr, &x.Pr, &x.Pc, &x.Rho, &x.Qc, &x.Rr, &x.Rc, &x.V1a, &x.V1b, &x.V2a,
+                        &x.V2b, &x.end})
+            *f += used;
+        wsl[q] = x;
+        used = x.end;
+        batch.push_back(q);
+    }
+    flush();
+    PGX_CUDA(cudaMemcpyAsync(out, out_b.p, nfreq * sizeof(cd), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaStreamSynchronize(st));
+}
+
+}  // namespace pgx

@@ -29,6 +29,8 @@ template <typename TA, typename TB, typename TC> struct GemmProblem {
     const double* kscale;  // multiplies B(k, :) when non-null
     int accumulate;        // C += A B instead of C = A B
     int conj_a;            // use conj(A) (complex A only)
+    const int* a_iidx;     // row gather of A: A(i,k) uses row a_iidx[i] (nullable)
+    const int* b_jidx;     // column gather of B: B(k,j) uses column b_jidx[j] (nullable)
 };
 
 struct GemmTile {
@@ -97,7 +99,8 @@ __global__ void __launch_bounds__(GEMM_THREADS)
             TA v = zero_of<TA>();
             if (gi < p.M && gk < p.K) {
                 const long kq = p.a_kidx ? p.a_kidx[gk] : gk;
-                v = maybe_conj(p.A[gi * p.sa_i + kq * p.sa_k], p.conj_a);
+                const long iq = p.a_iidx ? p.a_iidx[gi] : gi;
+                v = maybe_conj(p.A[iq * p.sa_i + kq * p.sa_k], p.conj_a);
             }
             As[kk][ii] = v;
         }
@@ -110,7 +113,8 @@ __global__ void __launch_bounds__(GEMM_THREADS)
             TB v = zero_of<TB>();
             if (gj < p.N && gk < p.K) {
                 const long kq = p.b_kidx ? p.b_kidx[gk] : gk;
-                v = p.B[kq * p.sb_k + gj * p.sb_j];
+                const long jq = p.b_jidx ? p.b_jidx[gj] : gj;
+                v = p.B[kq * p.sb_k + jq * p.sb_j];
                 if (p.kscale) v = scale_by(v, p.kscale[gk]);
             }
             Bs[kk][jj] = v;

@@ -16,6 +16,24 @@ namespace pgx {
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), bytes(o.bytes) {
+        o.p = nullptr;
+        o.bytes = 0;
+    }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            bytes = o.bytes;
+            o.p = nullptr;
+            o.bytes = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
     void reserve(size_t n) {
         if (n <= bytes) return;
         release();
@@ -113,6 +131,8 @@ void run_susc(pgx_ctx* c, int opA, int opB, int nparts, const int32_t* outer, co
 void run_ensemble_average(pgx_ctx* c, int op, double* out);
 void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
             double coef_tol, int flags, double* out);
+void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
+                     double anchor_tol, double* out);
 void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_tol, double nz_tol, long long* count);
 
 }  // namespace pgx

@@ -269,6 +269,8 @@ PYBIND11_MODULE(_pomerol, m) {
              py::keep_alive<1, 6>(), py::keep_alive<1, 7>(), py::keep_alive<1, 8>())
         .def_readwrite("PoleResolution", &TwoParticleGF::PoleResolution)
         .def_readwrite("CoefficientTolerance", &TwoParticleGF::CoefficientTolerance)
+        .def_readwrite("AnchorTolerance", &TwoParticleGF::AnchorTolerance)
+        .def_readwrite("ExactSum", &TwoParticleGF::ExactSum)
         .def("prepare", &TwoParticleGF::prepare)
         .def("compute",
              [](TwoParticleGF& g, bool clear, std::vector<std::tuple<C, C, C>> const& f, int) {

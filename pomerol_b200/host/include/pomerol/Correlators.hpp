@@ -146,6 +146,10 @@ class TwoParticleGF : public Thermal, public ComputableObject {
 public:
     RealType PoleResolution = 1e-8;
     RealType CoefficientTolerance = 1e-16;
+    // Sub-terms are anchored on states with weight > min(CoefficientTolerance,
+    // AnchorTolerance); ExactSum = true sums every state quadruple instead.
+    RealType AnchorTolerance = 1e-15;
+    bool ExactSum = false;
 
     TwoParticleGF(StatesClassification const& S, Hamiltonian const& H, AnnihilationOperator const& C1,
                   AnnihilationOperator const& C2, CreationOperator const& CX3, CreationOperator const& CX4,

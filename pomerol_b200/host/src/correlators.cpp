@@ -269,8 +269,13 @@ std::vector<ComplexType> TwoParticleGF::values(FreqVec3 const& freqs) const {
     }
     DM.bind();
     Device& dev = H.device();
+    // anchored sum: sub-terms whose Boltzmann weight is below the anchor
+    // threshold are skipped (the same order as the coefficient filter);
+    // ExactSum evaluates every state quadruple.
+    const double anchor = std::min(CoefficientTolerance, AnchorTolerance);
     dev.check(pgx_g2(dev.ctx(), (int32_t)parts.size(), parts.data(), (int32_t)freqs.size(), z.data(), PoleResolution,
-                     CoefficientTolerance, PGX_G2_REFERENCE_RULE, reinterpret_cast<double*>(out.data())),
+                     ExactSum ? 0.0 : anchor, ExactSum ? PGX_G2_EXACT : PGX_G2_ANCHORED,
+                     reinterpret_cast<double*>(out.data())),
               "pgx_g2");
     return out;
 }

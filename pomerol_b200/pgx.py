@@ -15,7 +15,7 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "libpgx.so"
 
 PGX_OK, PGX_ERR_ARG, PGX_ERR_OOM, PGX_ERR_CUDA, PGX_ERR_TIMEOUT, PGX_ERR_NUMERIC, PGX_ERR_STATE, PGX_ERR_NODEV = range(8)
-PGX_G2_EXACT, PGX_G2_REFERENCE_RULE = 0, 1
+PGX_G2_EXACT, PGX_G2_REFERENCE_RULE, PGX_G2_ANCHORED = 0, 1, 2
 
 EXPORTS = [
     "pgx_version", "pgx_create", "pgx_destroy", "pgx_last_error", "pgx_set_blocks", "pgx_set_hamiltonian",

@@ -146,8 +146,10 @@ class EngineRun:
     """The G2 stage chain on one libpgx context with the Hamiltonian resident
     in HBM: eigensolve, weights, rotation of c^+ and c, G2 on the triples."""
 
-    def __init__(self, prob: Problem, device=0):
-        from .pgx import Engine
+    def __init__(self, prob: Problem, device=0, anchored=True, anchor_tol=1e-16):
+        from .pgx import PGX_G2_ANCHORED, PGX_G2_EXACT, Engine
+        self.flags = PGX_G2_ANCHORED if anchored else PGX_G2_EXACT
+        self.anchor_tol = anchor_tol if anchored else 0.0
         self.prob = prob
         blocks, self.actions, self.chains = prob.engine_inputs()
         self.eng = Engine(device)
@@ -171,4 +173,4 @@ class EngineRun:
         parts = [((slots[p[0]], slots[p[1]], slots[p[2]], self.cdag[d]), tuple(b), tuple(p), s)
                  for b, p, s in self.chains]
         self.parts = parts
-        return e.g2(parts, triples, pole_res=1e-8)
+        return e.g2(parts, triples, pole_res=1e-8, coef_tol=self.anchor_tol, flags=self.flags)

@@ -207,6 +207,67 @@ def test_anderson2pgf_golden(harness):
         assert np.abs(v - np.array(k["chi_uuuu"])).max() < k["tol"]
 
 
+def _anchored(g, parts, fz, tol=1e-16, pole_res=1e-8):
+    from pomerol_b200.pgx import PGX_G2_ANCHORED
+    return g.eng.g2(parts, fz, pole_res=pole_res, coef_tol=tol, flags=PGX_G2_ANCHORED)
+
+
+def test_anchored_g2_vertex4_and_anderson2pgf(harness):
+    """Weight-anchored sum reproduces the closed-form atom and the golden vector."""
+    from tests.test_oracle_golden import anderson2pgf_freqs, anderson2pgf_model
+    k, e = anderson2pgf_model()
+    m = M.make_model(e)
+    g = harness(m, k["beta"])
+    fz = np.array(anderson2pgf_freqs(k["beta"]))
+    i = m.info.getIndex("C", 0, M.UP)
+    parts = g.g2_parts(g.c(i), g.c(i), g.cdag(i), g.cdag(i))
+    v = _anchored(g, parts, fz, tol=1e-15, pole_res=k["pole_resolution"])
+    assert np.abs(v - np.array(k["chi_uuuu"])).max() < k["tol"]
+    exact = g.eng.g2(parts, fz, pole_res=k["pole_resolution"])
+    assert np.abs(v - exact).max() < 1e-10 * np.abs(exact).max()
+
+
+@pytest.mark.parametrize("beta", [2.0, 10.0])
+def test_anchored_g2_plaquette_matches_exact_oracle(harness, beta):
+    m = M.make_model(M.plaquette())
+    g = harness(m, beta)
+    ed = EDm.ED(m, beta)
+    u, d = m.info.getIndex("A", 0, 1), m.info.getIndex("A", 0, 0)
+    trip = [(a, b, x) for a in range(-4, 4) for b in range(-4, 4) for x in range(-4, 4)]
+    fz = np.array([L.fermionic(np.array(t), beta) for t in trip])
+    parts = g.g2_parts(g.c(u), g.c(d), g.cdag(u), g.cdag(d))
+    v = _anchored(g, parts, fz)
+    oparts = L.g2_parts(ed, ed.c(u), ed.c(d), ed.cdag(u), ed.cdag(d))
+    sel = list(range(0, len(trip), 29))
+    ref = L.g2_exact(ed, oparts, [tuple(fz[t]) for t in sel])
+    assert np.abs(v[sel] - ref).max() < 1e-10 * np.abs(ref).max()
+    # bosonic transfer 0 with equal energies exercises the delta branches
+    assert np.abs(v - g.eng.g2(parts, fz)).max() < 1e-10 * np.abs(v).max()
+
+
+def test_anchored_g2_anderson_a5_subset(harness):
+    """Anderson 1+5 (dim 4096, beta=20): anchored GPU sum vs the exact oracle
+    on the largest block chains and a subset of the 16^3 cube."""
+    U, epsd, eps, V, beta = M.anderson_a5_params(0)
+    m = M.make_model(M.anderson(U, epsd, eps, V))
+    g = harness(m, beta)
+    ed = EDm.ED(m, beta)
+    u, d = m.info.getIndex("C", 0, 1), m.info.getIndex("C", 0, 0)
+    n = np.arange(-8, 8)
+    trip = np.array([(a, b, x) for a in n for b in n for x in n])
+    fz = L.fermionic(trip, beta)
+    parts = g.g2_parts(g.c(u), g.c(d), g.cdag(u), g.cdag(d))
+    v = _anchored(g, parts, fz)
+    # dense GPU sum over every quadruple (exact mode) on the full cube
+    vx = g.eng.g2(parts, fz)
+    assert np.abs(v - vx).max() < 1e-9 * np.abs(vx).max()
+    # exact oracle on a few triples, all chains
+    oparts = L.g2_parts(ed, ed.c(u), ed.c(d), ed.cdag(u), ed.cdag(d))
+    sel = [0, 777, 2048, 4095]
+    ref = L.g2_exact(ed, oparts, [tuple(fz[t]) for t in sel])
+    assert np.abs(vx[sel] - ref).max() < 1e-9 * np.abs(ref).max()
+
+
 def test_plaquette_g2_matches_oracle(harness):
     """Plaquette (t=1, U=4, mu=2, beta=10), chi_(u0,d0,u0,d0) on n in [-4,3]^3."""
     beta = 10.0
