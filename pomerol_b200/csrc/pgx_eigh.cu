@@ -61,15 +61,14 @@ struct EighArgs {
     const double* H;           // packed input blocks (row-major)
     double* A;                 // workspace copy (destroyed)
     double* Zc;                // workspace, column-major accumulated factor
-    double* U;                 // output eigenvectors, row-major, columns = vectors
-    double* E;                 // output eigenvalues, ascending per block
-    int* status;               // set to PGX_ERR_NUMERIC on failure
+    double* tri;               // per block: diagonal then sub-diagonal (2 n)
 };
 
+// Householder reduction of one block and accumulation of its orthogonal
+// factor (column-major), one CTA per block.
 __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
     extern __shared__ double sh[];
     __shared__ double red[32];
-    __shared__ int s_state, s_m, s_nrot;
 
     const int b = g.order[blockIdx.x];
     const int n = g.dims[b];
@@ -77,8 +76,6 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
     const double* Hb = g.H + mo;
     double* A = g.A + mo;
     double* Z = g.Zc + mo;
-    double* U = g.U + mo;
-    double* E = g.E + eo;
     const int tid = threadIdx.x, nt = blockDim.x;
 
     double* v = sh;            // n   Householder vector   | later: cosines
@@ -190,9 +187,58 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
         }
         __syncthreads();
     }
-    // ---------------- implicit QL with Wilkinson shift ----------------
-    double* cs = v;
-    double* sn = w;
+    // hand the tridiagonal (diagonal, sub-diagonal) to the QL stage
+    for (int i = tid; i < n; i += nt) {
+        g.tri[2 * eo + i] = dg[i];
+        g.tri[2 * eo + n + i] = ed[i];
+    }
+}
+
+// Implicit QL with Wilkinson shift on the tridiagonal of one block, applied to
+// a slice of rows of the accumulated factor held in shared memory.  Rows of
+// Q evolve independently under right-multiplication by Givens rotations, so a
+// large block is split over many CTAs; each CTA regenerates the (identical)
+// rotation sequence with one thread and applies it to its rows.  The rows
+// then give the eigenvectors, sorted by a rank computation.
+struct QlItem {
+    int block, row0, nrows, pad;
+};
+
+struct QlArgs {
+    const QlItem* items;
+    const int* dims;
+    const long* moff;
+    const long* eoff;
+    const double* Zc;   // column-major factor per block
+    const double* tri;  // per block: n diagonal then n sub-diagonal entries
+    double* U;
+    double* E;
+    int* status;
+};
+
+__global__ void __launch_bounds__(128) ql_rows_kernel(QlArgs g) {
+    extern __shared__ double sh[];
+    __shared__ int s_state, s_m, s_nrot;
+    const QlItem it = g.items[blockIdx.x];
+    const int n = g.dims[it.block], nr = it.nrows, row0 = it.row0;
+    const long mo = g.moff[it.block], eo = g.eoff[it.block];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int ld = n + 1;  // odd row stride: rows of different threads fall in different banks
+    double* dg = sh;
+    double* ed = sh + n;
+    double* cs = sh + 2 * n;
+    double* sn = sh + 3 * n;
+    double* Zs = sh + 4 * n;  // nr x ld
+    for (int i = tid; i < n; i += nt) {
+        dg[i] = g.tri[2 * eo + i];
+        ed[i] = g.tri[2 * eo + n + i];
+    }
+    const double* Zc = g.Zc + mo;
+    for (long e = tid; e < (long)nr * n; e += nt) {
+        const int r = (int)(e % nr), j = (int)(e / nr);
+        Zs[r * ld + j] = Zc[(long)j * n + row0 + r];
+    }
+    __syncthreads();
     const double eps = 2.220446049250313e-16;
     for (int l = 0; l < n; ++l) {
         int iter = 0;
@@ -214,26 +260,34 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
                     double s = 1.0, c = 1.0, p = 0.0;
                     int i = m - 1, nrot = 0;
                     bool underflow = false;
+                    // one reciprocal square root per rotation keeps the
+                    // dependent chain short (the sweep is sequential);
+                    // d[i+1] of this step is the d[i] loaded one step earlier
+                    double d_hi = dg[m];
                     for (; i >= l; --i) {
-                        double f = s * ed[i], bb = c * ed[i];
-                        r = hyp(f, g);
-                        ed[i + 1] = r;
-                        if (r == 0.0) {
-                            dg[i + 1] -= p;
+                        const double ei = ed[i], d_lo = dg[i];
+                        const double f = s * ei, bb = c * ei;
+                        const double r2 = fma(f, f, g * g);
+                        if (r2 == 0.0) {
+                            ed[i + 1] = 0.0;
+                            dg[i + 1] = d_hi - p;
                             ed[m] = 0.0;
                             underflow = true;
                             break;
                         }
-                        s = f / r;
-                        c = g / r;
-                        g = dg[i + 1] - p;
-                        r = (dg[i] - g) * s + 2.0 * c * bb;
+                        const double rinv = rsqrt(r2);
+                        ed[i + 1] = r2 * rinv;
+                        s = f * rinv;
+                        c = g * rinv;
+                        g = d_hi - p;
+                        r = (d_lo - g) * s + 2.0 * c * bb;
                         p = s * r;
                         dg[i + 1] = g + p;
                         g = c * r - bb;
                         cs[nrot] = c;
                         sn[nrot] = s;
                         ++nrot;
+                        d_hi = d_lo;
                     }
                     if (!underflow) {
                         dg[l] -= p;
@@ -253,46 +307,37 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
             }
             if (st == 1) break;
             const int m = s_m, nrot = s_nrot;
-            // rotations at i = m-1, m-2, ..., m-nrot on columns (i, i+1)
-            // columns m-1-q are loaded eight at a time before the stores of
-            // the same group, so the loads overlap instead of waiting on them
-            for (int r = tid; r < n; r += nt) {
-                double carry = Z[(long)m * n + r];
-                for (int q0 = 0; q0 < nrot; q0 += 8) {
-                    double zi[8];
-#pragma unroll
-                    for (int u = 0; u < 8; ++u)
-                        if (q0 + u < nrot) zi[u] = Z[(long)(m - 1 - q0 - u) * n + r];
-#pragma unroll
-                    for (int u = 0; u < 8; ++u) {
-                        if (q0 + u < nrot) {
-                            const double s = sn[q0 + u], c = cs[q0 + u];
-                            Z[(long)(m - q0 - u) * n + r] = s * zi[u] + c * carry;
-                            carry = c * zi[u] - s * carry;
-                        }
-                    }
+            // rotations at i = m-1, ..., m-nrot on columns (i, i+1) of each row
+            for (int r = tid; r < nr; r += nt) {
+                double* row = Zs + r * ld;
+                double carry = row[m];
+                for (int q = 0; q < nrot; ++q) {
+                    const double zi = row[m - 1 - q], s = sn[q], c = cs[q];
+                    row[m - q] = s * zi + c * carry;
+                    carry = c * zi - s * carry;
                 }
-                if (nrot > 0) Z[(long)(m - nrot) * n + r] = carry;
+                if (nrot > 0) row[m - nrot] = carry;
             }
             __syncthreads();
         }
     }
     // ---------------- sort ascending (rank) and write E, U (row-major) ----------------
+    int* rank = reinterpret_cast<int*>(cs);
     for (int i = tid; i < n; i += nt) {
         const double di = dg[i];
-        int rank = 0;
+        int rk = 0;
         for (int j = 0; j < n; ++j) {
             const double dj = dg[j];
-            rank += (dj < di) || (dj == di && j < i);
+            rk += (dj < di) || (dj == di && j < i);
         }
-        ed[i] = (double)rank;  // reuse as rank storage
-        E[rank] = di;
+        rank[i] = rk;
+        if (row0 == 0) g.E[eo + rk] = di;
     }
     __syncthreads();
-    for (int i = 0; i < n; ++i) {
-        const int rank = (int)ed[i];
-        const double* col = Z + (long)i * n;
-        for (int r = tid; r < n; r += nt) U[(long)r * n + rank] = col[r];
+    double* U = g.U + mo;
+    for (long e = tid; e < (long)nr * n; e += nt) {
+        const int r = (int)(e / n), j = (int)(e % n);
+        U[(long)(row0 + r) * n + rank[j]] = Zs[r * ld + j];
     }
 }
 
@@ -302,6 +347,7 @@ void launch_eigh(Problem& P, cudaStream_t st) {
     const size_t smem = 4 * sizeof(double) * (size_t)std::max(P.dmax, 1);
     PGX_CHECK(smem <= 200 * 1024, PGX_ERR_ARG, "block too large for the single-CTA eigensolver (d > 6400)");
     PGX_CUDA(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    P.tri.reserve(2 * std::max<long>(P.esize, 1) * sizeof(double));
     EighArgs a;
     a.order = P.d_order;
     a.dims = P.d_dims;
@@ -310,11 +356,44 @@ void launch_eigh(Problem& P, cudaStream_t st) {
     a.H = P.d_H;
     a.A = P.d_work;
     a.Zc = P.d_work2;
-    a.U = P.d_U;
-    a.E = P.d_E;
-    a.status = P.d_status;
+    a.tri = P.tri.as<double>();
     eigh_kernel<<<P.nblocks, EIGH_THREADS, smem, st>>>(a);
     check_launch("eigh_kernel");
+
+    // QL stage: row slices sized to fill ~200 KB of shared memory per CTA,
+    // largest blocks first
+    const long cap = 200L * 1024 / sizeof(double);
+    std::vector<QlItem> items;
+    std::vector<int> order(P.nblocks);
+    for (int b = 0; b < P.nblocks; ++b) order[b] = b;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return P.dims[x] > P.dims[y]; });
+    long smem_ql = 0;
+    for (int b : order) {
+        const long n = P.dims[b];
+        const long rows = std::max<long>(1, std::min<long>(n, (cap - 4 * n) / (n + 1)));
+        PGX_CHECK(4 * n + rows * (n + 1) <= cap, PGX_ERR_ARG, "block too large for the QL stage");
+        for (long r0 = 0; r0 < n; r0 += rows) {
+            const int nr = (int)std::min(rows, n - r0);
+            items.push_back(QlItem{b, (int)r0, nr, 0});
+            smem_ql = std::max(smem_ql, (4 * n + (long)nr * (n + 1)) * (long)sizeof(double));
+        }
+    }
+    P.ql_items.reserve(items.size() * sizeof(QlItem));
+    PGX_CUDA(cudaMemcpyAsync(P.ql_items.p, items.data(), items.size() * sizeof(QlItem), cudaMemcpyHostToDevice, st));
+    PGX_CUDA(cudaFuncSetAttribute(ql_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ql));
+    QlArgs q;
+    q.items = P.ql_items.as<QlItem>();
+    q.dims = P.d_dims;
+    q.moff = P.d_moff;
+    q.eoff = P.d_eoff;
+    q.Zc = P.d_work2;
+    q.tri = P.tri.as<double>();
+    q.U = P.d_U;
+    q.E = P.d_E;
+    q.status = P.d_status;
+    ql_rows_kernel<<<(unsigned)items.size(), 128, smem_ql, st>>>(q);
+    check_launch("ql_rows_kernel");
+    PGX_CUDA(cudaStreamSynchronize(st));  // the host item list goes out of scope
 }
 
 }  // namespace pgx

@@ -67,33 +67,37 @@ template <> __device__ __forceinline__ cd zero_of<cd>() { return cd{0.0, 0.0}; }
 
 constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_THREADS = 256;
 
-template <typename TA, typename TB, typename TC>
+// Tile shapes: 64x64 (4x4 outputs per thread), 16x128 for problems with at
+// most 16 rows and 128x16 for at most 16 columns (1x8 / 8x1 per thread), so
+// the skinny products of the anchored G2 do not waste a 64-wide tile.
+template <typename TA, typename TB, typename TC, int BM, int BN>
 __global__ void __launch_bounds__(GEMM_THREADS)
     gemm_tiles_kernel(const GemmProblem<TA, TB, TC>* __restrict__ probs, const GemmTile* __restrict__ tiles) {
     using TAcc = typename std::conditional<is_cd<TA>::value || is_cd<TB>::value, cd, double>::type;
     constexpr int BK = (is_cd<TA>::value || is_cd<TB>::value) ? 8 : 16;
-    __shared__ TA As[BK][GEMM_BM + 1];
-    __shared__ TB Bs[BK][GEMM_BN + 1];
+    constexpr int TM = BM / 16, TN = BN / 16;
+    __shared__ TA As[BK][BM + 1];
+    __shared__ TB Bs[BK][BN + 1];
 
     const GemmTile t = tiles[blockIdx.x];
     const GemmProblem<TA, TB, TC> p = probs[t.prob];
-    const int i0 = t.tm * GEMM_BM, j0 = t.tn * GEMM_BN;
+    const int i0 = t.tm * BM, j0 = t.tn * BN;
     const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
 
-    TAcc acc[4][4];
+    TAcc acc[TM][TN];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < TM; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = zero_of<TAcc>();
+        for (int b = 0; b < TN; ++b) acc[a][b] = zero_of<TAcc>();
 
     const bool a_i_fast = (p.sa_i == 1);
     const bool b_j_fast = (p.sb_j == 1);
 
     for (int k0 = 0; k0 < p.K; k0 += BK) {
         // ---- A tile: BM x BK
-        for (int l = tid; l < GEMM_BM * BK; l += GEMM_THREADS) {
+        for (int l = tid; l < BM * BK; l += GEMM_THREADS) {
             int ii, kk;
-            if (a_i_fast) { ii = l % GEMM_BM; kk = l / GEMM_BM; }
+            if (a_i_fast) { ii = l % BM; kk = l / BM; }
             else { ii = l / BK; kk = l % BK; }
             const int gi = i0 + ii, gk = k0 + kk;
             TA v = zero_of<TA>();
@@ -105,9 +109,9 @@ __global__ void __launch_bounds__(GEMM_THREADS)
             As[kk][ii] = v;
         }
         // ---- B tile: BK x BN
-        for (int l = tid; l < GEMM_BN * BK; l += GEMM_THREADS) {
+        for (int l = tid; l < BN * BK; l += GEMM_THREADS) {
             int jj, kk;
-            if (b_j_fast) { jj = l % GEMM_BN; kk = l / GEMM_BN; }
+            if (b_j_fast) { jj = l % BN; kk = l / BN; }
             else { jj = l / BK; kk = l % BK; }
             const int gj = j0 + jj, gk = k0 + kk;
             TB v = zero_of<TB>();
@@ -122,26 +126,25 @@ __global__ void __launch_bounds__(GEMM_THREADS)
         __syncthreads();
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
-            TA a[4];
-            TB b[4];
+            TA a[TM];
+            TB b[TN];
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                a[q] = As[kk][ty + 16 * q];
-                b[q] = Bs[kk][tx + 16 * q];
-            }
+            for (int q = 0; q < TM; ++q) a[q] = As[kk][ty + 16 * q];
 #pragma unroll
-            for (int qa = 0; qa < 4; ++qa)
+            for (int q = 0; q < TN; ++q) b[q] = Bs[kk][tx + 16 * q];
 #pragma unroll
-                for (int qb = 0; qb < 4; ++qb) mac(acc[qa][qb], a[qa], b[qb]);
+            for (int qa = 0; qa < TM; ++qa)
+#pragma unroll
+                for (int qb = 0; qb < TN; ++qb) mac(acc[qa][qb], a[qa], b[qb]);
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int qa = 0; qa < 4; ++qa) {
+    for (int qa = 0; qa < TM; ++qa) {
         const int gi = i0 + ty + 16 * qa;
         if (gi >= p.M) continue;
 #pragma unroll
-        for (int qb = 0; qb < 4; ++qb) {
+        for (int qb = 0; qb < TN; ++qb) {
             const int gj = j0 + tx + 16 * qb;
             if (gj >= p.N) continue;
             store_c(p.C[gi * p.sc_i + gj * p.sc_j], acc[qa][qb], p.accumulate);
@@ -149,26 +152,53 @@ __global__ void __launch_bounds__(GEMM_THREADS)
     }
 }
 
-// Host helper: upload problems + tile list into scratch buffers and launch.
+// Tile class of a problem: 0 = 64x64, 1 = 16x128 (M <= 16), 2 = 128x16 (N <= 16).
+template <typename P> inline int gemm_class(const P& p) {
+    if (p.M <= 16 && p.N > 16) return 1;
+    if (p.N <= 16 && p.M > 16) return 2;
+    if (p.M <= 16 && p.N <= 16) return 1;
+    return 0;
+}
+
+// Host helper: upload problems + tile lists into scratch buffers and launch
+// one kernel per tile class.  Tile capacity computed for 64x64 tiles is an
+// upper bound for every class.
 template <typename TA, typename TB, typename TC>
 void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* d_probs, size_t probs_cap,
                        void* d_tiles, size_t tiles_cap, cudaStream_t st) {
     if (probs.empty()) return;
+    static const int BMs[3] = {64, 16, 128}, BNs[3] = {64, 128, 16};
     std::vector<GemmTile> tiles;
-    for (size_t q = 0; q < probs.size(); ++q) {
-        const int tm = ceil_div(probs[q].M, GEMM_BM), tn = ceil_div(probs[q].N, GEMM_BN);
-        if (probs[q].M <= 0 || probs[q].N <= 0) continue;
-        for (int a = 0; a < tm; ++a)
-            for (int b = 0; b < tn; ++b) tiles.push_back(GemmTile{(int)q, a, b, 0});
+    size_t start[4] = {0, 0, 0, 0};
+    for (int cls = 0; cls < 3; ++cls) {
+        start[cls] = tiles.size();
+        for (size_t q = 0; q < probs.size(); ++q) {
+            if (probs[q].M <= 0 || probs[q].N <= 0 || gemm_class(probs[q]) != cls) continue;
+            const int tm = ceil_div(probs[q].M, BMs[cls]), tn = ceil_div(probs[q].N, BNs[cls]);
+            for (int a = 0; a < tm; ++a)
+                for (int b = 0; b < tn; ++b) tiles.push_back(GemmTile{(int)q, a, b, 0});
+        }
     }
+    start[3] = tiles.size();
     if (tiles.empty()) return;
     PGX_CHECK(probs.size() * sizeof(probs[0]) <= probs_cap, PGX_ERR_ARG, "gemm problem list overflow");
     PGX_CHECK(tiles.size() * sizeof(GemmTile) <= tiles_cap, PGX_ERR_ARG, "gemm tile list overflow");
     PGX_CUDA(cudaMemcpyAsync(d_probs, probs.data(), probs.size() * sizeof(probs[0]), cudaMemcpyHostToDevice, st));
     PGX_CUDA(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(GemmTile), cudaMemcpyHostToDevice, st));
-    gemm_tiles_kernel<TA, TB, TC><<<(unsigned)tiles.size(), GEMM_THREADS, 0, st>>>(
-        static_cast<const GemmProblem<TA, TB, TC>*>(d_probs), static_cast<const GemmTile*>(d_tiles));
-    check_launch("gemm_tiles_kernel");
+    const auto* dp = static_cast<const GemmProblem<TA, TB, TC>*>(d_probs);
+    const auto* dt = static_cast<const GemmTile*>(d_tiles);
+    if (start[1] > start[0]) {
+        gemm_tiles_kernel<TA, TB, TC, 64, 64><<<(unsigned)(start[1] - start[0]), GEMM_THREADS, 0, st>>>(dp, dt + start[0]);
+        check_launch("gemm_tiles_kernel<64,64>");
+    }
+    if (start[2] > start[1]) {
+        gemm_tiles_kernel<TA, TB, TC, 16, 128><<<(unsigned)(start[2] - start[1]), GEMM_THREADS, 0, st>>>(dp, dt + start[1]);
+        check_launch("gemm_tiles_kernel<16,128>");
+    }
+    if (start[3] > start[2]) {
+        gemm_tiles_kernel<TA, TB, TC, 128, 16><<<(unsigned)(start[3] - start[2]), GEMM_THREADS, 0, st>>>(dp, dt + start[2]);
+        check_launch("gemm_tiles_kernel<128,16>");
+    }
 }
 
 }  // namespace pgx

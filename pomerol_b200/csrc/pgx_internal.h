@@ -85,7 +85,7 @@ struct Problem {
     double beta = 0.0, E0 = 0.0, Z = 0.0;
     std::vector<int> retained;
 
-    DevBuf H, work, work2, U, E, w, dims_d, moff_d, eoff_d, order_d, status;
+    DevBuf H, work, work2, U, E, w, dims_d, moff_d, eoff_d, order_d, status, tri, ql_items;
     int* d_dims = nullptr;
     long* d_moff = nullptr;
     long* d_eoff = nullptr;
