@@ -175,6 +175,24 @@ int pgx_g2(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, int32_t nfreq
 int pgx_g2_count(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, double coef_tol, double nz_tol,
                  long long* count);
 
+/* ------------------------------------------------------------------------
+ * Allocation-free eigensolve (no counterpart in the reference).
+ * For callers whose device memory belongs to an outer allocator (an
+ * application's caching pool or a fixed arena) and which must not let a
+ * library call cudaMalloc/cudaFree: diagonalises ONE real symmetric block of
+ * size n <= PGX_NOALLOC_MAX_DIM on buffers the caller owns, keeping its
+ * workspace in a static device array of the library (about 1 MiB per GPU,
+ * held until the process exits).  H (n*n, row-major, read only), E (n) and U
+ * (n*n, row-major, eigenvectors as columns, ascending eigenvalues) are DEVICE
+ * pointers; stream is a cudaStream_t (NULL: default stream).  The call waits
+ * for the stream before returning.  Larger n returns PGX_ERR_ARG.  All calls
+ * on a device share the workspace: calls that overlap on the GPU race and
+ * must be serialised by the caller.  The first call on a device looks up the
+ * workspace's address and should come before any stream capture.
+ * ------------------------------------------------------------------------ */
+#define PGX_NOALLOC_MAX_DIM 256
+int pgx_eigh_noalloc(const double* H, int32_t n, double* E, double* U, void* stream);
+
 /* Device-side timing of everything the context issues between the two
  * calls (CUDA events on the context's stream). */
 int pgx_timer_begin(pgx_ctx* ctx);

@@ -343,33 +343,17 @@ __global__ void __launch_bounds__(128) ql_rows_kernel(QlArgs g) {
 
 }  // namespace
 
-void launch_eigh(Problem& P, cudaStream_t st) {
-    const size_t smem = 4 * sizeof(double) * (size_t)std::max(P.dmax, 1);
-    PGX_CHECK(smem <= 200 * 1024, PGX_ERR_ARG, "block too large for the single-CTA eigensolver (d > 6400)");
-    PGX_CUDA(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    P.tri.reserve(2 * std::max<long>(P.esize, 1) * sizeof(double));
-    EighArgs a;
-    a.order = P.d_order;
-    a.dims = P.d_dims;
-    a.moff = P.d_moff;
-    a.eoff = P.d_eoff;
-    a.H = P.d_H;
-    a.A = P.d_work;
-    a.Zc = P.d_work2;
-    a.tri = P.tri.as<double>();
-    eigh_kernel<<<P.nblocks, EIGH_THREADS, smem, st>>>(a);
-    check_launch("eigh_kernel");
-
-    // QL stage: row slices sized to fill ~200 KB of shared memory per CTA,
-    // largest blocks first
+// QL work items of a block list: row slices sized to fill ~200 KB of shared
+// memory per CTA, largest blocks first.  Returns the dynamic shared memory
+// the QL kernel needs.
+static long ql_plan(const std::vector<int>& dims, std::vector<QlItem>& items) {
     const long cap = 200L * 1024 / sizeof(double);
-    std::vector<QlItem> items;
-    std::vector<int> order(P.nblocks);
-    for (int b = 0; b < P.nblocks; ++b) order[b] = b;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return P.dims[x] > P.dims[y]; });
+    std::vector<int> order(dims.size());
+    for (size_t b = 0; b < dims.size(); ++b) order[b] = (int)b;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return dims[x] > dims[y]; });
     long smem_ql = 0;
     for (int b : order) {
-        const long n = P.dims[b];
+        const long n = dims[b];
         const long rows = std::max<long>(1, std::min<long>(n, (cap - 4 * n) / (n + 1)));
         PGX_CHECK(4 * n + rows * (n + 1) <= cap, PGX_ERR_ARG, "block too large for the QL stage");
         for (long r0 = 0; r0 < n; r0 += rows) {
@@ -378,22 +362,71 @@ void launch_eigh(Problem& P, cudaStream_t st) {
             smem_ql = std::max(smem_ql, (4 * n + (long)nr * (n + 1)) * (long)sizeof(double));
         }
     }
-    P.ql_items.reserve(items.size() * sizeof(QlItem));
-    PGX_CUDA(cudaMemcpyAsync(P.ql_items.p, items.data(), items.size() * sizeof(QlItem), cudaMemcpyHostToDevice, st));
+    return smem_ql;
+}
+
+size_t eigh_ql_item_bytes(const std::vector<int>& dims) {
+    std::vector<QlItem> items;
+    ql_plan(dims, items);
+    return items.size() * sizeof(QlItem);
+}
+
+// Both eigensolver stages on caller-provided device buffers (no allocation).
+// `items_dev` must hold eigh_ql_item_bytes(dims) bytes; the function waits for
+// the stream before returning because the host item list is staged from it.
+void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, cudaStream_t st) {
+    int dmax = 1;
+    for (int x : dims) dmax = std::max(dmax, x);
+    const size_t smem = 4 * sizeof(double) * (size_t)dmax;
+    PGX_CHECK(smem <= 200 * 1024, PGX_ERR_ARG, "block too large for the single-CTA eigensolver (d > 6400)");
+    PGX_CUDA(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    EighArgs a;
+    a.order = d.order;
+    a.dims = d.dims;
+    a.moff = d.moff;
+    a.eoff = d.eoff;
+    a.H = d.H;
+    a.A = d.A;
+    a.Zc = d.Zc;
+    a.tri = d.tri;
+    eigh_kernel<<<(unsigned)dims.size(), EIGH_THREADS, smem, st>>>(a);
+    check_launch("eigh_kernel");
+    std::vector<QlItem> items;
+    const long smem_ql = ql_plan(dims, items);
+    PGX_CUDA(cudaMemcpyAsync(d.items, items.data(), items.size() * sizeof(QlItem), cudaMemcpyHostToDevice, st));
     PGX_CUDA(cudaFuncSetAttribute(ql_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ql));
     QlArgs q;
-    q.items = P.ql_items.as<QlItem>();
-    q.dims = P.d_dims;
-    q.moff = P.d_moff;
-    q.eoff = P.d_eoff;
-    q.Zc = P.d_work2;
-    q.tri = P.tri.as<double>();
-    q.U = P.d_U;
-    q.E = P.d_E;
-    q.status = P.d_status;
+    q.items = static_cast<const QlItem*>(d.items);
+    q.dims = d.dims;
+    q.moff = d.moff;
+    q.eoff = d.eoff;
+    q.Zc = d.Zc;
+    q.tri = d.tri;
+    q.U = d.U;
+    q.E = d.E;
+    q.status = d.status;
     ql_rows_kernel<<<(unsigned)items.size(), 128, smem_ql, st>>>(q);
     check_launch("ql_rows_kernel");
     PGX_CUDA(cudaStreamSynchronize(st));  // the host item list goes out of scope
+}
+
+void launch_eigh(Problem& P, cudaStream_t st) {
+    P.tri.reserve(2 * std::max<long>(P.esize, 1) * sizeof(double));
+    P.ql_items.reserve(eigh_ql_item_bytes(P.dims));
+    EighDev d;
+    d.order = P.d_order;
+    d.dims = P.d_dims;
+    d.moff = P.d_moff;
+    d.eoff = P.d_eoff;
+    d.H = P.d_H;
+    d.A = P.d_work;
+    d.Zc = P.d_work2;
+    d.tri = P.tri.as<double>();
+    d.items = P.ql_items.p;
+    d.U = P.d_U;
+    d.E = P.d_E;
+    d.status = P.d_status;
+    launch_eigh_raw(d, P.dims, st);
 }
 
 }  // namespace pgx

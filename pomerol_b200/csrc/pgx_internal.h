@@ -121,6 +121,24 @@ struct pgx_ctx {
 namespace pgx {
 
 void launch_eigh(Problem& P, cudaStream_t st);
+
+// Device buffers of one eigensolve (any number of blocks), all caller-owned.
+struct EighDev {
+    const int* order;    // CTA -> block, largest first
+    const int* dims;
+    const long* moff;
+    const long* eoff;
+    const double* H;     // packed blocks, row-major
+    double* A;           // workspace, sum d^2
+    double* Zc;          // workspace, sum d^2
+    double* tri;         // workspace, 2 sum d
+    void* items;         // workspace, eigh_ql_item_bytes(dims)
+    double* U;           // output, sum d^2
+    double* E;           // output, sum d
+    int* status;         // PGX_ERR_NUMERIC on non-convergence
+};
+size_t eigh_ql_item_bytes(const std::vector<int>& dims);
+void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, cudaStream_t st);
 void launch_weights(Problem& P, double beta, cudaStream_t st);
 void rotate_operator(Problem& P, Operator& op, cudaStream_t st);
 void adjoint_operator(Problem& P, const Operator& src, Operator& dst, cudaStream_t st);

@@ -22,7 +22,7 @@ EXPORTS = [
     "pgx_eigh", "pgx_get_eigensystem", "pgx_ground_energy", "pgx_weights", "pgx_truncate_blocks",
     "pgx_op_define", "pgx_op_rotate", "pgx_op_adjoint", "pgx_op_info", "pgx_op_read", "pgx_gf", "pgx_susc",
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
-    "pgx_launch_count",
+    "pgx_launch_count", "pgx_eigh_noalloc",
 ]
 
 
@@ -71,6 +71,7 @@ def load():
         lib.pgx_timer_begin.argtypes = [P]
         lib.pgx_timer_end.argtypes = [P, P]
         lib.pgx_launch_count.restype = C.c_longlong
+        lib.pgx_eigh_noalloc.argtypes = [P, I32, P, P, P]
         _lib = lib
     return _lib
 
