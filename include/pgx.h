@@ -181,7 +181,7 @@ int pgx_g2_count(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, double 
  * application's caching pool or a fixed arena) and which must not let a
  * library call cudaMalloc/cudaFree: diagonalises ONE real symmetric block of
  * size n <= PGX_NOALLOC_MAX_DIM on buffers the caller owns, keeping its
- * workspace in a static device array of the library (about 1 MiB per GPU,
+ * workspace in a static device array of the library (about 2.5 MiB per GPU,
  * held until the process exits).  H (n*n, row-major, read only), E (n) and U
  * (n*n, row-major, eigenvectors as columns, ascending eigenvalues) are DEVICE
  * pointers; stream is a cudaStream_t (NULL: default stream).  The call waits
@@ -203,6 +203,17 @@ long long pgx_launch_count(void);
 
 /* Device time (ms) of the last pgx_g2 call and its dominant GEMM stage. */
 int pgx_g2_last_timing(pgx_ctx* ctx, double* total_ms, double* gemm_ms, double* gemm_flops);
+
+/* Per-kernel profile of everything the context launches between the two
+ * calls: CUDA event pairs on the launching stream around each instrumented
+ * kernel, aggregated by kernel name and sorted by total time (largest first).
+ * flops and bytes are the kernel's ALGORITHMIC floating-point operations and
+ * DRAM bytes (minimum traffic) summed over its launches, 0 where not stated.
+ * pgx_profile_end waits for the stream and returns the number of kernels. */
+int pgx_profile_begin(pgx_ctx* ctx);
+int pgx_profile_end(pgx_ctx* ctx, int32_t* nkernels);
+int pgx_profile_kernel(pgx_ctx* ctx, int32_t i, char* name, int32_t name_cap, int32_t* launches, double* ms,
+                       double* flops, double* bytes);
 
 #ifdef __cplusplus
 }

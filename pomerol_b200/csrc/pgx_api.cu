@@ -14,6 +14,75 @@ long long& launch_counter() {
     static long long n = 0;
     return n;
 }
+
+Profiler*& active_profiler() {
+    static thread_local Profiler* p = nullptr;
+    return p;
+}
+
+cudaEvent_t Profiler::event() {
+    if (!spare.empty()) {
+        cudaEvent_t e = spare.back();
+        spare.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    PGX_CUDA(cudaEventCreate(&e));
+    return e;
+}
+
+void Profiler::clear() {
+    for (auto& r : open) {
+        spare.push_back(r.a);
+        spare.push_back(r.b);
+    }
+    open.clear();
+    stats.clear();
+}
+
+void Profiler::resolve() {
+    for (auto& r : open) {
+        PGX_CUDA(cudaEventSynchronize(r.b));
+        float t = 0.f;
+        PGX_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+        auto it = std::find_if(stats.begin(), stats.end(), [&](const KernelStat& k) { return k.name == r.name; });
+        if (it == stats.end()) {
+            stats.push_back(KernelStat{r.name});
+            it = stats.end() - 1;
+        }
+        it->launches += 1;
+        it->ms += t;
+        it->flops += r.flops;
+        it->bytes += r.bytes;
+        spare.push_back(r.a);
+        spare.push_back(r.b);
+    }
+    open.clear();
+    std::stable_sort(stats.begin(), stats.end(), [](const KernelStat& x, const KernelStat& y) { return x.ms > y.ms; });
+}
+
+Profiler::~Profiler() {
+    for (auto& r : open) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto e : spare) cudaEventDestroy(e);
+}
+
+ProfRange::ProfRange(const char* name, cudaStream_t st, double flops, double bytes) {
+    Profiler* p = active_profiler();
+    if (!p || !p->on) return;
+    Profiler::Range r{name, p->event(), p->event(), flops, bytes};
+    PGX_CUDA(cudaEventRecord(r.a, st));
+    p->open.push_back(r);
+    p_ = p;
+    st_ = st;
+    idx_ = p->open.size() - 1;
+}
+
+ProfRange::~ProfRange() {
+    if (p_) cudaEventRecord(p_->open[idx_].b, st_);
+}
 }
 
 using pgx::Error;
@@ -22,6 +91,11 @@ namespace {
 
 template <typename F> int guarded(pgx_ctx* c, F&& f) {
     if (!c) return PGX_ERR_ARG;
+    struct Scope {  // the context's profiler is visible to launch sites during the call
+        pgx::Profiler* saved;
+        explicit Scope(pgx::Profiler* p) : saved(pgx::active_profiler()) { pgx::active_profiler() = p; }
+        ~Scope() { pgx::active_profiler() = saved; }
+    } scope(&c->prof);
     try {
         PGX_CUDA(cudaSetDevice(c->device));
         f();
@@ -396,6 +470,39 @@ int pgx_timer_end(pgx_ctx* c, double* ms) {
 }
 
 long long pgx_launch_count(void) { return pgx::launch_counter(); }
+
+int pgx_profile_begin(pgx_ctx* c) {
+    return guarded(c, [&] {
+        c->prof.clear();
+        c->prof.on = true;
+    });
+}
+
+int pgx_profile_end(pgx_ctx* c, int32_t* nkernels) {
+    return guarded(c, [&] {
+        PGX_CHECK(c->prof.on, PGX_ERR_STATE, "pgx_profile_begin first");
+        c->prof.on = false;
+        c->prof.resolve();
+        if (nkernels) *nkernels = (int32_t)c->prof.stats.size();
+    });
+}
+
+int pgx_profile_kernel(pgx_ctx* c, int32_t i, char* name, int32_t name_cap, int32_t* launches, double* ms,
+                       double* flops, double* bytes) {
+    return guarded(c, [&] {
+        PGX_CHECK(i >= 0 && i < (int32_t)c->prof.stats.size(), PGX_ERR_ARG, "kernel index out of range");
+        const pgx::KernelStat& k = c->prof.stats[i];
+        if (name && name_cap > 0) {
+            const size_t n = std::min<size_t>(k.name.size(), (size_t)name_cap - 1);
+            std::copy(k.name.begin(), k.name.begin() + n, name);
+            name[n] = '\0';
+        }
+        if (launches) *launches = k.launches;
+        if (ms) *ms = k.ms;
+        if (flops) *flops = k.flops;
+        if (bytes) *bytes = k.bytes;
+    });
+}
 
 int pgx_g2_last_timing(pgx_ctx* c, double* total_ms, double* gemm_ms, double* gemm_flops) {
     return guarded(c, [&] {

@@ -1,23 +1,23 @@
-// K1: batched FP64 symmetric eigensolver, one CTA per symmetry block.
+// K1: batched FP64 symmetric eigensolver.
 //
 // Replaces Eigen::SelfAdjointEigenSolver as called by HamiltonianPart::computeImpl
-// (HamiltonianPart.cpp:90-102).  Method (Golub & Van Loan, "Matrix Computations",
-// 4th ed., sections 8.3.1 and 8.3.5): Householder reduction to tridiagonal form,
-// explicit accumulation of the orthogonal factor, implicit QL iterations with
-// Wilkinson shift whose Givens rotations are applied to the accumulated factor.
-//
-// Parallel layout inside a CTA:
-//   * the Householder step's symmetric mat-vec and rank-2 update run over all
-//     threads with coalesced column access (the trailing matrix is symmetric);
-//   * the factor Q is stored column-major so that a Givens rotation on columns
-//     (i, i+1) is a coalesced update over rows;
-//   * each QL sweep's rotation sequence is produced by one thread into shared
-//     memory and applied to all rows of Q in parallel (row r carries its
-//     running value through the sweep, one load and one store per rotation);
-//   * eigenvalues are sorted by a parallel rank computation.
-// Convergence failure sets a device status word instead of trapping.
+// (HamiltonianPart.cpp:90-102).  Stages:
+//   1. eigh_kernel, one CTA per block: Householder reduction to tridiagonal
+//      form T and explicit accumulation of the orthogonal factor Q
+//      (Golub & Van Loan, "Matrix Computations", 4th ed., 8.3.1).  The
+//      symmetric mat-vec and the rank-2 update run over all threads with
+//      coalesced column access; Q is stored column-major.
+//   2. bisect_kernel, one thread per eigenvalue: bisection with Sturm counts
+//      on the unreduced pieces of T (8.4.1).
+//   3. vector_kernel, one thread per cluster of close eigenvalues: twisted
+//      factorisation for the eigenvectors of T, inverse iteration with
+//      modified Gram-Schmidt inside a cluster; eigenvalues are ranked so that
+//      the output is ascending.
+//   4. U = Q Z as one batched FP64 GEMM over all blocks.
+// A non-finite eigenvector sets a device status word instead of trapping.
 
 #include "pgx_common.cuh"
+#include "pgx_gemm.cuh"
 #include "pgx_internal.h"
 
 namespace pgx {
@@ -25,7 +25,6 @@ namespace pgx {
 namespace {
 
 constexpr int EIGH_THREADS = 512;
-constexpr int QL_MAX_ITER = 90;
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -42,15 +41,6 @@ __device__ double block_sum(double v, double* red) {
     double r = (lane < nw) ? red[lane] : 0.0;
     r = warp_sum(r);
     return r;
-}
-
-// Hypotenuse without overflow for the QL sweep (scaled form).
-__device__ __forceinline__ double hyp(double a, double b) {
-    double x = fabs(a), y = fabs(b);
-    double m = fmax(x, y), n = fmin(x, y);
-    if (m == 0.0) return 0.0;
-    double r = n / m;
-    return m * sqrt(1.0 + r * r);
 }
 
 struct EighArgs {
@@ -78,8 +68,8 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
     double* Z = g.Zc + mo;
     const int tid = threadIdx.x, nt = blockDim.x;
 
-    double* v = sh;            // n   Householder vector   | later: cosines
-    double* w = sh + n;        // n   p / w vectors        | later: sines
+    double* v = sh;            // n   Householder vector
+    double* w = sh + n;        // n   p / w vectors
     double* dg = sh + 2 * n;   // n   diagonal
     double* ed = sh + 3 * n;   // n   sub-diagonal
 
@@ -187,194 +177,292 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
         }
         __syncthreads();
     }
-    // hand the tridiagonal (diagonal, sub-diagonal) to the QL stage
+    // hand the tridiagonal (diagonal, sub-diagonal) to the bisection stage
     for (int i = tid; i < n; i += nt) {
         g.tri[2 * eo + i] = dg[i];
         g.tri[2 * eo + n + i] = ed[i];
     }
 }
 
-// Implicit QL with Wilkinson shift on the tridiagonal of one block, applied to
-// a slice of rows of the accumulated factor held in shared memory.  Rows of
-// Q evolve independently under right-multiplication by Givens rotations, so a
-// large block is split over many CTAs; each CTA regenerates the (identical)
-// rotation sequence with one thread and applies it to its rows.  The rows
-// then give the eigenvectors, sorted by a rank computation.
-struct QlItem {
-    int block, row0, nrows, pad;
+// ----------------------------------------------------------------------------
+// Tridiagonal stage.  T (diagonal d, sub-diagonal e) is split into unreduced
+// pieces where |e_i| <= eps (|d_i| + |d_i+1|) or |e_i| <= 8 eps ||T|| (a
+// perturbation of T of the size of the Householder stage's own backward
+// error).  Exact degeneracies of H show up as such splits, so eigenvectors of
+// different pieces are orthogonal by support.
+//   * eigenvalues: bisection with Sturm counts, one thread per eigenvalue
+//     (Golub & Van Loan, 8.4.1);
+//   * eigenvectors: inverse iteration, one thread per chain of eigenvalues
+//     whose neighbours are closer than 1e-4 ||T|| (Golub & Van Loan, 8.2.2;
+//     Wilkinson's scheme as in LAPACK's stein).  Each solve factors
+//     T - lambda I by Gaussian elimination with partial pivoting; a chain
+//     member is orthogonalised (modified Gram-Schmidt, twice on the last
+//     pass) against earlier members closer than 1e-4 ||T||, and its shift is
+//     nudged above the previous one so that coincident eigenvalues get
+//     distinct vectors.  The start vector is a fixed hash of (index, row).
+struct TriItem {
+    int block, j0, j1, pad;
 };
 
-struct QlArgs {
-    const QlItem* items;
+struct TriArgs {
+    const TriItem* items;
     const int* dims;
     const long* moff;
     const long* eoff;
-    const double* Zc;   // column-major factor per block
-    const double* tri;  // per block: n diagonal then n sub-diagonal entries
-    double* U;
-    double* E;
+    const double* tri;  // per block: d (n), e (n)
+    double* lam;        // per block: eigenvalues, ascending inside each piece
+    int* sb;            // per block: 2 n ints (first and last row of the piece)
+    int* rank;          // per block: n ints (position in the ascending order)
+    double* Z;          // per block: n x n column-major eigenvectors of T, sorted
+    double* S;          // per block: 3 n x n scratch (LU factors, 3 n per eigenvalue)
+    double* E;          // eigenvalues, ascending
     int* status;
 };
 
-__global__ void __launch_bounds__(128) ql_rows_kernel(QlArgs g) {
+constexpr int TRI_THREADS = 128;
+constexpr double EPS = 2.220446049250313e-16;
+constexpr double SAFE_MIN = 2.2250738585072014e-308;
+constexpr double SPLIT_ABS = 8.0;   // absolute split threshold, units of eps ||T||
+constexpr double CHAIN_TOL = 1e-4;  // chain / orthogonalisation window, units of ||T||
+constexpr int INV_ITERS = 2;        // inverse iterations (one more for chain members)
+
+// Loads d and e of one block into shared memory, zeroes the split points and
+// returns ||T|| (max row sum); every thread of the CTA must call it.
+__device__ double load_tri(const double* tri, long eo, int n, double* d, double* e) {
+    __shared__ double red[TRI_THREADS / 32];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        d[i] = tri[2 * eo + i];
+        e[i] = (i < n - 1) ? tri[2 * eo + n + i] : 0.0;
+    }
+    __syncthreads();
+    double m = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+        m = fmax(m, fabs(d[i]) + fabs(e[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0));
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = m;
+    __syncthreads();
+    double tn = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tn = fmax(tn, red[w]);
+    for (int i = threadIdx.x; i < n - 1; i += blockDim.x)
+        if (fabs(e[i]) <= EPS * (fabs(d[i]) + fabs(d[i + 1])) || fabs(e[i]) <= SPLIT_ABS * EPS * tn) e[i] = 0.0;
+    __syncthreads();
+    return tn;
+}
+
+// number of eigenvalues of T[a..b] below x
+__device__ int sturm(const double* d, const double* e, int a, int b, double x, double pivmin) {
+    double q = d[a] - x;
+    if (fabs(q) < pivmin) q = -pivmin;
+    int cnt = q < 0.0;
+    for (int i = a + 1; i <= b; ++i) {
+        q = (d[i] - x) - e[i - 1] * (e[i - 1] / q);
+        if (fabs(q) < pivmin) q = -pivmin;
+        cnt += q < 0.0;
+    }
+    return cnt;
+}
+
+__device__ void piece_of(const double* e, int n, int j, int& a, int& b) {
+    a = j;
+    b = j;
+    while (a > 0 && e[a - 1] != 0.0) --a;
+    while (b < n - 1 && e[b] != 0.0) ++b;
+}
+
+__global__ void __launch_bounds__(TRI_THREADS) bisect_kernel(TriArgs g) {
     extern __shared__ double sh[];
-    __shared__ int s_state, s_m, s_nrot;
-    const QlItem it = g.items[blockIdx.x];
-    const int n = g.dims[it.block], nr = it.nrows, row0 = it.row0;
-    const long mo = g.moff[it.block], eo = g.eoff[it.block];
-    const int tid = threadIdx.x, nt = blockDim.x;
-    const int ld = n + 1;  // odd row stride: rows of different threads fall in different banks
-    double* dg = sh;
-    double* ed = sh + n;
-    double* cs = sh + 2 * n;
-    double* sn = sh + 3 * n;
-    double* Zs = sh + 4 * n;  // nr x ld
-    for (int i = tid; i < n; i += nt) {
-        dg[i] = g.tri[2 * eo + i];
-        ed[i] = g.tri[2 * eo + n + i];
+    const TriItem it = g.items[blockIdx.x];
+    const int n = g.dims[it.block];
+    const long eo = g.eoff[it.block];
+    double* d = sh;
+    double* e = sh + n;
+    load_tri(g.tri, eo, n, d, e);
+    for (int j = it.j0 + threadIdx.x; j < it.j1; j += blockDim.x) {
+        int a, b;
+        piece_of(e, n, j, a, b);
+        double lo = 1e300, hi = -1e300, em = 0.0;
+        for (int i = a; i <= b; ++i) {
+            const double r = (i > a ? fabs(e[i - 1]) : 0.0) + (i < b ? fabs(e[i]) : 0.0);
+            lo = fmin(lo, d[i] - r);
+            hi = fmax(hi, d[i] + r);
+            if (i < b) em = fmax(em, e[i] * e[i]);
+        }
+        const double pivmin = SAFE_MIN * fmax(1.0, em);
+        const double gn = fmax(fabs(lo), fabs(hi));
+        const double w = 2.0 * EPS * gn + pivmin;
+        lo -= w;
+        hi += w;
+        const double atol = 0.25 * EPS * gn + pivmin;
+        const int k = j - a;
+        for (int iter = 0; iter < 256; ++iter) {
+            if (hi - lo <= atol + 2.0 * EPS * fmin(fabs(lo), fabs(hi))) break;
+            const double mid = 0.5 * (lo + hi);
+            if (mid <= lo || mid >= hi) break;
+            if (sturm(d, e, a, b, mid, pivmin) > k) hi = mid;
+            else lo = mid;
+        }
+        g.lam[eo + j] = 0.5 * (lo + hi);
+        g.sb[2 * eo + j] = a;
+        g.sb[2 * eo + n + j] = b;
     }
-    const double* Zc = g.Zc + mo;
-    for (long e = tid; e < (long)nr * n; e += nt) {
-        const int r = (int)(e % nr), j = (int)(e / nr);
-        Zs[r * ld + j] = Zc[(long)j * n + row0 + r];
+}
+
+// pseudo-random start vector entry in [-1, 1) for eigen-index j, row i
+__device__ __forceinline__ double start_entry(int j, int i) {
+    unsigned x = (unsigned)j * 0x9E3779B1u + (unsigned)i * 0x85EBCA77u + 0x165667B1u;
+    x ^= x >> 15;
+    x *= 0x2C1B3C6Du;
+    x ^= x >> 12;
+    x *= 0x297A2D39u;
+    x ^= x >> 15;
+    return (double)x * (2.0 / 4294967296.0) - 1.0;
+}
+
+// z := (T[a..b] - lm I)^-1 z by Gaussian elimination with partial pivoting;
+// the factorisation and the forward elimination share one sweep, the upper
+// factor's three diagonals are kept in u1, u2, u3 for the back substitution.
+// Pivots smaller than pfloor in magnitude are replaced by +-pfloor.
+__device__ void lu_solve(const double* d, const double* e, int a, int b, double lm, double pfloor, double* z,
+                         double* u1, double* u2, double* u3) {
+    double p = d[a] - lm, q = (a < b) ? e[a] : 0.0;
+    for (int k = a; k < b; ++k) {
+        const double sub = e[k], dn = d[k + 1] - lm, en = (k + 1 < b) ? e[k + 1] : 0.0;
+        const double zk = z[k], zk1 = z[k + 1];
+        double np, nq;
+        if (fabs(sub) > fabs(p)) {  // row interchange
+            const double l = p / sub;
+            u1[k] = sub;
+            u2[k] = dn;
+            u3[k] = en;
+            np = q - l * dn;
+            nq = -l * en;
+            z[k] = zk1;
+            z[k + 1] = zk - l * zk1;
+        } else {
+            const double l = (p != 0.0) ? sub / p : 0.0;
+            u1[k] = p;
+            u2[k] = q;
+            u3[k] = 0.0;
+            np = dn - l * q;
+            nq = en;
+            z[k + 1] = zk1 - l * zk;
+        }
+        p = np;
+        q = nq;
     }
+    u1[b] = p;
+    for (int k = b; k >= a; --k) {
+        double piv = u1[k];
+        if (fabs(piv) < pfloor) piv = (piv >= 0.0) ? pfloor : -pfloor;
+        double r = z[k];
+        if (k + 1 <= b) r -= u2[k] * z[k + 1];
+        if (k + 2 <= b) r -= u3[k] * z[k + 2];
+        z[k] = r / piv;
+    }
+}
+
+// z /= ||z||; false when the norm is zero or not finite
+__device__ bool normalize(double* z, int a, int b) {
+    double nn = 0.0;
+    for (int i = a; i <= b; ++i) nn = fma(z[i], z[i], nn);
+    if (!(nn > 0.0) || !isfinite(nn)) return false;
+    const double inv = rsqrt(nn);
+    for (int i = a; i <= b; ++i) z[i] *= inv;
+    return true;
+}
+
+__global__ void __launch_bounds__(TRI_THREADS) vector_kernel(TriArgs g) {
+    extern __shared__ double sh[];
+    const TriItem it = g.items[blockIdx.x];
+    const int n = g.dims[it.block];
+    const long eo = g.eoff[it.block], mo = g.moff[it.block];
+    double* d = sh;
+    double* e = sh + n;
+    double* lam = sh + 2 * n;
+    const double tn = load_tri(g.tri, eo, n, d, e);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) lam[i] = g.lam[eo + i];
     __syncthreads();
-    const double eps = 2.220446049250313e-16;
-    for (int l = 0; l < n; ++l) {
-        int iter = 0;
-        while (true) {
-            if (tid == 0) {
-                int m = l;
-                for (; m < n - 1; ++m) {
-                    double dd = fabs(dg[m]) + fabs(dg[m + 1]);
-                    if (fabs(ed[m]) <= eps * dd) break;
-                }
-                if (m == l) {
-                    s_state = 1;
-                } else if (++iter > QL_MAX_ITER) {
-                    s_state = 2;
-                } else {
-                    double g = (dg[l + 1] - dg[l]) / (2.0 * ed[l]);
-                    double r = hyp(g, 1.0);
-                    g = dg[m] - dg[l] + ed[l] / (g + copysign(r, g));
-                    double s = 1.0, c = 1.0, p = 0.0;
-                    int i = m - 1, nrot = 0;
-                    bool underflow = false;
-                    // one reciprocal square root per rotation keeps the
-                    // dependent chain short (the sweep is sequential);
-                    // d[i+1] of this step is the d[i] loaded one step earlier
-                    double d_hi = dg[m];
-                    for (; i >= l; --i) {
-                        const double ei = ed[i], d_lo = dg[i];
-                        const double f = s * ei, bb = c * ei;
-                        const double r2 = fma(f, f, g * g);
-                        if (r2 == 0.0) {
-                            ed[i + 1] = 0.0;
-                            dg[i + 1] = d_hi - p;
-                            ed[m] = 0.0;
-                            underflow = true;
-                            break;
+    const double ortol = CHAIN_TOL * tn;
+    const double pfloor = (tn > 0.0) ? EPS * tn : 1.0;
+    const int* sa = g.sb + 2 * eo;
+    const int* sbe = sa + n;
+    double* Zb = g.Z + mo;
+    double* Sb = g.S + 3 * mo;
+    for (int j = it.j0 + threadIdx.x; j < it.j1; j += blockDim.x) {
+        const int a = sa[j], b = sbe[j];
+        if (j > a && lam[j] - lam[j - 1] <= ortol) continue;  // not the head of a chain
+        int jend = j;
+        while (jend < b && lam[jend + 1] - lam[jend] <= ortol) ++jend;
+        double prev = -1e308;
+        for (int jj = j; jj <= jend; ++jj) {
+            double lm = lam[jj];
+            const double sep = 10.0 * EPS * fmax(fabs(lm), 1e-3 * tn);
+            if (jj > j && lm < prev + sep) lm = prev + sep;  // distinct shifts inside a chain
+            prev = lm;
+            int rk = 0;
+            for (int i = 0; i < n; ++i) rk += (lam[i] < lam[jj]) || (lam[i] == lam[jj] && i < jj);
+            g.rank[eo + jj] = rk;
+            g.E[eo + rk] = lam[jj];
+            double* z = Zb + (long)rk * n;
+            for (int i = 0; i < a; ++i) z[i] = 0.0;
+            for (int i = b + 1; i < n; ++i) z[i] = 0.0;
+            bool ok = true;
+            if (a == b) {
+                z[a] = 1.0;
+            } else {
+                double* u1 = Sb + (long)3 * jj * n;
+                double* u2 = u1 + n;
+                double* u3 = u2 + n;
+                for (int i = a; i <= b; ++i) z[i] = start_entry(jj, i);
+                const int iters = INV_ITERS + (jj > j ? 1 : 0);
+                for (int t = 0; t < iters && ok; ++t) {
+                    lu_solve(d, e, a, b, lm, pfloor, z, u1, u2, u3);
+                    const int passes = (t == iters - 1) ? 2 : 1;
+                    for (int pass = 0; pass < passes && ok; ++pass) {
+                        for (int pp = jj - 1; pp >= j && lam[jj] - lam[pp] <= ortol; --pp) {
+                            const double* qv = Zb + (long)g.rank[eo + pp] * n;
+                            double dot = 0.0;
+                            for (int i = a; i <= b; ++i) dot = fma(qv[i], z[i], dot);
+                            for (int i = a; i <= b; ++i) z[i] = fma(-dot, qv[i], z[i]);
                         }
-                        const double rinv = rsqrt(r2);
-                        ed[i + 1] = r2 * rinv;
-                        s = f * rinv;
-                        c = g * rinv;
-                        g = d_hi - p;
-                        r = (d_lo - g) * s + 2.0 * c * bb;
-                        p = s * r;
-                        dg[i + 1] = g + p;
-                        g = c * r - bb;
-                        cs[nrot] = c;
-                        sn[nrot] = s;
-                        ++nrot;
-                        d_hi = d_lo;
+                        ok = normalize(z, a, b);
                     }
-                    if (!underflow) {
-                        dg[l] -= p;
-                        ed[l] = g;
-                        ed[m] = 0.0;
-                    }
-                    s_m = m;
-                    s_nrot = nrot;
-                    s_state = 0;
                 }
             }
-            __syncthreads();
-            const int st = s_state;
-            if (st == 2) {
-                if (tid == 0) atomicExch(g.status, PGX_ERR_NUMERIC);
-                return;
-            }
-            if (st == 1) break;
-            const int m = s_m, nrot = s_nrot;
-            // rotations at i = m-1, ..., m-nrot on columns (i, i+1) of each row
-            for (int r = tid; r < nr; r += nt) {
-                double* row = Zs + r * ld;
-                double carry = row[m];
-                for (int q = 0; q < nrot; ++q) {
-                    const double zi = row[m - 1 - q], s = sn[q], c = cs[q];
-                    row[m - q] = s * zi + c * carry;
-                    carry = c * zi - s * carry;
-                }
-                if (nrot > 0) row[m - nrot] = carry;
-            }
-            __syncthreads();
+            if (!ok) atomicExch(g.status, PGX_ERR_NUMERIC);
         }
-    }
-    // ---------------- sort ascending (rank) and write E, U (row-major) ----------------
-    int* rank = reinterpret_cast<int*>(cs);
-    for (int i = tid; i < n; i += nt) {
-        const double di = dg[i];
-        int rk = 0;
-        for (int j = 0; j < n; ++j) {
-            const double dj = dg[j];
-            rk += (dj < di) || (dj == di && j < i);
-        }
-        rank[i] = rk;
-        if (row0 == 0) g.E[eo + rk] = di;
-    }
-    __syncthreads();
-    double* U = g.U + mo;
-    for (long e = tid; e < (long)nr * n; e += nt) {
-        const int r = (int)(e / n), j = (int)(e % n);
-        U[(long)(row0 + r) * n + rank[j]] = Zs[r * ld + j];
     }
 }
 
 }  // namespace
 
-// QL work items of a block list: row slices sized to fill ~200 KB of shared
-// memory per CTA, largest blocks first.  Returns the dynamic shared memory
-// the QL kernel needs.
-static long ql_plan(const std::vector<int>& dims, std::vector<QlItem>& items) {
-    const long cap = 200L * 1024 / sizeof(double);
+static void tri_plan(const std::vector<int>& dims, std::vector<TriItem>& items) {
     std::vector<int> order(dims.size());
     for (size_t b = 0; b < dims.size(); ++b) order[b] = (int)b;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return dims[x] > dims[y]; });
-    long smem_ql = 0;
-    for (int b : order) {
-        const long n = dims[b];
-        const long rows = std::max<long>(1, std::min<long>(n, (cap - 4 * n) / (n + 1)));
-        PGX_CHECK(4 * n + rows * (n + 1) <= cap, PGX_ERR_ARG, "block too large for the QL stage");
-        for (long r0 = 0; r0 < n; r0 += rows) {
-            const int nr = (int)std::min(rows, n - r0);
-            items.push_back(QlItem{b, (int)r0, nr, 0});
-            smem_ql = std::max(smem_ql, (4 * n + (long)nr * (n + 1)) * (long)sizeof(double));
-        }
-    }
-    return smem_ql;
+    for (int b : order)
+        for (int j0 = 0; j0 < dims[b]; j0 += TRI_THREADS)
+            items.push_back(TriItem{b, j0, std::min(dims[b], j0 + TRI_THREADS), 0});
 }
 
-size_t eigh_ql_item_bytes(const std::vector<int>& dims) {
-    std::vector<QlItem> items;
-    ql_plan(dims, items);
-    return items.size() * sizeof(QlItem);
+size_t eigh_item_bytes(const std::vector<int>& dims) {
+    std::vector<TriItem> items;
+    tri_plan(dims, items);
+    return items.size() * sizeof(TriItem);
 }
 
-// Both eigensolver stages on caller-provided device buffers (no allocation).
-// `items_dev` must hold eigh_ql_item_bytes(dims) bytes; the function waits for
-// the stream before returning because the host item list is staged from it.
-void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, cudaStream_t st) {
+size_t eigh_gemm_bytes(const std::vector<int>& dims, size_t* tiles_bytes) {
+    long nt = 0;
+    for (int n : dims) nt += (long)ceil_div(n, GEMM_BM) * ceil_div(n, GEMM_BN);
+    if (tiles_bytes) *tiles_bytes = std::max<long>(nt, 1) * sizeof(GemmTile);
+    return std::max<size_t>(dims.size(), 1) * sizeof(GemmProblem<double, double, double>);
+}
+
+// All eigensolver stages on caller-provided device buffers (no allocation).
+// The function waits for the stream before returning because its host
+// descriptor lists are staged from host memory.
+void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::vector<long>& moff,
+                     cudaStream_t st) {
     int dmax = 1;
     for (int x : dims) dmax = std::max(dmax, x);
     const size_t smem = 4 * sizeof(double) * (size_t)dmax;
@@ -389,30 +477,88 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, cudaStream_
     a.A = d.A;
     a.Zc = d.Zc;
     a.tri = d.tri;
-    eigh_kernel<<<(unsigned)dims.size(), EIGH_THREADS, smem, st>>>(a);
-    check_launch("eigh_kernel");
-    std::vector<QlItem> items;
-    const long smem_ql = ql_plan(dims, items);
-    PGX_CUDA(cudaMemcpyAsync(d.items, items.data(), items.size() * sizeof(QlItem), cudaMemcpyHostToDevice, st));
-    PGX_CUDA(cudaFuncSetAttribute(ql_rows_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_ql));
-    QlArgs q;
-    q.items = static_cast<const QlItem*>(d.items);
-    q.dims = d.dims;
-    q.moff = d.moff;
-    q.eoff = d.eoff;
-    q.Zc = d.Zc;
-    q.tri = d.tri;
-    q.U = d.U;
-    q.E = d.E;
-    q.status = d.status;
-    ql_rows_kernel<<<(unsigned)items.size(), 128, smem_ql, st>>>(q);
-    check_launch("ql_rows_kernel");
-    PGX_CUDA(cudaStreamSynchronize(st));  // the host item list goes out of scope
+    {
+        // LAPACK operation counts: tridiagonalisation 4/3 n^3, forming Q 4/3 n^3;
+        // minimum DRAM traffic: read H, write Q and the tridiagonal
+        double fl = 0.0, by = 0.0;
+        for (int n : dims) {
+            fl += 8.0 / 3.0 * (double)n * n * n;
+            by += 16.0 * n * n + 16.0 * n;
+        }
+        ProfRange pr("eigh_kernel", st, fl, by);
+        eigh_kernel<<<(unsigned)dims.size(), EIGH_THREADS, smem, st>>>(a);
+        check_launch("eigh_kernel");
+    }
+
+    std::vector<TriItem> items;
+    tri_plan(dims, items);
+    PGX_CUDA(cudaMemcpyAsync(d.items, items.data(), items.size() * sizeof(TriItem), cudaMemcpyHostToDevice, st));
+    TriArgs t;
+    t.items = static_cast<const TriItem*>(d.items);
+    t.dims = d.dims;
+    t.moff = d.moff;
+    t.eoff = d.eoff;
+    t.tri = d.tri;
+    t.lam = d.lam;
+    t.sb = d.sb;
+    t.rank = d.rank;
+    t.Z = d.A;   // the Householder workspace is free again
+    t.S = d.S;
+    t.E = d.E;
+    t.status = d.status;
+    const size_t smem_b = 2 * sizeof(double) * (size_t)dmax, smem_v = 3 * sizeof(double) * (size_t)dmax;
+    PGX_CUDA(cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
+    PGX_CUDA(cudaFuncSetAttribute(vector_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_v));
+    double esum = 0.0, msum = 0.0;
+    for (int n : dims) {
+        esum += n;
+        msum += (double)n * n;
+    }
+    {
+        ProfRange pr("bisect_kernel", st, 0.0, 16.0 * esum + 8.0 * esum + 8.0 * esum);
+        bisect_kernel<<<(unsigned)items.size(), TRI_THREADS, smem_b, st>>>(t);
+        check_launch("bisect_kernel");
+    }
+    {
+        ProfRange pr("vector_kernel", st, 0.0, 8.0 * msum + 48.0 * esum);
+        vector_kernel<<<(unsigned)items.size(), TRI_THREADS, smem_v, st>>>(t);
+        check_launch("vector_kernel");
+    }
+
+    // U = Q Z: Q column-major (Zc), Z column-major (A), U row-major
+    std::vector<GemmProblem<double, double, double>> probs;
+    for (size_t b = 0; b < dims.size(); ++b) {
+        const int n = dims[b];
+        GemmProblem<double, double, double> g{};
+        g.A = d.Zc + moff[b];
+        g.B = d.A + moff[b];
+        g.C = d.U + moff[b];
+        g.M = n;
+        g.N = n;
+        g.K = n;
+        g.sa_i = 1;
+        g.sa_k = n;
+        g.sb_k = 1;
+        g.sb_j = n;
+        g.sc_i = n;
+        g.sc_j = 1;
+        probs.push_back(g);
+    }
+    size_t tiles_cap = 0;
+    const size_t probs_cap = eigh_gemm_bytes(dims, &tiles_cap);
+    launch_gemm_batch(probs, d.gemm_probs, probs_cap, d.gemm_tiles, tiles_cap, st);
+    PGX_CUDA(cudaStreamSynchronize(st));  // the host lists go out of scope
 }
 
 void launch_eigh(Problem& P, cudaStream_t st) {
-    P.tri.reserve(2 * std::max<long>(P.esize, 1) * sizeof(double));
-    P.ql_items.reserve(eigh_ql_item_bytes(P.dims));
+    // tri (2 sum d) | lam (sum d) | sb (2 sum d ints) | rank (sum d ints)
+    const long e = std::max<long>(P.esize, 1);
+    P.tri.reserve((2 * e + e) * sizeof(double) + 3 * e * sizeof(int) + 64);
+    P.tri_items.reserve(eigh_item_bytes(P.dims));
+    size_t tiles_b = 0;
+    const size_t probs_b = eigh_gemm_bytes(P.dims, &tiles_b);
+    P.eigh_gemm.reserve(((probs_b + 255) & ~size_t(255)) + tiles_b);
+    P.eigh_scratch.reserve(3 * std::max<long>(P.msize, 1) * sizeof(double));
     EighDev d;
     d.order = P.d_order;
     d.dims = P.d_dims;
@@ -422,11 +568,17 @@ void launch_eigh(Problem& P, cudaStream_t st) {
     d.A = P.d_work;
     d.Zc = P.d_work2;
     d.tri = P.tri.as<double>();
-    d.items = P.ql_items.p;
+    d.lam = d.tri + 2 * e;
+    d.sb = reinterpret_cast<int*>(d.lam + e);
+    d.rank = d.sb + 2 * e;
+    d.S = P.eigh_scratch.as<double>();
+    d.items = P.tri_items.p;
+    d.gemm_probs = P.eigh_gemm.p;
+    d.gemm_tiles = P.eigh_gemm.as<char>() + ((probs_b + 255) & ~size_t(255));
     d.U = P.d_U;
     d.E = P.d_E;
     d.status = P.d_status;
-    launch_eigh_raw(d, P.dims, st);
+    launch_eigh_raw(d, P.dims, P.moff, st);
 }
 
 }  // namespace pgx

@@ -409,6 +409,11 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
         PGX_CUDA(cudaMemcpyAsync(bd.p, dt.data(), dt.size() * sizeof(DTerm), cudaMemcpyHostToDevice, st));
         const long warps = (long)dt.size() * nfreq;
         const int blocks = (int)std::min<long>(ceil_div(warps * 32, 256), 148L * 16);
+        // 24 FP64 operations per (h, k, triple) element: two complex products,
+        // the denominator, its squared modulus, the kernel value, accumulation
+        double elems = 0.0;
+        for (const DTerm& d : dt) elems += (double)d.nh * d.nk * nfreq;
+        ProfRange pr("dterm_kernel", st, 24.0 * elems, 0.0);
         dterm_kernel<<<blocks, 256, 0, st>>>(bd.as<DTerm>(), (int)dt.size(), nfreq, P.beta, pole_res, d_out);
         check_launch("dterm_kernel");
     }

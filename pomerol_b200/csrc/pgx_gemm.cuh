@@ -9,10 +9,12 @@
 // (the signed row gather of a fermionic operator).
 #pragma once
 
+#include <string>
 #include <type_traits>
 #include <vector>
 
 #include "pgx_common.cuh"
+#include "pgx_internal.h"
 
 namespace pgx {
 
@@ -152,6 +154,13 @@ __global__ void __launch_bounds__(GEMM_THREADS)
     }
 }
 
+template <typename T> constexpr const char* type_tag() { return is_cd<T>::value ? "cd" : "double"; }
+template <typename TA, typename TB, typename TC> const char* gemm_name() {
+    static const std::string n =
+        std::string("gemm_tiles_kernel<") + type_tag<TA>() + ", " + type_tag<TB>() + ", " + type_tag<TC>() + ">";
+    return n.c_str();
+}
+
 // Tile class of a problem: 0 = 64x64, 1 = 16x128 (M <= 16), 2 = 128x16 (N <= 16).
 template <typename P> inline int gemm_class(const P& p) {
     if (p.M <= 16 && p.N > 16) return 1;
@@ -187,6 +196,17 @@ void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* 
     PGX_CUDA(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(GemmTile), cudaMemcpyHostToDevice, st));
     const auto* dp = static_cast<const GemmProblem<TA, TB, TC>*>(d_probs);
     const auto* dt = static_cast<const GemmTile*>(d_tiles);
+    // real x real 2, real x complex 4, complex x complex 8 operations per product term;
+    // minimum traffic: A, B and C once (C twice when accumulating)
+    constexpr double mac = (is_cd<TA>::value && is_cd<TB>::value) ? 8.0
+                           : (is_cd<TA>::value || is_cd<TB>::value) ? 4.0 : 2.0;
+    double fl = 0.0, by = 0.0;
+    for (const auto& q : probs) {
+        fl += mac * q.M * (double)q.N * q.K;
+        by += (double)q.M * q.K * sizeof(TA) + (double)q.K * q.N * sizeof(TB) +
+              (q.accumulate ? 2.0 : 1.0) * q.M * (double)q.N * sizeof(TC);
+    }
+    ProfRange pr(gemm_name<TA, TB, TC>(), st, fl, by);
     if (start[1] > start[0]) {
         gemm_tiles_kernel<TA, TB, TC, 64, 64><<<(unsigned)(start[1] - start[0]), GEMM_THREADS, 0, st>>>(dp, dt + start[0]);
         check_launch("gemm_tiles_kernel<64,64>");

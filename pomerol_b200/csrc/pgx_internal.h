@@ -85,7 +85,8 @@ struct Problem {
     double beta = 0.0, E0 = 0.0, Z = 0.0;
     std::vector<int> retained;
 
-    DevBuf H, work, work2, U, E, w, dims_d, moff_d, eoff_d, order_d, status, tri, ql_items;
+    DevBuf H, work, work2, U, E, w, dims_d, moff_d, eoff_d, order_d, status, tri, tri_items, eigh_gemm,
+        eigh_scratch;
     int* d_dims = nullptr;
     long* d_moff = nullptr;
     long* d_eoff = nullptr;
@@ -105,6 +106,48 @@ struct G2Timing {
     double total_ms = 0, gemm_ms = 0, gemm_flops = 0;
 };
 
+// Per-kernel device times of a context, on request (pgx_profile_begin/end):
+// each instrumented launch site brackets its kernel with an event pair on the
+// launching stream and states the kernel's algorithmic FLOPs and DRAM bytes.
+struct KernelStat {
+    std::string name;
+    int launches = 0;
+    double ms = 0, flops = 0, bytes = 0;
+};
+
+struct Profiler {
+    struct Range {
+        std::string name;
+        cudaEvent_t a, b;
+        double flops, bytes;
+    };
+    bool on = false;
+    std::vector<Range> open;
+    std::vector<cudaEvent_t> spare;
+    std::vector<KernelStat> stats;
+    cudaEvent_t event();
+    void clear();
+    void resolve();  // waits for the recorded events and folds them into stats
+    ~Profiler();
+};
+
+// Profiler of the context whose entry point runs on this thread (or null).
+Profiler*& active_profiler();
+
+// Brackets the launches of its scope on stream st when profiling is on.
+class ProfRange {
+  public:
+    ProfRange(const char* name, cudaStream_t st, double flops, double bytes);
+    ~ProfRange();
+    ProfRange(const ProfRange&) = delete;
+    ProfRange& operator=(const ProfRange&) = delete;
+
+  private:
+    Profiler* p_ = nullptr;
+    cudaStream_t st_ = nullptr;
+    size_t idx_ = 0;
+};
+
 }  // namespace pgx
 
 struct pgx_ctx {
@@ -113,6 +156,7 @@ struct pgx_ctx {
     std::string last_error;
     pgx::Problem P;
     pgx::G2Timing g2t;
+    pgx::Profiler prof;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
     // scratch for G2 and Lehmann kernels
     pgx::DevBuf scratch[12];
@@ -129,16 +173,24 @@ struct EighDev {
     const long* moff;
     const long* eoff;
     const double* H;     // packed blocks, row-major
-    double* A;           // workspace, sum d^2
+    double* A;           // workspace, sum d^2 (later the eigenvectors of T)
     double* Zc;          // workspace, sum d^2
-    double* tri;         // workspace, 2 sum d
-    void* items;         // workspace, eigh_ql_item_bytes(dims)
+    double* tri;         // workspace, 2 sum d (diagonal, sub-diagonal)
+    double* lam;         // workspace, sum d
+    int* sb;             // workspace, 2 sum d
+    int* rank;           // workspace, sum d
+    double* S;           // workspace, 3 sum d^2
+    void* items;         // workspace, eigh_item_bytes(dims)
+    void* gemm_probs;    // workspace, eigh_gemm_bytes(dims, ...)
+    void* gemm_tiles;    // workspace, tile bytes from eigh_gemm_bytes
     double* U;           // output, sum d^2
     double* E;           // output, sum d
-    int* status;         // PGX_ERR_NUMERIC on non-convergence
+    int* status;         // PGX_ERR_NUMERIC when a vector is not finite
 };
-size_t eigh_ql_item_bytes(const std::vector<int>& dims);
-void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, cudaStream_t st);
+size_t eigh_item_bytes(const std::vector<int>& dims);
+size_t eigh_gemm_bytes(const std::vector<int>& dims, size_t* tiles_bytes);
+void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::vector<long>& moff,
+                     cudaStream_t st);
 void launch_weights(Problem& P, double beta, cudaStream_t st);
 void rotate_operator(Problem& P, Operator& op, cudaStream_t st);
 void adjoint_operator(Problem& P, const Operator& src, Operator& dst, cudaStream_t st);

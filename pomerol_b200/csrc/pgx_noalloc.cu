@@ -7,9 +7,11 @@
 // block on buffers the caller passes in, and keeps its own workspace in the
 // file-scope array below instead of allocating.
 //
-// The array holds the Householder workspace, the accumulated factor, the
-// tridiagonal and the small descriptors of one block of at most
-// PGX_NOALLOC_MAX_DIM states (about 1 MiB).  Every GPU that loads this
+// The array holds the Householder workspace (reused for the eigenvectors of
+// the tridiagonal), the accumulated factor, the inverse-iteration scratch,
+// the tridiagonal with its eigenvalues and index arrays, and the small
+// descriptor lists of one block of at most PGX_NOALLOC_MAX_DIM states
+// (about 2.5 MiB).  Every GPU that loads this
 // library holds it until the process exits.  All calls on a device share it
 // and it keeps the last call's contents: calls whose work overlaps on the GPU
 // (different streams, or host threads racing) corrupt each other and must be
@@ -28,12 +30,19 @@
 namespace {
 
 constexpr long NA_N = PGX_NOALLOC_MAX_DIM;
-// layout in doubles: A (n^2) | Zc (n^2) | tri (2n) | QL items (32 doubles) | descriptors (8 doubles)
+// layout in doubles:
+//   A (n^2) | Zc (n^2) | S (3 n^2) | tri (2n) | lam (n) | sb, rank (3n ints = 2n doubles)
+//   | bisection items (32) | GEMM problem (32) | GEMM tiles (64) | descriptors (8)
 constexpr long NA_A = 0;
 constexpr long NA_ZC = NA_A + NA_N * NA_N;
-constexpr long NA_TRI = NA_ZC + NA_N * NA_N;
-constexpr long NA_ITEMS = NA_TRI + 2 * NA_N;
-constexpr long NA_META = NA_ITEMS + 32;
+constexpr long NA_S = NA_ZC + NA_N * NA_N;
+constexpr long NA_TRI = NA_S + 3 * NA_N * NA_N;
+constexpr long NA_LAM = NA_TRI + 2 * NA_N;
+constexpr long NA_INT = NA_LAM + NA_N;
+constexpr long NA_ITEMS = NA_INT + 2 * NA_N;
+constexpr long NA_GPROB = NA_ITEMS + 32;
+constexpr long NA_GTILE = NA_GPROB + 32;
+constexpr long NA_META = NA_GTILE + 64;
 constexpr long NA_TOTAL = NA_META + 8;
 
 static __device__ __align__(256) double g_noalloc_scratch[NA_TOTAL];
@@ -85,7 +94,10 @@ extern "C" int pgx_eigh_noalloc(const double* H, int32_t n, double* E, double* U
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     try {
         const std::vector<int> dims{n};
-        PGX_CHECK(pgx::eigh_ql_item_bytes(dims) <= 32 * sizeof(double), PGX_ERR_ARG, "QL item list too long");
+        size_t tile_bytes = 0;
+        PGX_CHECK(pgx::eigh_item_bytes(dims) <= 32 * sizeof(double), PGX_ERR_ARG, "item list too long");
+        PGX_CHECK(pgx::eigh_gemm_bytes(dims, &tile_bytes) <= 32 * sizeof(double) && tile_bytes <= 64 * sizeof(double),
+                  PGX_ERR_ARG, "GEMM lists too long");
         NaMeta* meta = reinterpret_cast<NaMeta*>(base + NA_META);
         const NaMeta h{0, n, 0, 0, 0, 0};
         PGX_CUDA(cudaMemcpyAsync(meta, &h, sizeof(h), cudaMemcpyHostToDevice, st));
@@ -98,11 +110,17 @@ extern "C" int pgx_eigh_noalloc(const double* H, int32_t n, double* E, double* U
         d.A = base + NA_A;
         d.Zc = base + NA_ZC;
         d.tri = base + NA_TRI;
+        d.lam = base + NA_LAM;
+        d.sb = reinterpret_cast<int*>(base + NA_INT);
+        d.rank = d.sb + 2 * n;
+        d.S = base + NA_S;
         d.items = base + NA_ITEMS;
+        d.gemm_probs = base + NA_GPROB;
+        d.gemm_tiles = base + NA_GTILE;
         d.U = U;
         d.E = E;
         d.status = &meta->status;
-        pgx::launch_eigh_raw(d, dims, st);  // waits for the stream
+        pgx::launch_eigh_raw(d, dims, {0L}, st);  // waits for the stream
         int status = 0;
         PGX_CUDA(cudaMemcpyAsync(&status, &meta->status, sizeof(int), cudaMemcpyDeviceToHost, st));
         PGX_CUDA(cudaStreamSynchronize(st));

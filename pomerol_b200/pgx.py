@@ -22,7 +22,7 @@ EXPORTS = [
     "pgx_eigh", "pgx_get_eigensystem", "pgx_ground_energy", "pgx_weights", "pgx_truncate_blocks",
     "pgx_op_define", "pgx_op_rotate", "pgx_op_adjoint", "pgx_op_info", "pgx_op_read", "pgx_gf", "pgx_susc",
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
-    "pgx_launch_count", "pgx_eigh_noalloc",
+    "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
 ]
 
 
@@ -72,6 +72,9 @@ def load():
         lib.pgx_timer_end.argtypes = [P, P]
         lib.pgx_launch_count.restype = C.c_longlong
         lib.pgx_eigh_noalloc.argtypes = [P, I32, P, P, P]
+        lib.pgx_profile_begin.argtypes = [P]
+        lib.pgx_profile_end.argtypes = [P, P]
+        lib.pgx_profile_kernel.argtypes = [P, I32, C.c_char_p, I32, P, P, P, P]
         _lib = lib
     return _lib
 
@@ -263,5 +266,29 @@ def _timer_end(self):
     return float(ms[0])
 
 
+def _profile_begin(self):
+    """Start recording per-kernel device times (CUDA event pairs on the
+    context's stream) for the instrumented kernels."""
+    self._ck(self.lib.pgx_profile_begin(self.h))
+
+
+def _profile_end(self):
+    """Stop recording; per kernel name: launches, total ms, algorithmic
+    FLOPs and DRAM bytes summed over the launches (largest time first)."""
+    n = np.zeros(1, dtype=np.int32)
+    self._ck(self.lib.pgx_profile_end(self.h, _p(n)))
+    out = []
+    for i in range(int(n[0])):
+        name = C.create_string_buffer(128)
+        nl = np.zeros(1, dtype=np.int32)
+        v = np.zeros(3)
+        self._ck(self.lib.pgx_profile_kernel(self.h, i, name, 128, _p(nl), _p(v[0:1]), _p(v[1:2]), _p(v[2:3])))
+        out.append({"name": name.value.decode(), "launches": int(nl[0]), "ms": float(v[0]),
+                    "flops": float(v[1]), "bytes": float(v[2])})
+    return out
+
+
 Engine.timer_begin = _timer_begin
 Engine.timer_end = _timer_end
+Engine.profile_begin = _profile_begin
+Engine.profile_end = _profile_end
