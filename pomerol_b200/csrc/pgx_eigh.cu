@@ -2,19 +2,24 @@
 //
 // Replaces Eigen::SelfAdjointEigenSolver as called by HamiltonianPart::computeImpl
 // (HamiltonianPart.cpp:90-102).  Stages:
-//   1. eigh_kernel, one CTA per block: Householder reduction to tridiagonal
-//      form T and explicit accumulation of the orthogonal factor Q
-//      (Golub & Van Loan, "Matrix Computations", 4th ed., 8.3.1).  The
-//      symmetric mat-vec and the rank-2 update run over all threads with
-//      coalesced column access; Q is stored column-major.
+//   1. Householder reduction to tridiagonal form T and explicit accumulation
+//      of the orthogonal factor Q (Golub & Van Loan, "Matrix Computations",
+//      4th ed., 8.3.1):
+//      eigh_cluster_kernel, one thread-block cluster of 1-8 CTAs per block
+//      with the matrix in distributed shared memory (blocks up to 464 states);
+//      eigh_kernel, one CTA per block with the matrix in global memory
+//      (larger blocks).  Q is stored column-major.
 //   2. bisect_kernel, one thread per eigenvalue: bisection with Sturm counts
 //      on the unreduced pieces of T (8.4.1).
-//   3. vector_kernel, one thread per cluster of close eigenvalues: twisted
-//      factorisation for the eigenvectors of T, inverse iteration with
-//      modified Gram-Schmidt inside a cluster; eigenvalues are ranked so that
-//      the output is ascending.
+//   3. vector_kernel, one thread per chain of close eigenvalues: inverse
+//      iteration with a partial-pivoting tridiagonal LU, modified Gram-Schmidt
+//      inside a chain; eigenvalues are ranked so that the output is ascending.
 //   4. U = Q Z as one batched FP64 GEMM over all blocks.
 // A non-finite eigenvector sets a device status word instead of trapping.
+
+#include <cooperative_groups.h>
+
+#include <cstring>
 
 #include "pgx_common.cuh"
 #include "pgx_gemm.cuh"
@@ -181,6 +186,174 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
     for (int i = tid; i < n; i += nt) {
         g.tri[2 * eo + i] = dg[i];
         g.tri[2 * eo + n + i] = ed[i];
+    }
+}
+
+// ----------------------------------------------------------------------------
+// Householder stage on a thread-block cluster (blocks whose matrix fits in
+// the shared memory of up to 8 CTAs: 464 states at 220 KB per CTA).
+//
+// The C CTAs of a cluster hold the block's symmetric matrix in distributed
+// shared memory, row r in CTA r mod C (cyclic, so the shrinking trailing
+// matrix stays spread over all CTAs).  Step k of the reduction:
+//   (A) cluster barrier; every CTA reads row k (= the column below the
+//       diagonal) from its owner and forms the Householder vector v, tau;
+//   each CTA computes p = tau B v on its own rows and its share of v.p;
+//   (B) cluster barrier; every CTA gathers all of p and the v.p shares,
+//       forms w = p - (tau/2)(v.p) v and applies B -= v w^T + w v^T to its
+//       own rows.
+// CTA 0 stores d_k, e_k and sqrt(tau) v (row k of V in global memory).
+// Q = H_0 ... H_{n-3} is then formed from V with the CTAs owning columns
+// j = c (mod C) of Q: a column's update needs only that column, so this
+// phase has no cross-CTA traffic.  The outputs (tridiagonal, column-major Q)
+// are those of eigh_kernel.
+constexpr int CL_THREADS = 512;
+constexpr int CL_MAX_DIM = CL_THREADS + 1;  // the prefetch of a reflector uses one element per thread
+
+struct ClusterArgs {
+    const int* blocks;  // cluster -> block
+    const int* dims;
+    const long* moff;
+    const long* eoff;
+    const double* H;
+    double* V;          // per block n x n: row k holds sqrt(tau_k) v_k in columns k+1..n-1
+    double* Zc;         // per block: Q column-major
+    double* tri;
+};
+
+__host__ __device__ inline size_t cluster_smem_doubles(int n, int C) {
+    const int R = (n + C - 1) / C;
+    return (size_t)R * n + 2 * (size_t)n + R + 2;
+}
+
+__global__ void __launch_bounds__(CL_THREADS) eigh_cluster_kernel(ClusterArgs g) {
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ double sh[];
+    __shared__ double red[32];
+    const int C = (int)cl.num_blocks();
+    const int c = (int)cl.block_rank();
+    const int b = g.blocks[blockIdx.x / C];
+    const int n = g.dims[b];
+    const long mo = g.moff[b], eo = g.eoff[b];
+    const int R = (n + C - 1) / C;
+    const int nrows = (n - c + C - 1) / C;  // rows (and later columns) c, c + C, ...
+    double* slab = sh;                      // R x n rows | later R x n columns of Q
+    double* v = sh + (size_t)R * n;         // n
+    double* w = v + n;                      // n
+    double* p = w + n;                      // R
+    double* dslot = p + R;                  // 1
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+    const double* Hb = g.H + mo;
+    double* V = g.V + mo;
+
+    for (long idx = tid; idx < (long)nrows * n; idx += nt) {
+        const int lr = (int)(idx / n), j = (int)(idx % n);
+        slab[idx] = Hb[(long)(c + C * lr) * n + j];
+    }
+    for (int k = 0; k + 2 < n; ++k) {
+        const int m = n - k - 1;
+        cl.sync();  // (A) row k is final; the p slots of the previous step are free
+        const double* rowk = cl.map_shared_rank(slab, k % C) + (size_t)(k / C) * n;
+        double part = 0.0;
+        for (int i = tid; i < m; i += nt) {
+            const double x = rowk[k + 1 + i];
+            v[i] = x;
+            if (i > 0) part += x * x;
+        }
+        const double sigma = block_sum(part, red);
+        const double x0 = v[0];
+        const double dk = rowk[k];
+        double tau = 0.0, alpha = x0, v0 = x0;
+        if (sigma != 0.0) {
+            const double mu = sqrt(x0 * x0 + sigma);
+            alpha = (x0 > 0.0) ? -mu : mu;  // v0 = x0 - alpha without cancellation
+            v0 = x0 - alpha;
+            tau = 2.0 / (sigma + v0 * v0);
+        }
+        __syncthreads();
+        if (tid == 0) v[0] = v0;
+        __syncthreads();
+        // p = tau B v on own rows r >= k+1 (one warp per row)
+        const int lr0 = (k + 1 - c + C - 1) / C;
+        double dpart = 0.0;
+        for (int lr = lr0 + wid; lr < nrows; lr += nw) {
+            const double* row = slab + (size_t)lr * n + (k + 1);
+            double s = 0.0;
+            for (int j = lane; j < m; j += 32) s = fma(row[j], v[j], s);
+            s = warp_sum(s) * tau;
+            if (lane == 0) {
+                p[lr] = s;
+                dpart += v[c + C * lr - (k + 1)] * s;
+            }
+        }
+        const double dsum = block_sum(dpart, red);
+        if (tid == 0) dslot[0] = dsum;
+        cl.sync();  // (B) p and the v.p shares of every CTA are complete
+        double dtot = 0.0;
+        for (int q = 0; q < C; ++q) dtot += cl.map_shared_rank(dslot, q)[0];
+        const double K = 0.5 * tau * dtot;
+        for (int i = tid; i < m; i += nt) {
+            const int r = k + 1 + i;
+            w[i] = cl.map_shared_rank(p, r % C)[r / C] - K * v[i];
+        }
+        __syncthreads();
+        for (int lr = lr0 + wid; lr < nrows; lr += nw) {
+            double* row = slab + (size_t)lr * n + (k + 1);
+            const int i = c + C * lr - (k + 1);
+            const double vi = v[i], wi = w[i];
+            for (int j = lane; j < m; j += 32) row[j] -= vi * w[j] + wi * v[j];
+        }
+        if (c == 0) {
+            if (tid == 0) {
+                g.tri[2 * eo + k] = dk;
+                g.tri[2 * eo + n + k] = alpha;
+            }
+            const double st = sqrt(tau);
+            for (int i = tid; i < m; i += nt) V[(size_t)k * n + k + 1 + i] = v[i] * st;
+        }
+    }
+    cl.sync();
+    if (c == 0 && tid == 0) {
+        auto elem = [&](int r, int j) { return cl.map_shared_rank(slab, r % C)[(size_t)(r / C) * n + j]; };
+        if (n >= 2) {
+            g.tri[2 * eo + n - 2] = elem(n - 2, n - 2);
+            g.tri[2 * eo + n + n - 2] = elem(n - 1, n - 2);
+        }
+        g.tri[2 * eo + n - 1] = elem(n - 1, n - 1);
+        g.tri[2 * eo + n + n - 1] = 0.0;
+    }
+    __threadfence();
+    cl.sync();  // V is visible to every CTA; no CTA reads another's shared memory after this point
+
+    // ---- Q = H_0 ... H_{n-3}, columns j = c + C t of Q in shared memory (column-major)
+    double* Qs = slab;
+    double* u = v;
+    for (long idx = tid; idx < (long)nrows * n; idx += nt) {
+        const int t = (int)(idx / n), i = (int)(idx % n);
+        Qs[idx] = (i == c + C * t) ? 1.0 : 0.0;
+    }
+    double pre = 0.0;
+    if (n >= 3 && tid < 2) pre = V[(size_t)(n - 3) * n + (n - 2) + tid];
+    for (int k = n - 3; k >= 0; --k) {
+        const int m = n - k - 1;
+        __syncthreads();  // the previous reflector is no longer read
+        if (tid < m) u[tid] = pre;
+        __syncthreads();
+        if (k >= 1 && tid < m + 1) pre = V[(size_t)(k - 1) * n + k + tid];
+        const int t0 = (k + 1 - c + C - 1) / C;
+        for (int t = t0 + wid; t < nrows; t += nw) {
+            double* col = Qs + (size_t)t * n + (k + 1);
+            double s = 0.0;
+            for (int i = lane; i < m; i += 32) s = fma(u[i], col[i], s);
+            s = warp_sum(s);
+            for (int i = lane; i < m; i += 32) col[i] -= u[i] * s;
+        }
+    }
+    __syncthreads();
+    for (long idx = tid; idx < (long)nrows * n; idx += nt) {
+        const int t = (int)(idx / n), i = (int)(idx % n);
+        g.Zc[mo + (long)(c + C * t) * n + i] = Qs[idx];
     }
 }
 
@@ -445,10 +618,38 @@ static void tri_plan(const std::vector<int>& dims, std::vector<TriItem>& items) 
             items.push_back(TriItem{b, j0, std::min(dims[b], j0 + TRI_THREADS), 0});
 }
 
+constexpr int CL_SIZES[4] = {1, 2, 4, 8};
+constexpr size_t CL_SMEM_MAX = 220 * 1024;
+
+// Householder stage plan: the block list of each cluster size (largest
+// blocks first) and the blocks left to the single-CTA global-memory kernel.
+struct HhPlan {
+    std::vector<int> cls[4];
+    std::vector<int> global;
+};
+
+static HhPlan hh_plan(const std::vector<int>& dims) {
+    std::vector<int> order(dims.size());
+    for (size_t b = 0; b < dims.size(); ++b) order[b] = (int)b;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return dims[x] > dims[y]; });
+    HhPlan h;
+    for (int b : order) {
+        const int n = dims[b];
+        int q = -1;
+        if (n <= CL_MAX_DIM)
+            for (int i = 0; i < 4 && q < 0; ++i)
+                if (cluster_smem_doubles(n, CL_SIZES[i]) * sizeof(double) <= CL_SMEM_MAX) q = i;
+        if (q < 0) h.global.push_back(b);
+        else h.cls[q].push_back(b);
+    }
+    return h;
+}
+
+// descriptor bytes: bisection items, then one int per block (Householder lists)
 size_t eigh_item_bytes(const std::vector<int>& dims) {
     std::vector<TriItem> items;
     tri_plan(dims, items);
-    return items.size() * sizeof(TriItem);
+    return items.size() * sizeof(TriItem) + dims.size() * sizeof(int);
 }
 
 size_t eigh_gemm_bytes(const std::vector<int>& dims, size_t* tiles_bytes) {
@@ -465,34 +666,109 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
                      cudaStream_t st) {
     int dmax = 1;
     for (int x : dims) dmax = std::max(dmax, x);
-    const size_t smem = 4 * sizeof(double) * (size_t)dmax;
-    PGX_CHECK(smem <= 200 * 1024, PGX_ERR_ARG, "block too large for the single-CTA eigensolver (d > 6400)");
-    PGX_CUDA(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    EighArgs a;
-    a.order = d.order;
-    a.dims = d.dims;
-    a.moff = d.moff;
-    a.eoff = d.eoff;
-    a.H = d.H;
-    a.A = d.A;
-    a.Zc = d.Zc;
-    a.tri = d.tri;
-    {
-        // LAPACK operation counts: tridiagonalisation 4/3 n^3, forming Q 4/3 n^3;
-        // minimum DRAM traffic: read H, write Q and the tridiagonal
-        double fl = 0.0, by = 0.0;
-        for (int n : dims) {
-            fl += 8.0 / 3.0 * (double)n * n * n;
-            by += 16.0 * n * n + 16.0 * n;
-        }
-        ProfRange pr("eigh_kernel", st, fl, by);
-        eigh_kernel<<<(unsigned)dims.size(), EIGH_THREADS, smem, st>>>(a);
-        check_launch("eigh_kernel");
-    }
-
+    // descriptors: bisection items and the Householder block lists, one upload
     std::vector<TriItem> items;
     tri_plan(dims, items);
-    PGX_CUDA(cudaMemcpyAsync(d.items, items.data(), items.size() * sizeof(TriItem), cudaMemcpyHostToDevice, st));
+    HhPlan hp = hh_plan(dims);
+    // a cluster size the device cannot schedule falls back to the global-memory kernel
+    ClusterArgs ca;
+    ca.dims = d.dims;
+    ca.moff = d.moff;
+    ca.eoff = d.eoff;
+    ca.H = d.H;
+    ca.V = d.A;
+    ca.Zc = d.Zc;
+    ca.tri = d.tri;
+    size_t cl_smem[4] = {0, 0, 0, 0};
+    for (int q = 0; q < 4; ++q) {
+        if (hp.cls[q].empty()) continue;
+        for (int b : hp.cls[q]) cl_smem[q] = std::max(cl_smem[q], cluster_smem_doubles(dims[b], CL_SIZES[q]) * sizeof(double));
+        PGX_CUDA(cudaFuncSetAttribute(eigh_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CL_SMEM_MAX));
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CL_SIZES[q];
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3((unsigned)CL_SIZES[q]);
+        cfg.blockDim = dim3(CL_THREADS);
+        cfg.dynamicSmemBytes = cl_smem[q];
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (cudaOccupancyMaxActiveClusters(&nclusters, eigh_cluster_kernel, &cfg) != cudaSuccess || nclusters < 1) {
+            cudaGetLastError();
+            hp.global.insert(hp.global.end(), hp.cls[q].begin(), hp.cls[q].end());
+            hp.cls[q].clear();
+        }
+    }
+    std::vector<int> lists(hp.global);
+    size_t cl_off[4];
+    for (int q = 0; q < 4; ++q) {
+        cl_off[q] = lists.size();
+        lists.insert(lists.end(), hp.cls[q].begin(), hp.cls[q].end());
+    }
+    std::vector<char> host(items.size() * sizeof(TriItem) + lists.size() * sizeof(int));
+    std::memcpy(host.data(), items.data(), items.size() * sizeof(TriItem));
+    std::memcpy(host.data() + items.size() * sizeof(TriItem), lists.data(), lists.size() * sizeof(int));
+    PGX_CUDA(cudaMemcpyAsync(d.items, host.data(), host.size(), cudaMemcpyHostToDevice, st));
+    const int* d_lists = reinterpret_cast<const int*>(static_cast<const char*>(d.items) + items.size() * sizeof(TriItem));
+
+    // LAPACK operation counts: tridiagonalisation 4/3 n^3, forming Q 4/3 n^3;
+    // minimum DRAM traffic: read H, write Q and the tridiagonal
+    auto hh_work = [&](const std::vector<int>& bl, double& fl, double& by) {
+        fl = by = 0.0;
+        for (int b : bl) {
+            const double n = dims[b];
+            fl += 8.0 / 3.0 * n * n * n;
+            by += 16.0 * n * n + 16.0 * n;
+        }
+    };
+    if (!hp.global.empty()) {
+        int gmax = 1;
+        for (int b : hp.global) gmax = std::max(gmax, dims[b]);
+        const size_t smem = 4 * sizeof(double) * (size_t)gmax;
+        PGX_CHECK(smem <= 200 * 1024, PGX_ERR_ARG, "block too large for the single-CTA eigensolver (d > 6400)");
+        PGX_CUDA(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        EighArgs a;
+        a.order = d_lists;
+        a.dims = d.dims;
+        a.moff = d.moff;
+        a.eoff = d.eoff;
+        a.H = d.H;
+        a.A = d.A;
+        a.Zc = d.Zc;
+        a.tri = d.tri;
+        double fl, by;
+        hh_work(hp.global, fl, by);
+        ProfRange pr("eigh_kernel", st, fl, by);
+        eigh_kernel<<<(unsigned)hp.global.size(), EIGH_THREADS, smem, st>>>(a);
+        check_launch("eigh_kernel");
+    }
+    for (int q = 0; q < 4; ++q) {
+        if (hp.cls[q].empty()) continue;
+        ca.blocks = d_lists + cl_off[q];
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CL_SIZES[q];
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3((unsigned)(hp.cls[q].size() * CL_SIZES[q]));
+        cfg.blockDim = dim3(CL_THREADS);
+        cfg.dynamicSmemBytes = cl_smem[q];
+        cfg.stream = st;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        double fl, by;
+        hh_work(hp.cls[q], fl, by);
+        static const char* names[4] = {"eigh_cluster_kernel<1>", "eigh_cluster_kernel<2>", "eigh_cluster_kernel<4>",
+                                       "eigh_cluster_kernel<8>"};
+        ProfRange pr(names[q], st, fl, by);
+        PGX_CUDA(cudaLaunchKernelEx(&cfg, eigh_cluster_kernel, ca));
+        check_launch("eigh_cluster_kernel");
+    }
+
     TriArgs t;
     t.items = static_cast<const TriItem*>(d.items);
     t.dims = d.dims;
@@ -560,7 +836,6 @@ void launch_eigh(Problem& P, cudaStream_t st) {
     P.eigh_gemm.reserve(((probs_b + 255) & ~size_t(255)) + tiles_b);
     P.eigh_scratch.reserve(3 * std::max<long>(P.msize, 1) * sizeof(double));
     EighDev d;
-    d.order = P.d_order;
     d.dims = P.d_dims;
     d.moff = P.d_moff;
     d.eoff = P.d_eoff;

@@ -168,7 +168,6 @@ void launch_eigh(Problem& P, cudaStream_t st);
 
 // Device buffers of one eigensolve (any number of blocks), all caller-owned.
 struct EighDev {
-    const int* order;    // CTA -> block, largest first
     const int* dims;
     const long* moff;
     const long* eoff;

@@ -102,7 +102,6 @@ extern "C" int pgx_eigh_noalloc(const double* H, int32_t n, double* E, double* U
         const NaMeta h{0, n, 0, 0, 0, 0};
         PGX_CUDA(cudaMemcpyAsync(meta, &h, sizeof(h), cudaMemcpyHostToDevice, st));
         pgx::EighDev d;
-        d.order = &meta->order;
         d.dims = &meta->dims;
         d.moff = &meta->moff;
         d.eoff = &meta->eoff;

@@ -13,6 +13,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", default="a5")
     ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--kernels", action="store_true", help="per-kernel event times of the last step")
     a = ap.parse_args()
     import torch  # noqa: F401  (CUDA context for the process)
     from .workloads import EngineRun, Problem, matsubara_cube
@@ -21,9 +22,16 @@ def main():
     run = EngineRun(prob)
     for s in range(a.steps):
         t0 = time.perf_counter()
+        last = a.kernels and s == a.steps - 1
+        if last:
+            run.eng.profile_begin()
         run.eng.timer_begin()
         v = run.step(z)
         ms = run.eng.timer_end()
+        if last:
+            for k in run.eng.profile_end():
+                print(f"  {k['name']:40s} x{k['launches']:<3d} {k['ms']:9.3f} ms  "
+                      f"{k['flops'] / max(k['ms'], 1e-9) / 1e9:9.3f} TFLOP/s  {k['bytes'] / max(k['ms'], 1e-9) / 1e6:9.2f} GB/s")
         print(f"step {s}: device {ms:.1f} ms, wall {1e3 * (time.perf_counter() - t0):.1f} ms, "
               f"g2 {run.eng.g2_timing()}, |v|max {np.abs(v).max():.4e}", flush=True)
 

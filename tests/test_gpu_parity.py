@@ -75,6 +75,41 @@ def test_eigh_larger_blocks(harness):
         assert np.abs(e - np.linalg.eigvalsh(h)).max() < 1e-11 * scale
 
 
+def test_eigh_every_householder_class():
+    """One eigensolve whose blocks reach every Householder launch: thread-block
+    clusters of 1, 2, 4 and 8 CTAs (blocks whose matrix fits in 8 x 220 KB of
+    distributed shared memory, up to 464 states) and the single-CTA
+    global-memory kernel (larger blocks).
+    Spectra: random, tightly clustered (1e-9 spacings), two-level degenerate."""
+    rng = np.random.default_rng(11)
+    dims = [150, 200, 256, 300, 401, 464, 465, 514, 640]
+    blocks = []
+    for i, d in enumerate(dims):
+        q, _ = np.linalg.qr(rng.standard_normal((d, d)))
+        if i % 3 == 0:
+            a = rng.standard_normal((d, d))
+            h = (a + a.T) / 2
+        elif i % 3 == 1:
+            ev = np.r_[np.arange(d - 4) * 1e-9, [1.0, 2.0, 3.0, 4.0]]
+            h = (q * ev) @ q.T
+        else:
+            ev = np.r_[np.zeros(d // 2), np.ones(d - d // 2)]
+            h = (q * ev) @ q.T
+        blocks.append((h + h.T) / 2)
+    from pomerol_b200.pgx import Engine
+    eng = Engine()
+    eng.set_blocks(dims)
+    eng.set_hamiltonian(blocks)
+    eng.eigh()
+    E, U = eng.eigensystem()
+    for h, e, u in zip(blocks, E, U):
+        scale = max(1.0, np.abs(e).max())
+        assert np.all(np.diff(e) >= 0)
+        assert np.abs(h @ u - u * e[None, :]).max() < 1e-10 * scale
+        assert np.abs(u.T @ u - np.eye(len(e))).max() < 1e-11
+        assert np.abs(e - np.linalg.eigvalsh(h)).max() < 1e-11 * scale
+
+
 def test_hamiltonian_ground_energy(harness):
     e = M.CoulombS("A", 1.0, -0.5) + M.CoulombS("B", 2.0, -1.0) + M.Hopping("A", "B", -1.0)
     g = harness(M.make_model(e), 10.0)
