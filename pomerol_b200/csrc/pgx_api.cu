@@ -159,6 +159,11 @@ int pgx_destroy(pgx_ctx* c) {
     for (auto& b : c->scratch) b.release();
     if (c->ev_begin) cudaEventDestroy(c->ev_begin);
     if (c->ev_end) cudaEventDestroy(c->ev_end);
+    for (int i = 0; i < 3; ++i) {
+        if (c->aux[i]) cudaStreamDestroy(c->aux[i]);
+        if (c->join[i]) cudaEventDestroy(c->join[i]);
+    }
+    if (c->fork) cudaEventDestroy(c->fork);
     cudaStreamDestroy(c->stream);
     delete c;
     return PGX_OK;
@@ -242,7 +247,7 @@ int pgx_eigh(pgx_ctx* c) {
         PGX_CHECK(P.have_H, PGX_ERR_STATE, "pgx_set_hamiltonian first");
         PGX_CHECK(!P.is_complex, PGX_ERR_ARG, "complex Hermitian blocks are not supported by this build");
         PGX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int), c->stream));
-        pgx::launch_eigh(P, c->stream);
+        pgx::launch_eigh(c);
         int st = 0;
         PGX_CUDA(cudaMemcpyAsync(&st, P.d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
         PGX_CUDA(cudaStreamSynchronize(c->stream));

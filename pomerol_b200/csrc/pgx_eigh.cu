@@ -724,6 +724,13 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
             by += 16.0 * n * n + 16.0 * n;
         }
     };
+    // the launches are independent: with side streams, cluster class q > 0 runs
+    // on aux[q - 1] while the main stream runs the global-memory kernel and class 0
+    const bool fork = d.aux[0] && d.aux[1] && d.aux[2] && d.fork;
+    if (fork) {
+        PGX_CUDA(cudaEventRecord(d.fork, st));
+        for (int i = 0; i < 3; ++i) PGX_CUDA(cudaStreamWaitEvent(d.aux[i], d.fork, 0));
+    }
     if (!hp.global.empty()) {
         int gmax = 1;
         for (int b : hp.global) gmax = std::max(gmax, dims[b]);
@@ -747,6 +754,7 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     }
     for (int q = 0; q < 4; ++q) {
         if (hp.cls[q].empty()) continue;
+        const cudaStream_t sq = (fork && q > 0) ? d.aux[q - 1] : st;
         ca.blocks = d_lists + cl_off[q];
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute attr[1];
@@ -757,16 +765,22 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
         cfg.gridDim = dim3((unsigned)(hp.cls[q].size() * CL_SIZES[q]));
         cfg.blockDim = dim3(CL_THREADS);
         cfg.dynamicSmemBytes = cl_smem[q];
-        cfg.stream = st;
+        cfg.stream = sq;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         double fl, by;
         hh_work(hp.cls[q], fl, by);
         static const char* names[4] = {"eigh_cluster_kernel<1>", "eigh_cluster_kernel<2>", "eigh_cluster_kernel<4>",
                                        "eigh_cluster_kernel<8>"};
-        ProfRange pr(names[q], st, fl, by);
+        ProfRange pr(names[q], sq, fl, by);
         PGX_CUDA(cudaLaunchKernelEx(&cfg, eigh_cluster_kernel, ca));
         check_launch("eigh_cluster_kernel");
+    }
+    if (fork) {
+        for (int i = 0; i < 3; ++i) {
+            PGX_CUDA(cudaEventRecord(d.join[i], d.aux[i]));
+            PGX_CUDA(cudaStreamWaitEvent(st, d.join[i], 0));
+        }
     }
 
     TriArgs t;
@@ -826,7 +840,16 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     PGX_CUDA(cudaStreamSynchronize(st));  // the host lists go out of scope
 }
 
-void launch_eigh(Problem& P, cudaStream_t st) {
+void launch_eigh(pgx_ctx* c) {
+    Problem& P = c->P;
+    cudaStream_t st = c->stream;
+    if (!c->fork) {
+        PGX_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+        for (int i = 0; i < 3; ++i) {
+            PGX_CUDA(cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking));
+            PGX_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
+        }
+    }
     // tri (2 sum d) | lam (sum d) | sb (2 sum d ints) | rank (sum d ints)
     const long e = std::max<long>(P.esize, 1);
     P.tri.reserve((2 * e + e) * sizeof(double) + 3 * e * sizeof(int) + 64);
@@ -853,6 +876,11 @@ void launch_eigh(Problem& P, cudaStream_t st) {
     d.U = P.d_U;
     d.E = P.d_E;
     d.status = P.d_status;
+    for (int i = 0; i < 3; ++i) {
+        d.aux[i] = c->aux[i];
+        d.join[i] = c->join[i];
+    }
+    d.fork = c->fork;
     launch_eigh_raw(d, P.dims, P.moff, st);
 }
 

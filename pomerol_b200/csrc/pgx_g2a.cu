@@ -68,9 +68,12 @@ struct DTerm {
     long b1, b3, bh, bk;
     const double *Ek, *Eh, *wh;
     const int* hot;       // anchor states (inner indices) of the anchor block
-    const int* ti1;       // per triple: index of z1 in the plan
-    const int* ti3;       // per triple: index of z3 in the plan
     const cd* ts;         // per triple: s of this sub-term
+    const int* gt;        // triples grouped by (z1, z3): triple ids
+    const int* goff;      // group g holds gt[goff[g] .. goff[g+1])
+    const int* gi1;       // per group: index of z1 in the plan
+    const int* gi3;       // per group: index of z3 in the plan
+    int ng;
     int nh, nk;
     int va_cplx, vb_cplx; // operand element types
     int va_hstate, vb_hstate;  // h stride applies to the anchor's state index instead of its position
@@ -82,46 +85,88 @@ __device__ __forceinline__ cd load_v(const void* p, int cplx, long idx) {
     return cplx ? static_cast<const cd*>(p)[idx] : cd{static_cast<const double*>(p)[idx], 0.0};
 }
 
-// One warp per (sub-term, triple): lanes over the summed index k.
-__global__ void __launch_bounds__(256) dterm_kernel(const DTerm* terms, int nterms, int nfreq, double beta,
-                                                    double tol, cd* out) {
-    const long nwork = (long)nterms * nfreq;
-    const int lane = threadIdx.x & 31;
-    for (long wk = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; wk < nwork;
-         wk += ((long)gridDim.x * blockDim.x) >> 5) {
-        const int q = (int)(wk / nfreq), t = (int)(wk % nfreq);
-        const DTerm& d = terms[q];
-        const int i1 = d.ti1[t], i3 = d.ti3[t];
-        const cd s = d.ts[t];
-        double ax = 0.0, ay = 0.0;
+// Triples of one (z1, z3) group handled together: the operand product
+// VA * VB does not depend on z2, so it is loaded once for DG triples.
+constexpr int DG = 8;
+
+template <bool DELTA>
+__device__ void dterm_group(const DTerm& d, int g, double beta, double tol2, cd* out, int lane) {
+    const int i1 = d.gi1[g], i3 = d.gi3[g];
+    const int tb = d.goff[g], te = d.goff[g + 1];
+    for (int t0 = tb; t0 < te; t0 += DG) {
+        const int cnt = min(DG, te - t0);
+        double sx[DG], sy[DG], ax[DG], ay[DG];
+        int tt[DG];
+#pragma unroll
+        for (int q = 0; q < DG; ++q) {
+            const int t = d.gt[t0 + min(q, cnt - 1)];  // a short group repeats its last triple
+            const cd sv = d.ts[t];
+            tt[q] = t;
+            sx[q] = sv.x;
+            sy[q] = sv.y;
+            ax[q] = 0.0;
+            ay[q] = 0.0;
+        }
         for (int h = 0; h < d.nh; ++h) {
             const int hs = d.hot[h];
             const double eh = d.Eh[hs], w = d.wh[hs];
+            const double cw = d.cnum * w, cdl = d.cdelta * beta * w;
             const long oa = i1 * d.a1 + i3 * d.a3 + (long)(d.va_hstate ? hs : h) * d.ah;
             const long ob = i1 * d.b1 + i3 * d.b3 + (long)(d.vb_hstate ? hs : h) * d.bh;
             for (int k = lane; k < d.nk; k += 32) {
                 const cd ab = load_v(d.VA, d.va_cplx, oa + k * d.ak) * load_v(d.VB, d.vb_cplx, ob + k * d.bk);
-                const cd D{s.x - d.sgn * (d.Ek[k] - eh), s.y};
-                cd K;
-                if (d.use_delta && sqrt(abs2(D)) <= tol) {
-                    K = cd{d.cdelta * beta * w, 0.0};
-                } else {
-                    const double r = d.cnum * w / abs2(D);
-                    K = cd{D.x * r, -D.y * r};
+                const double de = d.sgn * (d.Ek[k] - eh);
+#pragma unroll
+                for (int q = 0; q < DG; ++q) {
+                    const double Dx = sx[q] - de, Dy = sy[q];
+                    const double m2 = Dx * Dx + Dy * Dy;
+                    double Kx, Ky;
+                    if (DELTA && m2 <= tol2) {
+                        Kx = cdl;
+                        Ky = 0.0;
+                    } else {
+                        const double r = cw / m2;
+                        Kx = Dx * r;
+                        Ky = -Dy * r;
+                    }
+                    ax[q] += ab.x * Kx - ab.y * Ky;
+                    ay[q] += ab.x * Ky + ab.y * Kx;
                 }
-                const cd v = ab * K;
-                ax += v.x;
-                ay += v.y;
             }
         }
-        for (int o = 16; o > 0; o >>= 1) {
-            ax += __shfl_xor_sync(0xffffffffu, ax, o);
-            ay += __shfl_xor_sync(0xffffffffu, ay, o);
+#pragma unroll
+        for (int q = 0; q < DG; ++q) {
+            double x = ax[q], y = ay[q];
+            for (int o = 16; o > 0; o >>= 1) {
+                x += __shfl_xor_sync(0xffffffffu, x, o);
+                y += __shfl_xor_sync(0xffffffffu, y, o);
+            }
+            if (lane == 0 && q < cnt && (x != 0.0 || y != 0.0)) {
+                atomicAdd(&out[tt[q]].x, d.pref * x);
+                atomicAdd(&out[tt[q]].y, d.pref * y);
+            }
         }
-        if (lane == 0 && (ax != 0.0 || ay != 0.0)) {
-            atomicAdd(&out[t].x, d.pref * ax);
-            atomicAdd(&out[t].y, d.pref * ay);
+    }
+}
+
+// One warp per (sub-term, (z1, z3) group); lanes over the summed index k.
+// woff[q] = first work item of term q (prefix sum of the group counts).
+__global__ void __launch_bounds__(256) dterm_kernel(const DTerm* terms, const int* woff, int nterms, double beta,
+                                                    double tol2, cd* out) {
+    const int lane = threadIdx.x & 31;
+    const int nwork = woff[nterms];
+    for (int wk = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5); wk < nwork;
+         wk += (int)(((long)gridDim.x * blockDim.x) >> 5)) {
+        int lo = 0, hi = nterms - 1;  // last q with woff[q] <= wk
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (woff[mid] <= wk) lo = mid;
+            else hi = mid - 1;
         }
+        const DTerm& d = terms[lo];
+        const int g = wk - woff[lo];
+        if (d.use_delta) dterm_group<true>(d, g, beta, tol2, out, lane);
+        else dterm_group<false>(d, g, beta, tol2, out, lane);
     }
 }
 
@@ -129,9 +174,11 @@ struct APlan {
     std::vector<cd> Z1, Z3;
     std::vector<int> i1, i3;
     std::vector<cd> s[4];
+    std::vector<int> gt, goff, gi1, gi3;  // triples grouped by (i1, i3)
     DevBuf buf;
     cd *dZ1 = nullptr, *dZ3 = nullptr, *ds[4] = {nullptr, nullptr, nullptr, nullptr};
     int *di1 = nullptr, *di3 = nullptr;
+    int *dgt = nullptr, *dgoff = nullptr, *dgi1 = nullptr, *dgi3 = nullptr;
 };
 
 struct KeyC {
@@ -158,8 +205,22 @@ void build_aplan(APlan& pl, const int perm[3], int nfreq, const double* z, cudaS
         pl.s[2][t] = a + b;
         pl.s[3][t] = b + c;
     }
-    const size_t n1 = pl.Z1.size(), n3 = pl.Z3.size(), nf = nfreq;
-    pl.buf.reserve((n1 + n3 + 4 * nf) * sizeof(cd) + 2 * nf * sizeof(int) + 256);
+    pl.gt.resize(nfreq);
+    for (int t = 0; t < nfreq; ++t) pl.gt[t] = t;
+    std::stable_sort(pl.gt.begin(), pl.gt.end(), [&](int x, int y) {
+        return std::make_pair(pl.i1[x], pl.i3[x]) < std::make_pair(pl.i1[y], pl.i3[y]);
+    });
+    for (int q = 0; q < nfreq; ++q) {
+        const int t = pl.gt[q];
+        if (q == 0 || pl.i1[t] != pl.i1[pl.gt[q - 1]] || pl.i3[t] != pl.i3[pl.gt[q - 1]]) {
+            pl.goff.push_back(q);
+            pl.gi1.push_back(pl.i1[t]);
+            pl.gi3.push_back(pl.i3[t]);
+        }
+    }
+    pl.goff.push_back(nfreq);
+    const size_t n1 = pl.Z1.size(), n3 = pl.Z3.size(), nf = nfreq, ng = pl.gi1.size();
+    pl.buf.reserve((n1 + n3 + 4 * nf) * sizeof(cd) + (3 * nf + 3 * ng + 1) * sizeof(int) + 256);
     char* p = pl.buf.as<char>();
     auto take = [&](size_t b) {
         char* r = p;
@@ -171,6 +232,10 @@ void build_aplan(APlan& pl, const int perm[3], int nfreq, const double* z, cudaS
     for (int k = 0; k < 4; ++k) pl.ds[k] = reinterpret_cast<cd*>(take(nf * sizeof(cd)));
     pl.di1 = reinterpret_cast<int*>(take(nf * sizeof(int)));
     pl.di3 = reinterpret_cast<int*>(take(nf * sizeof(int)));
+    pl.dgt = reinterpret_cast<int*>(take(nf * sizeof(int)));
+    pl.dgoff = reinterpret_cast<int*>(take((ng + 1) * sizeof(int)));
+    pl.dgi1 = reinterpret_cast<int*>(take(ng * sizeof(int)));
+    pl.dgi3 = reinterpret_cast<int*>(take(ng * sizeof(int)));
     auto up = [&](void* d, const void* h, size_t b) {
         if (b) PGX_CUDA(cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, st));
     };
@@ -179,6 +244,10 @@ void build_aplan(APlan& pl, const int perm[3], int nfreq, const double* z, cudaS
     for (int k = 0; k < 4; ++k) up(pl.ds[k], pl.s[k].data(), nf * sizeof(cd));
     up(pl.di1, pl.i1.data(), nf * sizeof(int));
     up(pl.di3, pl.i3.data(), nf * sizeof(int));
+    up(pl.dgt, pl.gt.data(), nf * sizeof(int));
+    up(pl.dgoff, pl.goff.data(), (ng + 1) * sizeof(int));
+    up(pl.dgi1, pl.gi1.data(), ng * sizeof(int));
+    up(pl.dgi3, pl.gi3.data(), ng * sizeof(int));
 }
 
 // Workspace of one chain inside a batch (element offsets into one cd pool).
@@ -347,9 +416,12 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
             d.hot = d_hot + hot_off[S[anchor]];
             d.nh = nh;
             d.nk = nk;
-            d.ti1 = pl.di1;
-            d.ti3 = pl.di3;
             d.ts = pl.ds[sidx];
+            d.gt = pl.dgt;
+            d.goff = pl.dgoff;
+            d.gi1 = pl.dgi1;
+            d.gi3 = pl.dgi3;
+            d.ng = (int)pl.gi1.size();
             d.sgn = sgn;
             d.use_delta = use_delta;
             d.cdelta = cd_;
@@ -404,17 +476,24 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
         }
     }
     if (!dt.empty()) {
+        std::vector<int> woff(dt.size() + 1, 0);
+        double elems = 0.0;
+        for (size_t q = 0; q < dt.size(); ++q) {
+            woff[q + 1] = woff[q] + dt[q].ng;
+            elems += (double)dt[q].nh * dt[q].nk * nfreq;
+        }
         DevBuf& bd = c->scratch[3];
-        bd.reserve(dt.size() * sizeof(DTerm));
+        const size_t tb = (dt.size() * sizeof(DTerm) + 255) & ~size_t(255);
+        bd.reserve(tb + woff.size() * sizeof(int));
         PGX_CUDA(cudaMemcpyAsync(bd.p, dt.data(), dt.size() * sizeof(DTerm), cudaMemcpyHostToDevice, st));
-        const long warps = (long)dt.size() * nfreq;
-        const int blocks = (int)std::min<long>(ceil_div(warps * 32, 256), 148L * 16);
+        PGX_CUDA(cudaMemcpyAsync(bd.as<char>() + tb, woff.data(), woff.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        const long warps = woff.back();
+        const int blocks = (int)std::max<long>(1, std::min<long>(ceil_div(warps * 32, 256), 148L * 16));
         // 24 FP64 operations per (h, k, triple) element: two complex products,
         // the denominator, its squared modulus, the kernel value, accumulation
-        double elems = 0.0;
-        for (const DTerm& d : dt) elems += (double)d.nh * d.nk * nfreq;
         ProfRange pr("dterm_kernel", st, 24.0 * elems, 0.0);
-        dterm_kernel<<<blocks, 256, 0, st>>>(bd.as<DTerm>(), (int)dt.size(), nfreq, P.beta, pole_res, d_out);
+        dterm_kernel<<<blocks, 256, 0, st>>>(bd.as<DTerm>(), reinterpret_cast<const int*>(bd.as<char>() + tb),
+                                             (int)dt.size(), P.beta, pole_res * pole_res, d_out);
         check_launch("dterm_kernel");
     }
     // the scratch descriptor buffers are reused by the next batch

@@ -158,13 +158,16 @@ struct pgx_ctx {
     pgx::G2Timing g2t;
     pgx::Profiler prof;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
+    // side streams (and their fork / join events) for independent launches
+    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
     // scratch for G2 and Lehmann kernels
     pgx::DevBuf scratch[12];
 };
 
 namespace pgx {
 
-void launch_eigh(Problem& P, cudaStream_t st);
+void launch_eigh(pgx_ctx* c);
 
 // Device buffers of one eigensolve (any number of blocks), all caller-owned.
 struct EighDev {
@@ -185,6 +188,10 @@ struct EighDev {
     double* U;           // output, sum d^2
     double* E;           // output, sum d
     int* status;         // PGX_ERR_NUMERIC when a vector is not finite
+    // optional: streams on which independent Householder launches run
+    // concurrently with the main stream (all null: everything on one stream)
+    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
 };
 size_t eigh_item_bytes(const std::vector<int>& dims);
 size_t eigh_gemm_bytes(const std::vector<int>& dims, size_t* tiles_bytes);
