@@ -21,10 +21,11 @@
 //   T4a   s  sum_4 [O2[h,:] C(z3)]_4 [X4 A(z1)[:,h]]_4 (delta ? -beta w2 : w2/D)
 //   T4b   s  sum_2 [O2 C(z3)[:,h]]_2 [X4[h,:] A(z1)]_2 (delta ? 0 : -w4/D)
 // (Z = z1+z2+z3, D = s - (E_b - E_a) with s = z1+z2 for T3 and z2+z3 for T4).
-// Stages, each one launch for a batch of chains: dressing of A(z1), C(z3);
-// anchored products per frequency (gather GEMMs); products per (z1, z3)
-// stacked into GEMMs over all anchors; contractions per triple (warp per
-// (sub-term, triple), resonant delta test in FP64).
+// Stages, each one launch for a batch of chains: anchored products per
+// frequency (gather GEMMs); products per (z1, z3) stacked into GEMMs over all
+// anchors; contractions per triple (warp per (sub-term, (z1, z3) group),
+// resonant delta test in FP64).  A(z1) and C(z3) are never stored: the GEMM
+// tile loads dress O1 and O3 with the frequency as they read them.
 
 #include <array>
 #include <map>
@@ -37,29 +38,6 @@
 namespace pgx {
 
 namespace {
-
-struct DressItem {
-    const void* O;  // d_a x d_b operator block (double or cd)
-    const double *Ea, *Eb;
-    const cd* z;
-    int nz, da, db;
-    cd* out;        // nz x da x db
-};
-
-template <typename T>
-__global__ void dress_list_kernel(const DressItem* items, int nitems) {
-    const DressItem it = items[blockIdx.y];
-    const long n = (long)it.da * it.db;
-    const long total = n * it.nz;
-    const T* O = static_cast<const T*>(it.O);
-    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < total; e += (long)gridDim.x * blockDim.x) {
-        const int iz = (int)(e / n);
-        const long r = e % n;
-        const int a = (int)(r / it.db), b = (int)(r % it.db);
-        const cd zz = it.z[iz];
-        it.out[e] = tocd(O[r]) * inv(cd{zz.x - (it.Eb[b] - it.Ea[a]), zz.y});
-    }
-}
 
 struct DTerm {
     const void* VA;
@@ -252,12 +230,20 @@ void build_aplan(APlan& pl, const int perm[3], int nfreq, const double* z, cudaS
 
 // Workspace of one chain inside a batch (element offsets into one cd pool).
 struct ChainWs {
-    long A1, C3, Lc, Lr, Pr, Pc, Rho, Qc, Rr, Rc, V1a, V1b, V2a, V2b, end;
+    long Lc, Lr, Pr, Pc, Rho, Qc, Rr, Rc, V1a, V1b, V2a, V2b, end;
+};
+
+// Frequency dressing of a Lehmann factor: the operator block (rows in block
+// Sa, columns in Sb) divided elementwise by z - (E_Sb - E_Sa).
+struct Dress {
+    const double *Ea, *Eb;
+    cd z;
 };
 
 template <typename TA, typename TB>
-GemmProblem<TA, TB, cd> gp(const TA* A, long sai, long sak, const TB* B, long sbk, long sbj, cd* C, long sci, int M, int N,
-                           int K, const int* aii = nullptr, const int* bjj = nullptr) {
+GemmProblem<TA, TB, cd> gp(const typename src_t<TA>::type* A, long sai, long sak, const typename src_t<TB>::type* B,
+                           long sbk, long sbj, cd* C, long sci, int M, int N, int K, const int* aii = nullptr,
+                           const int* bjj = nullptr, Dress dr = Dress{nullptr, nullptr, cd{0.0, 0.0}}) {
     GemmProblem<TA, TB, cd> g{};
     g.A = A;
     g.B = B;
@@ -273,6 +259,9 @@ GemmProblem<TA, TB, cd> gp(const TA* A, long sai, long sak, const TB* B, long sb
     g.sc_j = 1;
     g.a_iidx = aii;
     g.b_jidx = bjj;
+    g.dEa = dr.Ea;
+    g.dEb = dr.Eb;
+    g.dz = dr.z;
     return g;
 }
 
@@ -286,33 +275,14 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
     Problem& P = c->P;
     cudaStream_t st = c->stream;
     constexpr bool TC = is_cd<T>::value;
-    // ---- dressing
-    std::vector<DressItem> di;
-    for (int q : idx) {
-        const pgx_g2_part& g = parts[q];
-        const APlan& pl = plans[part_plan[q]];
-        const ChainWs& w = wsl[q];
-        const int S1 = g.block[0], S2 = g.block[1], S3 = g.block[2], S4 = g.block[3];
-        const Operator &o1 = P.ops[g.op[0]], &o3 = P.ops[g.op[2]];
-        di.push_back(DressItem{o1.mat.as<T>() + o1.parts[o1.by_left[S1]].off, P.d_E + P.eoff[S1], P.d_E + P.eoff[S2],
-                               pl.dZ1, (int)pl.Z1.size(), P.dims[S1], P.dims[S2], pool + w.A1});
-        di.push_back(DressItem{o3.mat.as<T>() + o3.parts[o3.by_left[S3]].off, P.d_E + P.eoff[S3], P.d_E + P.eoff[S4],
-                               pl.dZ3, (int)pl.Z3.size(), P.dims[S3], P.dims[S4], pool + w.C3});
-    }
-    DevBuf& bi = c->scratch[2];
-    bi.reserve(di.size() * sizeof(DressItem));
-    PGX_CUDA(cudaMemcpyAsync(bi.p, di.data(), di.size() * sizeof(DressItem), cudaMemcpyHostToDevice, st));
-    {
-        long maxe = 1;
-        for (auto& x : di) maxe = std::max(maxe, (long)x.nz * x.da * x.db);
-        dim3 grid(std::min(ceil_div(maxe, 256), 1024), (unsigned)di.size());
-        dress_list_kernel<T><<<grid, 256, 0, st>>>(bi.as<DressItem>(), (int)di.size());
-        check_launch("dress_list_kernel");
-    }
-    // ---- anchored products per frequency
-    std::vector<GemmProblem<T, cd, cd>> pa;  // operator x dressed
-    std::vector<GemmProblem<cd, T, cd>> pb;  // dressed x operator
-    std::vector<GemmProblem<cd, cd, cd>> pc;  // per (z1, z3), all anchors stacked
+    // ---- anchored products per frequency and stacked products per (z1, z3);
+    // A1(z1) = O1 / (z1 - (E2 - E1)) and C3(z3) = O3 / (z3 - (E4 - E3)) are
+    // dressed inside the GEMM tile loads (Dressed<T> operands)
+    using DT = Dressed<T>;
+    std::vector<GemmProblem<T, DT, cd>> pa;   // operator x dressed
+    std::vector<GemmProblem<DT, T, cd>> pb;   // dressed x operator
+    std::vector<GemmProblem<DT, cd, cd>> pc;  // dressed x stacked anchors (per z1 or z3)
+    std::vector<GemmProblem<cd, DT, cd>> pd;  // stacked anchors x dressed
     for (int q : idx) {
         const pgx_g2_part& g = parts[q];
         const APlan& pl = plans[part_plan[q]];
@@ -321,43 +291,50 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
         const int d1 = P.dims[S1], d2 = P.dims[S2], d3 = P.dims[S3], d4 = P.dims[S4];
         const int r1 = rs[q][0], r2 = rs[q][1], r3 = rs[q][2], r4 = rs[q][3];
         const int N1 = (int)pl.Z1.size(), N3 = (int)pl.Z3.size();
-        const Operator &o2 = P.ops[g.op[1]], &o4 = P.ops[g.op[3]];
+        const Operator &o1 = P.ops[g.op[0]], &o2 = P.ops[g.op[1]], &o3 = P.ops[g.op[2]], &o4 = P.ops[g.op[3]];
+        const T* O1 = o1.mat.as<T>() + o1.parts[o1.by_left[S1]].off;
         const T* O2 = o2.mat.as<T>() + o2.parts[o2.by_left[S2]].off;
+        const T* O3 = o3.mat.as<T>() + o3.parts[o3.by_left[S3]].off;
         const T* X4 = o4.mat.as<T>() + o4.parts[o4.by_left[S4]].off;
+        const double *E1 = P.d_E + P.eoff[S1], *E2 = P.d_E + P.eoff[S2], *E3 = P.d_E + P.eoff[S3],
+                     *E4 = P.d_E + P.eoff[S4];
         const int *H1 = d_hot + hot_off[S1], *H2 = d_hot + hot_off[S2], *H3 = d_hot + hot_off[S3], *H4 = d_hot + hot_off[S4];
-        const long s12 = (long)d1 * d2, s34 = (long)d3 * d4;
         for (int i = 0; i < N1; ++i) {
-            const cd* A1 = pool + w.A1 + i * s12;
-            if (r2) pa.push_back(gp<T, cd>(X4, d1, 1, A1, d2, 1, pool + w.Lc + (long)i * r2, (long)N1 * r2, d4, r2, d1,
-                                           nullptr, H2));                                     // Lc = X4 A1[:,H2]
-            if (r4) pa.push_back(gp<T, cd>(X4, d1, 1, A1, d2, 1, pool + w.Lr + (long)i * r4 * d2, d2, r4, d2, d1, H4));  // Lr
-            if (r1) pb.push_back(gp<cd, T>(A1, d2, 1, O2, d3, 1, pool + w.Pr + (long)i * r1 * d3, d3, r1, d3, d2, H1));  // Pr
-            if (r3) pb.push_back(gp<cd, T>(A1, d2, 1, O2, d3, 1, pool + w.Pc + (long)i * d1 * r3, r3, d1, r3, d2,
-                                           nullptr, H3));                                     // Pc = A1 O2[:,H3]
+            const Dress A1{E1, E2, pl.Z1[i]};  // A1 = O1 dressed with z1: d1 x d2, row-major
+            if (r2) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lc + (long)i * r2, (long)N1 * r2, d4, r2, d1,
+                                           nullptr, H2, A1));                                 // Lc = X4 A1[:,H2]
+            if (r4) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lr + (long)i * r4 * d2, d2, r4, d2, d1, H4,
+                                           nullptr, A1));                                     // Lr = X4[H4,:] A1
+            if (r1) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pr + (long)i * r1 * d3, d3, r1, d3, d2, H1,
+                                           nullptr, A1));                                     // Pr = A1[H1,:] O2
+            if (r3) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pc + (long)i * d1 * r3, r3, d1, r3, d2,
+                                           nullptr, H3, A1));                                 // Pc = A1 O2[:,H3]
         }
         for (int i = 0; i < N3; ++i) {
-            const cd* C3 = pool + w.C3 + i * s34;
-            if (r3) pb.push_back(gp<cd, T>(C3, d4, 1, X4, d1, 1, pool + w.Rho + (long)i * r3 * d1, d1, r3, d1, d4, H3));  // rho
-            if (r1) pb.push_back(gp<cd, T>(C3, d4, 1, X4, d1, 1, pool + w.Qc + (long)i * d3 * r1, r1, d3, r1, d4,
-                                           nullptr, H1));                                     // Qc = C3 X4[:,H1]
-            if (r2) pa.push_back(gp<T, cd>(O2, d3, 1, C3, d4, 1, pool + w.Rr + (long)i * r2 * d4, d4, r2, d4, d3, H2));  // Rr
-            if (r4) pa.push_back(gp<T, cd>(O2, d3, 1, C3, d4, 1, pool + w.Rc + (long)i * r4, (long)N3 * r4, d2, r4, d3,
-                                           nullptr, H4));                                     // Rc = O2 C3[:,H4]
+            const Dress C3{E3, E4, pl.Z3[i]};  // C3 = O3 dressed with z3: d3 x d4, row-major
+            if (r3) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Rho + (long)i * r3 * d1, d1, r3, d1, d4, H3,
+                                           nullptr, C3));                                     // rho = C3[H3,:] X4
+            if (r1) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Qc + (long)i * d3 * r1, r1, d3, r1, d4,
+                                           nullptr, H1, C3));                                 // Qc = C3 X4[:,H1]
+            if (r2) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rr + (long)i * r2 * d4, d4, r2, d4, d3, H2,
+                                           nullptr, C3));                                     // Rr = O2[H2,:] C3
+            if (r4) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rc + (long)i * r4, (long)N3 * r4, d2, r4, d3,
+                                           nullptr, H4, C3));                                 // Rc = O2 C3[:,H4]
         }
         // products over (z1, z3): anchors of all frequencies stacked as columns / rows
         for (int i = 0; i < N3; ++i) {
-            const cd* C3 = pool + w.C3 + i * s34;
-            if (r2) pc.push_back(gp<cd, cd>(C3, d4, 1, pool + w.Lc, (long)N1 * r2, 1, pool + w.V1a + (long)i * d3 * N1 * r2,
-                                            (long)N1 * r2, d3, N1 * r2, d4));                 // V1a = C3 LcAll
-            if (r1) pc.push_back(gp<cd, cd>(pool + w.Pr, d3, 1, C3, d4, 1, pool + w.V2a + (long)i * N1 * r1 * d4, d4,
-                                            N1 * r1, d4, d3));                                // V2a = PrAll C3
+            const Dress C3{E3, E4, pl.Z3[i]};
+            if (r2) pc.push_back(gp<DT, cd>(O3, d4, 1, pool + w.Lc, (long)N1 * r2, 1, pool + w.V1a + (long)i * d3 * N1 * r2,
+                                            (long)N1 * r2, d3, N1 * r2, d4, nullptr, nullptr, C3));  // V1a = C3 LcAll
+            if (r1) pd.push_back(gp<cd, DT>(pool + w.Pr, d3, 1, O3, d4, 1, pool + w.V2a + (long)i * N1 * r1 * d4, d4,
+                                            N1 * r1, d4, d3, nullptr, nullptr, C3));                 // V2a = PrAll C3
         }
         for (int i = 0; i < N1; ++i) {
-            const cd* A1 = pool + w.A1 + i * s12;
-            if (r3) pc.push_back(gp<cd, cd>(pool + w.Rho, d1, 1, A1, d2, 1, pool + w.V1b + (long)i * N3 * r3 * d2, d2,
-                                            N3 * r3, d2, d1));                                // V1b = rhoAll A1
-            if (r4) pc.push_back(gp<cd, cd>(A1, d2, 1, pool + w.Rc, (long)N3 * r4, 1, pool + w.V2b + (long)i * d1 * N3 * r4,
-                                            (long)N3 * r4, d1, N3 * r4, d2));                 // V2b = A1 RcAll
+            const Dress A1{E1, E2, pl.Z1[i]};
+            if (r3) pd.push_back(gp<cd, DT>(pool + w.Rho, d1, 1, O1, d2, 1, pool + w.V1b + (long)i * N3 * r3 * d2, d2,
+                                            N3 * r3, d2, d1, nullptr, nullptr, A1));                 // V1b = rhoAll A1
+            if (r4) pc.push_back(gp<DT, cd>(O1, d2, 1, pool + w.Rc, (long)N3 * r4, 1, pool + w.V2b + (long)i * d1 * N3 * r4,
+                                            (long)N3 * r4, d1, N3 * r4, d2, nullptr, nullptr, A1));  // V2b = A1 RcAll
         }
     }
     // descriptor buffers sized once for the largest list, before any launch
@@ -367,8 +344,8 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
             for (auto& g : probs) nt += (long)ceil_div(g.M, GEMM_BM) * ceil_div(g.N, GEMM_BN);
             return nt;
         };
-        const long nprob = (long)(pa.size() + pb.size() + pc.size());
-        const long nt = tiles(pa) + tiles(pb) + tiles(pc);
+        const long nprob = (long)std::max({pa.size(), pb.size(), pc.size(), pd.size()});
+        const long nt = std::max({tiles(pa), tiles(pb), tiles(pc), tiles(pd)});
         c->scratch[7].reserve(std::max<long>(nprob, 1) * sizeof(GemmProblem<cd, cd, cd>));
         c->scratch[8].reserve(std::max<long>(nt, 1) * sizeof(GemmTile));
     }
@@ -376,17 +353,11 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
         if (probs.empty()) return;
         launch_gemm_batch(probs, c->scratch[7].p, c->scratch[7].bytes, c->scratch[8].p, c->scratch[8].bytes, st);
     };
-    if constexpr (TC) {
-        // complex operators: all products are complex x complex
-        std::vector<GemmProblem<cd, cd, cd>> all;
-        for (auto& g : pa) all.push_back(g);
-        for (auto& g : pb) all.push_back(g);
-        launch(all);
-    } else {
-        launch(pa);
-        launch(pb);
-    }
+    // the stacked products read Lc, Pr, rho and Rc written by the first two launches
+    launch(pa);
+    launch(pb);
     launch(pc);
+    launch(pd);
     // ---- contractions per triple
     std::vector<DTerm> dt;
     for (int q : idx) {
@@ -577,8 +548,6 @@ void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq
             o += (n + 1) & ~1L;  // keep 32-byte alignment of complex doubles
             return r0;
         };
-        x.A1 = take(N1 * d[0] * d[1]);
-        x.C3 = take(N3 * d[2] * d[3]);
         x.Lc = take((long)d[3] * N1 * r[1]);
         x.Lr = take(N1 * r[3] * d[1]);
         x.Pr = take(N1 * r[0] * d[2]);
@@ -593,7 +562,7 @@ void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq
         x.V2b = take(N1 * d[0] * N3 * r[3]);
         x.end = o;
         if (used > 0 && used + x.end > budget) flush();
-        for (long* f : {&x.A1, &x.C3, &x.Lc, &x.Lr, &x.Pr, &x.Pc, &x.Rho, &x.Qc, &x.Rr, &x.Rc, &x.V1a, &x.V1b, &x.V2a,
+        for (long* f : {&x.Lc, &x.Lr, &x.Pr, &x.Pc, &x.Rho, &x.Qc, &x.Rr, &x.Rc, &x.V1a, &x.V1b, &x.V2a,
                         &x.V2b, &x.end})
             *f += used;
         wsl[q] = x;

@@ -18,9 +18,21 @@
 
 namespace pgx {
 
+// An operand declared Dressed<T> is stored as the operator block X (type T,
+// rows a, columns b in the block's own orientation) and enters the product as
+// the complex matrix X[a][b] / (z - (Eb[b] - Ea[a])): the frequency dressing of
+// a Lehmann factor, computed as the tile is loaded instead of materialised.
+template <typename T> struct Dressed {};
+template <typename T> struct is_dressed : std::false_type {};
+template <typename T> struct is_dressed<Dressed<T>> : std::true_type {};
+template <typename T> struct src_t { using type = T; };
+template <typename T> struct src_t<Dressed<T>> { using type = T; };
+template <typename T> struct val_t { using type = T; };
+template <typename T> struct val_t<Dressed<T>> { using type = cd; };
+
 template <typename TA, typename TB, typename TC> struct GemmProblem {
-    const TA* A;
-    const TB* B;
+    const typename src_t<TA>::type* A;
+    const typename src_t<TB>::type* B;
     TC* C;
     int M, N, K;
     long sa_i, sa_k;   // A(i,k) = A[i*sa_i + k'*sa_k], k' = a_kidx ? a_kidx[k] : k
@@ -33,6 +45,9 @@ template <typename TA, typename TB, typename TC> struct GemmProblem {
     int conj_a;            // use conj(A) (complex A only)
     const int* a_iidx;     // row gather of A: A(i,k) uses row a_iidx[i] (nullable)
     const int* b_jidx;     // column gather of B: B(k,j) uses column b_jidx[j] (nullable)
+    const double* dEa;     // dressing of the Dressed<T> operand: energies of its rows,
+    const double* dEb;     // of its columns (after the gathers),
+    cd dz;                 // and the frequency
 };
 
 struct GemmTile {
@@ -54,6 +69,9 @@ __device__ __forceinline__ void mac(cd& c, cd a, cd b) {
     c.y = fma(a.x, b.y, c.y);
     c.y = fma(a.y, b.x, c.y);
 }
+template <typename T> __device__ __forceinline__ cd dress(T x, double ea, double eb, cd z) {
+    return tocd(x) * inv(cd{z.x - (eb - ea), z.y});
+}
 __device__ __forceinline__ double scale_by(double a, double s) { return a * s; }
 __device__ __forceinline__ cd scale_by(cd a, double s) { return cd{a.x * s, a.y * s}; }
 __device__ __forceinline__ double maybe_conj(double a, int) { return a; }
@@ -72,14 +90,21 @@ constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_THREADS = 256;
 // Tile shapes: 64x64 (4x4 outputs per thread), 16x128 for problems with at
 // most 16 rows and 128x16 for at most 16 columns (1x8 / 8x1 per thread), so
 // the skinny products of the anchored G2 do not waste a 64-wide tile.
+// Shared memory is double-buffered: the next k-tile's global loads are issued
+// into registers before the current tile's products, so their latency
+// overlaps the arithmetic, and one barrier per k-tile suffices.
 template <typename TA, typename TB, typename TC, int BM, int BN>
-__global__ void __launch_bounds__(GEMM_THREADS)
+__global__ void __launch_bounds__(GEMM_THREADS, 2)
     gemm_tiles_kernel(const GemmProblem<TA, TB, TC>* __restrict__ probs, const GemmTile* __restrict__ tiles) {
-    using TAcc = typename std::conditional<is_cd<TA>::value || is_cd<TB>::value, cd, double>::type;
-    constexpr int BK = (is_cd<TA>::value || is_cd<TB>::value) ? 8 : 16;
+    using VA = typename val_t<TA>::type;  // operand values as they enter the product
+    using VB = typename val_t<TB>::type;
+    using TAcc = typename std::conditional<is_cd<VA>::value || is_cd<VB>::value, cd, double>::type;
+    constexpr int BK = (is_cd<VA>::value || is_cd<VB>::value) ? 8 : 16;
     constexpr int TM = BM / 16, TN = BN / 16;
-    __shared__ TA As[BK][BM + 1];
-    __shared__ TB Bs[BK][BN + 1];
+    constexpr int LA = (BM * BK + GEMM_THREADS - 1) / GEMM_THREADS;
+    constexpr int LB = (BN * BK + GEMM_THREADS - 1) / GEMM_THREADS;
+    __shared__ VA As[2][BK][BM + 1];
+    __shared__ VB Bs[2][BK][BN + 1];
 
     const GemmTile t = tiles[blockIdx.x];
     const GemmProblem<TA, TB, TC> p = probs[t.prob];
@@ -94,52 +119,113 @@ __global__ void __launch_bounds__(GEMM_THREADS)
 
     const bool a_i_fast = (p.sa_i == 1);
     const bool b_j_fast = (p.sb_j == 1);
+    VA ra[LA];
+    VB rb[LB];
+    // position (row or column, k) inside the tile of element l of a k-tile
+    auto a_pos = [&](int l, int& ii, int& kk) {
+        if (a_i_fast) {
+            ii = l % BM;
+            kk = l / BM;
+        } else {
+            ii = l / BK;
+            kk = l % BK;
+        }
+    };
+    auto b_pos = [&](int l, int& jj, int& kk) {
+        if (b_j_fast) {
+            jj = l % BN;
+            kk = l / BN;
+        } else {
+            jj = l / BK;
+            kk = l % BK;
+        }
+    };
+    auto load = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < LA; ++q) {
+            const int l = tid + q * GEMM_THREADS;
+            VA v = zero_of<VA>();
+            if (l < BM * BK) {
+                int ii, kk;
+                a_pos(l, ii, kk);
+                const int gi = i0 + ii, gk = k0 + kk;
+                if (gi < p.M && gk < p.K) {
+                    const long kq = p.a_kidx ? p.a_kidx[gk] : gk;
+                    const long iq = p.a_iidx ? p.a_iidx[gi] : gi;
+                    if constexpr (is_dressed<TA>::value)
+                        v = dress(p.A[iq * p.sa_i + kq * p.sa_k], p.dEa[iq], p.dEb[kq], p.dz);
+                    else
+                        v = maybe_conj(p.A[iq * p.sa_i + kq * p.sa_k], p.conj_a);
+                }
+            }
+            ra[q] = v;
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int l = tid + q * GEMM_THREADS;
+            VB v = zero_of<VB>();
+            if (l < BN * BK) {
+                int jj, kk;
+                b_pos(l, jj, kk);
+                const int gj = j0 + jj, gk = k0 + kk;
+                if (gj < p.N && gk < p.K) {
+                    const long kq = p.b_kidx ? p.b_kidx[gk] : gk;
+                    const long jq = p.b_jidx ? p.b_jidx[gj] : gj;
+                    if constexpr (is_dressed<TB>::value) {
+                        v = dress(p.B[kq * p.sb_k + jq * p.sb_j], p.dEa[kq], p.dEb[jq], p.dz);
+                    } else {
+                        v = p.B[kq * p.sb_k + jq * p.sb_j];
+                        if (p.kscale) v = scale_by(v, p.kscale[gk]);
+                    }
+                }
+            }
+            rb[q] = v;
+        }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int q = 0; q < LA; ++q) {
+            const int l = tid + q * GEMM_THREADS;
+            if (l < BM * BK) {
+                int ii, kk;
+                a_pos(l, ii, kk);
+                As[buf][kk][ii] = ra[q];
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+            const int l = tid + q * GEMM_THREADS;
+            if (l < BN * BK) {
+                int jj, kk;
+                b_pos(l, jj, kk);
+                Bs[buf][kk][jj] = rb[q];
+            }
+        }
+    };
 
+    load(0);
+    store(0);
+    __syncthreads();
+    int buf = 0;
     for (int k0 = 0; k0 < p.K; k0 += BK) {
-        // ---- A tile: BM x BK
-        for (int l = tid; l < BM * BK; l += GEMM_THREADS) {
-            int ii, kk;
-            if (a_i_fast) { ii = l % BM; kk = l / BM; }
-            else { ii = l / BK; kk = l % BK; }
-            const int gi = i0 + ii, gk = k0 + kk;
-            TA v = zero_of<TA>();
-            if (gi < p.M && gk < p.K) {
-                const long kq = p.a_kidx ? p.a_kidx[gk] : gk;
-                const long iq = p.a_iidx ? p.a_iidx[gi] : gi;
-                v = maybe_conj(p.A[iq * p.sa_i + kq * p.sa_k], p.conj_a);
-            }
-            As[kk][ii] = v;
-        }
-        // ---- B tile: BK x BN
-        for (int l = tid; l < BN * BK; l += GEMM_THREADS) {
-            int jj, kk;
-            if (b_j_fast) { jj = l % BN; kk = l / BN; }
-            else { jj = l / BK; kk = l % BK; }
-            const int gj = j0 + jj, gk = k0 + kk;
-            TB v = zero_of<TB>();
-            if (gj < p.N && gk < p.K) {
-                const long kq = p.b_kidx ? p.b_kidx[gk] : gk;
-                const long jq = p.b_jidx ? p.b_jidx[gj] : gj;
-                v = p.B[kq * p.sb_k + jq * p.sb_j];
-                if (p.kscale) v = scale_by(v, p.kscale[gk]);
-            }
-            Bs[kk][jj] = v;
-        }
-        __syncthreads();
+        const bool more = k0 + BK < p.K;
+        if (more) load(k0 + BK);
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
-            TA a[TM];
-            TB b[TN];
+            VA a[TM];
+            VB b[TN];
 #pragma unroll
-            for (int q = 0; q < TM; ++q) a[q] = As[kk][ty + 16 * q];
+            for (int q = 0; q < TM; ++q) a[q] = As[buf][kk][ty + 16 * q];
 #pragma unroll
-            for (int q = 0; q < TN; ++q) b[q] = Bs[kk][tx + 16 * q];
+            for (int q = 0; q < TN; ++q) b[q] = Bs[buf][kk][tx + 16 * q];
 #pragma unroll
             for (int qa = 0; qa < TM; ++qa)
 #pragma unroll
                 for (int qb = 0; qb < TN; ++qb) mac(acc[qa][qb], a[qa], b[qb]);
         }
+        if (more) store(buf ^ 1);
         __syncthreads();
+        buf ^= 1;
     }
 #pragma unroll
     for (int qa = 0; qa < TM; ++qa) {
@@ -154,7 +240,13 @@ __global__ void __launch_bounds__(GEMM_THREADS)
     }
 }
 
-template <typename T> constexpr const char* type_tag() { return is_cd<T>::value ? "cd" : "double"; }
+template <typename T> struct type_tag_s {
+    static const char* get() { return is_cd<T>::value ? "cd" : "double"; }
+};
+template <typename T> struct type_tag_s<Dressed<T>> {
+    static const char* get() { return is_cd<T>::value ? "dressed<cd>" : "dressed<double>"; }
+};
+template <typename T> const char* type_tag() { return type_tag_s<T>::get(); }
 template <typename TA, typename TB, typename TC> const char* gemm_name() {
     static const std::string n =
         std::string("gemm_tiles_kernel<") + type_tag<TA>() + ", " + type_tag<TB>() + ", " + type_tag<TC>() + ">";
@@ -198,12 +290,14 @@ void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* 
     const auto* dt = static_cast<const GemmTile*>(d_tiles);
     // real x real 2, real x complex 4, complex x complex 8 operations per product term;
     // minimum traffic: A, B and C once (C twice when accumulating)
-    constexpr double mac = (is_cd<TA>::value && is_cd<TB>::value) ? 8.0
-                           : (is_cd<TA>::value || is_cd<TB>::value) ? 4.0 : 2.0;
+    using VA = typename val_t<TA>::type;
+    using VB = typename val_t<TB>::type;
+    constexpr double mac = (is_cd<VA>::value && is_cd<VB>::value) ? 8.0
+                           : (is_cd<VA>::value || is_cd<VB>::value) ? 4.0 : 2.0;
     double fl = 0.0, by = 0.0;
     for (const auto& q : probs) {
         fl += mac * q.M * (double)q.N * q.K;
-        by += (double)q.M * q.K * sizeof(TA) + (double)q.K * q.N * sizeof(TB) +
+        by += (double)q.M * q.K * sizeof(typename src_t<TA>::type) + (double)q.K * q.N * sizeof(typename src_t<TB>::type) +
               (q.accumulate ? 2.0 : 1.0) * q.M * (double)q.N * sizeof(TC);
     }
     ProfRange pr(gemm_name<TA, TB, TC>(), st, fl, by);
