@@ -204,6 +204,11 @@ long long pgx_launch_count(void);
 /* Device time (ms) of the last pgx_g2 call and its dominant GEMM stage. */
 int pgx_g2_last_timing(pgx_ctx* ctx, double* total_ms, double* gemm_ms, double* gemm_flops);
 
+/* Numerics check of the device reciprocal used in the Lehmann kernels
+ * (Newton-Raphson from a single-precision seed): out[i] = 1/x[i] for x[i] > 0,
+ * host arrays, computed on the current device. */
+int pgx_recip_check(const double* x, int32_t n, double* out);
+
 /* Per-kernel profile of everything the context launches between the two
  * calls: CUDA event pairs on the launching stream around each instrumented
  * kernel, aggregated by kernel name and sorted by total time (largest first).

@@ -89,6 +89,11 @@ using pgx::Error;
 
 namespace {
 
+__global__ void recip_check_kernel(const double* x, double* y, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y[i] = pgx::recip_pos(x[i]);
+}
+
 template <typename F> int guarded(pgx_ctx* c, F&& f) {
     if (!c) return PGX_ERR_ARG;
     struct Scope {  // the context's profiler is visible to launch sites during the call
@@ -475,6 +480,26 @@ int pgx_timer_end(pgx_ctx* c, double* ms) {
 }
 
 long long pgx_launch_count(void) { return pgx::launch_counter(); }
+
+int pgx_recip_check(const double* x, int32_t n, double* out) {
+    if (!x || !out || n < 1) return PGX_ERR_ARG;
+    double *dx = nullptr, *dy = nullptr;
+    int rc = PGX_OK;
+    if (cudaMalloc(&dx, n * sizeof(double)) != cudaSuccess || cudaMalloc(&dy, n * sizeof(double)) != cudaSuccess) {
+        rc = PGX_ERR_OOM;
+    } else if (cudaMemcpy(dx, x, n * sizeof(double), cudaMemcpyHostToDevice) != cudaSuccess) {
+        rc = PGX_ERR_CUDA;
+    } else {
+        recip_check_kernel<<<(n + 255) / 256, 256>>>(dx, dy, n);
+        ++pgx::launch_counter();
+        if (cudaGetLastError() != cudaSuccess || cudaMemcpy(out, dy, n * sizeof(double), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = PGX_ERR_CUDA;
+    }
+    cudaGetLastError();
+    if (dx) cudaFree(dx);
+    if (dy) cudaFree(dy);
+    return rc;
+}
 
 int pgx_profile_begin(pgx_ctx* c) {
     return guarded(c, [&] {

@@ -33,6 +33,34 @@ __host__ __device__ __forceinline__ cd inv(cd a) {
 }
 __host__ __device__ __forceinline__ cd div(cd a, cd b) { return a * inv(b); }
 
+#ifdef __CUDACC__
+// 1/x for x > 0 by the Newton-Raphson iteration y <- y + y (1 - x y), which
+// doubles the number of correct bits per step (Muller et al., "Handbook of
+// Floating-Point Arithmetic", 2nd ed., sec. 4.7), seeded with the hardware
+// single-precision approximation (PTX rcp.approx.ftz.f32, at most 1 ulp of
+// single precision): two steps bring the error to the double rounding level.
+// Outside [1e-30, 1e30] (where the seed could leave the single-precision
+// range) the IEEE division is used.
+// The iteration alone, valid for x in [1e-30, 1e30]; callers that test the
+// range once for several values keep their arithmetic free of branches.
+__device__ __forceinline__ double recip_newton(double x) {
+    float xf = (float)x, yf;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
+    double y = (double)yf;
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+__device__ __forceinline__ bool recip_in_range(double x) { return x > 1e-30 && x < 1e30; }
+__device__ __forceinline__ double recip_pos(double x) { return recip_in_range(x) ? recip_newton(x) : 1.0 / x; }
+// 1/a = conj(a) / |a|^2 with recip_pos for the real reciprocal.
+__device__ __forceinline__ cd inv_fast(cd a) {
+    const double r = recip_pos(abs2(a));
+    return cd{a.x * r, -a.y * r};
+}
+#endif
+
 // Scalar-type helpers used by templated kernels (double or cd).
 __host__ __device__ __forceinline__ cd tocd(double a) { return cd{a, 0.0}; }
 __host__ __device__ __forceinline__ cd tocd(cd a) { return a; }

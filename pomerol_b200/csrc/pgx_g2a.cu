@@ -94,21 +94,31 @@ __device__ void dterm_group(const DTerm& d, int g, double beta, double tol2, cd*
             for (int k = lane; k < d.nk; k += 32) {
                 const cd ab = load_v(d.VA, d.va_cplx, oa + k * d.ak) * load_v(d.VB, d.vb_cplx, ob + k * d.bk);
                 const double de = d.sgn * (d.Ek[k] - eh);
+                double Dx[DG], m2[DG], rc[DG];
+                bool in_range = true;
 #pragma unroll
                 for (int q = 0; q < DG; ++q) {
-                    const double Dx = sx[q] - de, Dy = sy[q];
-                    const double m2 = Dx * Dx + Dy * Dy;
-                    double Kx, Ky;
-                    if (DELTA && m2 <= tol2) {
-                        Kx = cdl;
-                        Ky = 0.0;
-                    } else {
-                        const double r = cw / m2;
-                        Kx = Dx * r;
-                        Ky = -Dy * r;
-                    }
-                    ax[q] += ab.x * Kx - ab.y * Ky;
-                    ay[q] += ab.x * Ky + ab.y * Kx;
+                    Dx[q] = sx[q] - de;
+                    m2[q] = fma(Dx[q], Dx[q], sy[q] * sy[q]);
+                    in_range = in_range && recip_in_range(m2[q]);
+                }
+                // one range test per element keeps the DG reciprocal chains
+                // branch-free, so they interleave
+                if (in_range) {
+#pragma unroll
+                    for (int q = 0; q < DG; ++q) rc[q] = recip_newton(m2[q]);
+                } else {
+#pragma unroll
+                    for (int q = 0; q < DG; ++q) rc[q] = 1.0 / m2[q];
+                }
+#pragma unroll
+                for (int q = 0; q < DG; ++q) {
+                    const double r = cw * rc[q];
+                    const bool delta = DELTA && m2[q] <= tol2;
+                    const double Kx = delta ? cdl : Dx[q] * r;
+                    const double Ky = delta ? 0.0 : -sy[q] * r;
+                    ax[q] = fma(ab.x, Kx, fma(-ab.y, Ky, ax[q]));
+                    ay[q] = fma(ab.x, Ky, fma(ab.y, Kx, ay[q]));
                 }
             }
         }

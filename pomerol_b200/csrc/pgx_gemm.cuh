@@ -70,7 +70,7 @@ __device__ __forceinline__ void mac(cd& c, cd a, cd b) {
     c.y = fma(a.y, b.x, c.y);
 }
 template <typename T> __device__ __forceinline__ cd dress(T x, double ea, double eb, cd z) {
-    return tocd(x) * inv(cd{z.x - (eb - ea), z.y});
+    return tocd(x) * inv_fast(cd{z.x - (eb - ea), z.y});
 }
 __device__ __forceinline__ double scale_by(double a, double s) { return a * s; }
 __device__ __forceinline__ cd scale_by(cd a, double s) { return cd{a.x * s, a.y * s}; }
@@ -253,12 +253,35 @@ template <typename TA, typename TB, typename TC> const char* gemm_name() {
     return n.c_str();
 }
 
-// Tile class of a problem: 0 = 64x64, 1 = 16x128 (M <= 16), 2 = 128x16 (N <= 16).
+// Tile classes (BM x BN).  A problem takes the class that pads it least
+// (ties: the larger tile); the classes other than 64x64 are used only when
+// their short side covers the problem's M or N in one tile, so the tile count
+// never exceeds that of 64x64 tiles.
+constexpr int GEMM_NCLS = 7;
+constexpr int GEMM_CLS_M[GEMM_NCLS] = {64, 16, 128, 64, 64, 32, 48};
+constexpr int GEMM_CLS_N[GEMM_NCLS] = {64, 128, 16, 32, 48, 64, 64};
+
 template <typename P> inline int gemm_class(const P& p) {
-    if (p.M <= 16 && p.N > 16) return 1;
-    if (p.N <= 16 && p.M > 16) return 2;
-    if (p.M <= 16 && p.N <= 16) return 1;
-    return 0;
+    int best = 0;
+    long best_area = (long)ceil_div(p.M, 64) * 64 * ((long)ceil_div(p.N, 64) * 64);
+    for (int c = 1; c < GEMM_NCLS; ++c) {
+        const int bm = GEMM_CLS_M[c], bn = GEMM_CLS_N[c];
+        if (bm < 64 && p.M > bm) continue;
+        if (bn < 64 && p.N > bn) continue;
+        const long area = (long)ceil_div(p.M, bm) * bm * ((long)ceil_div(p.N, bn) * bn);
+        if (area < best_area) {
+            best = c;
+            best_area = area;
+        }
+    }
+    return best;
+}
+
+template <typename TA, typename TB, typename TC, int BM, int BN>
+void launch_gemm_class(const GemmProblem<TA, TB, TC>* dp, const GemmTile* dt, size_t b, size_t e, cudaStream_t st) {
+    if (e <= b) return;
+    gemm_tiles_kernel<TA, TB, TC, BM, BN><<<(unsigned)(e - b), GEMM_THREADS, 0, st>>>(dp, dt + b);
+    check_launch("gemm_tiles_kernel");
 }
 
 // Host helper: upload problems + tile lists into scratch buffers and launch
@@ -268,19 +291,20 @@ template <typename TA, typename TB, typename TC>
 void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* d_probs, size_t probs_cap,
                        void* d_tiles, size_t tiles_cap, cudaStream_t st) {
     if (probs.empty()) return;
-    static const int BMs[3] = {64, 16, 128}, BNs[3] = {64, 128, 16};
     std::vector<GemmTile> tiles;
-    size_t start[4] = {0, 0, 0, 0};
-    for (int cls = 0; cls < 3; ++cls) {
-        start[cls] = tiles.size();
+    size_t start[GEMM_NCLS + 1] = {};
+    std::vector<int> cls(probs.size());
+    for (size_t q = 0; q < probs.size(); ++q) cls[q] = gemm_class(probs[q]);
+    for (int c = 0; c < GEMM_NCLS; ++c) {
+        start[c] = tiles.size();
         for (size_t q = 0; q < probs.size(); ++q) {
-            if (probs[q].M <= 0 || probs[q].N <= 0 || gemm_class(probs[q]) != cls) continue;
-            const int tm = ceil_div(probs[q].M, BMs[cls]), tn = ceil_div(probs[q].N, BNs[cls]);
+            if (probs[q].M <= 0 || probs[q].N <= 0 || cls[q] != c) continue;
+            const int tm = ceil_div(probs[q].M, GEMM_CLS_M[c]), tn = ceil_div(probs[q].N, GEMM_CLS_N[c]);
             for (int a = 0; a < tm; ++a)
                 for (int b = 0; b < tn; ++b) tiles.push_back(GemmTile{(int)q, a, b, 0});
         }
     }
-    start[3] = tiles.size();
+    start[GEMM_NCLS] = tiles.size();
     if (tiles.empty()) return;
     PGX_CHECK(probs.size() * sizeof(probs[0]) <= probs_cap, PGX_ERR_ARG, "gemm problem list overflow");
     PGX_CHECK(tiles.size() * sizeof(GemmTile) <= tiles_cap, PGX_ERR_ARG, "gemm tile list overflow");
@@ -301,18 +325,13 @@ void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* 
               (q.accumulate ? 2.0 : 1.0) * q.M * (double)q.N * sizeof(TC);
     }
     ProfRange pr(gemm_name<TA, TB, TC>(), st, fl, by);
-    if (start[1] > start[0]) {
-        gemm_tiles_kernel<TA, TB, TC, 64, 64><<<(unsigned)(start[1] - start[0]), GEMM_THREADS, 0, st>>>(dp, dt + start[0]);
-        check_launch("gemm_tiles_kernel<64,64>");
-    }
-    if (start[2] > start[1]) {
-        gemm_tiles_kernel<TA, TB, TC, 16, 128><<<(unsigned)(start[2] - start[1]), GEMM_THREADS, 0, st>>>(dp, dt + start[1]);
-        check_launch("gemm_tiles_kernel<16,128>");
-    }
-    if (start[3] > start[2]) {
-        gemm_tiles_kernel<TA, TB, TC, 128, 16><<<(unsigned)(start[3] - start[2]), GEMM_THREADS, 0, st>>>(dp, dt + start[2]);
-        check_launch("gemm_tiles_kernel<128,16>");
-    }
+    launch_gemm_class<TA, TB, TC, 64, 64>(dp, dt, start[0], start[1], st);
+    launch_gemm_class<TA, TB, TC, 16, 128>(dp, dt, start[1], start[2], st);
+    launch_gemm_class<TA, TB, TC, 128, 16>(dp, dt, start[2], start[3], st);
+    launch_gemm_class<TA, TB, TC, 64, 32>(dp, dt, start[3], start[4], st);
+    launch_gemm_class<TA, TB, TC, 64, 48>(dp, dt, start[4], start[5], st);
+    launch_gemm_class<TA, TB, TC, 32, 64>(dp, dt, start[5], start[6], st);
+    launch_gemm_class<TA, TB, TC, 48, 64>(dp, dt, start[6], start[7], st);
 }
 
 }  // namespace pgx

@@ -23,6 +23,7 @@ EXPORTS = [
     "pgx_op_define", "pgx_op_rotate", "pgx_op_adjoint", "pgx_op_info", "pgx_op_read", "pgx_gf", "pgx_susc",
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
+    "pgx_recip_check",
 ]
 
 
@@ -75,6 +76,7 @@ def load():
         lib.pgx_profile_begin.argtypes = [P]
         lib.pgx_profile_end.argtypes = [P, P]
         lib.pgx_profile_kernel.argtypes = [P, I32, C.c_char_p, I32, P, P, P, P]
+        lib.pgx_recip_check.argtypes = [P, I32, P]
         _lib = lib
     return _lib
 

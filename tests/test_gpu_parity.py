@@ -318,3 +318,20 @@ def test_plaquette_g2_matches_oracle(harness):
     sel = list(range(0, len(trip), 37))
     ref = L.g2_exact(ed, oparts, [tuple(fz[t]) for t in sel])
     assert np.abs(v[sel] - ref).max() < 1e-10 * np.abs(ref).max()
+
+
+def test_device_reciprocal_error_bound():
+    """The Newton-Raphson reciprocal of the Lehmann kernels against the
+    correctly rounded 1/x: at most 2 ulp over 1e-40..1e40 (both the iterated
+    range and the IEEE-division fallback outside [1e-30, 1e30])."""
+    import ctypes
+    from pomerol_b200 import pgx
+    rng = np.random.default_rng(5)
+    x = np.concatenate([10.0 ** rng.uniform(-40, 40, 200000), rng.uniform(0.5, 2.0, 50000),
+                        np.array([1e-30 * (1 + 1e-15), 1e30 * (1 - 1e-15), 1.0, 3.0, 7.0])])
+    out = np.empty_like(x)
+    rc = pgx.load().pgx_recip_check(x.ctypes.data_as(ctypes.c_void_p), len(x), out.ctypes.data_as(ctypes.c_void_p))
+    assert rc == pgx.PGX_OK
+    ref = 1.0 / x
+    ulp = np.abs(out - ref) / np.spacing(ref)
+    assert ulp.max() <= 2.0
