@@ -3,6 +3,7 @@
 // exception crosses the ABI.
 
 #include <algorithm>
+#include <cstring>
 #include <numeric>
 
 #include "pgx_common.cuh"
@@ -69,6 +70,58 @@ Profiler::~Profiler() {
     for (auto e : spare) cudaEventDestroy(e);
 }
 
+HostArena*& active_arena() {
+    static thread_local HostArena* a = nullptr;
+    return a;
+}
+
+void* HostArena::put(const void* src, size_t n) {
+    const size_t need = (n + 15) & ~size_t(15);
+    while (cur < blocks.size() && used + need > blocks[cur].second) {
+        ++cur;
+        used = 0;
+    }
+    if (cur == blocks.size()) {
+        const size_t cap = std::max<size_t>(need, std::max<size_t>(size_t(1) << 20, blocks.empty() ? 0 : 2 * blocks.back().second));
+        void* p = nullptr;
+        if (cudaMallocHost(&p, cap) != cudaSuccess) {
+            cudaGetLastError();
+            throw Error{PGX_ERR_OOM, "cudaMallocHost(" + std::to_string(cap) + " bytes) failed"};
+        }
+        blocks.emplace_back(static_cast<char*>(p), cap);
+        used = 0;
+    }
+    char* dst = blocks[cur].first + used;
+    std::memcpy(dst, src, n);
+    used += need;
+    dirty = true;
+    return dst;
+}
+
+void HostArena::recycle(cudaStream_t st) {
+    if (!dirty) return;
+    const cudaError_t q = cudaStreamQuery(st);
+    if (q == cudaErrorNotReady) {
+        cudaGetLastError();  // not an error: copies are still pending, keep appending
+        return;
+    }
+    if (q != cudaSuccess) return;
+    cur = 0;
+    used = 0;
+    dirty = false;
+}
+
+HostArena::~HostArena() {
+    for (auto& b : blocks) cudaFreeHost(b.first);
+}
+
+void h2d(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+    if (!bytes) return;
+    HostArena* a = active_arena();
+    const void* s = a ? a->put(src, bytes) : src;
+    PGX_CUDA(cudaMemcpyAsync(dst, s, bytes, cudaMemcpyHostToDevice, st));
+}
+
 ProfRange::ProfRange(const char* name, cudaStream_t st, double flops, double bytes) {
     Profiler* p = active_profiler();
     if (!p || !p->on) return;
@@ -96,14 +149,22 @@ __global__ void recip_check_kernel(const double* x, double* y, int n) {
 
 template <typename F> int guarded(pgx_ctx* c, F&& f) {
     if (!c) return PGX_ERR_ARG;
-    struct Scope {  // the context's profiler is visible to launch sites during the call
-        pgx::Profiler* saved;
-        explicit Scope(pgx::Profiler* p) : saved(pgx::active_profiler()) { pgx::active_profiler() = p; }
-        ~Scope() { pgx::active_profiler() = saved; }
-    } scope(&c->prof);
+    struct Scope {  // the context's profiler and upload arena are visible to launch sites during the call
+        pgx::Profiler* saved_p;
+        pgx::HostArena* saved_a;
+        explicit Scope(pgx_ctx* c) : saved_p(pgx::active_profiler()), saved_a(pgx::active_arena()) {
+            pgx::active_profiler() = &c->prof;
+            pgx::active_arena() = &c->arena;
+        }
+        ~Scope() {
+            pgx::active_profiler() = saved_p;
+            pgx::active_arena() = saved_a;
+        }
+    } scope(c);
     try {
         PGX_CUDA(cudaSetDevice(c->device));
         f();
+        c->arena.recycle(c->stream);
         c->last_error.clear();
         return PGX_OK;
     } catch (const Error& e) {

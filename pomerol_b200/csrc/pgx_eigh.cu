@@ -653,15 +653,12 @@ size_t eigh_item_bytes(const std::vector<int>& dims) {
 }
 
 size_t eigh_gemm_bytes(const std::vector<int>& dims, size_t* tiles_bytes) {
-    long nt = 0;
-    for (int n : dims) nt += (long)ceil_div(n, GEMM_BM) * ceil_div(n, GEMM_BN);
-    if (tiles_bytes) *tiles_bytes = std::max<long>(nt, 1) * sizeof(GemmTile);
+    if (tiles_bytes) *tiles_bytes = gemm_index_bytes(dims.size());
     return std::max<size_t>(dims.size(), 1) * sizeof(GemmProblem<double, double, double>);
 }
 
-// All eigensolver stages on caller-provided device buffers (no allocation).
-// The function waits for the stream before returning because its host
-// descriptor lists are staged from host memory.
+// All eigensolver stages on caller-provided device buffers (no allocation),
+// enqueued on stream st (asynchronous).
 void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::vector<long>& moff,
                      cudaStream_t st) {
     int dmax = 1;
@@ -711,7 +708,7 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     std::vector<char> host(items.size() * sizeof(TriItem) + lists.size() * sizeof(int));
     std::memcpy(host.data(), items.data(), items.size() * sizeof(TriItem));
     std::memcpy(host.data() + items.size() * sizeof(TriItem), lists.data(), lists.size() * sizeof(int));
-    PGX_CUDA(cudaMemcpyAsync(d.items, host.data(), host.size(), cudaMemcpyHostToDevice, st));
+    h2d(d.items, host.data(), host.size(), st);
     const int* d_lists = reinterpret_cast<const int*>(static_cast<const char*>(d.items) + items.size() * sizeof(TriItem));
 
     // LAPACK operation counts: tridiagonalisation 4/3 n^3, forming Q 4/3 n^3;
@@ -837,7 +834,6 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     size_t tiles_cap = 0;
     const size_t probs_cap = eigh_gemm_bytes(dims, &tiles_cap);
     launch_gemm_batch(probs, d.gemm_probs, probs_cap, d.gemm_tiles, tiles_cap, st);
-    PGX_CUDA(cudaStreamSynchronize(st));  // the host lists go out of scope
 }
 
 void launch_eigh(pgx_ctx* c) {

@@ -274,7 +274,7 @@ void upload_plan(Plan& pl, cudaStream_t st) {
     pl.dptr = reinterpret_cast<int*>(take((np + 1) * sizeof(int)));
     pl.dslot = reinterpret_cast<int*>(take(nf * sizeof(int)));
     auto up = [&](void* d, const void* h, size_t b) {
-        if (b) PGX_CUDA(cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, st));
+        if (b) h2d(d, h, b, st);
     };
     up(pl.dZ1, pl.Z1.data(), n1 * sizeof(cd));
     up(pl.dZ3, pl.Z3.data(), n3 * sizeof(cd));
@@ -527,7 +527,7 @@ void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const d
     S[5].reserve(nR * sizeof(cd));
     S[6].reserve(pair_budget * sizeof(cd));
     S[7].reserve(nprob * sizeof(GemmProblem<cd, cd, cd>));
-    S[8].reserve(ntile * sizeof(GemmTile));
+    S[8].reserve(gemm_index_bytes(nprob));
     S[9].reserve(std::max(nfreq, 1) * sizeof(cd));
     ws.A1 = S[0].as<cd>();
     ws.C3 = S[1].as<cd>();

@@ -225,7 +225,7 @@ void build_aplan(APlan& pl, const int perm[3], int nfreq, const double* z, cudaS
     pl.dgi1 = reinterpret_cast<int*>(take(ng * sizeof(int)));
     pl.dgi3 = reinterpret_cast<int*>(take(ng * sizeof(int)));
     auto up = [&](void* d, const void* h, size_t b) {
-        if (b) PGX_CUDA(cudaMemcpyAsync(d, h, b, cudaMemcpyHostToDevice, st));
+        if (b) h2d(d, h, b, st);
     };
     up(pl.dZ1, pl.Z1.data(), n1 * sizeof(cd));
     up(pl.dZ3, pl.Z3.data(), n3 * sizeof(cd));
@@ -244,16 +244,19 @@ struct ChainWs {
 };
 
 // Frequency dressing of a Lehmann factor: the operator block (rows in block
-// Sa, columns in Sb) divided elementwise by z - (E_Sb - E_Sa).
+// Sa, columns in Sb) divided elementwise by z - (E_Sb - E_Sa), with z taken
+// per batch item from the plan's frequency list.
 struct Dress {
     const double *Ea, *Eb;
-    cd z;
+    const cd* z;
 };
 
+// One product per frequency of a list (nb items): only the output moves, by
+// bc elements per item; the dressed operand takes the item's frequency.
 template <typename TA, typename TB>
 GemmProblem<TA, TB, cd> gp(const typename src_t<TA>::type* A, long sai, long sak, const typename src_t<TB>::type* B,
-                           long sbk, long sbj, cd* C, long sci, int M, int N, int K, const int* aii = nullptr,
-                           const int* bjj = nullptr, Dress dr = Dress{nullptr, nullptr, cd{0.0, 0.0}}) {
+                           long sbk, long sbj, cd* C, long sci, int M, int N, int K, const int* aii, const int* bjj,
+                           Dress dr, int nb, long bc) {
     GemmProblem<TA, TB, cd> g{};
     g.A = A;
     g.B = B;
@@ -271,7 +274,9 @@ GemmProblem<TA, TB, cd> gp(const typename src_t<TA>::type* A, long sai, long sak
     g.b_jidx = bjj;
     g.dEa = dr.Ea;
     g.dEb = dr.Eb;
-    g.dz = dr.z;
+    g.dzs = dr.z;
+    g.nb = nb;
+    g.bc = bc;
     return g;
 }
 
@@ -309,55 +314,40 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
         const double *E1 = P.d_E + P.eoff[S1], *E2 = P.d_E + P.eoff[S2], *E3 = P.d_E + P.eoff[S3],
                      *E4 = P.d_E + P.eoff[S4];
         const int *H1 = d_hot + hot_off[S1], *H2 = d_hot + hot_off[S2], *H3 = d_hot + hot_off[S3], *H4 = d_hot + hot_off[S4];
-        for (int i = 0; i < N1; ++i) {
-            const Dress A1{E1, E2, pl.Z1[i]};  // A1 = O1 dressed with z1: d1 x d2, row-major
-            if (r2) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lc + (long)i * r2, (long)N1 * r2, d4, r2, d1,
-                                           nullptr, H2, A1));                                 // Lc = X4 A1[:,H2]
-            if (r4) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lr + (long)i * r4 * d2, d2, r4, d2, d1, H4,
-                                           nullptr, A1));                                     // Lr = X4[H4,:] A1
-            if (r1) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pr + (long)i * r1 * d3, d3, r1, d3, d2, H1,
-                                           nullptr, A1));                                     // Pr = A1[H1,:] O2
-            if (r3) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pc + (long)i * d1 * r3, r3, d1, r3, d2,
-                                           nullptr, H3, A1));                                 // Pc = A1 O2[:,H3]
-        }
-        for (int i = 0; i < N3; ++i) {
-            const Dress C3{E3, E4, pl.Z3[i]};  // C3 = O3 dressed with z3: d3 x d4, row-major
-            if (r3) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Rho + (long)i * r3 * d1, d1, r3, d1, d4, H3,
-                                           nullptr, C3));                                     // rho = C3[H3,:] X4
-            if (r1) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Qc + (long)i * d3 * r1, r1, d3, r1, d4,
-                                           nullptr, H1, C3));                                 // Qc = C3 X4[:,H1]
-            if (r2) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rr + (long)i * r2 * d4, d4, r2, d4, d3, H2,
-                                           nullptr, C3));                                     // Rr = O2[H2,:] C3
-            if (r4) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rc + (long)i * r4, (long)N3 * r4, d2, r4, d3,
-                                           nullptr, H4, C3));                                 // Rc = O2 C3[:,H4]
-        }
+        const Dress A1{E1, E2, pl.dZ1};  // A1(z1) = O1 dressed with z1: d1 x d2, row-major
+        const Dress C3{E3, E4, pl.dZ3};  // C3(z3) = O3 dressed with z3: d3 x d4, row-major
+        // anchored products, one item per z1 (or z3)
+        if (r2) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lc, (long)N1 * r2, d4, r2, d1, nullptr, H2, A1, N1,
+                                       r2));                                              // Lc = X4 A1[:,H2]
+        if (r4) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lr, d2, r4, d2, d1, H4, nullptr, A1, N1,
+                                       (long)r4 * d2));                                   // Lr = X4[H4,:] A1
+        if (r1) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pr, d3, r1, d3, d2, H1, nullptr, A1, N1,
+                                       (long)r1 * d3));                                   // Pr = A1[H1,:] O2
+        if (r3) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pc, r3, d1, r3, d2, nullptr, H3, A1, N1,
+                                       (long)d1 * r3));                                   // Pc = A1 O2[:,H3]
+        if (r3) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Rho, d1, r3, d1, d4, H3, nullptr, C3, N3,
+                                       (long)r3 * d1));                                   // rho = C3[H3,:] X4
+        if (r1) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Qc, r1, d3, r1, d4, nullptr, H1, C3, N3,
+                                       (long)d3 * r1));                                   // Qc = C3 X4[:,H1]
+        if (r2) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rr, d4, r2, d4, d3, H2, nullptr, C3, N3,
+                                       (long)r2 * d4));                                   // Rr = O2[H2,:] C3
+        if (r4) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rc, (long)N3 * r4, d2, r4, d3, nullptr, H4, C3,
+                                       N3, r4));                                          // Rc = O2 C3[:,H4]
         // products over (z1, z3): anchors of all frequencies stacked as columns / rows
-        for (int i = 0; i < N3; ++i) {
-            const Dress C3{E3, E4, pl.Z3[i]};
-            if (r2) pc.push_back(gp<DT, cd>(O3, d4, 1, pool + w.Lc, (long)N1 * r2, 1, pool + w.V1a + (long)i * d3 * N1 * r2,
-                                            (long)N1 * r2, d3, N1 * r2, d4, nullptr, nullptr, C3));  // V1a = C3 LcAll
-            if (r1) pd.push_back(gp<cd, DT>(pool + w.Pr, d3, 1, O3, d4, 1, pool + w.V2a + (long)i * N1 * r1 * d4, d4,
-                                            N1 * r1, d4, d3, nullptr, nullptr, C3));                 // V2a = PrAll C3
-        }
-        for (int i = 0; i < N1; ++i) {
-            const Dress A1{E1, E2, pl.Z1[i]};
-            if (r3) pd.push_back(gp<cd, DT>(pool + w.Rho, d1, 1, O1, d2, 1, pool + w.V1b + (long)i * N3 * r3 * d2, d2,
-                                            N3 * r3, d2, d1, nullptr, nullptr, A1));                 // V1b = rhoAll A1
-            if (r4) pc.push_back(gp<DT, cd>(O1, d2, 1, pool + w.Rc, (long)N3 * r4, 1, pool + w.V2b + (long)i * d1 * N3 * r4,
-                                            (long)N3 * r4, d1, N3 * r4, d2, nullptr, nullptr, A1));  // V2b = A1 RcAll
-        }
+        if (r2) pc.push_back(gp<DT, cd>(O3, d4, 1, pool + w.Lc, (long)N1 * r2, 1, pool + w.V1a, (long)N1 * r2, d3, N1 * r2,
+                                        d4, nullptr, nullptr, C3, N3, (long)d3 * N1 * r2));   // V1a = C3 LcAll
+        if (r1) pd.push_back(gp<cd, DT>(pool + w.Pr, d3, 1, O3, d4, 1, pool + w.V2a, d4, N1 * r1, d4, d3, nullptr, nullptr,
+                                        C3, N3, (long)N1 * r1 * d4));                         // V2a = PrAll C3
+        if (r3) pd.push_back(gp<cd, DT>(pool + w.Rho, d1, 1, O1, d2, 1, pool + w.V1b, d2, N3 * r3, d2, d1, nullptr, nullptr,
+                                        A1, N1, (long)N3 * r3 * d2));                         // V1b = rhoAll A1
+        if (r4) pc.push_back(gp<DT, cd>(O1, d2, 1, pool + w.Rc, (long)N3 * r4, 1, pool + w.V2b, (long)N3 * r4, d1, N3 * r4,
+                                        d2, nullptr, nullptr, A1, N1, (long)d1 * N3 * r4));   // V2b = A1 RcAll
     }
     // descriptor buffers sized once for the largest list, before any launch
     {
-        auto tiles = [](auto& probs) {
-            long nt = 0;
-            for (auto& g : probs) nt += (long)ceil_div(g.M, GEMM_BM) * ceil_div(g.N, GEMM_BN);
-            return nt;
-        };
         const long nprob = (long)std::max({pa.size(), pb.size(), pc.size(), pd.size()});
-        const long nt = std::max({tiles(pa), tiles(pb), tiles(pc), tiles(pd)});
         c->scratch[7].reserve(std::max<long>(nprob, 1) * sizeof(GemmProblem<cd, cd, cd>));
-        c->scratch[8].reserve(std::max<long>(nt, 1) * sizeof(GemmTile));
+        c->scratch[8].reserve(gemm_index_bytes(nprob));
     }
     auto launch = [&](auto& probs) {
         if (probs.empty()) return;
@@ -466,8 +456,8 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
         DevBuf& bd = c->scratch[3];
         const size_t tb = (dt.size() * sizeof(DTerm) + 255) & ~size_t(255);
         bd.reserve(tb + woff.size() * sizeof(int));
-        PGX_CUDA(cudaMemcpyAsync(bd.p, dt.data(), dt.size() * sizeof(DTerm), cudaMemcpyHostToDevice, st));
-        PGX_CUDA(cudaMemcpyAsync(bd.as<char>() + tb, woff.data(), woff.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        h2d(bd.p, dt.data(), dt.size() * sizeof(DTerm), st);
+        h2d(bd.as<char>() + tb, woff.data(), woff.size() * sizeof(int), st);
         const long warps = woff.back();
         const int blocks = (int)std::max<long>(1, std::min<long>(ceil_div(warps * 32, 256), 148L * 16));
         // 24 FP64 operations per (h, k, triple) element: two complex products,
@@ -477,8 +467,7 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
                                              (int)dt.size(), P.beta, pole_res * pole_res, d_out);
         check_launch("dterm_kernel");
     }
-    // the scratch descriptor buffers are reused by the next batch
-    PGX_CUDA(cudaStreamSynchronize(st));
+    // the next batch reuses the device descriptor buffers in stream order
 }
 
 void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
@@ -486,9 +475,8 @@ void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq
     Problem& P = c->P;
     cudaStream_t st = c->stream;
     // anchor states per block (weights above the threshold)
-    std::vector<double> w(P.esize);
-    PGX_CUDA(cudaMemcpyAsync(w.data(), P.d_w, P.esize * sizeof(double), cudaMemcpyDeviceToHost, st));
-    PGX_CUDA(cudaStreamSynchronize(st));
+    const std::vector<double>& w = P.w_host;  // copied when the weights were computed
+    PGX_CHECK((long)w.size() == P.esize, PGX_ERR_STATE, "pgx_weights first");
     std::vector<int> hot;
     std::vector<long> hot_off(P.nblocks + 1, 0);
     std::vector<int> nhot(P.nblocks, 0);
@@ -501,7 +489,7 @@ void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq
     hot_off[P.nblocks] = (long)hot.size();
     DevBuf& bh = c->scratch[11];
     bh.reserve(std::max<size_t>(hot.size(), 1) * sizeof(int));
-    if (!hot.empty()) PGX_CUDA(cudaMemcpyAsync(bh.p, hot.data(), hot.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    if (!hot.empty()) h2d(bh.p, hot.data(), hot.size() * sizeof(int), st);
     // frequency plans per permutation
     std::map<std::tuple<int, int, int>, int> perm_id;
     std::vector<APlan> plans;

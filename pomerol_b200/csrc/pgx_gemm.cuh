@@ -47,12 +47,16 @@ template <typename TA, typename TB, typename TC> struct GemmProblem {
     const int* b_jidx;     // column gather of B: B(k,j) uses column b_jidx[j] (nullable)
     const double* dEa;     // dressing of the Dressed<T> operand: energies of its rows,
     const double* dEb;     // of its columns (after the gathers),
-    cd dz;                 // and the frequency
+    cd dz;                 // and the frequency (or dzs[b] for batch item b when dzs is set)
+    // batch of nb products with the same shapes (nb <= 0 counts as 1): item b
+    // uses A + b*ba, B + b*bb, C + b*bc
+    int nb;
+    long ba, bb, bc;
+    const cd* dzs;
 };
 
-struct GemmTile {
-    int prob, tm, tn, pad;
-};
+// Bytes of the per-class tile index a launch_gemm_batch of nprobs problems needs.
+inline size_t gemm_index_bytes(size_t nprobs) { return (nprobs + 16) * sizeof(int); }
 
 __device__ __forceinline__ void mac(double& c, double a, double b) { c = fma(a, b, c); }
 __device__ __forceinline__ void mac(cd& c, cd a, double b) {
@@ -87,29 +91,50 @@ template <> __device__ __forceinline__ cd zero_of<cd>() { return cd{0.0, 0.0}; }
 
 constexpr int GEMM_BM = 64, GEMM_BN = 64, GEMM_THREADS = 256;
 
-// Tile shapes: 64x64 (4x4 outputs per thread), 16x128 for problems with at
-// most 16 rows and 128x16 for at most 16 columns (1x8 / 8x1 per thread), so
-// the skinny products of the anchored G2 do not waste a 64-wide tile.
+// Tile shapes (BM x BN, outputs per thread): 64x64 (4x4); 16x128, 128x16
+// (1x8, 8x1); 64x32, 64x48, 32x64, 48x64 (4x2, 4x3, 2x4, 3x4); 4x128, 128x4
+// (1x2, 2x1) for products with at most 4 rows or columns, so the skinny
+// products of the anchored G2 do not run in a wide tile.
 // Shared memory is double-buffered: the next k-tile's global loads are issued
 // into registers before the current tile's products, so their latency
 // overlaps the arithmetic, and one barrier per k-tile suffices.
 template <typename TA, typename TB, typename TC, int BM, int BN>
 __global__ void __launch_bounds__(GEMM_THREADS, 2)
-    gemm_tiles_kernel(const GemmProblem<TA, TB, TC>* __restrict__ probs, const GemmTile* __restrict__ tiles) {
+    gemm_tiles_kernel(const GemmProblem<TA, TB, TC>* __restrict__ probs, const int* __restrict__ tile0, int nprobs) {
     using VA = typename val_t<TA>::type;  // operand values as they enter the product
     using VB = typename val_t<TB>::type;
     using TAcc = typename std::conditional<is_cd<VA>::value || is_cd<VB>::value, cd, double>::type;
     constexpr int BK = (is_cd<VA>::value || is_cd<VB>::value) ? 8 : 16;
-    constexpr int TM = BM / 16, TN = BN / 16;
+    // thread grid NY x NX (256 threads), each thread an TM x TN sub-tile
+    constexpr int NX = (BM == 4) ? 64 : (BN == 4) ? 4 : 16;
+    constexpr int NY = GEMM_THREADS / NX;
+    constexpr int TM = BM / NY, TN = BN / NX;
+    static_assert(TM * NY == BM && TN * NX == BN, "tile shape does not fit the thread grid");
     constexpr int LA = (BM * BK + GEMM_THREADS - 1) / GEMM_THREADS;
     constexpr int LB = (BN * BK + GEMM_THREADS - 1) / GEMM_THREADS;
     __shared__ VA As[2][BK][BM + 1];
     __shared__ VB Bs[2][BK][BN + 1];
 
-    const GemmTile t = tiles[blockIdx.x];
-    const GemmProblem<TA, TB, TC> p = probs[t.prob];
-    const int i0 = t.tm * BM, j0 = t.tn * BN;
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    // tile0[q] = first tile of problem q (prefix sum); find this CTA's problem
+    const int tile = blockIdx.x;
+    int lo = 0, hi = nprobs - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (tile0[mid] <= tile) lo = mid;
+        else hi = mid - 1;
+    }
+    GemmProblem<TA, TB, TC> p = probs[lo];
+    const int tn_count = (p.N + BN - 1) / BN, per_item = ((p.M + BM - 1) / BM) * tn_count;
+    const int local = tile - tile0[lo];
+    const int item = local / per_item, rem = local % per_item;
+    const int i0 = (rem / tn_count) * BM, j0 = (rem % tn_count) * BN;
+    if (item > 0) {
+        p.A += item * p.ba;
+        p.B += item * p.bb;
+        p.C += item * p.bc;
+    }
+    if (p.dzs) p.dz = p.dzs[item];
+    const int tid = threadIdx.x, tx = tid % NX, ty = tid / NX;
 
     TAcc acc[TM][TN];
 #pragma unroll
@@ -215,9 +240,9 @@ __global__ void __launch_bounds__(GEMM_THREADS, 2)
             VA a[TM];
             VB b[TN];
 #pragma unroll
-            for (int q = 0; q < TM; ++q) a[q] = As[buf][kk][ty + 16 * q];
+            for (int q = 0; q < TM; ++q) a[q] = As[buf][kk][ty + NY * q];
 #pragma unroll
-            for (int q = 0; q < TN; ++q) b[q] = Bs[buf][kk][tx + 16 * q];
+            for (int q = 0; q < TN; ++q) b[q] = Bs[buf][kk][tx + NX * q];
 #pragma unroll
             for (int qa = 0; qa < TM; ++qa)
 #pragma unroll
@@ -229,11 +254,11 @@ __global__ void __launch_bounds__(GEMM_THREADS, 2)
     }
 #pragma unroll
     for (int qa = 0; qa < TM; ++qa) {
-        const int gi = i0 + ty + 16 * qa;
+        const int gi = i0 + ty + NY * qa;
         if (gi >= p.M) continue;
 #pragma unroll
         for (int qb = 0; qb < TN; ++qb) {
-            const int gj = j0 + tx + 16 * qb;
+            const int gj = j0 + tx + NX * qb;
             if (gj >= p.N) continue;
             store_c(p.C[gi * p.sc_i + gj * p.sc_j], acc[qa][qb], p.accumulate);
         }
@@ -255,11 +280,10 @@ template <typename TA, typename TB, typename TC> const char* gemm_name() {
 
 // Tile classes (BM x BN).  A problem takes the class that pads it least
 // (ties: the larger tile); the classes other than 64x64 are used only when
-// their short side covers the problem's M or N in one tile, so the tile count
-// never exceeds that of 64x64 tiles.
-constexpr int GEMM_NCLS = 7;
-constexpr int GEMM_CLS_M[GEMM_NCLS] = {64, 16, 128, 64, 64, 32, 48};
-constexpr int GEMM_CLS_N[GEMM_NCLS] = {64, 128, 16, 32, 48, 64, 64};
+// their short side covers the problem's M or N in one tile.
+constexpr int GEMM_NCLS = 9;
+constexpr int GEMM_CLS_M[GEMM_NCLS] = {64, 16, 128, 64, 64, 32, 48, 4, 128};
+constexpr int GEMM_CLS_N[GEMM_NCLS] = {64, 128, 16, 32, 48, 64, 64, 128, 4};
 
 template <typename P> inline int gemm_class(const P& p) {
     int best = 0;
@@ -278,40 +302,51 @@ template <typename P> inline int gemm_class(const P& p) {
 }
 
 template <typename TA, typename TB, typename TC, int BM, int BN>
-void launch_gemm_class(const GemmProblem<TA, TB, TC>* dp, const GemmTile* dt, size_t b, size_t e, cudaStream_t st) {
-    if (e <= b) return;
-    gemm_tiles_kernel<TA, TB, TC, BM, BN><<<(unsigned)(e - b), GEMM_THREADS, 0, st>>>(dp, dt + b);
+void launch_gemm_class(const GemmProblem<TA, TB, TC>* dp, const int* d_index, size_t pb, size_t pe, int ntiles,
+                       cudaStream_t st) {
+    if (pe <= pb || ntiles <= 0) return;
+    gemm_tiles_kernel<TA, TB, TC, BM, BN><<<(unsigned)ntiles, GEMM_THREADS, 0, st>>>(dp + pb, d_index, (int)(pe - pb));
     check_launch("gemm_tiles_kernel");
 }
 
-// Host helper: upload problems + tile lists into scratch buffers and launch
-// one kernel per tile class.  Tile capacity computed for 64x64 tiles is an
-// upper bound for every class.
+// Host helper: upload the problems (grouped by tile class) and, per class, the
+// prefix sums of their tile counts into scratch buffers, and launch one kernel
+// per tile class.  The index needs gemm_index_bytes(probs.size()) bytes.
 template <typename TA, typename TB, typename TC>
 void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* d_probs, size_t probs_cap,
-                       void* d_tiles, size_t tiles_cap, cudaStream_t st) {
+                       void* d_index, size_t index_cap, cudaStream_t st) {
     if (probs.empty()) return;
-    std::vector<GemmTile> tiles;
-    size_t start[GEMM_NCLS + 1] = {};
+    std::vector<GemmProblem<TA, TB, TC>> sorted;
+    sorted.reserve(probs.size());
+    std::vector<int> index;  // per class: prefix over its problems, then the total
+    index.reserve(probs.size() + 2 * GEMM_NCLS);
+    size_t pstart[GEMM_NCLS + 1] = {}, istart[GEMM_NCLS] = {};
+    int ntiles[GEMM_NCLS] = {};
     std::vector<int> cls(probs.size());
     for (size_t q = 0; q < probs.size(); ++q) cls[q] = gemm_class(probs[q]);
     for (int c = 0; c < GEMM_NCLS; ++c) {
-        start[c] = tiles.size();
+        pstart[c] = sorted.size();
+        istart[c] = index.size();
+        long t = 0;
         for (size_t q = 0; q < probs.size(); ++q) {
-            if (probs[q].M <= 0 || probs[q].N <= 0 || cls[q] != c) continue;
-            const int tm = ceil_div(probs[q].M, GEMM_CLS_M[c]), tn = ceil_div(probs[q].N, GEMM_CLS_N[c]);
-            for (int a = 0; a < tm; ++a)
-                for (int b = 0; b < tn; ++b) tiles.push_back(GemmTile{(int)q, a, b, 0});
+            const auto& g = probs[q];
+            if (g.M <= 0 || g.N <= 0 || cls[q] != c) continue;
+            sorted.push_back(g);
+            index.push_back((int)t);
+            t += (long)std::max(g.nb, 1) * ceil_div(g.M, GEMM_CLS_M[c]) * ceil_div(g.N, GEMM_CLS_N[c]);
         }
+        PGX_CHECK(t < (1L << 31), PGX_ERR_ARG, "gemm batch too large");
+        index.push_back((int)t);
+        ntiles[c] = (int)t;
     }
-    start[GEMM_NCLS] = tiles.size();
-    if (tiles.empty()) return;
-    PGX_CHECK(probs.size() * sizeof(probs[0]) <= probs_cap, PGX_ERR_ARG, "gemm problem list overflow");
-    PGX_CHECK(tiles.size() * sizeof(GemmTile) <= tiles_cap, PGX_ERR_ARG, "gemm tile list overflow");
-    PGX_CUDA(cudaMemcpyAsync(d_probs, probs.data(), probs.size() * sizeof(probs[0]), cudaMemcpyHostToDevice, st));
-    PGX_CUDA(cudaMemcpyAsync(d_tiles, tiles.data(), tiles.size() * sizeof(GemmTile), cudaMemcpyHostToDevice, st));
+    pstart[GEMM_NCLS] = sorted.size();
+    if (sorted.empty()) return;
+    PGX_CHECK(sorted.size() * sizeof(sorted[0]) <= probs_cap, PGX_ERR_ARG, "gemm problem list overflow");
+    PGX_CHECK(index.size() * sizeof(int) <= index_cap, PGX_ERR_ARG, "gemm tile index overflow");
+    h2d(d_probs, sorted.data(), sorted.size() * sizeof(sorted[0]), st);
+    h2d(d_index, index.data(), index.size() * sizeof(int), st);
     const auto* dp = static_cast<const GemmProblem<TA, TB, TC>*>(d_probs);
-    const auto* dt = static_cast<const GemmTile*>(d_tiles);
+    const int* di = static_cast<const int*>(d_index);
     // real x real 2, real x complex 4, complex x complex 8 operations per product term;
     // minimum traffic: A, B and C once (C twice when accumulating)
     using VA = typename val_t<TA>::type;
@@ -319,19 +354,23 @@ void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* 
     constexpr double mac = (is_cd<VA>::value && is_cd<VB>::value) ? 8.0
                            : (is_cd<VA>::value || is_cd<VB>::value) ? 4.0 : 2.0;
     double fl = 0.0, by = 0.0;
-    for (const auto& q : probs) {
-        fl += mac * q.M * (double)q.N * q.K;
-        by += (double)q.M * q.K * sizeof(typename src_t<TA>::type) + (double)q.K * q.N * sizeof(typename src_t<TB>::type) +
-              (q.accumulate ? 2.0 : 1.0) * q.M * (double)q.N * sizeof(TC);
+    for (const auto& q : sorted) {
+        const double nb = std::max(q.nb, 1);
+        fl += nb * mac * q.M * (double)q.N * q.K;
+        by += nb * ((double)q.M * q.K * sizeof(typename src_t<TA>::type) +
+                    (double)q.K * q.N * sizeof(typename src_t<TB>::type) +
+                    (q.accumulate ? 2.0 : 1.0) * q.M * (double)q.N * sizeof(TC));
     }
     ProfRange pr(gemm_name<TA, TB, TC>(), st, fl, by);
-    launch_gemm_class<TA, TB, TC, 64, 64>(dp, dt, start[0], start[1], st);
-    launch_gemm_class<TA, TB, TC, 16, 128>(dp, dt, start[1], start[2], st);
-    launch_gemm_class<TA, TB, TC, 128, 16>(dp, dt, start[2], start[3], st);
-    launch_gemm_class<TA, TB, TC, 64, 32>(dp, dt, start[3], start[4], st);
-    launch_gemm_class<TA, TB, TC, 64, 48>(dp, dt, start[4], start[5], st);
-    launch_gemm_class<TA, TB, TC, 32, 64>(dp, dt, start[5], start[6], st);
-    launch_gemm_class<TA, TB, TC, 48, 64>(dp, dt, start[6], start[7], st);
+    launch_gemm_class<TA, TB, TC, 64, 64>(dp, di + istart[0], pstart[0], pstart[1], ntiles[0], st);
+    launch_gemm_class<TA, TB, TC, 16, 128>(dp, di + istart[1], pstart[1], pstart[2], ntiles[1], st);
+    launch_gemm_class<TA, TB, TC, 128, 16>(dp, di + istart[2], pstart[2], pstart[3], ntiles[2], st);
+    launch_gemm_class<TA, TB, TC, 64, 32>(dp, di + istart[3], pstart[3], pstart[4], ntiles[3], st);
+    launch_gemm_class<TA, TB, TC, 64, 48>(dp, di + istart[4], pstart[4], pstart[5], ntiles[4], st);
+    launch_gemm_class<TA, TB, TC, 32, 64>(dp, di + istart[5], pstart[5], pstart[6], ntiles[5], st);
+    launch_gemm_class<TA, TB, TC, 48, 64>(dp, di + istart[6], pstart[6], pstart[7], ntiles[6], st);
+    launch_gemm_class<TA, TB, TC, 4, 128>(dp, di + istart[7], pstart[7], pstart[8], ntiles[7], st);
+    launch_gemm_class<TA, TB, TC, 128, 4>(dp, di + istart[8], pstart[8], pstart[9], ntiles[8], st);
 }
 
 }  // namespace pgx

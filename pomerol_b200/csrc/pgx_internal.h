@@ -87,6 +87,8 @@ struct Problem {
 
     DevBuf H, work, work2, U, E, w, dims_d, moff_d, eoff_d, order_d, status, tri, tri_items, eigh_gemm,
         eigh_scratch;
+    DevBuf op_probs, op_tiles, op_meta;  // descriptor lists of operator rotation / adjoint
+    std::vector<double> w_host;          // host copy of the weights (set with them)
     int* d_dims = nullptr;
     long* d_moff = nullptr;
     long* d_eoff = nullptr;
@@ -105,6 +107,30 @@ struct Problem {
 struct G2Timing {
     double total_ms = 0, gemm_ms = 0, gemm_flops = 0;
 };
+
+// Pinned host staging for descriptor uploads.  Append-only while copies from
+// it may be pending, so the source of every asynchronous copy stays intact
+// until the copy has run; recycled at the end of an entry-point call whose
+// stream is idle (every call that returns results ends that way).  Blocks are
+// kept across calls.
+struct HostArena {
+    std::vector<std::pair<char*, size_t>> blocks;  // (pinned pointer, capacity)
+    size_t cur = 0, used = 0;                      // block in use, bytes used in it
+    bool dirty = false;                            // copies may be pending
+    void* put(const void* src, size_t n);
+    void recycle(cudaStream_t st);
+    HostArena() = default;
+    HostArena(const HostArena&) = delete;
+    HostArena& operator=(const HostArena&) = delete;
+    ~HostArena();
+};
+
+// Arena of the context whose entry point runs on this thread (or null).
+HostArena*& active_arena();
+
+// Host-to-device copy of a descriptor list on stream st: staged through the
+// active context's pinned arena (fully asynchronous), else a pageable copy.
+void h2d(void* dst, const void* src, size_t bytes, cudaStream_t st);
 
 // Per-kernel device times of a context, on request (pgx_profile_begin/end):
 // each instrumented launch site brackets its kernel with an event pair on the
@@ -157,6 +183,7 @@ struct pgx_ctx {
     pgx::Problem P;
     pgx::G2Timing g2t;
     pgx::Profiler prof;
+    pgx::HostArena arena;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
     // side streams (and their fork / join events) for independent launches
     cudaStream_t aux[3] = {nullptr, nullptr, nullptr};

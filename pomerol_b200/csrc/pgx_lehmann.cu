@@ -200,7 +200,9 @@ void launch_weights(Problem& P, double beta, cudaStream_t st) {
     weights_kernel<<<1, 1024, 0, st>>>(P.d_E, P.d_w, P.esize, beta, tmp);
     check_launch("weights_kernel");
     double h[2];
+    P.w_host.resize(P.esize);
     PGX_CUDA(cudaMemcpyAsync(h, tmp, sizeof(h), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaMemcpyAsync(P.w_host.data(), P.d_w, P.esize * sizeof(double), cudaMemcpyDeviceToHost, st));
     PGX_CUDA(cudaStreamSynchronize(st));
     P.E0 = h[0];
     P.Z = h[1];
@@ -217,10 +219,9 @@ void rotate_operator(Problem& P, Operator& op, cudaStream_t st) {
     const int np = (int)op.parts.size();
     const size_t esz = P.is_complex ? sizeof(cd) : sizeof(double);
     op.mat.reserve(std::max<long>(op.total, 1) * esz);
-    DevBuf probs_b, tiles_b;
-    long ntiles = 0;
-    for (auto& pt : op.parts) ntiles += (long)ceil_div(pt.dl, GEMM_BM) * ceil_div(pt.dr, GEMM_BN);
-    tiles_b.reserve(std::max<long>(ntiles, 1) * sizeof(GemmTile));
+    DevBuf& probs_b = P.op_probs;
+    DevBuf& tiles_b = P.op_tiles;
+    tiles_b.reserve(gemm_index_bytes(op.parts.size()));
     const int* kA = op.target.as<int>();
     const int* kB = kA + op.act_off.back();
     const double* ks = op.coef.as<double>();
@@ -277,9 +278,6 @@ void rotate_operator(Problem& P, Operator& op, cudaStream_t st) {
         probs_b.reserve(probs.size() * sizeof(probs[0]));
         launch_gemm_batch(probs, probs_b.p, probs_b.bytes, tiles_b.p, tiles_b.bytes, st);
     }
-    PGX_CUDA(cudaStreamSynchronize(st));
-    probs_b.release();
-    tiles_b.release();
     op.rotated = true;
     op.is_complex = P.is_complex;
 }
@@ -311,14 +309,13 @@ void adjoint_operator(Problem& P, const Operator& src, Operator& dst, cudaStream
         cols[q] = src.parts[q].dr;
         maxe = std::max(maxe, rows[q] * cols[q]);
     }
-    DevBuf meta;
+    DevBuf& meta = P.op_meta;
     meta.reserve(np * (2 * sizeof(long) + 2 * sizeof(int)) + 64);
     char* m = meta.as<char>();
-    PGX_CUDA(cudaMemcpyAsync(m, so.data(), np * sizeof(long), cudaMemcpyHostToDevice, st));
-    PGX_CUDA(cudaMemcpyAsync(m + np * sizeof(long), dof.data(), np * sizeof(long), cudaMemcpyHostToDevice, st));
-    PGX_CUDA(cudaMemcpyAsync(m + 2 * np * sizeof(long), rows.data(), np * sizeof(int), cudaMemcpyHostToDevice, st));
-    PGX_CUDA(cudaMemcpyAsync(m + 2 * np * sizeof(long) + np * sizeof(int), cols.data(), np * sizeof(int),
-                             cudaMemcpyHostToDevice, st));
+    h2d(m, so.data(), np * sizeof(long), st);
+    h2d(m + np * sizeof(long), dof.data(), np * sizeof(long), st);
+    h2d(m + 2 * np * sizeof(long), rows.data(), np * sizeof(int), st);
+    h2d(m + 2 * np * sizeof(long) + np * sizeof(int), cols.data(), np * sizeof(int), st);
     if (np > 0) {
         dim3 grid(std::min(ceil_div(maxe, 256), 1024), np);
         const long* dso = reinterpret_cast<const long*>(m);
@@ -332,8 +329,6 @@ void adjoint_operator(Problem& P, const Operator& src, Operator& dst, cudaStream
                                                          dcols, np);
         check_launch("adjoint_kernel");
     }
-    PGX_CUDA(cudaStreamSynchronize(st));
-    meta.release();
     dst.rotated = true;
     dst.is_complex = P.is_complex;
 }
@@ -372,8 +367,8 @@ static void run_pair(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* ou
     bz.reserve(std::max(nz, 1) * sizeof(cd));
     bout.reserve((std::max(nz, 1) + 1) * sizeof(cd));
     if (!pp.empty())
-        PGX_CUDA(cudaMemcpyAsync(bparts.p, pp.data(), pp.size() * sizeof(PairPart), cudaMemcpyHostToDevice, st));
-    if (nz > 0) PGX_CUDA(cudaMemcpyAsync(bz.p, z, nz * sizeof(cd), cudaMemcpyHostToDevice, st));
+        h2d(bparts.p, pp.data(), pp.size() * sizeof(PairPart), st);
+    if (nz > 0) h2d(bz.p, z, nz * sizeof(cd), st);
     PGX_CUDA(cudaMemsetAsync(bout.p, 0, (nz + 1) * sizeof(cd), st));
     cd* d_out = bout.as<cd>();
     double* d_zero = reinterpret_cast<double*>(d_out + nz);
@@ -452,9 +447,9 @@ void run_ensemble_average(pgx_ctx* c, int op, double* out) {
     int* d_dims = reinterpret_cast<int*>(d_eo + n);
     PGX_CUDA(cudaMemsetAsync(d_out, 0, 2 * sizeof(double), st));
     if (n > 0) {
-        PGX_CUDA(cudaMemcpyAsync(d_offs, offs.data(), n * sizeof(long), cudaMemcpyHostToDevice, st));
-        PGX_CUDA(cudaMemcpyAsync(d_eo, eo.data(), n * sizeof(long), cudaMemcpyHostToDevice, st));
-        PGX_CUDA(cudaMemcpyAsync(d_dims, dims.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
+        h2d(d_offs, offs.data(), n * sizeof(long), st);
+        h2d(d_eo, eo.data(), n * sizeof(long), st);
+        h2d(d_dims, dims.data(), n * sizeof(int), st);
         if (P.is_complex)
             ensemble_kernel<cd><<<n, 128, 0, st>>>(A.mat.as<cd>(), d_offs, d_eo, d_dims, n, P.d_w, d_out);
         else

@@ -119,7 +119,7 @@ extern "C" int pgx_eigh_noalloc(const double* H, int32_t n, double* E, double* U
         d.U = U;
         d.E = E;
         d.status = &meta->status;
-        pgx::launch_eigh_raw(d, dims, {0L}, st);  // waits for the stream
+        pgx::launch_eigh_raw(d, dims, {0L}, st);
         int status = 0;
         PGX_CUDA(cudaMemcpyAsync(&status, &meta->status, sizeof(int), cudaMemcpyDeviceToHost, st));
         PGX_CUDA(cudaStreamSynchronize(st));
