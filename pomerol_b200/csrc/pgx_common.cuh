@@ -41,8 +41,9 @@ __host__ __device__ __forceinline__ cd div(cd a, cd b) { return a * inv(b); }
 // single precision): two steps bring the error to the double rounding level.
 // Outside [1e-30, 1e30] (where the seed could leave the single-precision
 // range) the IEEE division is used.
-// The iteration alone, valid for x in [1e-30, 1e30]; callers that test the
-// range once for several values keep their arithmetic free of branches.
+// The iteration alone, valid for |x| in [1e-30, 1e30] (either sign); callers
+// that test the range once for several values keep their arithmetic free of
+// branches.
 __device__ __forceinline__ double recip_newton(double x) {
     float xf = (float)x, yf;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(yf) : "f"(xf));
@@ -52,7 +53,10 @@ __device__ __forceinline__ double recip_newton(double x) {
     e = fma(-x, y, 1.0);
     return fma(y, e, y);
 }
-__device__ __forceinline__ bool recip_in_range(double x) { return x > 1e-30 && x < 1e30; }
+__device__ __forceinline__ bool recip_in_range(double x) {
+    const double a = fabs(x);
+    return a > 1e-30 && a < 1e30;
+}
 __device__ __forceinline__ double recip_pos(double x) { return recip_in_range(x) ? recip_newton(x) : 1.0 / x; }
 // 1/a = conj(a) / |a|^2 with recip_pos for the real reciprocal.
 __device__ __forceinline__ cd inv_fast(cd a) {

@@ -364,7 +364,7 @@ __global__ void __launch_bounds__(CL_THREADS) eigh_cluster_kernel(ClusterArgs g)
 // error).  Exact degeneracies of H show up as such splits, so eigenvectors of
 // different pieces are orthogonal by support.
 //   * eigenvalues: bisection with Sturm counts, one thread per eigenvalue
-//     (Golub & Van Loan, 8.4.1);
+//     (Golub & Van Loan, 8.4.1), as 32-point multisection by one warp;
 //   * eigenvectors: inverse iteration, one thread per chain of eigenvalues
 //     whose neighbours are closer than 1e-4 ||T|| (Golub & Van Loan, 8.2.2;
 //     Wilkinson's scheme as in LAPACK's stein).  Each solve factors
@@ -402,7 +402,7 @@ constexpr int INV_ITERS = 2;        // inverse iterations (one more for chain me
 // Loads d and e of one block into shared memory, zeroes the split points and
 // returns ||T|| (max row sum); every thread of the CTA must call it.
 __device__ double load_tri(const double* tri, long eo, int n, double* d, double* e) {
-    __shared__ double red[TRI_THREADS / 32];
+    __shared__ double red[32];
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         d[i] = tri[2 * eo + i];
         e[i] = (i < n - 1) ? tri[2 * eo + n + i] : 0.0;
@@ -422,6 +422,19 @@ __device__ double load_tri(const double* tri, long eo, int n, double* d, double*
     return tn;
 }
 
+__device__ void piece_of(const double* e, int n, int j, int& a, int& b) {
+    a = j;
+    b = j;
+    while (a > 0 && e[a - 1] != 0.0) --a;
+    while (b < n - 1 && e[b] != 0.0) ++b;
+}
+
+// Multisection with one warp per eigenvalue: each round the 32 lanes take the
+// Sturm counts at 32 equally spaced interior points of the bracketing
+// interval, narrowing it 33-fold (about 11 rounds to full precision).
+constexpr int BIS_WARPS = 8;  // eigenvalues per CTA
+constexpr int BIS_THREADS = 32 * BIS_WARPS;
+
 // number of eigenvalues of T[a..b] below x
 __device__ int sturm(const double* d, const double* e, int a, int b, double x, double pivmin) {
     double q = d[a] - x;
@@ -435,45 +448,47 @@ __device__ int sturm(const double* d, const double* e, int a, int b, double x, d
     return cnt;
 }
 
-__device__ void piece_of(const double* e, int n, int j, int& a, int& b) {
-    a = j;
-    b = j;
-    while (a > 0 && e[a - 1] != 0.0) --a;
-    while (b < n - 1 && e[b] != 0.0) ++b;
-}
-
-__global__ void __launch_bounds__(TRI_THREADS) bisect_kernel(TriArgs g) {
+__global__ void __launch_bounds__(BIS_THREADS) bisect_kernel(TriArgs g, const TriItem* bitems) {
     extern __shared__ double sh[];
-    const TriItem it = g.items[blockIdx.x];
+    const TriItem it = bitems[blockIdx.x];
     const int n = g.dims[it.block];
     const long eo = g.eoff[it.block];
     double* d = sh;
     double* e = sh + n;
     load_tri(g.tri, eo, n, d, e);
-    for (int j = it.j0 + threadIdx.x; j < it.j1; j += blockDim.x) {
-        int a, b;
-        piece_of(e, n, j, a, b);
-        double lo = 1e300, hi = -1e300, em = 0.0;
-        for (int i = a; i <= b; ++i) {
-            const double r = (i > a ? fabs(e[i - 1]) : 0.0) + (i < b ? fabs(e[i]) : 0.0);
-            lo = fmin(lo, d[i] - r);
-            hi = fmax(hi, d[i] + r);
-            if (i < b) em = fmax(em, e[i] * e[i]);
-        }
-        const double pivmin = SAFE_MIN * fmax(1.0, em);
-        const double gn = fmax(fabs(lo), fabs(hi));
-        const double w = 2.0 * EPS * gn + pivmin;
-        lo -= w;
-        hi += w;
-        const double atol = 0.25 * EPS * gn + pivmin;
-        const int k = j - a;
-        for (int iter = 0; iter < 256; ++iter) {
-            if (hi - lo <= atol + 2.0 * EPS * fmin(fabs(lo), fabs(hi))) break;
-            const double mid = 0.5 * (lo + hi);
-            if (mid <= lo || mid >= hi) break;
-            if (sturm(d, e, a, b, mid, pivmin) > k) hi = mid;
-            else lo = mid;
-        }
+    const int lane = threadIdx.x & 31;
+    const int j = it.j0 + (int)(threadIdx.x >> 5);
+    if (j >= it.j1) return;
+    int a, b;
+    piece_of(e, n, j, a, b);
+    double lo = 1e300, hi = -1e300, em = 0.0;
+    for (int i = a; i <= b; ++i) {
+        const double r = (i > a ? fabs(e[i - 1]) : 0.0) + (i < b ? fabs(e[i]) : 0.0);
+        lo = fmin(lo, d[i] - r);
+        hi = fmax(hi, d[i] + r);
+        if (i < b) em = fmax(em, e[i] * e[i]);
+    }
+    const double pivmin = SAFE_MIN * fmax(1.0, em);
+    const double gn = fmax(fabs(lo), fabs(hi));
+    const double w = 2.0 * EPS * gn + pivmin;
+    lo -= w;
+    hi += w;
+    const double atol = 0.25 * EPS * gn + pivmin;
+    const int k = j - a;
+    // every lane holds the same lo, hi: the loop and its exits are warp-uniform
+    for (int round = 0; round < 64; ++round) {
+        if (hi - lo <= atol + 2.0 * EPS * fmin(fabs(lo), fabs(hi))) break;
+        const double step = (hi - lo) / 33.0;
+        if (!(lo + step > lo && lo + step * 32.0 < hi)) break;  // interval at the resolution of doubles
+        const int cnt = sturm(d, e, a, b, lo + step * (lane + 1), pivmin);
+        // counts grow with x: the eigenvalue lies between point `below` and `below + 1`
+        const int below = __popc(__ballot_sync(0xffffffffu, cnt <= k));
+        const double nlo = (below > 0) ? lo + step * below : lo;
+        const double nhi = (below < 32) ? lo + step * (below + 1) : hi;
+        lo = nlo;
+        hi = nhi;
+    }
+    if (lane == 0) {
         g.lam[eo + j] = 0.5 * (lo + hi);
         g.sb[2 * eo + j] = a;
         g.sb[2 * eo + n + j] = b;
@@ -609,13 +624,20 @@ __global__ void __launch_bounds__(TRI_THREADS) vector_kernel(TriArgs g) {
 
 }  // namespace
 
-static void tri_plan(const std::vector<int>& dims, std::vector<TriItem>& items) {
+// Work items, largest blocks first: vector_kernel takes TRI_THREADS
+// eigen-indices per CTA, bisect_kernel BIS_WARPS; both lists go into one
+// descriptor upload (vector items, then bisection items).
+static void tri_plan(const std::vector<int>& dims, std::vector<TriItem>& items, size_t* n_vec = nullptr) {
     std::vector<int> order(dims.size());
     for (size_t b = 0; b < dims.size(); ++b) order[b] = (int)b;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return dims[x] > dims[y]; });
     for (int b : order)
         for (int j0 = 0; j0 < dims[b]; j0 += TRI_THREADS)
             items.push_back(TriItem{b, j0, std::min(dims[b], j0 + TRI_THREADS), 0});
+    if (n_vec) *n_vec = items.size();
+    for (int b : order)
+        for (int j0 = 0; j0 < dims[b]; j0 += BIS_WARPS)
+            items.push_back(TriItem{b, j0, std::min(dims[b], j0 + BIS_WARPS), 0});
 }
 
 constexpr int CL_SIZES[4] = {1, 2, 4, 8};
@@ -665,7 +687,9 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     for (int x : dims) dmax = std::max(dmax, x);
     // descriptors: bisection items and the Householder block lists, one upload
     std::vector<TriItem> items;
-    tri_plan(dims, items);
+    size_t n_vec = 0;
+    tri_plan(dims, items, &n_vec);
+    const size_t n_bis = items.size() - n_vec;
     HhPlan hp = hh_plan(dims);
     // a cluster size the device cannot schedule falls back to the global-memory kernel
     ClusterArgs ca;
@@ -794,6 +818,7 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     t.E = d.E;
     t.status = d.status;
     const size_t smem_b = 2 * sizeof(double) * (size_t)dmax, smem_v = 3 * sizeof(double) * (size_t)dmax;
+    const TriItem* bis_items = static_cast<const TriItem*>(d.items) + n_vec;
     PGX_CUDA(cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
     PGX_CUDA(cudaFuncSetAttribute(vector_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_v));
     double esum = 0.0, msum = 0.0;
@@ -803,12 +828,12 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     }
     {
         ProfRange pr("bisect_kernel", st, 0.0, 16.0 * esum + 8.0 * esum + 8.0 * esum);
-        bisect_kernel<<<(unsigned)items.size(), TRI_THREADS, smem_b, st>>>(t);
+        bisect_kernel<<<(unsigned)n_bis, BIS_THREADS, smem_b, st>>>(t, bis_items);
         check_launch("bisect_kernel");
     }
     {
         ProfRange pr("vector_kernel", st, 0.0, 8.0 * msum + 48.0 * esum);
-        vector_kernel<<<(unsigned)items.size(), TRI_THREADS, smem_v, st>>>(t);
+        vector_kernel<<<(unsigned)n_vec, TRI_THREADS, smem_v, st>>>(t);
         check_launch("vector_kernel");
     }
 

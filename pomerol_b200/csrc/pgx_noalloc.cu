@@ -32,7 +32,7 @@ namespace {
 constexpr long NA_N = PGX_NOALLOC_MAX_DIM;
 // layout in doubles:
 //   A (n^2) | Zc (n^2) | S (3 n^2) | tri (2n) | lam (n) | sb, rank (3n ints = 2n doubles)
-//   | bisection items (32) | GEMM problem (32) | GEMM tiles (64) | descriptors (8)
+//   | work items (128) | GEMM problem (32) | GEMM tile index (64) | descriptors (8)
 constexpr long NA_A = 0;
 constexpr long NA_ZC = NA_A + NA_N * NA_N;
 constexpr long NA_S = NA_ZC + NA_N * NA_N;
@@ -40,7 +40,7 @@ constexpr long NA_TRI = NA_S + 3 * NA_N * NA_N;
 constexpr long NA_LAM = NA_TRI + 2 * NA_N;
 constexpr long NA_INT = NA_LAM + NA_N;
 constexpr long NA_ITEMS = NA_INT + 2 * NA_N;
-constexpr long NA_GPROB = NA_ITEMS + 32;
+constexpr long NA_GPROB = NA_ITEMS + 128;
 constexpr long NA_GTILE = NA_GPROB + 32;
 constexpr long NA_META = NA_GTILE + 64;
 constexpr long NA_TOTAL = NA_META + 8;
@@ -95,7 +95,7 @@ extern "C" int pgx_eigh_noalloc(const double* H, int32_t n, double* E, double* U
     try {
         const std::vector<int> dims{n};
         size_t tile_bytes = 0;
-        PGX_CHECK(pgx::eigh_item_bytes(dims) <= 32 * sizeof(double), PGX_ERR_ARG, "item list too long");
+        PGX_CHECK(pgx::eigh_item_bytes(dims) <= 128 * sizeof(double), PGX_ERR_ARG, "item list too long");
         PGX_CHECK(pgx::eigh_gemm_bytes(dims, &tile_bytes) <= 32 * sizeof(double) && tile_bytes <= 64 * sizeof(double),
                   PGX_ERR_ARG, "GEMM lists too long");
         NaMeta* meta = reinterpret_cast<NaMeta*>(base + NA_META);
