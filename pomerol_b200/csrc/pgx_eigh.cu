@@ -510,42 +510,80 @@ __device__ __forceinline__ double start_entry(int j, int i) {
 // the factorisation and the forward elimination share one sweep, the upper
 // factor's three diagonals are kept in u1, u2, u3 for the back substitution.
 // Pivots smaller than pfloor in magnitude are replaced by +-pfloor.
-__device__ void lu_solve(const double* d, const double* e, int a, int b, double lm, double pfloor, double* z,
-                         double* u1, double* u2, double* u3) {
+// Both sweeps are a chain of dependent divisions; the values the chain
+// passes on stay in registers, and the vector entries each sweep reads are
+// loaded LU_BATCH rows ahead, so a batch waits for memory once.
+constexpr int LU_BATCH = 8;
+
+__device__ void lu_solve(const double* d, const double* e, int a, int b, double lm, double pfloor,
+                         double* __restrict__ z, double* __restrict__ u1, double* __restrict__ u2,
+                         double* __restrict__ u3) {
     double p = d[a] - lm, q = (a < b) ? e[a] : 0.0;
-    for (int k = a; k < b; ++k) {
-        const double sub = e[k], dn = d[k + 1] - lm, en = (k + 1 < b) ? e[k + 1] : 0.0;
-        const double zk = z[k], zk1 = z[k + 1];
-        double np, nq;
-        if (fabs(sub) > fabs(p)) {  // row interchange
-            const double l = p / sub;
-            u1[k] = sub;
-            u2[k] = dn;
-            u3[k] = en;
-            np = q - l * dn;
-            nq = -l * en;
-            z[k] = zk1;
-            z[k + 1] = zk - l * zk1;
-        } else {
-            const double l = (p != 0.0) ? sub / p : 0.0;
-            u1[k] = p;
-            u2[k] = q;
-            u3[k] = 0.0;
-            np = dn - l * q;
-            nq = en;
-            z[k + 1] = zk1 - l * zk;
+    double zk = z[a];
+    for (int k0 = a; k0 < b; k0 += LU_BATCH) {
+        double zn[LU_BATCH];
+#pragma unroll
+        for (int t = 0; t < LU_BATCH; ++t)
+            if (k0 + t < b) zn[t] = z[k0 + t + 1];
+#pragma unroll
+        for (int t = 0; t < LU_BATCH; ++t) {
+            const int k = k0 + t;
+            if (k >= b) break;
+            const double sub = e[k], dn = d[k + 1] - lm, en = (k + 1 < b) ? e[k + 1] : 0.0;
+            const double zk1 = zn[t];
+            double np, nq, zout, znext;
+            if (fabs(sub) > fabs(p)) {  // row interchange
+                const double l = p / sub;
+                u1[k] = sub;
+                u2[k] = dn;
+                u3[k] = en;
+                np = q - l * dn;
+                nq = -l * en;
+                zout = zk1;
+                znext = zk - l * zk1;
+            } else {
+                const double l = (p != 0.0) ? sub / p : 0.0;
+                u1[k] = p;
+                u2[k] = q;
+                u3[k] = 0.0;
+                np = dn - l * q;
+                nq = en;
+                zout = zk;
+                znext = zk1 - l * zk;
+            }
+            z[k] = zout;
+            zk = znext;
+            p = np;
+            q = nq;
         }
-        p = np;
-        q = nq;
     }
-    u1[b] = p;
-    for (int k = b; k >= a; --k) {
-        double piv = u1[k];
-        if (fabs(piv) < pfloor) piv = (piv >= 0.0) ? pfloor : -pfloor;
-        double r = z[k];
-        if (k + 1 <= b) r -= u2[k] * z[k + 1];
-        if (k + 2 <= b) r -= u3[k] * z[k + 2];
-        z[k] = r / piv;
+    // back substitution; x1, x2 carry the two solution entries below row k
+    double x1 = 0.0, x2 = 0.0;
+    for (int k0 = b; k0 >= a; k0 -= LU_BATCH) {
+        double v1[LU_BATCH], v2[LU_BATCH], v3[LU_BATCH], vz[LU_BATCH];
+#pragma unroll
+        for (int t = 0; t < LU_BATCH; ++t) {
+            const int k = k0 - t;
+            if (k < a) break;
+            v1[t] = (k == b) ? p : u1[k];
+            vz[t] = (k == b) ? zk : z[k];
+            v2[t] = (k + 1 <= b) ? u2[k] : 0.0;
+            v3[t] = (k + 2 <= b) ? u3[k] : 0.0;
+        }
+#pragma unroll
+        for (int t = 0; t < LU_BATCH; ++t) {
+            const int k = k0 - t;
+            if (k < a) break;
+            double piv = v1[t];
+            if (fabs(piv) < pfloor) piv = (piv >= 0.0) ? pfloor : -pfloor;
+            double r = vz[t];
+            if (k + 1 <= b) r -= v2[t] * x1;
+            if (k + 2 <= b) r -= v3[t] * x2;
+            const double xk = r / piv;
+            z[k] = xk;
+            x2 = x1;
+            x1 = xk;
+        }
     }
 }
 
