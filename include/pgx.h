@@ -181,7 +181,7 @@ int pgx_g2_count(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, double 
  * application's caching pool or a fixed arena) and which must not let a
  * library call cudaMalloc/cudaFree: diagonalises ONE real symmetric block of
  * size n <= PGX_NOALLOC_MAX_DIM on buffers the caller owns, keeping its
- * workspace in a static device array of the library (about 2.5 MiB per GPU,
+ * workspace in a static device array of the library (about 3 MiB per GPU,
  * held until the process exits).  H (n*n, row-major, read only), E (n) and U
  * (n*n, row-major, eigenvectors as columns, ascending eigenvalues) are DEVICE
  * pointers; stream is a cudaStream_t (NULL: default stream).  The call waits

@@ -11,9 +11,10 @@
 //      (larger blocks).  Q is stored column-major.
 //   2. bisect_kernel, one thread per eigenvalue: bisection with Sturm counts
 //      on the unreduced pieces of T (8.4.1).
-//   3. vector_kernel, one thread per chain of close eigenvalues: inverse
-//      iteration with a partial-pivoting tridiagonal LU, modified Gram-Schmidt
-//      inside a chain; eigenvalues are ranked so that the output is ascending.
+//   3. vector_kernel, one thread per eigenvalue: inverse iteration with a
+//      partial-pivoting tridiagonal LU; ortho_kernel: modified Gram-Schmidt
+//      inside chains of close eigenvalues; eigenvalues are ranked so that the
+//      output is ascending.
 //   4. U = Q Z as one batched FP64 GEMM over all blocks.
 // A non-finite eigenvector sets a device status word instead of trapping.
 
@@ -365,16 +366,18 @@ __global__ void __launch_bounds__(CL_THREADS) eigh_cluster_kernel(ClusterArgs g)
 // different pieces are orthogonal by support.
 //   * eigenvalues: bisection with Sturm counts, one thread per eigenvalue
 //     (Golub & Van Loan, 8.4.1), as 32-point multisection by one warp;
-//   * eigenvectors: inverse iteration, one thread per chain of eigenvalues
-//     whose neighbours are closer than 1e-4 ||T|| (Golub & Van Loan, 8.2.2;
-//     Wilkinson's scheme as in LAPACK's stein).  Each solve factors
-//     T - lambda I by Gaussian elimination with partial pivoting; a chain
-//     member is orthogonalised (modified Gram-Schmidt, twice on the last
-//     pass) against earlier members closer than 1e-4 ||T||, and its shift is
-//     nudged above the previous one so that coincident eigenvalues get
-//     distinct vectors.  The start vector is a fixed hash of (index, row).
+//   * eigenvectors: two steps of inverse iteration, one thread per
+//     eigenvalue (Golub & Van Loan, 8.2.2).  Each solve factors T - lambda I
+//     by Gaussian elimination with partial pivoting.  In a chain of
+//     eigenvalues whose neighbours are closer than 1e-4 ||T|| the shifts are
+//     nudged apart, so coincident eigenvalues get distinct vectors, and a
+//     second kernel orthogonalises each member (modified Gram-Schmidt, twice)
+//     against the earlier members closer than 1e-4 ||T||; mixing only among
+//     such close eigenvalues keeps the residuals at the eps ||T|| level.  The
+//     start vector is a fixed hash of (index, row).
 struct TriItem {
     int block, j0, j1, pad;
+    long soff;  // vector_kernel: this CTA's scratch, 4 n TRI_THREADS doubles at S + soff
 };
 
 struct TriArgs {
@@ -387,17 +390,17 @@ struct TriArgs {
     int* sb;            // per block: 2 n ints (first and last row of the piece)
     int* rank;          // per block: n ints (position in the ascending order)
     double* Z;          // per block: n x n column-major eigenvectors of T, sorted
-    double* S;          // per block: 3 n x n scratch (LU factors, 3 n per eigenvalue)
+    double* S;          // per vector_kernel CTA: 4 arrays of n x TRI_THREADS, thread-interleaved
     double* E;          // eigenvalues, ascending
     int* status;
 };
 
-constexpr int TRI_THREADS = 128;
+constexpr int TRI_THREADS = 32;  // vector_kernel: one warp per CTA, so the CTAs spread over all SMs
 constexpr double EPS = 2.220446049250313e-16;
 constexpr double SAFE_MIN = 2.2250738585072014e-308;
 constexpr double SPLIT_ABS = 8.0;   // absolute split threshold, units of eps ||T||
 constexpr double CHAIN_TOL = 1e-4;  // chain / orthogonalisation window, units of ||T||
-constexpr int INV_ITERS = 2;        // inverse iterations (one more for chain members)
+constexpr int INV_ITERS = 2;        // inverse iterations per eigenvector
 
 // Loads d and e of one block into shared memory, zeroes the split points and
 // returns ||T|| (max row sum); every thread of the CTA must call it.
@@ -512,46 +515,42 @@ __device__ __forceinline__ double start_entry(int j, int i) {
 // Pivots smaller than pfloor in magnitude are replaced by +-pfloor.
 // Both sweeps are a chain of dependent divisions; the values the chain
 // passes on stay in registers, and the vector entries each sweep reads are
-// loaded LU_BATCH rows ahead, so a batch waits for memory once.
+// loaded LU_BATCH rows ahead, so a batch waits for memory once.  Entry i of
+// each vector is at index i * st: the lanes of a warp interleave their
+// vectors, so a warp at the same row reads and writes one contiguous segment.
 constexpr int LU_BATCH = 8;
 
 __device__ void lu_solve(const double* d, const double* e, int a, int b, double lm, double pfloor,
                          double* __restrict__ z, double* __restrict__ u1, double* __restrict__ u2,
-                         double* __restrict__ u3) {
+                         double* __restrict__ u3, int st) {
     double p = d[a] - lm, q = (a < b) ? e[a] : 0.0;
-    double zk = z[a];
+    double zk = z[(long)a * st];
     for (int k0 = a; k0 < b; k0 += LU_BATCH) {
         double zn[LU_BATCH];
 #pragma unroll
         for (int t = 0; t < LU_BATCH; ++t)
-            if (k0 + t < b) zn[t] = z[k0 + t + 1];
+            if (k0 + t < b) zn[t] = z[(long)(k0 + t + 1) * st];
 #pragma unroll
         for (int t = 0; t < LU_BATCH; ++t) {
             const int k = k0 + t;
             if (k >= b) break;
             const double sub = e[k], dn = d[k + 1] - lm, en = (k + 1 < b) ? e[k + 1] : 0.0;
             const double zk1 = zn[t];
-            double np, nq, zout, znext;
-            if (fabs(sub) > fabs(p)) {  // row interchange
-                const double l = p / sub;
-                u1[k] = sub;
-                u2[k] = dn;
-                u3[k] = en;
-                np = q - l * dn;
-                nq = -l * en;
-                zout = zk1;
-                znext = zk - l * zk1;
-            } else {
-                const double l = (p != 0.0) ? sub / p : 0.0;
-                u1[k] = p;
-                u2[k] = q;
-                u3[k] = 0.0;
-                np = dn - l * q;
-                nq = en;
-                zout = zk;
-                znext = zk1 - l * zk;
-            }
-            z[k] = zout;
+            // row interchange when the sub-diagonal entry is the larger pivot; both
+            // cases share one division and are selected without branching
+            const bool sw = fabs(sub) > fabs(p);
+            const double num = sw ? p : sub, den = sw ? sub : p;
+            const double l = (den != 0.0) ? num / den : 0.0;
+            const double w1 = sw ? sub : p, w2 = sw ? dn : q, w3 = sw ? en : 0.0;
+            const double np = sw ? q - l * dn : dn - l * q;
+            const double nq = sw ? -l * en : en;
+            const double zout = sw ? zk1 : zk;
+            const double znext = sw ? zk - l * zk1 : zk1 - l * zk;
+            const long o = (long)k * st;
+            u1[o] = w1;
+            u2[o] = w2;
+            u3[o] = w3;
+            z[o] = zout;
             zk = znext;
             p = np;
             q = nq;
@@ -565,10 +564,11 @@ __device__ void lu_solve(const double* d, const double* e, int a, int b, double 
         for (int t = 0; t < LU_BATCH; ++t) {
             const int k = k0 - t;
             if (k < a) break;
-            v1[t] = (k == b) ? p : u1[k];
-            vz[t] = (k == b) ? zk : z[k];
-            v2[t] = (k + 1 <= b) ? u2[k] : 0.0;
-            v3[t] = (k + 2 <= b) ? u3[k] : 0.0;
+            const long o = (long)k * st;
+            v1[t] = (k == b) ? p : u1[o];
+            vz[t] = (k == b) ? zk : z[o];
+            v2[t] = (k + 1 <= b) ? u2[o] : 0.0;
+            v3[t] = (k + 2 <= b) ? u3[o] : 0.0;
         }
 #pragma unroll
         for (int t = 0; t < LU_BATCH; ++t) {
@@ -580,23 +580,27 @@ __device__ void lu_solve(const double* d, const double* e, int a, int b, double 
             if (k + 1 <= b) r -= v2[t] * x1;
             if (k + 2 <= b) r -= v3[t] * x2;
             const double xk = r / piv;
-            z[k] = xk;
+            z[(long)k * st] = xk;
             x2 = x1;
             x1 = xk;
         }
     }
 }
 
-// z /= ||z||; false when the norm is zero or not finite
-__device__ bool normalize(double* z, int a, int b) {
+// z /= ||z|| over rows a..b (stride st); false when the norm is zero or not finite
+__device__ bool normalize(double* z, int a, int b, int st) {
     double nn = 0.0;
-    for (int i = a; i <= b; ++i) nn = fma(z[i], z[i], nn);
+    for (int i = a; i <= b; ++i) nn = fma(z[(long)i * st], z[(long)i * st], nn);
     if (!(nn > 0.0) || !isfinite(nn)) return false;
     const double inv = rsqrt(nn);
-    for (int i = a; i <= b; ++i) z[i] *= inv;
+    for (int i = a; i <= b; ++i) z[(long)i * st] *= inv;
     return true;
 }
 
+// One thread per eigenvalue, the same work in every thread: two steps of
+// inverse iteration.  Within a chain (neighbours closer than CHAIN_TOL ||T||)
+// the shifts are nudged apart so coincident eigenvalues start from distinct
+// shifts; ortho_kernel then orthogonalises the members of each chain.
 __global__ void __launch_bounds__(TRI_THREADS) vector_kernel(TriArgs g) {
     extern __shared__ double sh[];
     const TriItem it = g.items[blockIdx.x];
@@ -613,50 +617,77 @@ __global__ void __launch_bounds__(TRI_THREADS) vector_kernel(TriArgs g) {
     const int* sa = g.sb + 2 * eo;
     const int* sbe = sa + n;
     double* Zb = g.Z + mo;
-    double* Sb = g.S + 3 * mo;
+    // this thread's working vector and LU diagonals, interleaved with the CTA's other threads
+    const int st = blockDim.x;
+    double* zt = g.S + it.soff + threadIdx.x;
+    double* u1 = zt + (long)n * st;
+    double* u2 = u1 + (long)n * st;
+    double* u3 = u2 + (long)n * st;
+    for (int j = it.j0 + threadIdx.x; j < it.j1; j += blockDim.x) {
+        const int a = sa[j], b = sbe[j];
+        // shift: the eigenvalue, raised above its chain predecessor's shift where they coincide
+        int h = j;
+        while (h > a && lam[h] - lam[h - 1] <= ortol) --h;
+        double lm = -1e308;
+        for (int t = h; t <= j; ++t) {
+            const double lt = lam[t], sep = 10.0 * EPS * fmax(fabs(lt), 1e-3 * tn);
+            lm = (t > h && lt < lm + sep) ? lm + sep : lt;
+        }
+        int rk = 0;
+        for (int i = 0; i < n; ++i) rk += (lam[i] < lam[j]) || (lam[i] == lam[j] && i < j);
+        g.rank[eo + j] = rk;
+        g.E[eo + rk] = lam[j];
+        double* z = Zb + (long)rk * n;
+        bool ok = true;
+        if (a == b) {
+            for (int i = 0; i < n; ++i) z[i] = (i == a) ? 1.0 : 0.0;
+        } else {
+            for (int i = a; i <= b; ++i) zt[(long)i * st] = start_entry(j, i);
+            for (int t = 0; t < INV_ITERS && ok; ++t) {
+                lu_solve(d, e, a, b, lm, pfloor, zt, u1, u2, u3, st);
+                ok = normalize(zt, a, b, st);
+            }
+            for (int i = 0; i < n; ++i) z[i] = (i >= a && i <= b) ? zt[(long)i * st] : 0.0;
+        }
+        if (!ok) atomicExch(g.status, PGX_ERR_NUMERIC);
+    }
+}
+
+// Modified Gram-Schmidt, applied twice, of each chain member against the
+// earlier members closer than CHAIN_TOL ||T||; one thread per chain head.
+__global__ void __launch_bounds__(TRI_THREADS) ortho_kernel(TriArgs g) {
+    extern __shared__ double sh[];
+    const TriItem it = g.items[blockIdx.x];
+    const int n = g.dims[it.block];
+    const long eo = g.eoff[it.block], mo = g.moff[it.block];
+    double* d = sh;
+    double* e = sh + n;
+    double* lam = sh + 2 * n;
+    const double tn = load_tri(g.tri, eo, n, d, e);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) lam[i] = g.lam[eo + i];
+    __syncthreads();
+    const double ortol = CHAIN_TOL * tn;
+    const int* sa = g.sb + 2 * eo;
+    const int* sbe = sa + n;
+    const int* rank = g.rank + eo;
+    double* Zb = g.Z + mo;
     for (int j = it.j0 + threadIdx.x; j < it.j1; j += blockDim.x) {
         const int a = sa[j], b = sbe[j];
         if (j > a && lam[j] - lam[j - 1] <= ortol) continue;  // not the head of a chain
-        int jend = j;
-        while (jend < b && lam[jend + 1] - lam[jend] <= ortol) ++jend;
-        double prev = -1e308;
-        for (int jj = j; jj <= jend; ++jj) {
-            double lm = lam[jj];
-            const double sep = 10.0 * EPS * fmax(fabs(lm), 1e-3 * tn);
-            if (jj > j && lm < prev + sep) lm = prev + sep;  // distinct shifts inside a chain
-            prev = lm;
-            int rk = 0;
-            for (int i = 0; i < n; ++i) rk += (lam[i] < lam[jj]) || (lam[i] == lam[jj] && i < jj);
-            g.rank[eo + jj] = rk;
-            g.E[eo + rk] = lam[jj];
-            double* z = Zb + (long)rk * n;
-            for (int i = 0; i < a; ++i) z[i] = 0.0;
-            for (int i = b + 1; i < n; ++i) z[i] = 0.0;
-            bool ok = true;
-            if (a == b) {
-                z[a] = 1.0;
-            } else {
-                double* u1 = Sb + (long)3 * jj * n;
-                double* u2 = u1 + n;
-                double* u3 = u2 + n;
-                for (int i = a; i <= b; ++i) z[i] = start_entry(jj, i);
-                const int iters = INV_ITERS + (jj > j ? 1 : 0);
-                for (int t = 0; t < iters && ok; ++t) {
-                    lu_solve(d, e, a, b, lm, pfloor, z, u1, u2, u3);
-                    const int passes = (t == iters - 1) ? 2 : 1;
-                    for (int pass = 0; pass < passes && ok; ++pass) {
-                        for (int pp = jj - 1; pp >= j && lam[jj] - lam[pp] <= ortol; --pp) {
-                            const double* qv = Zb + (long)g.rank[eo + pp] * n;
-                            double dot = 0.0;
-                            for (int i = a; i <= b; ++i) dot = fma(qv[i], z[i], dot);
-                            for (int i = a; i <= b; ++i) z[i] = fma(-dot, qv[i], z[i]);
-                        }
-                        ok = normalize(z, a, b);
-                    }
+        bool ok = true;
+        for (int jj = j + 1; jj <= b && lam[jj] - lam[jj - 1] <= ortol; ++jj) {
+            double* z = Zb + (long)rank[jj] * n;
+            for (int pass = 0; pass < 2 && ok; ++pass) {
+                for (int pp = jj - 1; pp >= j && lam[jj] - lam[pp] <= ortol; --pp) {
+                    const double* qv = Zb + (long)rank[pp] * n;
+                    double dot = 0.0;
+                    for (int i = a; i <= b; ++i) dot = fma(qv[i], z[i], dot);
+                    for (int i = a; i <= b; ++i) z[i] = fma(-dot, qv[i], z[i]);
                 }
+                ok = normalize(z, a, b, 1);
             }
-            if (!ok) atomicExch(g.status, PGX_ERR_NUMERIC);
         }
+        if (!ok) atomicExch(g.status, PGX_ERR_NUMERIC);
     }
 }
 
@@ -669,13 +700,23 @@ static void tri_plan(const std::vector<int>& dims, std::vector<TriItem>& items, 
     std::vector<int> order(dims.size());
     for (size_t b = 0; b < dims.size(); ++b) order[b] = (int)b;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return dims[x] > dims[y]; });
+    long soff = 0;
     for (int b : order)
-        for (int j0 = 0; j0 < dims[b]; j0 += TRI_THREADS)
-            items.push_back(TriItem{b, j0, std::min(dims[b], j0 + TRI_THREADS), 0});
+        for (int j0 = 0; j0 < dims[b]; j0 += TRI_THREADS) {
+            items.push_back(TriItem{b, j0, std::min(dims[b], j0 + TRI_THREADS), 0, soff});
+            soff += 4L * dims[b] * TRI_THREADS;
+        }
     if (n_vec) *n_vec = items.size();
     for (int b : order)
         for (int j0 = 0; j0 < dims[b]; j0 += BIS_WARPS)
-            items.push_back(TriItem{b, j0, std::min(dims[b], j0 + BIS_WARPS), 0});
+            items.push_back(TriItem{b, j0, std::min(dims[b], j0 + BIS_WARPS), 0, 0});
+}
+
+// doubles of vector_kernel scratch (EighDev::S)
+size_t eigh_vec_scratch_doubles(const std::vector<int>& dims) {
+    size_t s = 0;
+    for (int n : dims) s += 4 * (size_t)n * TRI_THREADS * ((n + TRI_THREADS - 1) / TRI_THREADS);
+    return std::max<size_t>(s, 1);
 }
 
 constexpr int CL_SIZES[4] = {1, 2, 4, 8};
@@ -859,6 +900,7 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     const TriItem* bis_items = static_cast<const TriItem*>(d.items) + n_vec;
     PGX_CUDA(cudaFuncSetAttribute(bisect_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
     PGX_CUDA(cudaFuncSetAttribute(vector_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_v));
+    PGX_CUDA(cudaFuncSetAttribute(ortho_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_v));
     double esum = 0.0, msum = 0.0;
     for (int n : dims) {
         esum += n;
@@ -873,6 +915,11 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
         ProfRange pr("vector_kernel", st, 0.0, 8.0 * msum + 48.0 * esum);
         vector_kernel<<<(unsigned)n_vec, TRI_THREADS, smem_v, st>>>(t);
         check_launch("vector_kernel");
+    }
+    {
+        ProfRange pr("ortho_kernel", st, 0.0, 0.0);
+        ortho_kernel<<<(unsigned)n_vec, TRI_THREADS, smem_v, st>>>(t);
+        check_launch("ortho_kernel");
     }
 
     // U = Q Z: Q column-major (Zc), Z column-major (A), U row-major
@@ -916,7 +963,7 @@ void launch_eigh(pgx_ctx* c) {
     size_t tiles_b = 0;
     const size_t probs_b = eigh_gemm_bytes(P.dims, &tiles_b);
     P.eigh_gemm.reserve(((probs_b + 255) & ~size_t(255)) + tiles_b);
-    P.eigh_scratch.reserve(3 * std::max<long>(P.msize, 1) * sizeof(double));
+    P.eigh_scratch.reserve(eigh_vec_scratch_doubles(P.dims) * sizeof(double));
     EighDev d;
     d.dims = P.d_dims;
     d.moff = P.d_moff;

@@ -208,7 +208,7 @@ struct EighDev {
     double* lam;         // workspace, sum d
     int* sb;             // workspace, 2 sum d
     int* rank;           // workspace, sum d
-    double* S;           // workspace, 3 sum d^2
+    double* S;           // workspace, eigh_vec_scratch_doubles(dims)
     void* items;         // workspace, eigh_item_bytes(dims)
     void* gemm_probs;    // workspace, eigh_gemm_bytes(dims, ...)
     void* gemm_tiles;    // workspace, tile bytes from eigh_gemm_bytes
@@ -222,6 +222,7 @@ struct EighDev {
 };
 size_t eigh_item_bytes(const std::vector<int>& dims);
 size_t eigh_gemm_bytes(const std::vector<int>& dims, size_t* tiles_bytes);
+size_t eigh_vec_scratch_doubles(const std::vector<int>& dims);
 void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::vector<long>& moff,
                      cudaStream_t st);
 void launch_weights(Problem& P, double beta, cudaStream_t st);

@@ -11,7 +11,7 @@
 // the tridiagonal), the accumulated factor, the inverse-iteration scratch,
 // the tridiagonal with its eigenvalues and index arrays, and the small
 // descriptor lists of one block of at most PGX_NOALLOC_MAX_DIM states
-// (about 2.5 MiB).  Every GPU that loads this
+// (about 3 MiB).  Every GPU that loads this
 // library holds it until the process exits.  All calls on a device share it
 // and it keeps the last call's contents: calls whose work overlaps on the GPU
 // (different streams, or host threads racing) corrupt each other and must be
@@ -31,12 +31,12 @@ namespace {
 
 constexpr long NA_N = PGX_NOALLOC_MAX_DIM;
 // layout in doubles:
-//   A (n^2) | Zc (n^2) | S (3 n^2) | tri (2n) | lam (n) | sb, rank (3n ints = 2n doubles)
+//   A (n^2) | Zc (n^2) | S (4 n^2) | tri (2n) | lam (n) | sb, rank (3n ints = 2n doubles)
 //   | work items (128) | GEMM problem (32) | GEMM tile index (64) | descriptors (8)
 constexpr long NA_A = 0;
 constexpr long NA_ZC = NA_A + NA_N * NA_N;
 constexpr long NA_S = NA_ZC + NA_N * NA_N;
-constexpr long NA_TRI = NA_S + 3 * NA_N * NA_N;
+constexpr long NA_TRI = NA_S + 4 * NA_N * NA_N;
 constexpr long NA_LAM = NA_TRI + 2 * NA_N;
 constexpr long NA_INT = NA_LAM + NA_N;
 constexpr long NA_ITEMS = NA_INT + 2 * NA_N;
@@ -96,6 +96,7 @@ extern "C" int pgx_eigh_noalloc(const double* H, int32_t n, double* E, double* U
         const std::vector<int> dims{n};
         size_t tile_bytes = 0;
         PGX_CHECK(pgx::eigh_item_bytes(dims) <= 128 * sizeof(double), PGX_ERR_ARG, "item list too long");
+        PGX_CHECK(pgx::eigh_vec_scratch_doubles(dims) <= (size_t)(NA_TRI - NA_S), PGX_ERR_ARG, "vector scratch too small");
         PGX_CHECK(pgx::eigh_gemm_bytes(dims, &tile_bytes) <= 32 * sizeof(double) && tile_bytes <= 64 * sizeof(double),
                   PGX_ERR_ARG, "GEMM lists too long");
         NaMeta* meta = reinterpret_cast<NaMeta*>(base + NA_META);
