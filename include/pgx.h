@@ -61,6 +61,27 @@ int pgx_set_blocks(pgx_ctx* ctx, int32_t nblocks, const int32_t* dims, int32_t i
  * elements, blocks in order.  Host -> device copy only. */
 int pgx_set_hamiltonian(pgx_ctx* ctx, const double* H);
 
+/* Assemble the block Hamiltonians on the device from their monomial terms
+ * (in place of pgx_set_hamiltonian; replaces the dense assembly of
+ * HamiltonianPart::prepare, HamiltonianPart.cpp:56-76).  Term t is the product
+ * of the operators ops[t*PGX_TERM_OPS .. t*PGX_TERM_OPS+PGX_TERM_OPS-1] read
+ * left to right (entry 2*mode + 1 for c^+_mode, 2*mode for c_mode, -1 to pad
+ * the tail) times the complex coefficient (coef[2t], coef[2t+1]; real blocks
+ * use the real part).  It acts on a Fock state from its rightmost operator,
+ * with the Jordan-Wigner sign (-1)^(occupied modes below) for each operator.
+ * fock lists the Fock state of every block position, blocks in the order of
+ * pgx_set_blocks (sum of dims entries); state_block[s] and state_inner[s]
+ * give, for every s < 2^nmodes, its block and position (nmodes <= 30).
+ * Returns PGX_ERR_ARG if the tables disagree or a term maps a state out of
+ * its block. */
+#define PGX_TERM_OPS 8
+int pgx_assemble_hamiltonian(pgx_ctx* ctx, int32_t nterms, const int32_t* ops, const double* coef, int32_t nmodes,
+                             const uint64_t* fock, const int32_t* state_block, const int32_t* state_inner);
+
+/* Copy the block Hamiltonians on the device (uploaded or assembled) to the
+ * host, packed like pgx_set_hamiltonian's input. */
+int pgx_get_hamiltonian(pgx_ctx* ctx, double* H);
+
 /* Diagonalise every block in one launch (FP64).  Eigenvalues ascending per
  * block; eigenvectors are the columns of each block's U.  The uploaded
  * Hamiltonian is kept, so this can be re-run. */

@@ -179,15 +179,22 @@ template <typename F> int guarded(pgx_ctx* c, F&& f) {
     }
 }
 
+// A new problem on the context: metadata is reset, device buffers keep their
+// capacity (DevBuf::reserve grows them when needed), so a context reused for
+// problems of similar size allocates and frees nothing.
 void reset_problem(pgx::Problem& P) {
-    for (auto* b : {&P.H, &P.work, &P.work2, &P.U, &P.E, &P.w, &P.dims_d, &P.moff_d, &P.eoff_d, &P.order_d, &P.status})
-        b->release();
-    for (auto& op : P.ops) {
-        op.mat.release();
-        op.target.release();
-        op.coef.release();
-    }
-    P = pgx::Problem();
+    pgx::Problem fresh;
+    pgx::DevBuf pgx::Problem::*bufs[] = {&pgx::Problem::H,       &pgx::Problem::work,      &pgx::Problem::work2,
+                                         &pgx::Problem::U,       &pgx::Problem::E,         &pgx::Problem::w,
+                                         &pgx::Problem::dims_d,  &pgx::Problem::moff_d,    &pgx::Problem::eoff_d,
+                                         &pgx::Problem::order_d, &pgx::Problem::status,    &pgx::Problem::tri,
+                                         &pgx::Problem::tri_items, &pgx::Problem::eigh_gemm, &pgx::Problem::eigh_scratch,
+                                         &pgx::Problem::op_probs, &pgx::Problem::op_tiles, &pgx::Problem::op_meta,
+                                         &pgx::Problem::asm_buf};
+    for (auto m : bufs) fresh.*m = std::move(P.*m);
+    fresh.spare_ops = std::move(P.spare_ops);
+    for (auto& op : P.ops) fresh.spare_ops.push_back(std::move(op));
+    P = std::move(fresh);
 }
 
 }  // namespace
@@ -307,6 +314,32 @@ int pgx_set_hamiltonian(pgx_ctx* c, const double* H) {
     });
 }
 
+int pgx_assemble_hamiltonian(pgx_ctx* c, int32_t nterms, const int32_t* ops, const double* coef, int32_t nmodes,
+                             const uint64_t* fock, const int32_t* state_block, const int32_t* state_inner) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.nblocks > 0, PGX_ERR_STATE, "pgx_set_blocks first");
+        PGX_CHECK(nterms >= 0 && (nterms == 0 || (ops && coef)), PGX_ERR_ARG, "bad term list");
+        PGX_CHECK(nmodes >= 0 && nmodes <= 30, PGX_ERR_ARG, "nmodes must be in [0, 30]");
+        PGX_CHECK(fock && state_block && state_inner, PGX_ERR_ARG, "null state table");
+        PGX_CHECK(P.esize <= (1L << nmodes), PGX_ERR_ARG, "more block states than Fock states");
+        pgx::assemble_hamiltonian(c, nterms, ops, coef, nmodes, fock, state_block, state_inner);
+        P.have_H = true;
+        P.have_eig = P.have_w = false;
+        for (auto& op : P.ops) op.rotated = false;
+    });
+}
+
+int pgx_get_hamiltonian(pgx_ctx* c, double* H) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.have_H && H, PGX_ERR_STATE, "no Hamiltonian on the device");
+        const size_t sc = P.is_complex ? 2 : 1;
+        PGX_CUDA(cudaMemcpyAsync(H, P.d_H, P.msize * sc * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+    });
+}
+
 int pgx_eigh(pgx_ctx* c) {
     return guarded(c, [&] {
         pgx::Problem& P = c->P;
@@ -385,7 +418,7 @@ int pgx_op_define(pgx_ctx* c, int32_t nparts, const int32_t* right_block, const 
         PGX_CHECK(P.nblocks > 0, PGX_ERR_STATE, "pgx_set_blocks first");
         PGX_CHECK(nparts >= 0 && op_id && (nparts == 0 || (right_block && left_block && target && coef)),
                   PGX_ERR_ARG, "bad operator description");
-        pgx::Operator op;
+        pgx::Operator op = pgx::take_operator(P);
         op.by_left.assign(P.nblocks, -1);
         op.by_right.assign(P.nblocks, -1);
         std::vector<int> kA, kB;
@@ -443,7 +476,7 @@ int pgx_op_adjoint(pgx_ctx* c, int32_t src, int32_t* op_id) {
         pgx::Problem& P = c->P;
         PGX_CHECK(src >= 0 && src < (int)P.ops.size() && op_id, PGX_ERR_ARG, "bad operator id");
         PGX_CHECK(P.ops[src].rotated, PGX_ERR_STATE, "rotate the source operator first");
-        pgx::Operator dst;
+        pgx::Operator dst = pgx::take_operator(P);
         pgx::adjoint_operator(P, P.ops[src], dst, c->stream);
         P.ops.push_back(std::move(dst));
         *op_id = (int32_t)P.ops.size() - 1;

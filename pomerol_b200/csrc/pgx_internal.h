@@ -88,6 +88,7 @@ struct Problem {
     DevBuf H, work, work2, U, E, w, dims_d, moff_d, eoff_d, order_d, status, tri, tri_items, eigh_gemm,
         eigh_scratch;
     DevBuf op_probs, op_tiles, op_meta;  // descriptor lists of operator rotation / adjoint
+    DevBuf asm_buf;                      // term list and state tables of the Hamiltonian assembly
     std::vector<double> w_host;          // host copy of the weights (set with them)
     int* d_dims = nullptr;
     long* d_moff = nullptr;
@@ -102,7 +103,22 @@ struct Problem {
     double* d_w = nullptr;
 
     std::vector<Operator> ops;
+    std::vector<Operator> spare_ops;  // released operators whose device buffers are reused
 };
+
+// An operator with the device buffers of a released one, if any.
+inline Operator take_operator(Problem& P) {
+    if (P.spare_ops.empty()) return Operator();
+    Operator op = std::move(P.spare_ops.back());
+    P.spare_ops.pop_back();
+    op.parts.clear();
+    op.by_left.clear();
+    op.by_right.clear();
+    op.act_off.clear();
+    op.rotated = op.is_complex = false;
+    op.total = 0;
+    return op;
+}
 
 struct G2Timing {
     double total_ms = 0, gemm_ms = 0, gemm_flops = 0;
@@ -226,6 +242,8 @@ size_t eigh_vec_scratch_doubles(const std::vector<int>& dims);
 void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::vector<long>& moff,
                      cudaStream_t st);
 void launch_weights(Problem& P, double beta, cudaStream_t st);
+void assemble_hamiltonian(pgx_ctx* c, int nterms, const int32_t* ops, const double* coef, int nmodes,
+                          const uint64_t* fock, const int32_t* state_block, const int32_t* state_inner);
 void rotate_operator(Problem& P, Operator& op, cudaStream_t st);
 void adjoint_operator(Problem& P, const Operator& src, Operator& dst, cudaStream_t st);
 void run_gf(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,

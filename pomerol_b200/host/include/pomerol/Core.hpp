@@ -70,7 +70,8 @@ struct Thermal {
 };
 
 // One GPU context shared by every object of an ED problem (owned through
-// the Hamiltonian).  Throws std::runtime_error on any non-OK status.
+// the Hamiltonian), taken from and returned to a per-GPU pool of contexts.
+// Throws std::runtime_error on any non-OK status.
 class Device {
 public:
     explicit Device(int device = 0);
@@ -85,6 +86,7 @@ public:
     RealType weights_beta = -1.0;
 
 private:
+    int device_ = 0;
     pgx_ctx* ctx_ = nullptr;
 };
 

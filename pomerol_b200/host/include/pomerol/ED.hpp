@@ -155,7 +155,7 @@ public:
     // GPU context shared by every object built on this Hamiltonian.
     Device& device() const { return *Dev; }
     StatesClassification const& getStates() const { return S; }
-    std::vector<RealType> const& hostBlocks() const { return HPacked; }
+    std::vector<RealType> const& hostBlocks() const;  // packed blocks, fetched from the device when needed
     std::vector<long> const& matrixOffsets() const { return MOff; }
     std::vector<RealType> const& eigenvectors() const;  // packed, lazily fetched
 
@@ -164,7 +164,7 @@ private:
     StatesClassification const& S;
     std::shared_ptr<Device> Dev;
     bool Complex = false;
-    std::vector<RealType> HPacked;
+    mutable std::vector<RealType> HPacked;
     std::vector<long> MOff;
     std::vector<std::vector<RealType>> Eigenvalues;
     mutable std::vector<RealType> UPacked;

@@ -4,8 +4,9 @@
 // invariant-subspace partition (HilbertSpace.hpp:144-169: connected
 // components of H, then merges so that every c / c^+ maps a block into at
 // most one block) and assembly of the dense block Hamiltonians
-// (HamiltonianPart.cpp:56-76).  Eigensolve, weights and operator rotation
-// run on the GPU through libpgx.
+// (HamiltonianPart.cpp:56-76), which runs on the GPU (pgx_assemble_hamiltonian)
+// from the terms' Fock action.  Eigensolve, weights and operator rotation run
+// on the GPU through libpgx.
 #include <algorithm>
 #include <numeric>
 #include <unordered_map>
@@ -192,32 +193,75 @@ void Hamiltonian::prepareImpl(HilbertSpace const& HS, MPI_Comm const&) {
         dims[b] = (int32_t)S.getBlockSize(b);
         MOff[b + 1] = MOff[b] + (long)dims[b] * dims[b];
     }
-    HPacked.assign(MOff[nb] * sc, 0.0);
-    for (BlockNumber b = 0; b < nb; ++b) {
-        auto const& st = S.getFockStates(b);
-        const long d = dims[b];
-        double* Hb = HPacked.data() + MOff[b] * sc;
-        for (long j = 0; j < d; ++j) {
-            for (auto const& t : HS.getHTerms()) {
-                QuantumState o;
-                double sg;
-                if (!t.first.apply(st[j], o, sg)) continue;
-                if (S.getBlockNumber(o) != b) throw std::logic_error("Hamiltonian connects different blocks");
-                const long i = (long)S.getInnerState(o);
-                if (Complex) {
-                    Hb[2 * (i * d + j)] += sg * t.second.real();
-                    Hb[2 * (i * d + j) + 1] += sg * t.second.imag();
-                } else {
-                    Hb[i * d + j] += sg * t.second.real();
+    Dev->check(pgx_set_blocks(Dev->ctx(), nb, dims.data(), Complex ? 1 : 0), "pgx_set_blocks");
+    auto const& terms = HS.getHTerms();
+    const QuantumState dim = HS.getDim();
+    int nmodes = 0;
+    while ((QuantumState(1) << nmodes) < dim) ++nmodes;
+    bool device_assembly = nmodes <= 30 && S.getNumberOfStates() == dim;
+    for (auto const& t : terms) device_assembly = device_assembly && t.first.ops.size() <= PGX_TERM_OPS;
+    HPacked.clear();
+    if (device_assembly) {
+        // the GPU builds the dense blocks from the terms' Fock action
+        std::vector<int32_t> ops(std::max<std::size_t>(terms.size(), 1) * PGX_TERM_OPS, -1);
+        std::vector<double> coef(std::max<std::size_t>(terms.size(), 1) * 2, 0.0);
+        for (std::size_t t = 0; t < terms.size(); ++t) {
+            auto const& m = terms[t].first.ops;
+            for (std::size_t k = 0; k < m.size(); ++k) ops[t * PGX_TERM_OPS + k] = 2 * m[k].second + (m[k].first ? 1 : 0);
+            coef[2 * t] = terms[t].second.real();
+            coef[2 * t + 1] = terms[t].second.imag();
+        }
+        std::vector<uint64_t> fock;
+        fock.reserve(dim);
+        std::vector<int32_t> sb(dim, -1), si(dim, -1);
+        for (BlockNumber b = 0; b < nb; ++b) {
+            auto const& st = S.getFockStates(b);
+            for (std::size_t i = 0; i < st.size(); ++i) {
+                fock.push_back(st[i]);
+                sb[st[i]] = b;
+                si[st[i]] = (int32_t)i;
+            }
+        }
+        Dev->check(pgx_assemble_hamiltonian(Dev->ctx(), (int32_t)terms.size(), ops.data(), coef.data(), nmodes,
+                                            fock.data(), sb.data(), si.data()),
+                   "pgx_assemble_hamiltonian");
+    } else {
+        // monomials longer than PGX_TERM_OPS operators: dense blocks built here
+        HPacked.assign(MOff[nb] * sc, 0.0);
+        for (BlockNumber b = 0; b < nb; ++b) {
+            auto const& st = S.getFockStates(b);
+            const long d = dims[b];
+            double* Hb = HPacked.data() + MOff[b] * sc;
+            for (long j = 0; j < d; ++j) {
+                for (auto const& t : terms) {
+                    QuantumState o;
+                    double sg;
+                    if (!t.first.apply(st[j], o, sg)) continue;
+                    if (S.getBlockNumber(o) != b) throw std::logic_error("Hamiltonian connects different blocks");
+                    const long i = (long)S.getInnerState(o);
+                    if (Complex) {
+                        Hb[2 * (i * d + j)] += sg * t.second.real();
+                        Hb[2 * (i * d + j) + 1] += sg * t.second.imag();
+                    } else {
+                        Hb[i * d + j] += sg * t.second.real();
+                    }
                 }
             }
         }
+        Dev->check(pgx_set_hamiltonian(Dev->ctx(), HPacked.data()), "pgx_set_hamiltonian");
     }
-    Dev->check(pgx_set_blocks(Dev->ctx(), nb, dims.data(), Complex ? 1 : 0), "pgx_set_blocks");
-    Dev->check(pgx_set_hamiltonian(Dev->ctx(), HPacked.data()), "pgx_set_hamiltonian");
     parts.clear();
     for (BlockNumber b = 0; b < nb; ++b) parts.emplace_back(*this, b);
     setStatus(Prepared);
+}
+
+std::vector<RealType> const& Hamiltonian::hostBlocks() const {
+    if (getStatus() < Prepared) throw StatusMismatch("Hamiltonian is not prepared yet.");
+    if (HPacked.empty()) {
+        HPacked.resize(MOff.back() * (Complex ? 2 : 1));
+        Dev->check(pgx_get_hamiltonian(Dev->ctx(), HPacked.data()), "pgx_get_hamiltonian");
+    }
+    return HPacked;
 }
 
 void Hamiltonian::compute(MPI_Comm const&) {
@@ -244,7 +288,7 @@ void Hamiltonian::compute(MPI_Comm const&) {
 std::vector<RealType> const& Hamiltonian::eigenvectors() const {
     if (getStatus() < Computed) throw StatusMismatch("Hamiltonian is not computed yet.");
     if (UPacked.empty()) {
-        UPacked.resize(HPacked.size());
+        UPacked.resize(MOff.back() * (Complex ? 2 : 1));
         Dev->check(pgx_get_eigensystem(Dev->ctx(), nullptr, UPacked.data()), "pgx_get_eigensystem");
     }
     return UPacked;
@@ -279,7 +323,7 @@ RealType HamiltonianPart::getMinimumEigenvalue() const {
 }
 std::vector<RealType> HamiltonianPart::getMatrix() const {
     const int sc = H->Complex ? 2 : 1;
-    auto const& src = (H->getStatus() >= ComputableObject::Computed) ? H->eigenvectors() : H->HPacked;
+    auto const& src = (H->getStatus() >= ComputableObject::Computed) ? H->eigenvectors() : H->hostBlocks();
     return std::vector<RealType>(src.begin() + H->MOff[Block] * sc, src.begin() + H->MOff[Block + 1] * sc);
 }
 std::vector<RealType> HamiltonianPart::getEigenState(InnerQuantumState state) const {

@@ -1,7 +1,10 @@
 // Lattice presets (same terms as LatticePresets.cpp:46-48, 75-83, 140-147,
 // Pairing/NupNdown/Spinflip/PairHopping, 402-409, 423-448) and the core
 // tables (Misc.cpp:41-66).
+#include <map>
+#include <mutex>
 #include <stdexcept>
+#include <vector>
 
 #include "pomerol.hpp"
 
@@ -17,13 +20,40 @@ std::array<Permutation4, 24> const permutations4 = {
      {{2, 1, 3, 0}, 1},  {{2, 3, 0, 1}, 1},  {{2, 3, 1, 0}, -1}, {{3, 0, 1, 2}, -1}, {{3, 0, 2, 1}, 1},
      {{3, 1, 0, 2}, 1},  {{3, 1, 2, 0}, -1}, {{3, 2, 0, 1}, -1}, {{3, 2, 1, 0}, 1}}};
 
-Device::Device(int device) {
+// Contexts of destroyed Devices are kept per GPU and handed to the next
+// Device on that GPU: its device buffers, streams and pinned staging memory
+// are reused (pgx_set_blocks resets the problem, not the allocations), so a
+// new Hamiltonian neither allocates nor frees device memory when a previous
+// one of similar size existed.  Pooled contexts live until the process ends.
+namespace {
+std::mutex& pool_mutex() {
+    static std::mutex m;
+    return m;
+}
+std::map<int, std::vector<pgx_ctx*>>& context_pool() {
+    static auto* p = new std::map<int, std::vector<pgx_ctx*>>();  // never destroyed: outlives static teardown
+    return *p;
+}
+}  // namespace
+
+Device::Device(int device) : device_(device) {
+    {
+        std::lock_guard<std::mutex> lk(pool_mutex());
+        auto& free = context_pool()[device];
+        if (!free.empty()) {
+            ctx_ = free.back();
+            free.pop_back();
+            return;
+        }
+    }
     int rc = pgx_create(device, &ctx_);
     if (rc != PGX_OK) throw std::runtime_error("libpgx: no usable CUDA device (status " + std::to_string(rc) + ")");
 }
 
 Device::~Device() {
-    if (ctx_) pgx_destroy(ctx_);
+    if (!ctx_) return;
+    std::lock_guard<std::mutex> lk(pool_mutex());
+    context_pool()[device_].push_back(ctx_);
 }
 
 void Device::check(int rc, char const* what) const {

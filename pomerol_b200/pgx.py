@@ -23,7 +23,7 @@ EXPORTS = [
     "pgx_op_define", "pgx_op_rotate", "pgx_op_adjoint", "pgx_op_info", "pgx_op_read", "pgx_gf", "pgx_susc",
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
-    "pgx_recip_check",
+    "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian",
 ]
 
 
@@ -77,6 +77,8 @@ def load():
         lib.pgx_profile_end.argtypes = [P, P]
         lib.pgx_profile_kernel.argtypes = [P, I32, C.c_char_p, I32, P, P, P, P]
         lib.pgx_recip_check.argtypes = [P, I32, P]
+        lib.pgx_assemble_hamiltonian.argtypes = [P, I32, P, P, I32, P, P, P]
+        lib.pgx_get_hamiltonian.argtypes = [P, P]
         _lib = lib
     return _lib
 
@@ -290,6 +292,45 @@ def _profile_end(self):
     return out
 
 
+PGX_TERM_OPS = 8
+
+
+def _assemble_hamiltonian(self, terms, nmodes, fock, state_block, state_inner):
+    """Device assembly of the block Hamiltonians: terms is a list of
+    (ops, coef) with ops a sequence of (dagger, mode) pairs, left to right."""
+    n = len(terms)
+    ops = np.full((max(n, 1), PGX_TERM_OPS), -1, dtype=np.int32)
+    coef = np.zeros((max(n, 1), 2))
+    for t, (mono, c) in enumerate(terms):
+        if len(mono) > PGX_TERM_OPS:
+            raise ValueError("monomial longer than PGX_TERM_OPS operators")
+        for k, (dag, mode) in enumerate(mono):
+            ops[t, k] = 2 * int(mode) + (1 if dag else 0)
+        coef[t] = (complex(c).real, complex(c).imag)
+    fock = np.ascontiguousarray(fock, dtype=np.uint64)
+    sb = np.ascontiguousarray(state_block, dtype=np.int32)
+    si = np.ascontiguousarray(state_inner, dtype=np.int32)
+    self._ck(self.lib.pgx_assemble_hamiltonian(self.h, n, _p(ops), _p(coef), int(nmodes), _p(fock), _p(sb), _p(si)))
+
+
+def _get_hamiltonian(self):
+    """The block Hamiltonians on the device, one dense array per block."""
+    total = sum(d * d for d in self.dims)
+    buf = np.zeros(total * (2 if self.is_complex else 1))
+    self._ck(self.lib.pgx_get_hamiltonian(self.h, _p(buf)))
+    out, o = [], 0
+    for d in self.dims:
+        if self.is_complex:
+            m = buf[2 * o:2 * (o + d * d)].view(complex).reshape(d, d)
+        else:
+            m = buf[o:o + d * d].reshape(d, d)
+        out.append(m.copy())
+        o += d * d
+    return out
+
+
+Engine.assemble_hamiltonian = _assemble_hamiltonian
+Engine.get_hamiltonian = _get_hamiltonian
 Engine.timer_begin = _timer_begin
 Engine.timer_end = _timer_end
 Engine.profile_begin = _profile_begin
