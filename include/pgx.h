@@ -134,6 +134,11 @@ int pgx_op_rotate(pgx_ctx* ctx, int32_t op_id);
  * (c from c^+).  Returns its id. */
 int pgx_op_adjoint(pgx_ctx* ctx, int32_t src, int32_t* op_id);
 
+/* Release an operator: its device memory is kept by the context and reused
+ * by the next pgx_op_define / pgx_op_adjoint (as when the reference destroys a
+ * MonomialOperator).  The id stays invalid afterwards. */
+int pgx_op_release(pgx_ctx* ctx, int32_t op_id);
+
 /* Number of parts, and per part (right block, left block). */
 int pgx_op_info(pgx_ctx* ctx, int32_t op_id, int32_t* nparts, int32_t* right_block, int32_t* left_block);
 

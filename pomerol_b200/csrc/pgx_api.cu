@@ -483,6 +483,17 @@ int pgx_op_adjoint(pgx_ctx* c, int32_t src, int32_t* op_id) {
     });
 }
 
+int pgx_op_release(pgx_ctx* c, int32_t op_id) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(op_id >= 0 && op_id < (int)P.ops.size(), PGX_ERR_ARG, "bad operator id");
+        // work already queued on the context's stream that reads the operator
+        // runs before anything that reuses its buffers (same stream)
+        P.spare_ops.push_back(std::move(P.ops[op_id]));
+        P.ops[op_id] = pgx::Operator();  // no parts, not rotated: every later use is rejected
+    });
+}
+
 int pgx_op_info(pgx_ctx* c, int32_t op_id, int32_t* nparts, int32_t* right_block, int32_t* left_block) {
     return guarded(c, [&] {
         pgx::Problem& P = c->P;

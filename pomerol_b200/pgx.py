@@ -23,7 +23,7 @@ EXPORTS = [
     "pgx_op_define", "pgx_op_rotate", "pgx_op_adjoint", "pgx_op_info", "pgx_op_read", "pgx_gf", "pgx_susc",
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
-    "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian",
+    "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
 ]
 
 
@@ -79,6 +79,7 @@ def load():
         lib.pgx_recip_check.argtypes = [P, I32, P]
         lib.pgx_assemble_hamiltonian.argtypes = [P, I32, P, P, I32, P, P, P]
         lib.pgx_get_hamiltonian.argtypes = [P, P]
+        lib.pgx_op_release.argtypes = [P, I32]
         _lib = lib
     return _lib
 
@@ -329,6 +330,12 @@ def _get_hamiltonian(self):
     return out
 
 
+def _op_release(self, op_id):
+    """Give an operator's device memory back to the context for reuse."""
+    self._ck(self.lib.pgx_op_release(self.h, int(op_id)))
+
+
+Engine.op_release = _op_release
 Engine.assemble_hamiltonian = _assemble_hamiltonian
 Engine.get_hamiltonian = _get_hamiltonian
 Engine.timer_begin = _timer_begin

@@ -168,7 +168,10 @@ class EngineRun:
         u, d = self.prob.u0, self.prob.d0
         for i in (u, d):
             e.op_rotate(self.cdag[i])
+        for op in getattr(self, "_adjoints", ()):  # the previous step's c operators
+            e.op_release(op)
         c = {i: e.op_adjoint(self.cdag[i]) for i in (u, d)}
+        self._adjoints = tuple(c.values())
         slots = (c[u], c[d], self.cdag[u])  # C1, C2, CX3 of chi_(u0,d0,u0,d0)
         parts = [((slots[p[0]], slots[p[1]], slots[p[2]], self.cdag[d]), tuple(b), tuple(p), s)
                  for b, p, s in self.chains]

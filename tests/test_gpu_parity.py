@@ -380,3 +380,56 @@ def test_device_hamiltonian_assembly_rejects_bad_tables():
         eng.assemble_hamiltonian(terms, nmodes, fock, sb, bad)
     with pytest.raises(PgxError):
         eng.assemble_hamiltonian([(((True, nmodes),), 1.0)], nmodes, fock, sb, si)
+
+
+def test_context_reused_across_problems_of_different_sizes():
+    """pgx_set_blocks keeps a context's device buffers: a larger problem grows
+    them, a smaller one reuses them; operator buffers of the previous problem
+    are reused by the next one's operators."""
+    from pomerol_b200.pgx import Engine
+    rng = np.random.default_rng(3)
+    eng = Engine()
+    for dims in ([5, 40], [300, 7, 120], [3, 9]):
+        blocks = []
+        for d in dims:
+            a = rng.standard_normal((d, d))
+            blocks.append((a + a.T) / 2)
+        eng.set_blocks(dims)
+        eng.set_hamiltonian(blocks)
+        eng.eigh()
+        E, U = eng.eigensystem()
+        for h, e, u in zip(blocks, E, U):
+            scale = max(1.0, np.abs(e).max())
+            assert np.abs(h @ u - u * e[None, :]).max() < 1e-10 * scale
+            assert np.abs(e - np.linalg.eigvalsh(h)).max() < 1e-11 * scale
+    from tests.pgx_harness import GpuED
+    k = KATS["gf4site"]
+    m = M.make_model(plaquette_expr())
+    dn = m.info.getIndex("A", 0, 0)
+    g = GpuED(m, k["beta"])
+    for _ in range(3):  # the same context, problem set up again: operators reuse released buffers
+        v = g.gf(g.c(dn), g.cdag(dn), L.fermionic(np.arange(10), k["beta"]))
+        assert np.abs(v - cplx(k["G_A_down"])).max() < k["tol"]
+        g.eng.set_blocks(m.block_sizes(), m.complex)
+        g.eng.set_hamiltonian([m.h_block(b) for b in range(len(m.blocks))])
+        g.eng.eigh()
+        g.E, g.U = g.eng.eigensystem()
+        g.w, g.Z = g.eng.weights(k["beta"])
+        g._cdag, g._c = {}, {}
+
+
+def test_released_operator_is_rejected_and_its_memory_reused(harness):
+    from pomerol_b200.pgx import PgxError
+    m = M.make_model(plaquette_expr())
+    g = harness(m, 10.0)
+    ix = m.info.getIndex("A", 0, 0)
+    cd = g.cdag(ix)
+    c1 = g.eng.op_adjoint(cd)
+    ref = [g.eng.op_read(c1, k) for k in range(len(g.eng.op_info(c1)))]
+    g.eng.op_release(c1)
+    assert g.eng.op_info(c1) == []
+    with pytest.raises(PgxError):
+        g.eng.op_adjoint(c1)
+    c2 = g.eng.op_adjoint(cd)  # takes the released buffers
+    for k, r in enumerate(ref):
+        assert np.array_equal(g.eng.op_read(c2, k), r)
