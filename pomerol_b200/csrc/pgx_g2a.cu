@@ -95,18 +95,32 @@ __device__ void dterm_group(const DTerm& d, int g, double beta, double tol2, cd*
                 const cd ab = load_v(d.VA, d.va_cplx, oa + k * d.ak) * load_v(d.VB, d.vb_cplx, ob + k * d.bk);
                 const double de = d.sgn * (d.Ek[k] - eh);
                 double Dx[DG], m2[DG], rc[DG];
+                bool dl[DG];
                 bool in_range = true;
 #pragma unroll
                 for (int q = 0; q < DG; ++q) {
                     Dx[q] = sx[q] - de;
-                    m2[q] = fma(Dx[q], Dx[q], sy[q] * sy[q]);
+                    const double mq = fma(Dx[q], Dx[q], sy[q] * sy[q]);
+                    dl[q] = DELTA && mq <= tol2;
+                    m2[q] = dl[q] ? 1.0 : mq;  // resonant: the kernel value does not use it
                     in_range = in_range && recip_in_range(m2[q]);
                 }
-                // one range test per element keeps the DG reciprocal chains
-                // branch-free, so they interleave
                 if (in_range) {
+                    // Montgomery's batch inversion: the DG reciprocals from one
+                    // reciprocal of their product (prefix products forward, then
+                    // peel one factor per step backward); with every value in
+                    // [1e-30, 1e30] the product of 8 stays inside the double range
+                    double pre[DG];
+                    pre[0] = m2[0];
 #pragma unroll
-                    for (int q = 0; q < DG; ++q) rc[q] = recip_newton(m2[q]);
+                    for (int q = 1; q < DG; ++q) pre[q] = pre[q - 1] * m2[q];
+                    double inv = 1.0 / pre[DG - 1];
+#pragma unroll
+                    for (int q = DG - 1; q > 0; --q) {
+                        rc[q] = inv * pre[q - 1];
+                        inv = inv * m2[q];
+                    }
+                    rc[0] = inv;
                 } else {
 #pragma unroll
                     for (int q = 0; q < DG; ++q) rc[q] = 1.0 / m2[q];
@@ -114,7 +128,7 @@ __device__ void dterm_group(const DTerm& d, int g, double beta, double tol2, cd*
 #pragma unroll
                 for (int q = 0; q < DG; ++q) {
                     const double r = cw * rc[q];
-                    const bool delta = DELTA && m2[q] <= tol2;
+                    const bool delta = dl[q];
                     const double Kx = delta ? cdl : Dx[q] * r;
                     const double Ky = delta ? 0.0 : -sy[q] * r;
                     ax[q] = fma(ab.x, Kx, fma(-ab.y, Ky, ax[q]));
