@@ -190,7 +190,10 @@ void reset_problem(pgx::Problem& P) {
                                          &pgx::Problem::order_d, &pgx::Problem::status,    &pgx::Problem::tri,
                                          &pgx::Problem::tri_items, &pgx::Problem::eigh_gemm, &pgx::Problem::eigh_scratch,
                                          &pgx::Problem::op_probs, &pgx::Problem::op_tiles, &pgx::Problem::op_meta,
-                                         &pgx::Problem::asm_buf};
+                                         &pgx::Problem::asm_buf, &pgx::Problem::cx_meta, &pgx::Problem::cx_H,
+                                         &pgx::Problem::cx_A,    &pgx::Problem::cx_Zc,   &pgx::Problem::cx_U,
+                                         &pgx::Problem::cx_E,    &pgx::Problem::cx_tri,  &pgx::Problem::cx_S,
+                                         &pgx::Problem::cx_items, &pgx::Problem::cx_gemm};
     for (auto m : bufs) fresh.*m = std::move(P.*m);
     fresh.spare_ops = std::move(P.spare_ops);
     for (auto& op : P.ops) fresh.spare_ops.push_back(std::move(op));
@@ -344,7 +347,6 @@ int pgx_eigh(pgx_ctx* c) {
     return guarded(c, [&] {
         pgx::Problem& P = c->P;
         PGX_CHECK(P.have_H, PGX_ERR_STATE, "pgx_set_hamiltonian first");
-        PGX_CHECK(!P.is_complex, PGX_ERR_ARG, "complex Hermitian blocks are not supported by this build");
         PGX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int), c->stream));
         pgx::launch_eigh(c);
         int st = 0;

@@ -20,6 +20,7 @@
 
 #include <cooperative_groups.h>
 
+#include <cmath>
 #include <cstring>
 
 #include "pgx_common.cuh"
@@ -691,6 +692,84 @@ __global__ void __launch_bounds__(TRI_THREADS) ortho_kernel(TriArgs g) {
     }
 }
 
+// ----------------------------------------------------------------------------
+// Complex Hermitian blocks.  H = R + iI (R symmetric, I antisymmetric) has the
+// real symmetric embedding [[R, -I], [I, R]] of twice the size; every
+// eigenvalue of H appears twice in it, and for a real eigenvector [a; b] of
+// the pair, a + ib is an eigenvector of H (unit norm).  The embedding is
+// diagonalised by the real stages above; cx_extract_kernel then forms the
+// complex eigenvectors.
+
+// block b of H (complex, row-major n x n) -> block b of the embedding (2n x 2n)
+__global__ void cx_embed_kernel(const int* dims, const long* moff, const long* moff2, const double* H, double* H2) {
+    const int b = blockIdx.y, n = dims[b];
+    const cd* Hb = reinterpret_cast<const cd*>(H) + moff[b];
+    double* E = H2 + moff2[b];
+    const long nn = (long)n * n, n2 = 2L * n;
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < nn; e += (long)gridDim.x * blockDim.x) {
+        const int i = (int)(e / n), j = (int)(e % n);
+        const cd h = Hb[e];
+        E[i * n2 + j] = h.x;
+        E[i * n2 + n + j] = -h.y;
+        E[(n + i) * n2 + j] = h.y;
+        E[(n + i) * n2 + n + j] = h.x;
+    }
+}
+
+// One thread per cluster of equal eigenvalues of the embedding (2m values):
+// the m complex eigenvectors of H are taken from the 2m candidates a + ib by
+// modified Gram-Schmidt (twice), keeping those with a residual norm above 1/2.
+// A cluster is a run of consecutive eigenvalues closer than tol.
+__global__ void cx_extract_kernel(const int* dims, const long* moff, const long* eoff, const long* moff2,
+                                  const long* eoff2, const double* E2, const double* U2, double* E, cd* U, double tol,
+                                  int* status) {
+    const int b = blockIdx.x, n = dims[b];
+    const long n2 = 2L * n;
+    const double* Eb2 = E2 + eoff2[b];
+    const double* Ub2 = U2 + moff2[b];
+    double* Eb = E + eoff[b];
+    cd* Ub = U + moff[b];
+    for (int j = threadIdx.x; j < 2 * n; j += blockDim.x) {
+        if (j > 0 && Eb2[j] - Eb2[j - 1] <= tol) continue;  // not the start of a cluster
+        int jend = j;
+        while (jend + 1 < 2 * n && Eb2[jend + 1] - Eb2[jend] <= tol) ++jend;
+        const int sz = jend - j + 1, m = sz / 2, c0 = j / 2;
+        if ((sz & 1) || (j & 1)) {
+            atomicExch(status, PGX_ERR_NUMERIC);
+            continue;
+        }
+        int acc = 0;
+        for (int k = 0; k < sz && acc < m; ++k) {
+            cd* v = Ub + (c0 + acc);  // column c0 + acc, stride n
+            for (int i = 0; i < n; ++i) v[(long)i * n] = cd{Ub2[i * n2 + j + k], Ub2[(n + i) * n2 + j + k]};
+            for (int pass = 0; pass < 2; ++pass)
+                for (int q = 0; q < acc; ++q) {
+                    const cd* u = Ub + (c0 + q);
+                    double px = 0.0, py = 0.0;  // u^H v
+                    for (int i = 0; i < n; ++i) {
+                        const cd a = u[(long)i * n], c = v[(long)i * n];
+                        px += a.x * c.x + a.y * c.y;
+                        py += a.x * c.y - a.y * c.x;
+                    }
+                    for (int i = 0; i < n; ++i) {
+                        const cd a = u[(long)i * n];
+                        v[(long)i * n].x -= px * a.x - py * a.y;
+                        v[(long)i * n].y -= px * a.y + py * a.x;
+                    }
+                }
+            double nn = 0.0;
+            for (int i = 0; i < n; ++i) nn += abs2(v[(long)i * n]);
+            if (nn > 0.25) {
+                const double inv = rsqrt(nn);
+                for (int i = 0; i < n; ++i) v[(long)i * n] = v[(long)i * n] * inv;
+                Eb[c0 + acc] = Eb2[j + 2 * acc];
+                ++acc;
+            }
+        }
+        if (acc < m) atomicExch(status, PGX_ERR_NUMERIC);
+    }
+}
+
 }  // namespace
 
 // Work items, largest blocks first: vector_kernel takes TRI_THREADS
@@ -946,6 +1025,86 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     launch_gemm_batch(probs, d.gemm_probs, probs_cap, d.gemm_tiles, tiles_cap, st);
 }
 
+// Complex Hermitian blocks: embedding, real eigensolve of the embedding,
+// extraction of the complex eigenvectors (see cx_extract_kernel).
+static void launch_eigh_complex(pgx_ctx* c) {
+    Problem& P = c->P;
+    cudaStream_t st = c->stream;
+    const int nb = P.nblocks;
+    std::vector<int> d2(nb);
+    std::vector<long> m2(nb), e2(nb);
+    long msz2 = 0, esz2 = 0;
+    for (int b = 0; b < nb; ++b) {
+        d2[b] = 2 * P.dims[b];
+        m2[b] = msz2;
+        e2[b] = esz2;
+        msz2 += (long)d2[b] * d2[b];
+        esz2 += d2[b];
+    }
+    // dims | moff | eoff of the embedding, on the device
+    const size_t off_m = (nb * sizeof(int) + 15) & ~size_t(15);
+    P.cx_meta.reserve(off_m + 2 * nb * sizeof(long));
+    int* dd2 = P.cx_meta.as<int>();
+    long* dm2 = reinterpret_cast<long*>(P.cx_meta.as<char>() + off_m);
+    long* de2 = dm2 + nb;
+    h2d(dd2, d2.data(), nb * sizeof(int), st);
+    h2d(dm2, m2.data(), nb * sizeof(long), st);
+    h2d(de2, e2.data(), nb * sizeof(long), st);
+    P.cx_H.reserve(msz2 * sizeof(double));
+    P.cx_A.reserve(msz2 * sizeof(double));
+    P.cx_Zc.reserve(msz2 * sizeof(double));
+    P.cx_U.reserve(msz2 * sizeof(double));
+    P.cx_E.reserve(esz2 * sizeof(double));
+    P.cx_tri.reserve((3 * esz2) * sizeof(double) + 3 * esz2 * sizeof(int) + 64);
+    P.cx_S.reserve(eigh_vec_scratch_doubles(d2) * sizeof(double));
+    P.cx_items.reserve(eigh_item_bytes(d2));
+    size_t tiles_b = 0;
+    const size_t probs_b = eigh_gemm_bytes(d2, &tiles_b);
+    P.cx_gemm.reserve(((probs_b + 255) & ~size_t(255)) + tiles_b);
+    int dmax = 1;
+    for (int x : P.dims) dmax = std::max(dmax, x);
+    {
+        dim3 g(std::min(ceil_div((long)dmax * dmax, 256), 1024), (unsigned)nb);
+        cx_embed_kernel<<<g, 256, 0, st>>>(P.d_dims, P.d_moff, dm2, P.d_H, P.cx_H.as<double>());
+        check_launch("cx_embed_kernel");
+    }
+    EighDev d;
+    d.dims = dd2;
+    d.moff = dm2;
+    d.eoff = de2;
+    d.H = P.cx_H.as<double>();
+    d.A = P.cx_A.as<double>();
+    d.Zc = P.cx_Zc.as<double>();
+    d.tri = P.cx_tri.as<double>();
+    d.lam = d.tri + 2 * esz2;
+    d.sb = reinterpret_cast<int*>(d.lam + esz2);
+    d.rank = d.sb + 2 * esz2;
+    d.S = P.cx_S.as<double>();
+    d.items = P.cx_items.p;
+    d.gemm_probs = P.cx_gemm.p;
+    d.gemm_tiles = P.cx_gemm.as<char>() + ((probs_b + 255) & ~size_t(255));
+    d.U = P.cx_U.as<double>();
+    d.E = P.cx_E.as<double>();
+    d.status = P.d_status;
+    for (int i = 0; i < 3; ++i) {
+        d.aux[i] = c->aux[i];
+        d.join[i] = c->join[i];
+    }
+    d.fork = c->fork;
+    launch_eigh_raw(d, d2, m2, st);
+    // pairs of the embedding agree to the eigensolver's accuracy, far inside
+    // this clustering tolerance; distinct eigenvalues of H closer than it are
+    // orthonormalised together
+    std::vector<double> e(esz2);
+    PGX_CUDA(cudaMemcpyAsync(e.data(), d.E, esz2 * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaStreamSynchronize(st));
+    double emax = 1.0;
+    for (double x : e) emax = std::max(emax, std::fabs(x));
+    cx_extract_kernel<<<nb, 128, 0, st>>>(P.d_dims, P.d_moff, P.d_eoff, dm2, de2, d.E, d.U, P.d_E,
+                                          reinterpret_cast<cd*>(P.d_U), 1e-10 * emax, P.d_status);
+    check_launch("cx_extract_kernel");
+}
+
 void launch_eigh(pgx_ctx* c) {
     Problem& P = c->P;
     cudaStream_t st = c->stream;
@@ -955,6 +1114,10 @@ void launch_eigh(pgx_ctx* c) {
             PGX_CUDA(cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking));
             PGX_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
         }
+    }
+    if (P.is_complex) {
+        launch_eigh_complex(c);
+        return;
     }
     // tri (2 sum d) | lam (sum d) | sb (2 sum d ints) | rank (sum d ints)
     const long e = std::max<long>(P.esize, 1);

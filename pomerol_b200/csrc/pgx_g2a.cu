@@ -65,7 +65,7 @@ __device__ __forceinline__ cd load_v(const void* p, int cplx, long idx) {
 
 // Triples of one (z1, z3) group handled together: the operand product
 // VA * VB does not depend on z2, so it is loaded once for DG triples.
-constexpr int DG = 8;
+constexpr int DG = 8;  // the batch inversion below is written out for eight
 
 template <bool DELTA>
 __device__ void dterm_group(const DTerm& d, int g, double beta, double tol2, cd* out, int lane) {
@@ -91,9 +91,22 @@ __device__ void dterm_group(const DTerm& d, int g, double beta, double tol2, cd*
             const double cw = d.cnum * w, cdl = d.cdelta * beta * w;
             const long oa = i1 * d.a1 + i3 * d.a3 + (long)(d.va_hstate ? hs : h) * d.ah;
             const long ob = i1 * d.b1 + i3 * d.b3 + (long)(d.vb_hstate ? hs : h) * d.bh;
+            // operands of the next k are loaded while the current one is computed
+            cd nva{0.0, 0.0}, nvb{0.0, 0.0};
+            double nek = 0.0;
+            if (lane < d.nk) {
+                nva = load_v(d.VA, d.va_cplx, oa + lane * d.ak);
+                nvb = load_v(d.VB, d.vb_cplx, ob + lane * d.bk);
+                nek = d.Ek[lane];
+            }
             for (int k = lane; k < d.nk; k += 32) {
-                const cd ab = load_v(d.VA, d.va_cplx, oa + k * d.ak) * load_v(d.VB, d.vb_cplx, ob + k * d.bk);
-                const double de = d.sgn * (d.Ek[k] - eh);
+                const cd ab = nva * nvb;
+                const double de = d.sgn * (nek - eh);
+                if (k + 32 < d.nk) {
+                    nva = load_v(d.VA, d.va_cplx, oa + (k + 32) * d.ak);
+                    nvb = load_v(d.VB, d.vb_cplx, ob + (k + 32) * d.bk);
+                    nek = d.Ek[k + 32];
+                }
                 double Dx[DG], m2[DG], rc[DG];
                 bool dl[DG];
                 bool in_range = true;
@@ -106,21 +119,24 @@ __device__ void dterm_group(const DTerm& d, int g, double beta, double tol2, cd*
                     in_range = in_range && recip_in_range(m2[q]);
                 }
                 if (in_range) {
-                    // Montgomery's batch inversion: the DG reciprocals from one
-                    // reciprocal of their product (prefix products forward, then
-                    // peel one factor per step backward); with every value in
-                    // [1e-30, 1e30] the product of 8 stays inside the double range
-                    double pre[DG];
-                    pre[0] = m2[0];
-#pragma unroll
-                    for (int q = 1; q < DG; ++q) pre[q] = pre[q - 1] * m2[q];
-                    double inv = 1.0 / pre[DG - 1];
-#pragma unroll
-                    for (int q = DG - 1; q > 0; --q) {
-                        rc[q] = inv * pre[q - 1];
-                        inv = inv * m2[q];
-                    }
-                    rc[0] = inv;
+                    // Montgomery's batch inversion in tree form: the eight
+                    // reciprocals from one division of the product of all eight
+                    // (pairwise products up, then each subtree's reciprocal times
+                    // its sibling's product down; depth 3 each way).  With every
+                    // value in [1e-30, 1e30] the product stays inside the double range.
+                    const double p01 = m2[0] * m2[1], p23 = m2[2] * m2[3], p45 = m2[4] * m2[5], p67 = m2[6] * m2[7];
+                    const double p03 = p01 * p23, p47 = p45 * p67;
+                    const double inv = 1.0 / (p03 * p47);
+                    const double i03 = inv * p47, i47 = inv * p03;
+                    const double i01 = i03 * p23, i23 = i03 * p01, i45 = i47 * p67, i67 = i47 * p45;
+                    rc[0] = i01 * m2[1];
+                    rc[1] = i01 * m2[0];
+                    rc[2] = i23 * m2[3];
+                    rc[3] = i23 * m2[2];
+                    rc[4] = i45 * m2[5];
+                    rc[5] = i45 * m2[4];
+                    rc[6] = i67 * m2[7];
+                    rc[7] = i67 * m2[6];
                 } else {
 #pragma unroll
                     for (int q = 0; q < DG; ++q) rc[q] = 1.0 / m2[q];

@@ -89,6 +89,8 @@ struct Problem {
         eigh_scratch;
     DevBuf op_probs, op_tiles, op_meta;  // descriptor lists of operator rotation / adjoint
     DevBuf asm_buf;                      // term list and state tables of the Hamiltonian assembly
+    // complex blocks: real embedding of twice the size and its eigensolver workspace
+    DevBuf cx_meta, cx_H, cx_A, cx_Zc, cx_U, cx_E, cx_tri, cx_S, cx_items, cx_gemm;
     std::vector<double> w_host;          // host copy of the weights (set with them)
     int* d_dims = nullptr;
     long* d_moff = nullptr;

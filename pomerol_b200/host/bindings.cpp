@@ -104,10 +104,15 @@ PYBIND11_MODULE(_pomerol, m) {
         .def("compute", &HilbertSpace::compute)
         .def("getDim", &HilbertSpace::getDim)
         .def("getNumberOfBlocks", &HilbertSpace::getNumberOfBlocks);
-    m.def("MakeHilbertSpace", [](IndexClassification const& ii, RealExpr const& e) { return new HilbertSpace(ii, e); },
-          py::keep_alive<0, 1>());
-    m.def("MakeHilbertSpace", [](IndexClassification const& ii, ComplexExpr const& e) { return new HilbertSpace(ii, e); },
-          py::keep_alive<0, 1>());
+    // one function for both expression types: keep_alive on the second of two
+    // overloads faulted in pybind11's post-call handling
+    m.def(
+        "MakeHilbertSpace",
+        [](IndexClassification const& ii, py::object const& e) -> HilbertSpace* {
+            if (py::isinstance<RealExpr>(e)) return new HilbertSpace(ii, e.cast<RealExpr const&>());
+            return new HilbertSpace(ii, e.cast<ComplexExpr const&>());
+        },
+        py::keep_alive<0, 1>());
 
     py::class_<StatesClassification>(m, "StatesClassification")
         .def(py::init<>())

@@ -433,3 +433,73 @@ def test_released_operator_is_rejected_and_its_memory_reused(harness):
     c2 = g.eng.op_adjoint(cd)  # takes the released buffers
     for k, r in enumerate(ref):
         assert np.array_equal(g.eng.op_read(c2, k), r)
+
+
+def test_complex_hermitian_eigh():
+    """Complex Hermitian blocks (real embedding of twice the size, complex
+    eigenvectors formed from its pairs): random, exactly degenerate and
+    near-degenerate spectra; residual, unitarity and eigenvalues."""
+    from pomerol_b200.pgx import Engine
+    rng = np.random.default_rng(21)
+    dims = [1, 2, 5, 40, 120, 240]
+    blocks = []
+    for i, d in enumerate(dims):
+        q, _ = np.linalg.qr(rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d)))
+        if i == 3:
+            ev = np.repeat(np.arange(d // 4 + 1, dtype=float), 4)[:d]
+        elif i == 4:
+            ev = np.r_[np.arange(d - 3) * 1e-9, [1.0, 2.0, 3.0]]
+        else:
+            a = rng.standard_normal((d, d)) + 1j * rng.standard_normal((d, d))
+            blocks.append((a + a.conj().T) / 2)
+            continue
+        h = (q * ev) @ q.conj().T
+        blocks.append((h + h.conj().T) / 2)
+    eng = Engine()
+    eng.set_blocks(dims, is_complex=True)
+    eng.set_hamiltonian(blocks)
+    eng.eigh()
+    E, U = eng.eigensystem()
+    for h, e, u in zip(blocks, E, U):
+        scale = max(1.0, np.abs(e).max())
+        assert np.all(np.diff(e) >= 0)
+        assert np.abs(h @ u - u * e[None, :]).max() < 1e-10 * scale
+        assert np.abs(u.conj().T @ u - np.eye(len(e))).max() < 1e-11
+        assert np.abs(e - np.linalg.eigvalsh(h)).max() < 1e-11 * scale
+
+
+def _anderson_complex_gf(J, s1, s2, n, mu=1.2, U=2.0, beta=10.0):
+    """Closed-form G_{s1 s2}(i w_n) of the atom CoulombS(U, -mu) with spin
+    mixing J c+_up c_dn + h.c. (AndersonComplexTest.cpp:39-85): eigenstates
+    0, (-mu -+ |J|), -2mu + U; the mixed components carry exp(+-i arg J)."""
+    E = np.array([0.0, -mu - abs(J), -mu + abs(J), -2 * mu + U])
+    w = np.exp(-beta * E)
+    w /= w.sum()
+    iw = 1j * np.pi * (2 * n + 1) / beta
+    tr = [(1, 0, -1), (2, 0, 1), (3, 1, 1), (3, 2, -1)]  # (upper, lower, sign of the spin-mixed residue)
+    res = 0
+    for a, b, sg in tr:
+        term = 0.5 * (w[a] + w[b]) / (iw - (E[a] - E[b]))
+        if s1 == s2:
+            res += term
+        else:
+            res += sg * np.exp(1j * np.angle(J) * (1 if s1 == M.UP else -1)) * term
+    return res
+
+
+@pytest.mark.parametrize("J", [0.1, -0.1, 0.1j, -0.1j, 0.1 + 0.1j, 0.1 - 0.1j, -0.1 + 0.1j, -0.1 - 0.1j])
+def test_anderson_complex_closed_form(harness, J):
+    """G of the bare Anderson atom with complex spin mixing (complex Hermitian
+    H) against its closed form at 1e-12, as AndersonComplexTest.cpp:131-148."""
+    mu, U, beta = 1.2, 2.0, 10.0
+    m = M.make_model(M.CoulombS("C", U, -mu) + M.HoppingS("C", "C", J, 0, 0, M.UP, M.DOWN))
+    assert m.complex == (complex(J).imag != 0)
+    g = harness(m, beta)
+    n = np.arange(10)
+    z = 1j * np.pi * (2 * n + 1) / beta
+    for s1 in (M.DOWN, M.UP):
+        for s2 in (M.DOWN, M.UP):
+            i1, i2 = m.info.getIndex("C", 0, s1), m.info.getIndex("C", 0, s2)
+            v = g.gf(g.c(i1), g.cdag(i2), z)
+            ref = np.array([_anderson_complex_gf(J, s1, s2, k) for k in n])
+            assert np.abs(v - ref).max() < 1e-12

@@ -324,3 +324,28 @@ def test_anderson2pgf_reference_case(P, split):
     chi = Chi4(u0, u0, u0, u0).element()
     v = np.array([chi(om + Om, 1j * (2 * i + 1) * np.pi / beta, om) for i in range(10)])
     assert np.abs(v - ref).max() < k["tol"]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("J", [0.1, -0.1, 0.1j, -0.1j, 0.1 + 0.1j, 0.1 - 0.1j, -0.1 + 0.1j, -0.1 - 0.1j])
+def test_anderson_complex_reference_case(P, J):
+    """AndersonComplexTest.cpp:89-148 through the drop-in classes: complex
+    Hermitian H from CoulombS + Hopping(C, C, J, 0, 0, up, down); all four
+    G_{s1 s2}(n), n < 10, against the closed form at 1e-12."""
+    from tests.test_gpu_parity import _anderson_complex_gf
+    from oracle import model as M
+    L = P.LatticePresets
+    mu, U, beta = 1.2, 2.0, 10.0
+    HExpr = P.add(L.CoulombS("C", U, -mu), L.Hopping("C", "C", complex(J), 0, 0, P.up, P.down))
+    ii, hs, S, H, rho, ops = _setup(P, HExpr, beta)
+    assert H.isComplex() == (complex(J).imag != 0)
+    spin_of = {P.down: M.DOWN, P.up: M.UP}
+    for s1 in (P.down, P.up):
+        for s2 in (P.down, P.up):
+            i1, i2 = ii.getIndex("C", 0, s1), ii.getIndex("C", 0, s2)
+            GF = P.GreensFunction(S, H, ops.getAnnihilationOperator(i1), ops.getCreationOperator(i2), rho)
+            GF.prepare()
+            GF.compute()
+            v = np.array([GF(n) for n in range(10)])
+            ref = np.array([_anderson_complex_gf(J, spin_of[s1], spin_of[s2], n, mu, U, beta) for n in range(10)])
+            assert np.abs(v - ref).max() < 1e-12
