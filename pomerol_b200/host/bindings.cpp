@@ -329,4 +329,14 @@ PYBIND11_MODULE(_pomerol, m) {
              py::return_value_policy::reference_internal)
         .def("isInContainer", [](TwoParticleGFContainer const& g, ParticleIndex i, ParticleIndex j, ParticleIndex k,
                                  ParticleIndex l) { return g.isInContainer(IndexCombination4(i, j, k, l)); });
+
+    py::class_<Vertex4>(m, "Vertex4")
+        .def(py::init<TwoParticleGF const&, GreensFunction const&, GreensFunction const&, GreensFunction const&,
+                      GreensFunction const&>(),
+             py::keep_alive<1, 2>(), py::keep_alive<1, 3>(), py::keep_alive<1, 4>(), py::keep_alive<1, 5>(),
+             py::keep_alive<1, 6>())
+        .def("compute", &Vertex4::compute, py::arg("NumberOfMatsubaras") = 0)
+        .def("__call__", &Vertex4::operator())
+        .def("value", &Vertex4::value)
+        .def("getNumberOfMatsubaras", &Vertex4::getNumberOfMatsubaras);
 }

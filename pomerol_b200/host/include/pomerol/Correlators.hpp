@@ -226,4 +226,33 @@ private:
     std::map<IndexCombination4, std::shared_ptr<TwoParticleGF>> NonTrivialElements;
 };
 
+// Two-particle vertex (Vertex4.hpp:38-104, Vertex4.cpp:34-53):
+//   Gamma(n1, n2, n3) = chi(n1, n2, n3) + beta G13(n1) G24(n2) [n1 == n3]
+//                                        - beta G14(n1) G23(n2) [n2 == n3].
+// compute(N) caches the values on the box of MatsubaraContainer4
+// (MatsubaraContainers.hpp:80-107: bosonic index Omega = n1 + n2 in
+// [-2N, 2N - 2], n1 and n3 over the 2N - |Omega + 1| fermionic indices that
+// keep n1, n2, n3 inside [-N, N)); chi is evaluated for the whole box in one
+// device call.
+class Vertex4 : public Thermal, public ComputableObject {
+public:
+    Vertex4(TwoParticleGF const& Chi, GreensFunction const& G13, GreensFunction const& G24, GreensFunction const& G14,
+            GreensFunction const& G23);
+    void compute(long NumberOfMatsubaras = 0);
+    ComplexType operator()(long MatsubaraNumber1, long MatsubaraNumber2, long MatsubaraNumber3) const;
+    ComplexType value(long MatsubaraNumber1, long MatsubaraNumber2, long MatsubaraNumber3) const;
+    long getNumberOfMatsubaras() const { return NumberOfMatsubaras; }
+
+private:
+    ComplexType disconnected(long n1, long n2, long n3) const;
+    TwoParticleGF const& Chi;
+    GreensFunction const& G13;
+    GreensFunction const& G24;
+    GreensFunction const& G14;
+    GreensFunction const& G23;
+    long NumberOfMatsubaras = 0;
+    std::vector<std::vector<ComplexType>> Values;  // per bosonic index: size x size, row n1, column n3
+    std::vector<long> Offset, Size;
+};
+
 }  // namespace Pomerol

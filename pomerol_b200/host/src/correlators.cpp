@@ -399,4 +399,59 @@ ElementWithPermFreq<TwoParticleGF>& TwoParticleGFContainer::operator()(IndexComb
     return e;
 }
 
+// ------------------------------------------------------------ Vertex4
+Vertex4::Vertex4(TwoParticleGF const& Chi, GreensFunction const& G13, GreensFunction const& G24,
+                 GreensFunction const& G14, GreensFunction const& G23)
+    : Thermal(Chi.beta), Chi(Chi), G13(G13), G24(G24), G14(G14), G23(G23) {}
+
+ComplexType Vertex4::disconnected(long n1, long n2, long n3) const {
+    ComplexType v = 0.0;
+    if (n1 == n3) v += beta * G13(n1) * G24(n2);
+    if (n2 == n3) v -= beta * G14(n1) * G23(n2);
+    return v;
+}
+
+ComplexType Vertex4::value(long n1, long n2, long n3) const { return Chi(n1, n2, n3) + disconnected(n1, n2, n3); }
+
+void Vertex4::compute(long N) {
+    if (getStatus() >= Computed) return;
+    NumberOfMatsubaras = N;
+    Values.assign(N > 0 ? 4 * N - 1 : 0, {});
+    Offset.assign(Values.size(), 0);
+    Size.assign(Values.size(), 0);
+    FreqVec3 freqs;
+    std::vector<std::tuple<long, long, long>> idx;
+    for (long bv = 0; bv < (long)Values.size(); ++bv) {
+        const long Om = bv - 2 * N;
+        Size[bv] = 2 * N - std::labs(Om + 1);
+        Offset[bv] = (Om < 0 ? 0 : Om + 1) - N;
+        for (long a = 0; a < Size[bv]; ++a)
+            for (long c = 0; c < Size[bv]; ++c) {
+                const long n1 = a + Offset[bv], n2 = Om - n1, n3 = c + Offset[bv];
+                idx.emplace_back(n1, n2, n3);
+                freqs.emplace_back(MatsubaraSpacing * RealType(2 * n1 + 1), MatsubaraSpacing * RealType(2 * n2 + 1),
+                                   MatsubaraSpacing * RealType(2 * n3 + 1));
+            }
+    }
+    const std::vector<ComplexType> chi = Chi.isVanishing() ? std::vector<ComplexType>(freqs.size(), 0.0) : Chi.values(freqs);
+    std::size_t q = 0;
+    for (long bv = 0; bv < (long)Values.size(); ++bv) {
+        Values[bv].resize(Size[bv] * Size[bv]);
+        for (long e = 0; e < Size[bv] * Size[bv]; ++e, ++q) {
+            const auto& t = idx[q];
+            Values[bv][e] = chi[q] + disconnected(std::get<0>(t), std::get<1>(t), std::get<2>(t));
+        }
+    }
+    setStatus(Computed);
+}
+
+ComplexType Vertex4::operator()(long n1, long n2, long n3) const {
+    const long bv = n1 + n2 + 2 * NumberOfMatsubaras;
+    if (NumberOfMatsubaras > 0 && bv >= 0 && bv < (long)Values.size()) {
+        const long a = n1 - Offset[bv], c = n3 - Offset[bv];
+        if (a >= 0 && a < Size[bv] && c >= 0 && c < Size[bv]) return Values[bv][a * Size[bv] + c];
+    }
+    return value(n1, n2, n3);  // outside the cached box
+}
+
 }  // namespace Pomerol

@@ -349,3 +349,41 @@ def test_anderson_complex_reference_case(P, J):
             v = np.array([GF(n) for n in range(10)])
             ref = np.array([_anderson_complex_gf(J, spin_of[s1], spin_of[s2], n, mu, U, beta) for n in range(10)])
             assert np.abs(v - ref).max() < 1e-12
+
+
+@pytest.mark.gpu
+def test_vertex4_class_reference_case(P):
+    """Vertex4Test.cpp:124-150 through the drop-in Vertex4: the connected
+    vertex of the Hubbard atom, Gamma(n1,n2,n3) = g(n1,n2,n3) G(n1)G(n2)G(n3)G(n4),
+    from Vertex4(chi_uuuu, G, G, G, G).compute(n_iw) at 1e-10; values outside
+    the cached box come from the direct evaluation."""
+    from tests.test_oracle_golden import _vertex4_refs
+    L = P.LatticePresets
+    U, beta, n_iw = 1.0, 40.0, 4
+    ii, hs, S, H, rho, ops = _setup(P, L.CoulombS("A", U, -U / 2), beta)
+    G = P.GFContainer(ii, S, H, rho, ops)
+    G.prepareAll()
+    G.computeAll()
+    Chi = P.TwoParticleGFContainer(ii, S, H, rho, ops)
+    Chi.PoleResolution = 1e-4
+    Chi.CoefficientTolerance = 1e-12
+    up = ii.getIndex("A", 0, P.up)
+    Chi.prepareAll([(up, up, up, up)])
+    Chi.computeAll()
+    g_uuuu, _, _ = _vertex4_refs(U, beta)
+    GF = G(up, up)
+    chi = Chi(up, up, up, up).element()
+    Gamma = P.Vertex4(chi, GF, GF, GF, GF)
+    Gamma.compute(n_iw)
+    assert Gamma.getNumberOfMatsubaras() == n_iw
+    for n1 in range(-n_iw, n_iw):
+        for n2 in range(-n_iw, n_iw):
+            for n3 in range(-n_iw, n_iw):
+                n4 = n1 + n2 - n3
+                ref = g_uuuu(n1, n2, n3) * GF(n1) * GF(n2) * GF(n3) * GF(n4)
+                assert abs(Gamma(n1, n2, n3) - ref) < 1e-10
+    for n1, n2, n3 in ((5, -7, 2), (-6, 6, 0)):  # outside the box
+        n4 = n1 + n2 - n3
+        ref = g_uuuu(n1, n2, n3) * GF(n1) * GF(n2) * GF(n3) * GF(n4)
+        assert abs(Gamma(n1, n2, n3) - ref) < 1e-10
+        assert abs(Gamma.value(n1, n2, n3) - Gamma(n1, n2, n3)) < 1e-14
