@@ -82,6 +82,22 @@ int pgx_assemble_hamiltonian(pgx_ctx* ctx, int32_t nterms, const int32_t* ops, c
  * host, packed like pgx_set_hamiltonian's input. */
 int pgx_get_hamiltonian(pgx_ctx* ctx, double* H);
 
+/* Reverse-mode derivative of a Green's function through the whole chain
+ * eigensolve -> weights -> operator rotation -> Lehmann sum (the reference
+ * has no derivatives).  G(z_n) is the function pgx_gf evaluates for the same
+ * (op1, op2, parts, z) without coefficient filtering; for a loss L with
+ * dL = Re sum_n lambda[n] dG(z_n) (lambda: nz complex, e.g. 2 conj(G - G_target)
+ * for sum |G - G_target|^2) it returns dterm[t] = dL/dc_t for every term of
+ * the last pgx_assemble_hamiltonian call (real part of the coefficient;
+ * a term and its Hermitian conjugate are separate terms, and the derivative
+ * assumes the perturbation of H stays symmetric), and, when dE is non-NULL,
+ * dL/dE_s for every state.  op1 and op2 are operators defined by their Fock
+ * action or adjoints of such operators.  Real Hamiltonians only; derivative
+ * terms between eigenvalues closer than 1e-10 max|E| are dropped (exact for
+ * G, which does not depend on the basis of a degenerate subspace). */
+int pgx_gf_vjp(pgx_ctx* ctx, int32_t op1, int32_t op2, int32_t nparts, const int32_t* outer, const int32_t* inner,
+               int32_t nz, const double* z, const double* lambda, double* dterm, double* dE);
+
 /* Diagonalise every block in one launch (FP64).  Eigenvalues ascending per
  * block; eigenvectors are the columns of each block's U.  The uploaded
  * Hamiltonian is kept, so this can be re-run. */

@@ -403,3 +403,27 @@ def anderson_a5_params(seed=0, nb=5):
     eps = rng.uniform(-2, 2, nb)
     V = rng.uniform(0.2, 0.8, nb)
     return 3.0, -1.5, eps, V, 20.0
+
+
+def kanamori_k(U, J, eps, V, imp="d"):
+    """Two-orbital Kanamori impurity (CoulombP with U' = U - 2J at half
+    filling, eps_d = -(3U - 5J)/2) and two bath sites per orbital, each
+    hybridised with its own orbital only: bath b{o}{k} has level eps[2o+k]
+    and hopping V[2o+k] to orbital o, both spins."""
+    e = CoulombP(imp, U, U - 2 * J, J, -(3 * U - 5 * J) / 2, 2)
+    for o in range(2):
+        for k in range(2):
+            b = f"b{o}{k}"
+            e += Level(b, float(eps[2 * o + k]))
+            for s in (UP, DOWN):
+                e += HoppingS(imp, b, float(V[2 * o + k]), o, 0, s, s)
+    return e
+
+
+def kanamori_k_params(seed=0):
+    """Bath of the differentiation workload: eps ~ U[-2,2] (4), then
+    V ~ U[0.2,0.8] (4); U=2.5, J=0.4, beta=30."""
+    rng = np.random.default_rng(seed)
+    eps = rng.uniform(-2, 2, 4)
+    V = rng.uniform(0.2, 0.8, 4)
+    return 2.5, 0.4, eps, V, 30.0

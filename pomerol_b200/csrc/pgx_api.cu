@@ -312,6 +312,7 @@ int pgx_set_hamiltonian(pgx_ctx* c, const double* H) {
         PGX_CUDA(cudaMemcpyAsync(P.d_H, H, P.msize * sc * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         PGX_CUDA(cudaStreamSynchronize(c->stream));
         P.have_H = true;
+        P.have_asm = false;  // H no longer comes from an assembled term list
         P.have_eig = P.have_w = false;
         for (auto& op : P.ops) op.rotated = false;
     });
@@ -330,6 +331,15 @@ int pgx_assemble_hamiltonian(pgx_ctx* c, int32_t nterms, const int32_t* ops, con
         P.have_H = true;
         P.have_eig = P.have_w = false;
         for (auto& op : P.ops) op.rotated = false;
+    });
+}
+
+int pgx_gf_vjp(pgx_ctx* c, int32_t op1, int32_t op2, int32_t nparts, const int32_t* outer, const int32_t* inner,
+               int32_t nz, const double* z, const double* lambda, double* dterm, double* dE) {
+    return guarded(c, [&] {
+        PGX_CHECK(nparts >= 0 && nz >= 0 && (nparts == 0 || (outer && inner)) && (nz == 0 || (z && lambda)) && dterm,
+                  PGX_ERR_ARG, "bad arguments");
+        pgx::run_gf_vjp(c, op1, op2, nparts, outer, inner, nz, z, lambda, dterm, dE);
     });
 }
 
@@ -480,6 +490,7 @@ int pgx_op_adjoint(pgx_ctx* c, int32_t src, int32_t* op_id) {
         PGX_CHECK(P.ops[src].rotated, PGX_ERR_STATE, "rotate the source operator first");
         pgx::Operator dst = pgx::take_operator(P);
         pgx::adjoint_operator(P, P.ops[src], dst, c->stream);
+        dst.adj_src = src;
         P.ops.push_back(std::move(dst));
         *op_id = (int32_t)P.ops.size() - 1;
     });

@@ -133,6 +133,12 @@ void assemble_hamiltonian(pgx_ctx* c, int nterms, const int32_t* ops, const doub
     PGX_CUDA(cudaMemcpyAsync(&status, P.d_status, sizeof(int), cudaMemcpyDeviceToHost, st));
     PGX_CUDA(cudaStreamSynchronize(st));
     PGX_CHECK(status == 0, PGX_ERR_ARG, "a Hamiltonian term connects different blocks");
+    P.have_asm = true;
+    P.asm_nterms = nterms;
+    P.d_asm_ops = d_ops;
+    P.d_asm_fock = d_fock;
+    P.d_asm_sb = d_sb;
+    P.d_asm_si = d_si;
 }
 
 }  // namespace pgx

@@ -71,6 +71,7 @@ struct Operator {
     bool rotated = false;
     bool is_complex = false;
     long total = 0;                       // elements in mat
+    int adj_src = -1;                     // for an adjoint: the operator it was formed from
 };
 
 // One exact-diagonalisation problem: blocks, eigensystem, weights, operators.
@@ -89,6 +90,14 @@ struct Problem {
         eigh_scratch;
     DevBuf op_probs, op_tiles, op_meta;  // descriptor lists of operator rotation / adjoint
     DevBuf asm_buf;                      // term list and state tables of the Hamiltonian assembly
+    // device copies of the last assembly's inputs (valid while have_asm)
+    bool have_asm = false;
+    int asm_nterms = 0;
+    const int* d_asm_ops = nullptr;
+    const uint64_t* d_asm_fock = nullptr;
+    const int* d_asm_sb = nullptr;
+    const int* d_asm_si = nullptr;
+    DevBuf vjp_buf;                      // gradient workspace of pgx_gf_vjp
     // complex blocks: real embedding of twice the size and its eigensolver workspace
     DevBuf cx_meta, cx_H, cx_A, cx_Zc, cx_U, cx_E, cx_tri, cx_S, cx_items, cx_gemm;
     std::vector<double> w_host;          // host copy of the weights (set with them)
@@ -119,6 +128,7 @@ inline Operator take_operator(Problem& P) {
     op.act_off.clear();
     op.rotated = op.is_complex = false;
     op.total = 0;
+    op.adj_src = -1;
     return op;
 }
 
@@ -246,6 +256,8 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
 void launch_weights(Problem& P, double beta, cudaStream_t st);
 void assemble_hamiltonian(pgx_ctx* c, int nterms, const int32_t* ops, const double* coef, int nmodes,
                           const uint64_t* fock, const int32_t* state_block, const int32_t* state_inner);
+void run_gf_vjp(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,
+                const double* z, const double* lambda, double* dterm, double* dE);
 void rotate_operator(Problem& P, Operator& op, cudaStream_t st);
 void adjoint_operator(Problem& P, const Operator& src, Operator& dst, cudaStream_t st);
 void run_gf(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,

@@ -24,6 +24,7 @@ EXPORTS = [
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
+    "pgx_gf_vjp",
 ]
 
 
@@ -80,6 +81,7 @@ def load():
         lib.pgx_assemble_hamiltonian.argtypes = [P, I32, P, P, I32, P, P, P]
         lib.pgx_get_hamiltonian.argtypes = [P, P]
         lib.pgx_op_release.argtypes = [P, I32]
+        lib.pgx_gf_vjp.argtypes = [P, I32, I32, I32, P, P, I32, P, P, P, P]
         _lib = lib
     return _lib
 
@@ -312,6 +314,7 @@ def _assemble_hamiltonian(self, terms, nmodes, fock, state_block, state_inner):
     sb = np.ascontiguousarray(state_block, dtype=np.int32)
     si = np.ascontiguousarray(state_inner, dtype=np.int32)
     self._ck(self.lib.pgx_assemble_hamiltonian(self.h, n, _p(ops), _p(coef), int(nmodes), _p(fock), _p(sb), _p(si)))
+    self._asm_nterms = n
 
 
 def _get_hamiltonian(self):
@@ -330,12 +333,30 @@ def _get_hamiltonian(self):
     return out
 
 
+def _gf_vjp(self, op1, op2, outer, inner, z, lam):
+    """Reverse-mode derivative of gf(op1, op2, outer, inner, z): for a loss
+    with dL = Re sum_n lam[n] dG(z_n), returns (dL/dc_t for every term of the
+    last assemble_hamiltonian call, dL/dE_s for every state)."""
+    z = np.ascontiguousarray(np.asarray(z, dtype=complex))
+    lam = np.ascontiguousarray(np.asarray(lam, dtype=complex))
+    if lam.shape != z.shape:
+        raise ValueError("lam needs one entry per frequency")
+    o = np.ascontiguousarray(outer, dtype=np.int32)
+    i = np.ascontiguousarray(inner, dtype=np.int32)
+    dterm = np.zeros(max(getattr(self, "_asm_nterms", 0), 1))
+    dE = np.zeros(int(sum(self.dims)))
+    self._ck(self.lib.pgx_gf_vjp(self.h, int(op1), int(op2), len(o), _p(o), _p(i), len(z), _p(z.view(np.float64)),
+                                 _p(lam.view(np.float64)), _p(dterm), _p(dE)))
+    return dterm[:getattr(self, "_asm_nterms", 0)], dE
+
+
 def _op_release(self, op_id):
     """Give an operator's device memory back to the context for reuse."""
     self._ck(self.lib.pgx_op_release(self.h, int(op_id)))
 
 
 Engine.op_release = _op_release
+Engine.gf_vjp = _gf_vjp
 Engine.assemble_hamiltonian = _assemble_hamiltonian
 Engine.get_hamiltonian = _get_hamiltonian
 Engine.timer_begin = _timer_begin

@@ -97,3 +97,65 @@ class GpuED:
     def g2(self, C1, C2, CX3, CX4, triples, pole_res=1e-8):
         parts = self.g2_parts(C1, C2, CX3, CX4)
         return self.eng.g2(parts, triples, pole_res=pole_res), parts
+
+
+class GfTermChain:
+    """G(z) = <c_i c^+_j>(z) as a function of the coefficients of the
+    Hamiltonian's terms, through the C ABI: pgx_assemble_hamiltonian ->
+    pgx_eigh -> pgx_weights -> pgx_op_rotate / pgx_op_adjoint -> pgx_gf
+    (forward) and pgx_gf_vjp (backward).  The backward pass uses the device
+    state of the last forward call."""
+
+    def __init__(self, mdl, beta, i, j, z, device=0):
+        self.m, self.beta, self.z = mdl, float(beta), np.asarray(z, dtype=complex)
+        self.keys = list(mdl.expr.terms)
+        self.monos = [tuple((dag, mdl.info.index[ix]) for dag, ix in k) for k in self.keys]
+        self.fock = np.concatenate([np.asarray(b, dtype=np.uint64) for b in mdl.blocks])
+        self.sb, self.si = np.asarray(mdl.block_of), np.asarray(mdl.inner)
+        self.eng = Engine(device)
+        self.eng.set_blocks(mdl.block_sizes(), mdl.complex)
+        self.g = GpuED.__new__(GpuED)  # operator helpers on this engine (no host Hamiltonian upload)
+        self.g.m, self.g.beta, self.g.eng = mdl, beta, self.eng
+        self.g.retained = np.ones(len(mdl.blocks), dtype=bool)
+        self.g._cdag, self.g._c = {}, {}
+        self.i, self.j = i, j
+        self.op1 = self.op2 = None
+
+    def forward(self, coef):
+        terms = [(mono, float(c)) for mono, c in zip(self.monos, coef)]
+        self.eng.assemble_hamiltonian(terms, self.m.info.size(), self.fock, self.sb, self.si)
+        self.eng.eigh()
+        self.eng.weights(self.beta)
+        if self.op1 is not None:
+            for op in {self.op1, self.op2}:
+                self.eng.op_release(op)
+            if self.j != self.i:
+                self.eng.op_release(self.g._cdag[self.i])
+        self.g._cdag, self.g._c = {}, {}
+        self.op2 = self.g.cdag(self.j)
+        self.op1 = self.g.c(self.i)
+        self.outer, self.inner = self.g.pair_parts(self.op1, self.op2)
+        return self.eng.gf(self.op1, self.op2, self.outer, self.inner, self.z, coef_tol=0.0)
+
+    def vjp(self, lam):
+        return self.eng.gf_vjp(self.op1, self.op2, self.outer, self.inner, self.z, lam)
+
+
+def gf_of_terms():
+    """torch.autograd.Function over GfTermChain: real coefficient tensor ->
+    complex G tensor.  For a real loss torch passes dL/dRe G + i dL/dIm G as
+    the output gradient, so lambda = conj(grad_output)."""
+    import torch
+
+    class GfOfTerms(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, coef, chain):
+            ctx.chain = chain
+            return torch.from_numpy(chain.forward(coef.detach().cpu().numpy()))
+
+        @staticmethod
+        def backward(ctx, grad_out):
+            dterm, _ = ctx.chain.vjp(np.conj(grad_out.detach().cpu().numpy()))
+            return torch.from_numpy(dterm), None
+
+    return GfOfTerms

@@ -503,3 +503,158 @@ def test_anderson_complex_closed_form(harness, J):
             v = g.gf(g.c(i1), g.cdag(i2), z)
             ref = np.array([_anderson_complex_gf(J, s1, s2, k) for k in n])
             assert np.abs(v - ref).max() < 1e-12
+
+
+def _anderson_expr(p):
+    """Anderson impurity C with bath sites b_k: U n_up n_dn - mu n + sum_k
+    eps_k n_k + V_k (c+_C b_k + h.c.) (+ field h on C)."""
+    e = M.CoulombS("C", p["U"], -p["mu"]) + M.Magnetization("C", p["h"])
+    for k, (ek, vk) in enumerate(zip(p["eps"], p["V"])):
+        e += M.Level(f"b{k}", ek) + M.Hopping("C", f"b{k}", vk)
+    return e
+
+
+def _term_coefs(p, keys):
+    terms = M.make_model(_anderson_expr(p)).expr.terms
+    assert set(terms) == set(keys)
+    return np.array([complex(terms[k]).real for k in keys])
+
+
+def _exact_gf(p, i, j, beta, z):
+    """<c_i c+_j>(z) of the oracle's dense eigensolve (no term filtering)."""
+    m = M.make_model(_anderson_expr(p))
+    ed = EDm.ED(m, beta)
+    return L.gf_eval(L.gf_terms(ed, EDm.adjoint(ed.cdag(i)), ed.cdag(j), rule=False), z)
+
+
+@pytest.mark.parametrize("field,offdiag", [(0.0, False), (0.15, False), (0.15, True)])
+def test_gf_vjp_against_finite_differences(field, offdiag):
+    """pgx_gf_vjp: dL/dc_t of every assembled term, contracted with dc_t/dtheta
+    for theta in (U, mu, eps_k, V_k, h), against central differences (step
+    1e-5) of L(theta) evaluated with the oracle's exact G.  L = sum_n |G(z_n) -
+    G_target(z_n)|^2 (lambda = 2 conj(G - G_target)) plus a random linear
+    functional Re sum_n lambda'_n G(z_n); relative tolerance 1e-6."""
+    from tests.pgx_harness import GpuED
+    beta = 8.0
+    p0 = {"U": 2.0, "mu": 0.9, "h": field, "eps": [-0.6, 0.35], "V": [0.45, 0.3]}
+    m = M.make_model(_anderson_expr(p0))
+    keys = list(m.expr.terms)
+    terms, nmodes, fock, sb, si = _assembly_inputs(m)
+    i = m.info.getIndex("C", 0, M.DOWN)
+    j = m.info.getIndex("b0", 0, M.DOWN) if offdiag else i
+    z = 1j * np.pi * (2 * np.arange(12) + 1) / beta
+    g = GpuED(m, beta)
+    g.eng.assemble_hamiltonian(terms, nmodes, fock, sb, si)
+    g.eng.eigh()
+    g.E, g.U = g.eng.eigensystem()
+    g.w, g.Z = g.eng.weights(beta)
+    op1, op2 = g.c(i), g.cdag(j)
+    outer, inner = g.pair_parts(op1, op2)
+    G = g.eng.gf(op1, op2, outer, inner, z, coef_tol=0.0)
+    ref = _exact_gf(p0, i, j, beta, z)
+    assert np.abs(G - ref).max() < 1e-12
+    rng = np.random.default_rng(11)
+    target = ref * (1 + 0.1 * rng.standard_normal(len(z))) + 0.01j
+    lin = rng.standard_normal(len(z)) + 1j * rng.standard_normal(len(z))
+    losses = {
+        "squared": (lambda G: float(np.sum(np.abs(G - target) ** 2)), 2 * np.conj(G - target)),
+        "linear": (lambda G: float(np.real(np.sum(lin * G))), lin),
+    }
+    h = 1e-5
+    thetas = [("U",), ("mu",), ("h",), ("eps", 0), ("eps", 1), ("V", 0), ("V", 1)]
+
+    def shifted(th, d):
+        q = {k: (list(v) if isinstance(v, list) else v) for k, v in p0.items()}
+        if len(th) == 1:
+            q[th[0]] += d
+        else:
+            q[th[0]][th[1]] += d
+        return q
+
+    for name, (loss, lam) in losses.items():
+        dterm, dE = g.eng.gf_vjp(op1, op2, outer, inner, z, lam)
+        assert dterm.shape == (len(keys),) and dE.shape == (int(sum(m.block_sizes())),)
+        assert abs(dE.sum()) < 1e-10 * max(1.0, np.abs(dE).max())  # G depends on energy differences only
+        for th in thetas:
+            if th == ("h",) and field == 0.0:
+                continue
+            qp, qm = shifted(th, h), shifted(th, -h)
+            dc = (_term_coefs(qp, keys) - _term_coefs(qm, keys)) / (2 * h)
+            got = float(dc @ dterm)
+            fd = (loss(_exact_gf(qp, i, j, beta, z)) - loss(_exact_gf(qm, i, j, beta, z))) / (2 * h)
+            assert abs(got - fd) <= 1e-6 * max(1.0, abs(fd)), (name, th, got, fd)
+
+
+def _k_theta_coefs(keys, eps, V, U, J):
+    from oracle import gradient as GR
+    return GR.term_coefficients(M.kanamori_k(U, J, eps, V), keys)
+
+
+def test_gf_vjp_kanamori_differentiation_workload():
+    """Differentiation workload: two-orbital Kanamori impurity (U=2.5, J=0.4,
+    U'=U-2J, half filling) with two bath sites per orbital (dim 4096),
+    beta=30, L = sum_{n<512} |G_d0dn(i w_n) - G_target(i w_n)|^2, the target
+    from the bath of seed 2.  The gradient of L with respect to the eight
+    bath parameters and U, from pgx_gf_vjp through the torch.autograd wrapper
+    of the test harness, against (1) the FP64 reference gradient of the oracle
+    (1e-9 relative), (2) central differences (h=1e-6) of L evaluated with the
+    GPU forward chain and (3) with the oracle's exact G (1e-6 relative)."""
+    import torch
+    from oracle import gradient as GR
+    from tests.pgx_harness import GfTermChain, gf_of_terms
+    U, J, eps, V, beta = M.kanamori_k_params(0)
+    _, _, eps_t, V_t, _ = M.kanamori_k_params(2)
+    m = M.make_model(M.kanamori_k(U, J, eps, V))
+    keys = list(m.expr.terms)
+    i = m.info.getIndex("d", 0, M.DOWN)
+    z = 1j * np.pi * (2 * np.arange(512) + 1) / beta
+    G_t = GR.gf_exact(M.make_model(M.kanamori_k(U, J, eps_t, V_t)), beta, i, i, z)
+    theta0 = np.concatenate([eps, V, [U]])
+
+    def coefs(th):
+        return _k_theta_coefs(keys, th[0:4], th[4:8], th[8], J)
+
+    # coefficients are linear in theta: the Jacobian from unit-sized differences is exact
+    Jac = np.stack([(coefs(theta0 + 0.5 * e) - coefs(theta0 - 0.5 * e)) for e in np.eye(9)], axis=1)
+    chain = GfTermChain(m, beta, i, i, z)
+    Fn = gf_of_terms()
+    theta = torch.tensor(theta0, dtype=torch.float64, requires_grad=True)
+    c0 = torch.from_numpy(coefs(theta0) - Jac @ theta0)
+    G = Fn.apply(c0 + torch.from_numpy(Jac) @ theta, chain)
+    loss = ((G - torch.from_numpy(G_t)).abs() ** 2).sum()
+    loss.backward()
+    grad = theta.grad.numpy()
+    # (1) the FP64 reference gradient
+    G_ref = GR.gf_exact(m, beta, i, i, z)
+    assert np.abs(G.detach().numpy() - G_ref).max() < 1e-11
+    dterm_ref, _ = GR.gf_term_gradient(m, beta, i, i, z, 2 * np.conj(G_ref - G_t))
+    ref = Jac.T @ dterm_ref
+    assert np.abs(grad - ref).max() <= 1e-9 * np.abs(ref).max(), (grad, ref)
+    # timing of one gradient call (device time between events on the context's stream)
+    lam = 2 * np.conj(G.detach().numpy() - G_t)
+    chain.vjp(lam)
+    chain.eng.profile_begin()
+    chain.eng.timer_begin()
+    chain.vjp(lam)
+    ms = chain.eng.timer_end()
+    prof = chain.eng.profile_end()
+    print(f"\npgx_gf_vjp Kanamori dim 4096, 512 frequencies: {ms:.3f} ms device time")
+    for k in prof:
+        print(f"  {k['name']:<40s} {k['launches']:3d} launches {k['ms']:8.3f} ms")
+
+    def loss_gpu(th):
+        return float(np.sum(np.abs(chain.forward(coefs(th)) - G_t) ** 2))
+
+    def loss_oracle(th):
+        mm = M.make_model(M.kanamori_k(th[8], J, th[0:4], th[4:8]))
+        return float(np.sum(np.abs(GR.gf_exact(mm, beta, i, i, z) - G_t) ** 2))
+
+    h = 1e-6
+    for k in range(9):
+        e = np.eye(9)[k] * h
+        fd = (loss_gpu(theta0 + e) - loss_gpu(theta0 - e)) / (2 * h)
+        assert abs(grad[k] - fd) <= 1e-6 * max(1.0, abs(fd)), (k, grad[k], fd)
+    for k in (0, 5, 8):  # one bath energy, one hybridisation, U
+        e = np.eye(9)[k] * h
+        fd = (loss_oracle(theta0 + e) - loss_oracle(theta0 - e)) / (2 * h)
+        assert abs(grad[k] - fd) <= 1e-6 * max(1.0, abs(fd)), (k, grad[k], fd)
