@@ -18,8 +18,10 @@ OUT = Path(__file__).with_name("reference_kats.json")
 NUM = r"[-+]?\d+\.?\d*(?:[eE][-+]?\d+)?"
 
 
-def block_after(text, marker):
-    i = text.index(marker)
+def block_after(text, marker, occurrence=0):
+    i = -1
+    for _ in range(occurrence + 1):
+        i = text.index(marker, i + 1)
     j = text.index(";", i)
     # drop // comments line by line before the entries are split
     return "\n".join(line.split("//")[0] for line in text[i:j].splitlines())
@@ -63,6 +65,8 @@ def main():
     ad = complex_list(block_after(t, "G_ref_down <<"))
     t = (REF / "test/HamiltonianTest.cpp").read_text()
     e0 = float(re.search(rf"E_ref = ({NUM})", t).group(1))
+    t = (REF / "test/3PSusc3siteTest.cpp").read_text()
+    chi3 = [complex_list(block_after(t, "chi3_ref <<", q)) for q in range(3)]
     kats = {
         "anderson2pgf": {
             "source": "test/Anderson2PGFTest.cpp:37-58,97-126",
@@ -89,6 +93,17 @@ def main():
             "source": "test/AndersonTest.cpp:31-124",
             "U": 3.7, "mu_over_U": 0.6, "h": 0.1, "V": 1.0, "epsilon": 2.3, "beta": 20.0,
             "G_up": au, "G_down": ad, "tol": 1e-8,
+        },
+        "chi3_3site": {
+            "source": "test/3PSusc3siteTest.cpp:24-157",
+            "U": 4.0, "mu": 2.4, "t": 1.0, "beta": 5.0,
+            "sites": ["A", "B", "C"],
+            "n": [-1, 0, 1],
+            "PP": {"ops": [["A", "up"], ["C", "up"], ["A", "down"], ["C", "down"]], "chi3": chi3[0]},
+            "PH": {"ops": [["A", "up"], ["A", "up"], ["C", "down"], ["C", "down"]], "chi3": chi3[1]},
+            "xPH": {"ops": [["A", "up"], ["C", "up"], ["C", "down"], ["A", "down"]], "chi3": chi3[2]},
+            "layout": "chi3[(n1 + 1) * 3 + (n2 + 1)] for n1, n2 in n",
+            "tol": 1e-10,
         },
         "hamiltonian": {
             "source": "test/HamiltonianTest.cpp:31-75",
