@@ -218,6 +218,37 @@ int pgx_g2_count(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, double 
                  long long* count);
 
 /* ------------------------------------------------------------------------
+ * K6 Three-point fermion-boson susceptibility.
+ * Replaces: ThreePointSusceptibility::compute / operator() and
+ * ThreePointSusceptibilityPart::computeImpl, addMultiterm and the term
+ * evaluation (ThreePointSusceptibility.cpp:144-230,
+ * ThreePointSusceptibilityPart.cpp:243-357, ThreePointSusceptibilityPart.hpp:516-538).
+ * ------------------------------------------------------------------------ */
+
+#define PGX_PP 0  /* channels, as the reference's Channel enum (Misc.hpp:160-164) */
+#define PGX_PH 1
+#define PGX_XPH 2
+
+/* One part <i|F1|j><j|F2|k><k|B1|m><m|B2|i> of ThreePointSusceptibility::prepare
+ * (ThreePointSusceptibility.cpp:77-134): f1, f2 are the part's first and
+ * second fermionic operators (already exchanged when swapped != 0), b1, b2
+ * the factors of the quadratic operator; block = {i, j, k, m}. */
+typedef struct pgx_chi3_part {
+    int32_t f1, f2, b1, b2;
+    int32_t block[4];
+    int32_t swapped;
+} pgx_chi3_part;
+
+/* out[t] = sum over parts of the three-point susceptibility at the duplet
+ * t = (z1, z2) (z: 2*nfreq complex; out: nfreq complex), summed over every
+ * state triple without the reference's coefficient filter and pole merge.
+ * The term type of a triple is chosen by |E_i - E_k| <= pole_res and the
+ * resonant delta by |z1 - xi z2| <= pole_res (xi = -1 for PP, 1 otherwise),
+ * as in the reference.  Needs pgx_weights (beta) first. */
+int pgx_chi3(pgx_ctx* ctx, int32_t channel, int32_t nparts, const pgx_chi3_part* parts, int32_t nfreq,
+             const double* z, double pole_res, double* out);
+
+/* ------------------------------------------------------------------------
  * Allocation-free eigensolve (no counterpart in the reference).
  * For callers whose device memory belongs to an outer allocator (an
  * application's caching pool or a fixed arena) and which must not let a

@@ -193,7 +193,8 @@ void reset_problem(pgx::Problem& P) {
                                          &pgx::Problem::asm_buf, &pgx::Problem::cx_meta, &pgx::Problem::cx_H,
                                          &pgx::Problem::cx_A,    &pgx::Problem::cx_Zc,   &pgx::Problem::cx_U,
                                          &pgx::Problem::cx_E,    &pgx::Problem::cx_tri,  &pgx::Problem::cx_S,
-                                         &pgx::Problem::cx_items, &pgx::Problem::cx_gemm};
+                                         &pgx::Problem::cx_items, &pgx::Problem::cx_gemm, &pgx::Problem::vjp_buf,
+                                         &pgx::Problem::chi3_small, &pgx::Problem::chi3_big};
     for (auto m : bufs) fresh.*m = std::move(P.*m);
     fresh.spare_ops = std::move(P.spare_ops);
     for (auto& op : P.ops) fresh.spare_ops.push_back(std::move(op));
@@ -340,6 +341,15 @@ int pgx_gf_vjp(pgx_ctx* c, int32_t op1, int32_t op2, int32_t nparts, const int32
         PGX_CHECK(nparts >= 0 && nz >= 0 && (nparts == 0 || (outer && inner)) && (nz == 0 || (z && lambda)) && dterm,
                   PGX_ERR_ARG, "bad arguments");
         pgx::run_gf_vjp(c, op1, op2, nparts, outer, inner, nz, z, lambda, dterm, dE);
+    });
+}
+
+int pgx_chi3(pgx_ctx* c, int32_t channel, int32_t nparts, const pgx_chi3_part* parts, int32_t nfreq,
+             const double* z, double pole_res, double* out) {
+    return guarded(c, [&] {
+        PGX_CHECK(nparts >= 0 && nfreq >= 0 && (nparts == 0 || parts) && (nfreq == 0 || (z && out)), PGX_ERR_ARG,
+                  "bad arguments");
+        pgx::run_chi3(c, channel, nparts, parts, nfreq, z, pole_res, out);
     });
 }
 

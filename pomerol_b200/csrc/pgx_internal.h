@@ -98,6 +98,7 @@ struct Problem {
     const int* d_asm_sb = nullptr;
     const int* d_asm_si = nullptr;
     DevBuf vjp_buf;                      // gradient workspace of pgx_gf_vjp
+    DevBuf chi3_small, chi3_big;         // per-part constants / frequency-dependent matrices of pgx_chi3
     // complex blocks: real embedding of twice the size and its eigensolver workspace
     DevBuf cx_meta, cx_H, cx_A, cx_Zc, cx_U, cx_E, cx_tri, cx_S, cx_items, cx_gemm;
     std::vector<double> w_host;          // host copy of the weights (set with them)
@@ -269,6 +270,8 @@ void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const d
             double coef_tol, int flags, double* out);
 void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
                      double anchor_tol, double* out);
+void run_chi3(pgx_ctx* c, int channel, int nparts, const pgx_chi3_part* parts, int nfreq, const double* z,
+              double pole_res, double* out);
 void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_tol, double nz_tol, long long* count);
 
 }  // namespace pgx

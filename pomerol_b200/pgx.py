@@ -24,7 +24,7 @@ EXPORTS = [
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
-    "pgx_gf_vjp",
+    "pgx_gf_vjp", "pgx_chi3",
 ]
 
 
@@ -82,6 +82,7 @@ def load():
         lib.pgx_get_hamiltonian.argtypes = [P, P]
         lib.pgx_op_release.argtypes = [P, I32]
         lib.pgx_gf_vjp.argtypes = [P, I32, I32, I32, P, P, I32, P, P, P, P]
+        lib.pgx_chi3.argtypes = [P, I32, I32, P, I32, P, D, P]
         _lib = lib
     return _lib
 
@@ -350,6 +351,23 @@ def _gf_vjp(self, op1, op2, outer, inner, z, lam):
     return dterm[:getattr(self, "_asm_nterms", 0)], dE
 
 
+PGX_PP, PGX_PH, PGX_XPH = 0, 1, 2
+
+
+def _chi3(self, channel, parts, freqs, pole_res=1e-8):
+    """Three-point susceptibility at (z1, z2) duplets.  parts: list of
+    (f1, f2, b1, b2, (i, j, k, m), swapped) as ThreePointSusceptibility::prepare
+    forms them (operators of the part, blocks <i|f1|j><j|f2|k><k|b1|m><m|b2|i>)."""
+    desc = np.zeros((max(len(parts), 1), 9), dtype=np.int32)
+    for q, (f1, f2, b1, b2, blk, sw) in enumerate(parts):
+        desc[q] = [f1, f2, b1, b2, *blk, 1 if sw else 0]
+    fz = np.ascontiguousarray(np.asarray(freqs, dtype=complex).reshape(-1, 2))
+    out = np.zeros(len(fz), dtype=complex)
+    self._ck(self.lib.pgx_chi3(self.h, int(channel), len(parts), _p(desc), len(fz), _p(fz.view(np.float64)),
+                               float(pole_res), _p(out.view(np.float64))))
+    return out
+
+
 def _op_release(self, op_id):
     """Give an operator's device memory back to the context for reuse."""
     self._ck(self.lib.pgx_op_release(self.h, int(op_id)))
@@ -357,6 +375,7 @@ def _op_release(self, op_id):
 
 Engine.op_release = _op_release
 Engine.gf_vjp = _gf_vjp
+Engine.chi3 = _chi3
 Engine.assemble_hamiltonian = _assemble_hamiltonian
 Engine.get_hamiltonian = _get_hamiltonian
 Engine.timer_begin = _timer_begin

@@ -94,6 +94,34 @@ class GpuED:
                 parts.append(((ops[o0], ops[o1], ops[o2], CX4), (S1, S2, S3, S4), perm, sign))
         return parts
 
+    def chi3_parts(self, channel, CX1, C2, CX3, C4):
+        """ThreePointSusceptibility::prepare (ThreePointSusceptibility.cpp:68-142)
+        over the operators' block maps."""
+        F1, F2, B1, B2 = {0: (CX1, CX3, C2, C4), 1: (CX1, C2, CX3, C4), 2: (CX1, C4, CX3, C2)}[channel]
+        f1_rl, f1_lr = self.maps(F1)
+        f2_rl, f2_lr = self.maps(F2)
+        b1_rl, _ = self.maps(B1)
+        b2_rl, _ = self.maps(B2)
+        ret = self.retained
+        parts = []
+        for b2r in sorted(b2_rl):
+            b2l = b2_rl[b2r]
+            b1l = b1_rl.get(b2l)
+            if b1l is None:
+                continue
+            j = f1_lr.get(b2r)
+            if j is not None and f2_rl.get(b1l) == j and ret[b2r] and ret[j] and ret[b1l]:
+                parts.append((F1, F2, B1, B2, (b2r, j, b1l, b2l), False))
+            j = f2_lr.get(b2r)
+            if j is not None and f1_rl.get(b1l) == j and ret[b2r] and ret[j] and ret[b1l]:
+                parts.append((F2, F1, B1, B2, (b2r, j, b1l, b2l), True))
+        return parts
+
+    def chi3(self, channel, ixs, freqs, pole_res=1e-8):
+        i1, i2, i3, i4 = ixs
+        parts = self.chi3_parts(channel, self.cdag(i1), self.c(i2), self.cdag(i3), self.c(i4))
+        return self.eng.chi3(channel, parts, freqs, pole_res), parts
+
     def g2(self, C1, C2, CX3, CX4, triples, pole_res=1e-8):
         parts = self.g2_parts(C1, C2, CX3, CX4)
         return self.eng.g2(parts, triples, pole_res=pole_res), parts

@@ -658,3 +658,105 @@ def test_gf_vjp_kanamori_differentiation_workload():
         e = np.eye(9)[k] * h
         fd = (loss_oracle(theta0 + e) - loss_oracle(theta0 - e)) / (2 * h)
         assert abs(grad[k] - fd) <= 1e-6 * max(1.0, abs(fd)), (k, grad[k], fd)
+
+
+@pytest.mark.parametrize("channel", ["PP", "PH", "xPH"])
+def test_chi3_three_site_golden(harness, channel):
+    """pgx_chi3 on the reference's three-site cluster (3PSusc3siteTest.cpp:24-157):
+    golden values at 1e-10 and the exact oracle at 1e-12."""
+    from oracle import chi3 as X
+    k = KATS["chi3_3site"]
+    e = M.Expr()
+    for s in k["sites"]:
+        e += M.CoulombS(s, k["U"], -k["mu"])
+    for a, b in (("A", "B"), ("B", "C"), ("C", "A")):
+        e += M.Hopping(a, b, -k["t"])
+    m = M.make_model(e)
+    g = harness(m, k["beta"])
+    spin = {"up": M.UP, "down": M.DOWN}
+    ixs = [m.info.getIndex(s, 0, spin[sp]) for s, sp in k[channel]["ops"]]
+    ch = {"PP": X.PP, "PH": X.PH, "xPH": X.XPH}[channel]
+    freqs = [(L.fermionic(a, k["beta"]), L.fermionic(b, k["beta"])) for a in k["n"] for b in k["n"]]
+    v, parts = g.chi3(ch, ixs, freqs)
+    assert np.abs(v - cplx(k[channel]["chi3"])).max() < k["tol"]
+    ed = EDm.ED(m, k["beta"])
+    oparts = X.chi3_parts(ed, ch, ed.cdag(ixs[0]), ed.c(ixs[1]), ed.cdag(ixs[2]), ed.c(ixs[3]))
+    assert len(parts) == len(oparts)
+    assert np.abs(v - X.chi3_exact(ed, oparts, ch, freqs)).max() < 1e-12
+
+
+@pytest.mark.parametrize("h", [0.0, 0.01])
+def test_chi3_hubbard_atom_closed_form(harness, h):
+    """All channels and spin combinations of the Hubbard atom against its
+    closed form (3PSusc1siteTest.cpp:38-209), including the resonant
+    beta delta at z1 = -xi z2, on a 12 x 12 grid."""
+    from oracle import chi3 as X
+    from tests.test_oracle_chi3 import AtomChi3
+    U, mu, beta, n_iw = 1.0, 0.4, 10.0, 6
+    m = M.make_model(M.CoulombS("A", U, -mu) + M.Magnetization("A", -h))
+    g = harness(m, beta)
+    up, dn = m.info.getIndex("A", 0, M.UP), m.info.getIndex("A", 0, M.DOWN)
+    ga = AtomChi3(beta, U, mu, h)
+    st = {up: 1, dn: 2}
+    om = lambda n: np.pi * (2 * n + 1) / beta
+    grid = [(a, b) for a in range(-n_iw, n_iw) for b in range(-n_iw, n_iw)]
+    freqs = [(1j * om(a), 1j * om(b)) for a, b in grid]
+    for i1 in (up, dn):
+        for i2 in (up, dn):
+            other = dn if i1 == up else up
+            v, parts = g.chi3(X.PP, (i1, i1, i2, i2), freqs)
+            if i1 == i2:
+                assert not parts and np.all(v == 0)
+            else:
+                ref = np.array([ga(3, st[i2], 0, -om(a), -om(b)) + ga(3, st[i1], 0, -om(b), -om(a)) for a, b in grid])
+                assert np.abs(v - ref).max() < 1e-13
+            if i1 == i2:
+                ref = np.array([ga(st[i1], 0, st[i1], -om(a), om(b)) + ga(3, st[other], 3, -om(a), om(b))
+                                for a, b in grid])
+                refx = -ref
+            else:
+                s = st[i2]
+                ref = np.array([ga(3, s, 3, -om(a), om(b)) - ga(s, 3, s, om(a), -om(b)) for a, b in grid])
+                refx = np.array([-ga(st[i1], 0, st[i2], -om(a), om(b)) - ga(st[i1], 3, st[i2], om(b), -om(a))
+                                 for a, b in grid])
+            v, _ = g.chi3(X.PH, (i1, i1, i2, i2), freqs)
+            assert np.abs(v - ref).max() < 1e-13
+            v, _ = g.chi3(X.XPH, (i1, i1, i2, i2), freqs)
+            assert np.abs(v - refx).max() < 1e-13
+
+
+@pytest.mark.parametrize("complex_h", [False, True])
+def test_chi3_random_duplets_against_exact_oracle(harness, complex_h):
+    """Anderson impurity with three bath sites (real, or with a complex
+    hopping): every channel for several operator quadruples on a list of
+    duplets that repeats values, contains the resonant z1 = -xi z2 pairs and
+    off-axis complex frequencies, against the exact oracle (1e-11 relative)."""
+    from oracle import chi3 as X
+    beta = 6.0
+    e = M.CoulombS("C", 2.2, -1.1) + M.Magnetization("C", 0.07)
+    for k, (ek, vk) in enumerate([(-0.8, 0.5), (0.3, 0.35), (1.1, 0.6)]):
+        e += M.Level(f"b{k}", ek) + M.Hopping("C", f"b{k}", vk)
+    if complex_h:
+        e += M.HoppingS("b0", "b1", 0.2 + 0.15j, 0, 0, M.UP, M.UP) + M.HoppingS("b0", "b1", 0.2 + 0.15j, 0, 0,
+                                                                                  M.DOWN, M.DOWN)
+    m = M.make_model(e)
+    assert m.complex == complex_h
+    g = harness(m, beta)
+    ed = EDm.ED(m, beta)
+    rng = np.random.default_rng(7)
+    n = rng.integers(-5, 5, size=(40, 2))
+    freqs = [(L.fermionic(a, beta), L.fermionic(b, beta)) for a, b in n]
+    freqs += [(L.fermionic(a, beta), L.fermionic(-a - 1, beta)) for a in range(-3, 3)]   # z1 + z2 = 0
+    freqs += [(L.fermionic(a, beta), L.fermionic(a, beta)) for a in range(-3, 3)]        # z1 - z2 = 0
+    freqs += [(0.3 + 0.7j, -0.2 + 1.1j), (1.5 + 0.2j, 0.4 - 0.9j)]
+    freqs += freqs[:5]
+    up, dn = M.UP, M.DOWN
+    c0 = lambda s: m.info.getIndex("C", 0, s)
+    b0 = lambda s: m.info.getIndex("b0", 0, s)
+    for ixs in [(c0(up), c0(up), c0(dn), c0(dn)), (c0(up), b0(up), c0(dn), b0(dn)), (c0(up), c0(dn), c0(dn), c0(up))]:
+        for ch in (X.PP, X.PH, X.XPH):
+            v, parts = g.chi3(ch, ixs, freqs)
+            oparts = X.chi3_parts(ed, ch, ed.cdag(ixs[0]), ed.c(ixs[1]), ed.cdag(ixs[2]), ed.c(ixs[3]))
+            assert len(parts) == len(oparts)
+            ref = X.chi3_exact(ed, oparts, ch, freqs)
+            assert np.abs(v - ref).max() <= 1e-11 * max(1.0, np.abs(ref).max()), (ixs, ch)
