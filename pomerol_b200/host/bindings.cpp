@@ -30,6 +30,7 @@ py::object as_matrix(std::vector<double> const& v, long rows, long cols, bool cp
 }
 
 FreqVec3 to_freqs(std::vector<std::tuple<C, C, C>> const& f) { return FreqVec3(f.begin(), f.end()); }
+FreqVec2 to_freqs2(std::vector<std::tuple<C, C>> const& f) { return FreqVec2(f.begin(), f.end()); }
 
 template <typename E> void bind_expr(py::module& m, char const* name) {
     py::class_<E>(m, name)
@@ -329,6 +330,73 @@ PYBIND11_MODULE(_pomerol, m) {
              py::return_value_policy::reference_internal)
         .def("isInContainer", [](TwoParticleGFContainer const& g, ParticleIndex i, ParticleIndex j, ParticleIndex k,
                                  ParticleIndex l) { return g.isInContainer(IndexCombination4(i, j, k, l)); });
+
+    py::enum_<Channel>(m, "Channel").value("PP", PP).value("PH", PH).value("xPH", xPH).export_values();
+
+    py::class_<ThreePointSusceptibility>(m, "ThreePointSusceptibility")
+        .def(py::init<Channel, StatesClassification const&, Hamiltonian const&, CreationOperator const&,
+                      AnnihilationOperator const&, CreationOperator const&, AnnihilationOperator const&,
+                      DensityMatrix const&>(),
+             py::keep_alive<1, 3>(), py::keep_alive<1, 4>(), py::keep_alive<1, 5>(), py::keep_alive<1, 6>(),
+             py::keep_alive<1, 7>(), py::keep_alive<1, 8>(), py::keep_alive<1, 9>())
+        .def_readwrite("PoleResolution", &ThreePointSusceptibility::PoleResolution)
+        .def_readwrite("CoefficientTolerance", &ThreePointSusceptibility::CoefficientTolerance)
+        .def("prepare", &ThreePointSusceptibility::prepare)
+        .def("compute",
+             [](ThreePointSusceptibility& g, bool clear, std::vector<std::tuple<C, C>> const& f, int) {
+                 return g.compute(clear, to_freqs2(f));
+             },
+             py::arg("clear") = false, py::arg("freqs") = std::vector<std::tuple<C, C>>(), py::arg("comm") = 0)
+        .def("__call__", py::overload_cast<long, long>(&ThreePointSusceptibility::operator(), py::const_))
+        .def("__call__", py::overload_cast<C, C>(&ThreePointSusceptibility::operator(), py::const_))
+        .def("values",
+             [](ThreePointSusceptibility const& g, std::vector<std::tuple<C, C>> const& f) {
+                 return g.values(to_freqs2(f));
+             })
+        .def("isVanishing", &ThreePointSusceptibility::isVanishing)
+        .def("getNumParts", &ThreePointSusceptibility::getNumParts)
+        .def("getIndex", &ThreePointSusceptibility::getIndex)
+        .def("parts", [](ThreePointSusceptibility const& g) {
+            std::vector<std::tuple<std::array<int, 4>, int>> r;
+            for (auto const& p : g.deviceParts())
+                r.emplace_back(std::array<int, 4>{p.block[0], p.block[1], p.block[2], p.block[3]}, p.swapped);
+            return r;
+        });
+
+    py::class_<ElementWithPermFreq<ThreePointSusceptibility>>(m, "ThreePointSusceptibilityElement")
+        .def("element", &ElementWithPermFreq<ThreePointSusceptibility>::element,
+             py::return_value_policy::reference_internal);
+
+    py::class_<ThreePointSusceptibilityContainer>(m, "ThreePointSusceptibilityContainer")
+        .def(py::init<Channel, IndexClassification const&, StatesClassification const&, Hamiltonian const&,
+                      DensityMatrix const&, FieldOperatorContainer const&>(),
+             py::keep_alive<1, 4>(), py::keep_alive<1, 5>(), py::keep_alive<1, 6>(), py::keep_alive<1, 7>())
+        .def_readwrite("PoleResolution", &ThreePointSusceptibilityContainer::PoleResolution)
+        .def_readwrite("CoefficientTolerance", &ThreePointSusceptibilityContainer::CoefficientTolerance)
+        .def("prepareAll",
+             [](ThreePointSusceptibilityContainer& g, std::vector<std::array<ParticleIndex, 4>> const& idx) {
+                 std::set<IndexCombination4> s;
+                 for (auto const& p : idx) s.emplace(p[0], p[1], p[2], p[3]);
+                 g.prepareAll(s);
+             },
+             py::arg("indices") = std::vector<std::array<ParticleIndex, 4>>())
+        .def("computeAll",
+             [](ThreePointSusceptibilityContainer& g, bool clear, std::vector<std::tuple<C, C>> const& f, int) {
+                 auto r = g.computeAll(clear, to_freqs2(f));
+                 std::map<std::tuple<int, int, int, int>, std::vector<C>> out;
+                 for (auto& kv : r)
+                     out[std::make_tuple(kv.first.Index1, kv.first.Index2, kv.first.Index3, kv.first.Index4)] = kv.second;
+                 return out;
+             },
+             py::arg("clear") = false, py::arg("freqs") = std::vector<std::tuple<C, C>>(), py::arg("comm") = 0)
+        .def("__call__",
+             [](ThreePointSusceptibilityContainer& g, ParticleIndex i, ParticleIndex j, ParticleIndex k,
+                ParticleIndex l) -> ElementWithPermFreq<ThreePointSusceptibility>& { return g(i, j, k, l); },
+             py::return_value_policy::reference_internal)
+        .def("isInContainer", [](ThreePointSusceptibilityContainer const& g, ParticleIndex i, ParticleIndex j,
+                                 ParticleIndex k, ParticleIndex l) {
+            return g.isInContainer(IndexCombination4(i, j, k, l));
+        });
 
     py::class_<Vertex4>(m, "Vertex4")
         .def(py::init<TwoParticleGF const&, GreensFunction const&, GreensFunction const&, GreensFunction const&,

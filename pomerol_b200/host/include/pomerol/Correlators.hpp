@@ -1,9 +1,11 @@
 // Correlators of the drop-in API: GreensFunction, GFContainer,
-// Susceptibility, EnsembleAverage, TwoParticleGF, TwoParticleGFContainer.
+// Susceptibility, EnsembleAverage, TwoParticleGF, TwoParticleGFContainer,
+// ThreePointSusceptibility, ThreePointSusceptibilityContainer, Vertex4.
 // Public members, signatures and frequency conventions follow the reference
 // (GreensFunction.hpp:83-147, GFContainer.hpp:40-111, Susceptibility.hpp:75-171,
 // EnsembleAverage.cpp:27-67, TwoParticleGF.hpp:111-187,
-// TwoParticleGFContainer.hpp:52-93, IndexContainer4.hpp:138-273).
+// TwoParticleGFContainer.hpp:52-93, IndexContainer4.hpp:138-273,
+// ThreePointSusceptibility.hpp:67-177, ThreePointSusceptibilityContainer.hpp:35-108).
 //
 // Evaluation runs on the GPU: point queries by Matsubara index are served
 // from a cache that is filled a whole frequency window (G, chi) or cube (G2)
@@ -224,6 +226,87 @@ private:
     FieldOperatorContainer const& Operators;
     std::map<IndexCombination4, ElementWithPermFreq<TwoParticleGF>> ElementsMap;
     std::map<IndexCombination4, std::shared_ptr<TwoParticleGF>> NonTrivialElements;
+};
+
+// ------------------------------------------------------------ three point
+// Channel of a three-point susceptibility (Misc.hpp:160-164).
+enum Channel : int { PP = PGX_PP, PH = PGX_PH, xPH = PGX_XPH };
+
+using FreqTuple2 = std::tuple<ComplexType, ComplexType>;
+using FreqVec2 = std::vector<FreqTuple2>;
+
+// Three-point fermion-boson susceptibility (ThreePointSusceptibility.hpp:67-158):
+// part selection on the host as ThreePointSusceptibility::prepare does, the
+// Lehmann sum over every state triple on the GPU (pgx_chi3).
+class ThreePointSusceptibility : public Thermal, public ComputableObject {
+public:
+    RealType PoleResolution = 1e-8;
+    RealType CoefficientTolerance = 1e-16;
+
+    ThreePointSusceptibility(Channel channel, StatesClassification const& S, Hamiltonian const& H,
+                             CreationOperator const& CX1, AnnihilationOperator const& C2, CreationOperator const& CX3,
+                             AnnihilationOperator const& C4, DensityMatrix const& DM);
+    void prepare();
+    std::vector<ComplexType> compute(bool clear = false, FreqVec2 const& freqs = {},
+                                     MPI_Comm const& comm = MPI_COMM_WORLD);
+    ParticleIndex getIndex(std::size_t Position) const;
+    ComplexType operator()(ComplexType z1, ComplexType z2) const;
+    ComplexType operator()(long MatsubaraNumber1, long MatsubaraNumber2) const;
+    bool isVanishing() const { return Vanishing; }
+    std::size_t getNumParts() const { return Parts.size(); }
+    // Evaluate at many duplets with one device call.
+    std::vector<ComplexType> values(FreqVec2 const& freqs) const;
+    std::vector<pgx_chi3_part> const& deviceParts() const { return Parts; }
+
+private:
+    MonomialOperator const& getF2() const;
+    MonomialOperator const& getB1() const;
+    MonomialOperator const& getB2() const;
+    Channel channel;
+    StatesClassification const& S;
+    Hamiltonian const& H;
+    CreationOperator const& CX1;
+    AnnihilationOperator const& C2;
+    CreationOperator const& CX3;
+    AnnihilationOperator const& C4;
+    DensityMatrix const& DM;
+    bool Vanishing = true;
+    std::vector<pgx_chi3_part> Parts;
+    std::vector<std::array<MonomialOperator const*, 4>> PartOps;
+    mutable std::map<std::pair<long, long>, ComplexType> Cache;
+};
+
+// Container of three-point susceptibilities over index quadruples
+// (ThreePointSusceptibilityContainer.hpp:35-108 on IndexContainer4.hpp:138-237).
+class ThreePointSusceptibilityContainer : public Thermal {
+public:
+    RealType PoleResolution = 1e-8;
+    RealType CoefficientTolerance = 1e-16;
+
+    ThreePointSusceptibilityContainer(Channel channel, IndexClassification const& IndexInfo,
+                                      StatesClassification const& S, Hamiltonian const& H, DensityMatrix const& DM,
+                                      FieldOperatorContainer const& Ops);
+    void prepareAll(std::set<IndexCombination4> const& Indices = {});
+    std::map<IndexCombination4, std::vector<ComplexType>> computeAll(bool clearTerms = false,
+                                                                     FreqVec2 const& freqs = {},
+                                                                     MPI_Comm const& comm = MPI_COMM_WORLD);
+    ElementWithPermFreq<ThreePointSusceptibility>& operator()(IndexCombination4 const& Indices);
+    ElementWithPermFreq<ThreePointSusceptibility>& operator()(ParticleIndex i, ParticleIndex j, ParticleIndex k,
+                                                              ParticleIndex l) {
+        return (*this)(IndexCombination4(i, j, k, l));
+    }
+    bool isInContainer(IndexCombination4 const& Indices) const { return ElementsMap.count(Indices) > 0; }
+
+private:
+    ElementWithPermFreq<ThreePointSusceptibility>& create(IndexCombination4 const& Indices);
+    Channel channel;
+    ParticleIndex NumIndices;
+    StatesClassification const& S;
+    Hamiltonian const& H;
+    DensityMatrix const& DM;
+    FieldOperatorContainer const& Operators;
+    std::map<IndexCombination4, ElementWithPermFreq<ThreePointSusceptibility>> ElementsMap;
+    std::map<IndexCombination4, std::shared_ptr<ThreePointSusceptibility>> NonTrivialElements;
 };
 
 // Two-particle vertex (Vertex4.hpp:38-104, Vertex4.cpp:34-53):

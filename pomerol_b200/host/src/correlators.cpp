@@ -455,3 +455,224 @@ ComplexType Vertex4::operator()(long n1, long n2, long n3) const {
 }
 
 }  // namespace Pomerol
+
+namespace Pomerol {
+
+// ------------------------------------------------------------ ThreePointSusceptibility
+ThreePointSusceptibility::ThreePointSusceptibility(Channel channel, StatesClassification const& S,
+                                                   Hamiltonian const& H, CreationOperator const& CX1,
+                                                   AnnihilationOperator const& C2, CreationOperator const& CX3,
+                                                   AnnihilationOperator const& C4, DensityMatrix const& DM)
+    : Thermal(DM.beta), channel(channel), S(S), H(H), CX1(CX1), C2(C2), CX3(CX3), C4(C4), DM(DM) {}
+
+// The operators of each channel (ThreePointSusceptibility.cpp:37-66): F1 = CX1;
+// PP: F2 = CX3, B = C2 C4; PH: F2 = C2, B = CX3 C4; xPH: F2 = C4, B = CX3 C2.
+MonomialOperator const& ThreePointSusceptibility::getF2() const {
+    switch (channel) {
+        case PP: return CX3;
+        case PH: return C2;
+        case xPH: return C4;
+    }
+    throw std::runtime_error("ThreePointSusceptibility: Wrong channel");
+}
+MonomialOperator const& ThreePointSusceptibility::getB1() const {
+    switch (channel) {
+        case PP: return C2;
+        case PH: return CX3;
+        case xPH: return CX3;
+    }
+    throw std::runtime_error("ThreePointSusceptibility: Wrong channel");
+}
+MonomialOperator const& ThreePointSusceptibility::getB2() const {
+    switch (channel) {
+        case PP: return C4;
+        case PH: return C4;
+        case xPH: return C2;
+    }
+    throw std::runtime_error("ThreePointSusceptibility: Wrong channel");
+}
+
+void ThreePointSusceptibility::prepare() {
+    if (getStatus() >= Prepared) return;
+    MonomialOperator const& F1 = CX1;
+    MonomialOperator const& F2 = getF2();
+    MonomialOperator const& B1 = getB1();
+    MonomialOperator const& B2 = getB2();
+    Parts.clear();
+    PartOps.clear();
+    auto add = [&](MonomialOperator const& Fa, MonomialOperator const& Fb, BlockNumber i, BlockNumber j,
+                   BlockNumber k, BlockNumber m, bool swapped) {
+        pgx_chi3_part p{};
+        p.block[0] = i;
+        p.block[1] = j;
+        p.block[2] = k;
+        p.block[3] = m;
+        p.swapped = swapped ? 1 : 0;
+        Parts.push_back(p);
+        PartOps.push_back({&Fa, &Fb, &B1, &B2});
+    };
+    for (auto const& kv : B2.getBlockMapping().right) {  // right block -> left block, ascending
+        const BlockNumber b2right = kv.first, b2left = kv.second;
+        const BlockNumber b1left = B1.getLeftIndex(b2left);
+        if (b1left == INVALID_BLOCK_NUMBER) continue;
+        // <b2right|F1|j><j|F2|b1left><b1left|B1|b2left><b2left|B2|b2right>
+        const BlockNumber f1right = F1.getRightIndex(b2right), f2left = F2.getLeftIndex(b1left);
+        if (f1right == f2left && f1right != INVALID_BLOCK_NUMBER && DM.isRetained(b2right) &&
+            DM.isRetained(f1right) && DM.isRetained(b1left))
+            add(F1, F2, b2right, f1right, b1left, b2left, false);
+        // <b2right|F2|j><j|F1|b1left><b1left|B1|b2left><b2left|B2|b2right>
+        const BlockNumber f2right = F2.getRightIndex(b2right), f1left = F1.getLeftIndex(b1left);
+        if (f2right == f1left && f2right != INVALID_BLOCK_NUMBER && DM.isRetained(b2right) &&
+            DM.isRetained(f2right) && DM.isRetained(b1left))
+            add(F2, F1, b2right, f2right, b1left, b2left, true);
+    }
+    Vanishing = Parts.empty();
+    setStatus(Prepared);
+}
+
+std::vector<ComplexType> ThreePointSusceptibility::values(FreqVec2 const& freqs) const {
+    std::vector<ComplexType> out(freqs.size(), 0.0);
+    if (Vanishing || freqs.empty()) return out;
+    std::vector<pgx_chi3_part> parts = Parts;
+    for (std::size_t q = 0; q < parts.size(); ++q) {
+        int32_t* ids[4] = {&parts[q].f1, &parts[q].f2, &parts[q].b1, &parts[q].b2};
+        for (int k = 0; k < 4; ++k) {
+            *ids[k] = PartOps[q][k]->deviceId();
+            if (*ids[k] < 0) throw StatusMismatch("ThreePointSusceptibility: operators are not computed");
+        }
+    }
+    std::vector<double> z(4 * freqs.size());
+    for (std::size_t t = 0; t < freqs.size(); ++t) {
+        const ComplexType a = std::get<0>(freqs[t]), b = std::get<1>(freqs[t]);
+        z[4 * t] = a.real();
+        z[4 * t + 1] = a.imag();
+        z[4 * t + 2] = b.real();
+        z[4 * t + 3] = b.imag();
+    }
+    DM.bind();
+    Device& dev = H.device();
+    dev.check(pgx_chi3(dev.ctx(), (int32_t)channel, (int32_t)parts.size(), parts.data(), (int32_t)freqs.size(),
+                       z.data(), PoleResolution, reinterpret_cast<double*>(out.data())),
+              "pgx_chi3");
+    return out;
+}
+
+std::vector<ComplexType> ThreePointSusceptibility::compute(bool clear, FreqVec2 const& freqs, MPI_Comm const&) {
+    (void)clear;
+    if (getStatus() < Prepared) throw StatusMismatch("ThreePointSusceptibility is not prepared yet.");
+    std::vector<ComplexType> m_data;
+    if (getStatus() >= Computed) return m_data;
+    if (!Vanishing) {
+        m_data.assign(freqs.size(), 0.0);
+        if (!freqs.empty()) m_data = values(freqs);
+    }
+    Cache.clear();
+    setStatus(Computed);
+    return m_data;
+}
+
+ParticleIndex ThreePointSusceptibility::getIndex(std::size_t Position) const {
+    switch (Position) {
+        case 0: return CX1.getIndex();
+        case 1: return C2.getIndex();
+        case 2: return CX3.getIndex();
+        case 3: return C4.getIndex();
+        default: throw std::runtime_error("ThreePointSusceptibility: Could not get operator index");
+    }
+}
+
+ComplexType ThreePointSusceptibility::operator()(ComplexType z1, ComplexType z2) const {
+    if (Vanishing) return 0.0;
+    return values({FreqTuple2{z1, z2}})[0];
+}
+
+ComplexType ThreePointSusceptibility::operator()(long n1, long n2) const {
+    if (Vanishing) return 0.0;
+    const auto key = std::make_pair(n1, n2);
+    auto it = Cache.find(key);
+    if (it != Cache.end()) return it->second;
+    // fill the square [-W, W)^2 that contains the point with one device call
+    long W = std::max({std::labs(n1) + 1, std::labs(n2) + 1, 16L});
+    W = (W + 7) / 8 * 8;
+    if (W > 128) return (*this)(MatsubaraSpacing * RealType(2 * n1 + 1), MatsubaraSpacing * RealType(2 * n2 + 1));
+    FreqVec2 f;
+    for (long a = -W; a < W; ++a)
+        for (long b = -W; b < W; ++b)
+            f.emplace_back(MatsubaraSpacing * RealType(2 * a + 1), MatsubaraSpacing * RealType(2 * b + 1));
+    auto v = values(f);
+    std::size_t q = 0;
+    for (long a = -W; a < W; ++a)
+        for (long b = -W; b < W; ++b) Cache[std::make_pair(a, b)] = v[q++];
+    return Cache[key];
+}
+
+// ------------------------------------------------------------ ThreePointSusceptibilityContainer
+ThreePointSusceptibilityContainer::ThreePointSusceptibilityContainer(Channel channel,
+                                                                     IndexClassification const& IndexInfo,
+                                                                     StatesClassification const& S,
+                                                                     Hamiltonian const& H, DensityMatrix const& DM,
+                                                                     FieldOperatorContainer const& Ops)
+    : Thermal(DM.beta), channel(channel), NumIndices(IndexInfo.getIndexSize()), S(S), H(H), DM(DM), Operators(Ops) {}
+
+// IndexContainer4::create (IndexContainer4.hpp:190-237): the element and its
+// aliases under exchange of the first or last two indices
+ElementWithPermFreq<ThreePointSusceptibility>& ThreePointSusceptibilityContainer::create(IndexCombination4 const& I) {
+    auto e = std::make_shared<ThreePointSusceptibility>(
+        channel, S, H, Operators.getCreationOperator(I.Index1), Operators.getAnnihilationOperator(I.Index2),
+        Operators.getCreationOperator(I.Index3), Operators.getAnnihilationOperator(I.Index4), DM);
+    auto it = ElementsMap.emplace(I, ElementWithPermFreq<ThreePointSusceptibility>{e, permutations4[0]}).first;
+    NonTrivialElements.emplace(I, e);
+    const bool sameC = I.Index1 == I.Index2, sameCX = I.Index3 == I.Index4;
+    if (!sameC)
+        ElementsMap.emplace(IndexCombination4(I.Index2, I.Index1, I.Index3, I.Index4),
+                            ElementWithPermFreq<ThreePointSusceptibility>{e, permutations4[6]});
+    if (!sameCX)
+        ElementsMap.emplace(IndexCombination4(I.Index1, I.Index2, I.Index4, I.Index3),
+                            ElementWithPermFreq<ThreePointSusceptibility>{e, permutations4[1]});
+    if (!sameC && !sameCX)
+        ElementsMap.emplace(IndexCombination4(I.Index2, I.Index1, I.Index4, I.Index3),
+                            ElementWithPermFreq<ThreePointSusceptibility>{e, permutations4[7]});
+    return it->second;
+}
+
+void ThreePointSusceptibilityContainer::prepareAll(std::set<IndexCombination4> const& Indices) {
+    ElementsMap.clear();
+    NonTrivialElements.clear();
+    std::set<IndexCombination4> II = Indices;
+    if (II.empty())
+        for (ParticleIndex i = 0; i < NumIndices; ++i)
+            for (ParticleIndex j = i; j < NumIndices; ++j)
+                for (ParticleIndex k = 0; k < NumIndices; ++k)
+                    for (ParticleIndex l = k; l < NumIndices; ++l) II.emplace(i, j, k, l);
+    for (auto const& ic : II)
+        if (!isInContainer(ic)) create(ic);
+    for (auto& kv : ElementsMap) {
+        ThreePointSusceptibility& g = kv.second.element();
+        g.PoleResolution = PoleResolution;
+        g.CoefficientTolerance = CoefficientTolerance;
+        g.prepare();
+    }
+}
+
+// ThreePointSusceptibilityContainer::computeAll (ThreePointSusceptibilityContainer.cpp:30-40):
+// every key of the map in order; an alias of an element computed earlier
+// yields an empty vector, as there.
+std::map<IndexCombination4, std::vector<ComplexType>> ThreePointSusceptibilityContainer::computeAll(
+    bool clearTerms, FreqVec2 const& freqs, MPI_Comm const& comm) {
+    std::map<IndexCombination4, std::vector<ComplexType>> out;
+    for (auto& kv : ElementsMap) out.emplace(kv.first, kv.second.element().compute(clearTerms, freqs, comm));
+    return out;
+}
+
+ElementWithPermFreq<ThreePointSusceptibility>& ThreePointSusceptibilityContainer::operator()(
+    IndexCombination4 const& I) {
+    auto it = ElementsMap.find(I);
+    if (it != ElementsMap.end()) return it->second;
+    auto& e = create(I);
+    e.element().PoleResolution = PoleResolution;
+    e.element().CoefficientTolerance = CoefficientTolerance;
+    e.element().prepare();
+    return e;
+}
+
+}  // namespace Pomerol

@@ -3,8 +3,8 @@
 CPU tests: expression algebra, index classification and the Hilbert-space
 partition agree with the oracle.  GPU tests: the reference's own test cases
 (HamiltonianTest, GF1site, GF2site, GF4site, Anderson, GF1siteAnomalous,
-Susceptibility, Vertex4, Anderson2PGF) written against this API, at the
-reference tests' tolerances."""
+Susceptibility, Vertex4, Anderson2PGF, 3PSusc1site, 3PSusc3site) written
+against this API, at the reference tests' tolerances."""
 import json
 import os
 
@@ -387,3 +387,96 @@ def test_vertex4_class_reference_case(P):
         ref = g_uuuu(n1, n2, n3) * GF(n1) * GF(n2) * GF(n3) * GF(n4)
         assert abs(Gamma(n1, n2, n3) - ref) < 1e-10
         assert abs(Gamma.value(n1, n2, n3) - Gamma(n1, n2, n3)) < 1e-14
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("h_field", [0.0, 0.01])
+def test_chi3_1site_reference_case(P, h_field):
+    """3PSusc1siteTest.cpp:65-250 through the drop-in ThreePointSusceptibility:
+    all channels and spin pairs of the Hubbard atom against the closed form
+    at 1e-14 (relative to 1), and the PH / xPH crossing symmetry."""
+    from tests.test_oracle_chi3 import AtomChi3
+    L = P.LatticePresets
+    U, mu, beta, n_iw = 1.0, 0.4, 10.0, 20
+    ii, hs, S, H, rho, ops = _setup(P, L.CoulombS("A", U, -mu) + L.Magnetization("A", -h_field), beta)
+    up, dn = ii.getIndex("A", 0, P.up), ii.getIndex("A", 0, P.down)
+    g = AtomChi3(beta, U, mu, h_field)
+    om = lambda n: np.pi * (2 * n + 1) / beta
+    st = {up: 1, dn: 2}
+    grid = [(a, b) for a in range(-n_iw, n_iw) for b in range(-n_iw, n_iw)]
+
+    def chi3(ch, i1, i2, i3, i4):
+        c = P.ThreePointSusceptibility(ch, S, H, ops.getCreationOperator(i1), ops.getAnnihilationOperator(i2),
+                                       ops.getCreationOperator(i3), ops.getAnnihilationOperator(i4), rho)
+        c.prepare()
+        c.compute()
+        return c
+
+    for i1 in (up, dn):
+        for i2 in (up, dn):
+            other = dn if i1 == up else up
+            c = chi3(P.PP, i1, i1, i2, i2)
+            if i1 == i2:
+                assert c.isVanishing()
+            else:
+                for a, b in grid:
+                    ref = g(3, st[i2], 0, -om(a), -om(b)) + g(3, st[i1], 0, -om(b), -om(a))
+                    assert abs(c(a, b) - ref) < 1e-14 * max(1.0, abs(ref))
+            cph, cx = chi3(P.PH, i1, i1, i2, i2), chi3(P.xPH, i1, i1, i2, i2)
+            for a, b in grid:
+                if i1 == i2:
+                    ref = g(st[i1], 0, st[i1], -om(a), om(b)) + g(3, st[other], 3, -om(a), om(b))
+                    refx = -ref
+                else:
+                    s = st[i2]
+                    ref = g(3, s, 3, -om(a), om(b)) - g(s, 3, s, om(a), -om(b))
+                    refx = -g(st[i1], 0, st[i2], -om(a), om(b)) - g(st[i1], 3, st[i2], om(b), -om(a))
+                assert abs(cph(a, b) - ref) < 1e-14 * max(1.0, abs(ref))
+                assert abs(cx(a, b) - refx) < 1e-14 * max(1.0, abs(refx))
+    ix = (up, dn)
+    for a in ix:
+        for b in ix:
+            for c3 in ix:
+                for d in ix:
+                    ph, xph = chi3(P.PH, a, b, c3, d), chi3(P.xPH, a, d, c3, b)
+                    for n1, n2 in grid[::7]:
+                        assert abs(xph(n1, n2) + ph(n1, n2)) < 1e-14
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("channel", ["PP", "PH", "xPH"])
+def test_chi3_3site_reference_case(P, channel):
+    """3PSusc3siteTest.cpp:24-157: chi3 of the three-site Hubbard cluster at
+    n1, n2 in {-1, 0, 1} against the golden values at 1e-10, through the
+    class and through ThreePointSusceptibilityContainer.computeAll."""
+    L = P.LatticePresets
+    k = KATS["chi3_3site"]
+    HExpr = P.RealExpr()
+    for s in k["sites"]:
+        HExpr += L.CoulombS(s, k["U"], -k["mu"])
+    for a, b in (("A", "B"), ("B", "C"), ("C", "A")):
+        HExpr += L.Hopping(a, b, -k["t"])
+    beta = k["beta"]
+    ii, hs, S, H, rho, ops = _setup(P, HExpr, beta)
+    spin = {"up": P.up, "down": P.down}
+    i1, i2, i3, i4 = [ii.getIndex(s, 0, spin[sp]) for s, sp in k[channel]["ops"]]
+    ch = {"PP": P.PP, "PH": P.PH, "xPH": P.xPH}[channel]
+    c = P.ThreePointSusceptibility(ch, S, H, ops.getCreationOperator(i1), ops.getAnnihilationOperator(i2),
+                                   ops.getCreationOperator(i3), ops.getAnnihilationOperator(i4), rho)
+    c.prepare()
+    c.compute()
+    ref = cplx(k[channel]["chi3"])
+    got = np.array([c(a, b) for a in k["n"] for b in k["n"]])
+    assert np.abs(got - ref).max() < k["tol"]
+    cont = P.ThreePointSusceptibilityContainer(ch, ii, S, H, rho, ops)
+    cont.prepareAll([(i1, i2, i3, i4)])
+    freqs = [(1j * np.pi * (2 * a + 1) / beta, 1j * np.pi * (2 * b + 1) / beta) for a in k["n"] for b in k["n"]]
+    res = cont.computeAll(False, freqs)
+    # the element and its index-exchange aliases share one object; computeAll
+    # visits the keys in order, so the first key of the group carries the
+    # values and the later ones the empty vector of an already computed
+    # element (ThreePointSusceptibilityContainer.cpp:30-40)
+    group = sorted({(i1, i2, i3, i4), (i2, i1, i3, i4), (i1, i2, i4, i3), (i2, i1, i4, i3)})
+    assert all(cont.isInContainer(*g) for g in group)
+    assert np.abs(np.array(res[group[0]]) - ref).max() < k["tol"]
+    assert all(len(res[g]) == 0 for g in group[1:])
