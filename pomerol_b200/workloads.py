@@ -142,6 +142,69 @@ class Problem:
         return blocks, actions, g2.parts()
 
 
+def matsubara_square(beta, n):
+    """Fermionic duplets (n1, n2) in [-n/2, n/2)^2 and their frequencies."""
+    k = np.arange(-n // 2, n // 2)
+    idx = np.array([(a, b) for a in k for b in k])
+    return idx, 1j * np.pi * (2 * idx + 1) / beta
+
+
+class Chi3Run:
+    """Three-point susceptibility chi3_PH(u0, u0, d0, d0) of a workload on one
+    libpgx context with the Hamiltonian resident in HBM: eigensolve, weights,
+    rotation of c^+ and c, chi3 on the duplets.  The parts are the ones the
+    drop-in ThreePointSusceptibility::prepare selects."""
+
+    def __init__(self, prob: Problem, channel=None, device=0):
+        from .pgx import PGX_PH, Engine
+        self.channel = PGX_PH if channel is None else channel
+        self.prob = prob
+        blocks, self.actions, _ = prob.engine_inputs()
+        H, rho, ops = self._dropin_parts()
+        self.eng = Engine(device)
+        self.eng.set_blocks(prob.dims)
+        self.eng.set_hamiltonian(blocks)
+        self.cdag = {i: self.eng.op_define([(r, l, np.asarray(t), np.asarray(c)) for r, l, t, c in a])
+                     for i, a in self.actions.items()}
+
+    def _dropin_parts(self):
+        pr = self.prob
+        H = P.Hamiltonian(pr.S, pr.device)
+        H.prepare(pr.HExpr, pr.hs)
+        H.compute()
+        rho = P.DensityMatrix(pr.S, H, pr.beta)
+        rho.prepare()
+        rho.compute()
+        ops = P.FieldOperatorContainer(pr.ii, pr.hs, pr.S, H, {pr.u0, pr.d0})
+        ops.prepareAll(pr.hs)
+        ops.computeAll()
+        u, d = pr.u0, pr.d0
+        chi = P.ThreePointSusceptibility(P.Channel(self.channel), pr.S, H, ops.getCreationOperator(u),
+                                         ops.getAnnihilationOperator(u), ops.getCreationOperator(d),
+                                         ops.getAnnihilationOperator(d), rho)
+        chi.prepare()
+        self.part_blocks = chi.parts()
+        return H, rho, ops
+
+    def step(self, duplets):
+        e = self.eng
+        e.eigh()
+        e.weights(self.prob.beta)
+        u, d = self.prob.u0, self.prob.d0
+        for i in (u, d):
+            e.op_rotate(self.cdag[i])
+        for op in getattr(self, "_adjoints", ()):
+            e.op_release(op)
+        c = {i: e.op_adjoint(self.cdag[i]) for i in (u, d)}
+        self._adjoints = tuple(c.values())
+        # operators CX1, C2, CX3, C4 = c+_u, c_u, c+_d, c_d -> (F1, F2, B1, B2) of the channel
+        CX1, C2, CX3, C4 = self.cdag[u], c[u], self.cdag[d], c[d]
+        F1, F2, B1, B2 = {0: (CX1, CX3, C2, C4), 1: (CX1, C2, CX3, C4), 2: (CX1, C4, CX3, C2)}[self.channel]
+        parts = [((F2, F1) if sw else (F1, F2)) + (B1, B2, tuple(blk), bool(sw)) for blk, sw in self.part_blocks]
+        self.parts = parts
+        return e.chi3(self.channel, parts, duplets)
+
+
 class EngineRun:
     """The G2 stage chain on one libpgx context with the Hamiltonian resident
     in HBM: eigensolve, weights, rotation of c^+ and c, G2 on the triples."""

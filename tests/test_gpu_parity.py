@@ -760,3 +760,27 @@ def test_chi3_random_duplets_against_exact_oracle(harness, complex_h):
             assert len(parts) == len(oparts)
             ref = X.chi3_exact(ed, oparts, ch, freqs)
             assert np.abs(v - ref).max() <= 1e-11 * max(1.0, np.abs(ref).max()), (ixs, ch)
+
+
+def test_chi3_anderson5_workload_sample(harness):
+    """chi3_PH(u0, u0, d0, d0) of the Anderson impurity with five bath sites
+    (dim 4096, 72 parts, blocks up to 400) on the 16 x 16 fermionic square:
+    three duplets, one of them resonant (z1 = z2), against the exact oracle
+    (1e-10 relative), and the crossing symmetry chi3_xPH(1, 4, 3, 2) =
+    -chi3_PH(1, 2, 3, 4) on the whole square (1e-12 relative)."""
+    from oracle import chi3 as X
+    U, epsd, eps, V, beta = M.anderson_a5_params(0)
+    m = M.make_model(M.anderson(U, epsd, eps, V))
+    g = harness(m, beta)
+    u0, d0 = m.info.getIndex("C", 0, M.UP), m.info.getIndex("C", 0, M.DOWN)
+    n = np.arange(-8, 8)
+    freqs = [(L.fermionic(a, beta), L.fermionic(b, beta)) for a in n for b in n]
+    v, parts = g.chi3(X.PH, (u0, u0, d0, d0), freqs)
+    assert len(parts) == 72
+    vx, _ = g.chi3(X.XPH, (u0, d0, d0, u0), freqs)
+    assert np.abs(vx + v).max() <= 1e-12 * np.abs(v).max()
+    ed = EDm.ED(m, beta)
+    oparts = X.chi3_parts(ed, X.PH, ed.cdag(u0), ed.c(u0), ed.cdag(d0), ed.c(d0))
+    sample = [freqs.index((L.fermionic(a, beta), L.fermionic(b, beta))) for a, b in ((1, 2), (-3, -3), (5, -8))]
+    ref = X.chi3_exact(ed, oparts, X.PH, [freqs[q] for q in sample])
+    assert np.abs(v[sample] - ref).max() <= 1e-10 * np.abs(ref).max()
