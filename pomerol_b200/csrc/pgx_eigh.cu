@@ -7,8 +7,8 @@
 //      4th ed., 8.3.1):
 //      eigh_cluster_kernel, one thread-block cluster of 1-8 CTAs per block
 //      with the matrix in distributed shared memory (blocks up to 464 states);
-//      eigh_kernel, one CTA per block with the matrix in global memory
-//      (larger blocks).  Q is stored column-major.
+//      larger blocks: a blocked reduction (panels of 32 columns, trailing
+//      updates and Q by GEMMs) over the whole GPU.  Q is stored column-major.
 //   2. bisect_kernel, one thread per eigenvalue: bisection with Sturm counts
 //      on the unreduced pieces of T (8.4.1).
 //   3. vector_kernel, one thread per eigenvalue: inverse iteration with a
@@ -31,7 +31,6 @@ namespace pgx {
 
 namespace {
 
-constexpr int EIGH_THREADS = 512;
 
 __device__ __forceinline__ double warp_sum(double v) {
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -50,145 +49,237 @@ __device__ double block_sum(double v, double* red) {
     return r;
 }
 
-struct EighArgs {
-    const int* order;          // CTA -> block (largest first)
+// ----------------------------------------------------------------------------
+// Householder stage for blocks too large for a cluster's shared memory
+// (n > 464): the blocked reduction of LAPACK's dsytrd / dlatrd (lower).
+// Panels of BHH_NB columns.  Column j of the panel that starts at k is first
+// brought up to date with the panel's earlier reflectors,
+//   a = A(j:, j) - V W(j, :)^T - W V(j, :)^T,
+// then reflected (v, tau; d_j = a_j, e_j = alpha) and
+//   w = tau (A(j+1:, j+1:) v - V (W^T v) - W (V^T v)),  w -= (tau/2)(w.v) v,
+// with A the matrix as it was at the start of the panel: the trailing matrix
+// is only read per column (bhh_symv_kernel) and written once per panel,
+// A(k+p:, k+p:) -= V W^T + W V^T, by one GEMM of inner size 2p.
+// The reflectors stay in the columns of A below the diagonal (zeros above),
+// and Q = H_0 ... H_{n-3} is formed panel by panel, from the last one, as
+// Q(k+1:, k+1:) += V (-T) (V^T Q(k+1:, k+1:)), where T is the upper
+// triangular factor of the panel's block reflector I - V T V^T (LAPACK
+// dlarft).  Every such block of a problem advances in the same launches.
+// The outputs (tridiagonal, column-major Q) are those of the cluster kernel.
+constexpr int BHH_NB = 32;  // panel width
+constexpr int BHH_COL_THREADS = 1024;
+constexpr int BHH_SYMV_THREADS = 256;
+constexpr int BHH_SYMV_ROWS = 32;  // trailing rows per symv CTA
+
+struct BigArgs {
+    const int* big;    // the large blocks, largest first
+    const long* boff;  // per entry of `big`: scratch offset in S (doubles)
+    int nact;          // entries of `big` this launch covers (a prefix)
     const int* dims;
-    const long* moff;          // matrix offset of block b (elements)
-    const long* eoff;          // vector offset of block b
-    const double* H;           // packed input blocks (row-major)
-    double* A;                 // workspace copy (destroyed)
-    double* Zc;                // workspace, column-major accumulated factor
-    double* tri;               // per block: diagonal then sub-diagonal (2 n)
+    const long* moff;
+    const long* eoff;
+    double* A;    // per block n x n row-major working copy of H
+    double* Zc;   // per block Q, column-major
+    double* S;    // scratch
+    double* tri;  // per block: d (n), e (n)
+    int k;        // first column of the current panel
+    int fin;      // column whose w is completed (-1: none)
+    int col;      // column to reflect (-1: none)
 };
 
-// Householder reduction of one block and accumulation of its orthogonal
-// factor (column-major), one CTA per block.
-__global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
-    extern __shared__ double sh[];
+// Scratch of one large block, in doubles: V and W (BHH_NB columns of n each),
+// y (n), tau (n), then per panel its Gram matrix and -T (BHH_NB^2 each).
+__host__ __device__ inline long bhh_panels(int n) { return n > 2 ? (n - 2 + BHH_NB - 1) / BHH_NB : 0; }
+__host__ __device__ inline long bhh_scratch_doubles(int n) {
+    return 2L * BHH_NB * n + 2L * n + 2 * bhh_panels(n) * BHH_NB * BHH_NB;
+}
+
+__global__ void __launch_bounds__(BHH_COL_THREADS) bhh_col_kernel(BigArgs g) {
     __shared__ double red[32];
-
-    const int b = g.order[blockIdx.x];
+    __shared__ double dots[2 * BHH_NB];
+    __shared__ double sv[BHH_NB], sw[BHH_NB];
+    __shared__ double hh[2];
+    const int b = g.big[blockIdx.x];
     const int n = g.dims[b];
-    const long mo = g.moff[b], eo = g.eoff[b];
-    const double* Hb = g.H + mo;
-    double* A = g.A + mo;
-    double* Z = g.Zc + mo;
-    const int tid = threadIdx.x, nt = blockDim.x;
-
-    double* v = sh;            // n   Householder vector
-    double* w = sh + n;        // n   p / w vectors
-    double* dg = sh + 2 * n;   // n   diagonal
-    double* ed = sh + 3 * n;   // n   sub-diagonal
-
-    for (long i = tid; i < (long)n * n; i += nt) A[i] = Hb[i];
-    __syncthreads();
-
-    // ---------------- Householder tridiagonalisation (lower) ----------------
-    for (int k = 0; k + 2 < n; ++k) {
-        const int m = n - k - 1;
-        const long base = (long)(k + 1) * n + (k + 1);  // B(i,j) = A[base + i*n + j]
-        double part = 0.0;
-        for (int i = tid; i < m; i += nt) {
-            double x = A[(long)(k + 1 + i) * n + k];
-            v[i] = x;
-            if (i > 0) part += x * x;
-        }
-        double sigma = block_sum(part, red);
-        const double x0 = v[0];
-        if (tid == 0) dg[k] = A[(long)k * n + k];
-        if (sigma == 0.0) {
-            if (tid == 0) ed[k] = x0;
+    double* A = g.A + g.moff[b];
+    double* V = g.S + g.boff[blockIdx.x];  // column t at V + t n
+    double* W = V + (long)BHH_NB * n;
+    const double* y = W + (long)BHH_NB * n;
+    double* tau = W + (long)BHH_NB * n + n;
+    const long eo = g.eoff[b];
+    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
+    const int last = n - 3;  // the last column with a reflector
+    // ---- complete w of column fin
+    if (g.fin >= 0 && g.fin <= last) {
+        const int f = g.fin, cf = f - g.k;
+        const double* v = V + (long)cf * n;
+        double* w = W + (long)cf * n;
+        const double t = tau[f];
+        if (t == 0.0) {
+            for (int r = tid; r < n; r += nt) w[r] = 0.0;
+        } else {
+            // dots[2s] = W_s . v, dots[2s + 1] = V_s . v (v vanishes above row f + 1)
+            for (int q = wid; q < 2 * cf; q += nw) {
+                const double* x = ((q & 1) ? V : W) + (long)(q >> 1) * n;
+                double acc = 0.0;
+                for (int r = f + 1 + lane; r < n; r += 32) acc = fma(x[r], v[r], acc);
+                acc = warp_sum(acc);
+                if (lane == 0) dots[q] = acc;
+            }
             __syncthreads();
-            if (tid == 0) A[(long)(k + 1) * n + k] = 0.0;  // marks tau = 0 below
-            continue;
-        }
-        const double mu = sqrt(x0 * x0 + sigma);
-        const double alpha = (x0 > 0.0) ? -mu : mu;   // v0 = x0 - alpha, no cancellation
-        const double v0 = x0 - alpha;
-        const double tau = 2.0 / (sigma + v0 * v0);
-        __syncthreads();
-        if (tid == 0) { v[0] = v0; ed[k] = alpha; }
-        __syncthreads();
-        // p = tau * B v  (B symmetric: p_i = sum_j B(j,i) v_j, coalesced over i);
-        // four independent accumulators keep several loads in flight
-        for (int i = tid; i < m; i += nt) {
-            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-            const double* col = A + base + i;
-            int j = 0;
-            for (; j + 3 < m; j += 4) {
-                const double b0 = col[(long)j * n], b1 = col[(long)(j + 1) * n], b2 = col[(long)(j + 2) * n],
-                             b3 = col[(long)(j + 3) * n];
-                a0 = fma(b0, v[j], a0);
-                a1 = fma(b1, v[j + 1], a1);
-                a2 = fma(b2, v[j + 2], a2);
-                a3 = fma(b3, v[j + 3], a3);
+            double part = 0.0;
+            for (int r = tid; r < n; r += nt) {
+                double wr = 0.0;
+                if (r > f) {
+                    double acc = y[r];
+                    for (int s2 = 0; s2 < cf; ++s2)
+                        acc -= V[(long)s2 * n + r] * dots[2 * s2] + W[(long)s2 * n + r] * dots[2 * s2 + 1];
+                    wr = t * acc;
+                    part = fma(wr, v[r], part);
+                }
+                w[r] = wr;
             }
-            for (; j < m; ++j) a0 = fma(col[(long)j * n], v[j], a0);
-            w[i] = tau * ((a0 + a1) + (a2 + a3));
+            const double K = 0.5 * t * block_sum(part, red);  // its barriers order the writes of w above
+            for (int r = f + 1 + tid; r < n; r += nt) w[r] -= K * v[r];
         }
-        __syncthreads();
-        part = 0.0;
-        for (int i = tid; i < m; i += nt) part += v[i] * w[i];
-        const double K = 0.5 * tau * block_sum(part, red);
-        __syncthreads();
-        for (int i = tid; i < m; i += nt) w[i] -= K * v[i];
-        __syncthreads();
-        // B -= v w^T + w v^T  (rows in groups of four: loads issued before stores)
-        for (int i = tid; i < m; i += nt) {
-            const double vi = v[i], wi = w[i];
-            double* colp = A + base + i;
-            int j = 0;
-            for (; j + 3 < m; j += 4) {
-                double b0 = colp[(long)j * n], b1 = colp[(long)(j + 1) * n], b2 = colp[(long)(j + 2) * n],
-                       b3 = colp[(long)(j + 3) * n];
-                b0 -= v[j] * wi + w[j] * vi;
-                b1 -= v[j + 1] * wi + w[j + 1] * vi;
-                b2 -= v[j + 2] * wi + w[j + 2] * vi;
-                b3 -= v[j + 3] * wi + w[j + 3] * vi;
-                colp[(long)j * n] = b0;
-                colp[(long)(j + 1) * n] = b1;
-                colp[(long)(j + 2) * n] = b2;
-                colp[(long)(j + 3) * n] = b3;
-            }
-            for (; j < m; ++j) colp[(long)j * n] -= v[j] * wi + w[j] * vi;
-        }
-        // keep v (scaled by sqrt(tau)) in column k below the diagonal
-        const double st = sqrt(tau);
-        for (int i = tid; i < m; i += nt) A[(long)(k + 1 + i) * n + k] = v[i] * st;
         __syncthreads();
     }
-    if (tid == 0) {
-        if (n >= 2) {
-            dg[n - 2] = A[(long)(n - 2) * n + (n - 2)];
-            ed[n - 2] = A[(long)(n - 1) * n + (n - 2)];
-            if (n == 2) ed[0] = A[(long)1 * n + 0];
+    // ---- reflect column col
+    if (g.col >= 0 && g.col <= last) {
+        const int j = g.col, cc = j - g.k;
+        for (int s2 = tid; s2 < cc; s2 += nt) {
+            sv[s2] = V[(long)s2 * n + j];
+            sw[s2] = W[(long)s2 * n + j];
         }
-        dg[n - 1] = A[(long)(n - 1) * n + (n - 1)];
-        ed[n - 1] = 0.0;
+        __syncthreads();
+        double* a = V + (long)cc * n;         // the updated column, then the reflector, in place
+        const double* Arow = A + (long)j * n;  // row j holds column j (A symmetric)
+        double part = 0.0;
+        for (int r = tid; r < n; r += nt) {
+            double x = 0.0;
+            if (r >= j) {
+                x = Arow[r];
+                for (int s2 = 0; s2 < cc; ++s2) x -= V[(long)s2 * n + r] * sw[s2] + W[(long)s2 * n + r] * sv[s2];
+                if (r >= j + 2) part = fma(x, x, part);
+            }
+            a[r] = x;
+        }
+        const double sigma = block_sum(part, red);
+        if (tid == 0) {
+            const double x0 = a[j + 1];
+            double alpha = x0, tj = 0.0, v0 = 0.0;
+            if (sigma != 0.0) {
+                const double mu = sqrt(x0 * x0 + sigma);
+                alpha = (x0 > 0.0) ? -mu : mu;  // v0 = x0 - alpha without cancellation
+                v0 = x0 - alpha;
+                tj = 2.0 / (sigma + v0 * v0);
+            }
+            hh[0] = tj;
+            hh[1] = v0;
+            g.tri[2 * eo + j] = a[j];
+            g.tri[2 * eo + n + j] = alpha;
+            tau[j] = tj;
+        }
+        __syncthreads();
+        const double tj = hh[0], v0 = hh[1];
+        for (int r = tid; r < n; r += nt) {
+            const double vr = (tj != 0.0 && r > j) ? ((r == j + 1) ? v0 : a[r]) : 0.0;
+            a[r] = vr;
+            A[(long)r * n + j] = vr;  // column j of A: zeros down to the diagonal, then v
+        }
     }
-    // ---------------- accumulate Q = H_0 ... H_{n-3} (column-major) ----------------
-    for (long i = tid; i < (long)n * n; i += nt) Z[i] = ((i / n) == (i % n)) ? 1.0 : 0.0;
+}
+
+// y(j+1:) = A(j+1:, j+1:) v for column j = col of every active block; one
+// warp per row, the CTAs of the active blocks in one flat grid.
+__global__ void __launch_bounds__(BHH_SYMV_THREADS) bhh_symv_kernel(BigArgs g) {
+    extern __shared__ double svec[];
+    int q = blockIdx.x, bi = 0, m = 0;
+    for (; bi < g.nact; ++bi) {
+        m = g.dims[g.big[bi]] - g.col - 1;
+        const int cnt = (m + BHH_SYMV_ROWS - 1) / BHH_SYMV_ROWS;
+        if (q < cnt) break;
+        q -= cnt;
+    }
+    if (bi >= g.nact) return;
+    const int b = g.big[bi];
+    const int n = g.dims[b], j = g.col, cc = j - g.k;
+    const double* A = g.A + g.moff[b];
+    const double* v = g.S + g.boff[bi] + (long)cc * n + (j + 1);
+    double* y = g.S + g.boff[bi] + 2L * BHH_NB * n + (j + 1);
+    for (int c = threadIdx.x; c < m; c += blockDim.x) svec[c] = v[c];
     __syncthreads();
-    const int lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
-    for (int k = n - 3; k >= 0; --k) {
-        const int m = n - k - 1;
-        for (int i = tid; i < m; i += nt) v[i] = A[(long)(k + 1 + i) * n + k];  // sqrt(tau) v
-        __syncthreads();
-        // columns j >= k+1: Q(:,j) -= u (u^T Q(:,j)),  u = sqrt(tau) v
-        for (int j = k + 1 + wid; j < n; j += nw) {
-            double* col = Z + (long)j * n + (k + 1);
-            double s = 0.0;
-            for (int i = lane; i < m; i += 32) s += v[i] * col[i];
-            s = warp_sum(s);
-            for (int i = lane; i < m; i += 32) col[i] -= v[i] * s;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int rr = wid; rr < BHH_SYMV_ROWS; rr += BHH_SYMV_THREADS / 32) {
+        const int r = q * BHH_SYMV_ROWS + rr;
+        if (r >= m) break;
+        const double* row = A + (long)(j + 1 + r) * n + (j + 1);
+        double s0 = 0.0, s1 = 0.0;
+        int c = lane;
+        for (; c + 32 < m; c += 64) {
+            s0 = fma(row[c], svec[c], s0);
+            s1 = fma(row[c + 32], svec[c + 32], s1);
         }
-        __syncthreads();
+        if (c < m) s0 = fma(row[c], svec[c], s0);
+        const double sum = warp_sum(s0 + s1);
+        if (lane == 0) y[r] = sum;
     }
-    // hand the tridiagonal (diagonal, sub-diagonal) to the bisection stage
-    for (int i = tid; i < n; i += nt) {
-        g.tri[2 * eo + i] = dg[i];
-        g.tri[2 * eo + n + i] = ed[i];
+}
+
+// the last 2 x 2 of the tridiagonal, and Q = I, per large block
+__global__ void bhh_finish_kernel(BigArgs g) {
+    const int b = g.big[blockIdx.x];
+    const int n = g.dims[b];
+    const double* A = g.A + g.moff[b];
+    double* Z = g.Zc + g.moff[b];
+    const long eo = g.eoff[b];
+    if (threadIdx.x == 0) {
+        if (n >= 2) {
+            g.tri[2 * eo + n - 2] = A[(long)(n - 2) * n + (n - 2)];
+            g.tri[2 * eo + n + n - 2] = A[(long)(n - 1) * n + (n - 2)];
+        }
+        g.tri[2 * eo + n - 1] = A[(long)(n - 1) * n + (n - 1)];
+        g.tri[2 * eo + n + n - 1] = 0.0;
     }
+    for (long i = threadIdx.x; i < (long)n * n; i += blockDim.x) Z[i] = ((i / n) == (i % n)) ? 1.0 : 0.0;
+}
+
+// -T of every panel's block reflector from its Gram matrix G = V^T V (LAPACK
+// dlarft, forward, columnwise): T_ii = tau_i, T(0:i, i) = -tau_i T(0:i, 0:i) G(0:i, i).
+// One warp per (block, panel); lane t owns row t of T.
+__global__ void bhh_tfactor_kernel(BigArgs g) {
+    int q = blockIdx.x, bi = 0;
+    for (; bi < g.nact; ++bi) {
+        const int np = (int)bhh_panels(g.dims[g.big[bi]]);
+        if (q < np) break;
+        q -= np;
+    }
+    if (bi >= g.nact) return;
+    const int n = g.dims[g.big[bi]];
+    const int k = q * BHH_NB, p = min(BHH_NB, n - 2 - k);
+    double* base = g.S + g.boff[bi];
+    const double* tau = base + 2L * BHH_NB * n + n + k;
+    const double* G = base + 2L * BHH_NB * n + 2L * n + (long)q * BHH_NB * BHH_NB;
+    double* nT = base + 2L * BHH_NB * n + 2L * n + (bhh_panels(n) + q) * BHH_NB * BHH_NB;
+    const int t = threadIdx.x;
+    double row[BHH_NB];
+#pragma unroll
+    for (int i = 0; i < BHH_NB; ++i) row[i] = 0.0;
+#pragma unroll
+    for (int i = 0; i < BHH_NB; ++i) {
+        if (i < p) {
+            if (t == i) row[i] = tau[i];
+            if (t < i) {
+                double acc = 0.0;
+#pragma unroll
+                for (int s2 = 0; s2 < BHH_NB; ++s2)
+                    if (s2 >= t && s2 < i) acc = fma(row[s2], G[s2 * BHH_NB + i], acc);
+                row[i] = -tau[i] * acc;
+            }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < BHH_NB; ++i) nT[t * BHH_NB + i] = -row[i];
 }
 
 // ----------------------------------------------------------------------------
@@ -208,7 +299,7 @@ __global__ void __launch_bounds__(EIGH_THREADS) eigh_kernel(EighArgs g) {
 // Q = H_0 ... H_{n-3} is then formed from V with the CTAs owning columns
 // j = c (mod C) of Q: a column's update needs only that column, so this
 // phase has no cross-CTA traffic.  The outputs (tridiagonal, column-major Q)
-// are those of eigh_kernel.
+// are those of the blocked large-block path.
 constexpr int CL_THREADS = 512;
 constexpr int CL_MAX_DIM = CL_THREADS + 1;  // the prefetch of a reflector uses one element per thread
 
@@ -791,15 +882,30 @@ static void tri_plan(const std::vector<int>& dims, std::vector<TriItem>& items, 
             items.push_back(TriItem{b, j0, std::min(dims[b], j0 + BIS_WARPS), 0, 0});
 }
 
-// doubles of vector_kernel scratch (EighDev::S)
-size_t eigh_vec_scratch_doubles(const std::vector<int>& dims) {
-    size_t s = 0;
-    for (int n : dims) s += 4 * (size_t)n * TRI_THREADS * ((n + TRI_THREADS - 1) / TRI_THREADS);
-    return std::max<size_t>(s, 1);
-}
-
 constexpr int CL_SIZES[4] = {1, 2, 4, 8};
 constexpr size_t CL_SMEM_MAX = 220 * 1024;
+
+// the smallest cluster class whose shared memory holds an n x n block, or -1
+// (the block then takes the large-block path)
+static int cluster_class(int n) {
+    if (n > CL_MAX_DIM) return -1;
+    for (int i = 0; i < 4; ++i)
+        if (cluster_smem_doubles(n, CL_SIZES[i]) * sizeof(double) <= CL_SMEM_MAX) return i;
+    return -1;
+}
+
+// doubles of vector_kernel scratch (EighDev::S); the large-block path uses
+// the same buffer before the vector stage (a -1 scale vector, then one
+// scratch per large block)
+size_t eigh_vec_scratch_doubles(const std::vector<int>& dims) {
+    size_t s = 0, big = 2 * BHH_NB;
+    for (int n : dims) {
+        s += 4 * (size_t)n * TRI_THREADS * ((n + TRI_THREADS - 1) / TRI_THREADS);
+        if (cluster_class(n) < 0) big += (size_t)bhh_scratch_doubles(n);
+    }
+    return std::max<size_t>(std::max(s, big), 1);
+}
+
 
 // Householder stage plan: the block list of each cluster size (largest
 // blocks first) and the blocks left to the single-CTA global-memory kernel.
@@ -814,27 +920,239 @@ static HhPlan hh_plan(const std::vector<int>& dims) {
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return dims[x] > dims[y]; });
     HhPlan h;
     for (int b : order) {
-        const int n = dims[b];
-        int q = -1;
-        if (n <= CL_MAX_DIM)
-            for (int i = 0; i < 4 && q < 0; ++i)
-                if (cluster_smem_doubles(n, CL_SIZES[i]) * sizeof(double) <= CL_SMEM_MAX) q = i;
+        const int q = cluster_class(dims[b]);
         if (q < 0) h.global.push_back(b);
         else h.cls[q].push_back(b);
     }
     return h;
 }
 
-// descriptor bytes: bisection items, then one int per block (Householder lists)
+// the large blocks (beyond the cluster path), largest first
+static std::vector<int> big_blocks(const std::vector<int>& dims) {
+    std::vector<int> big;
+    for (size_t b = 0; b < dims.size(); ++b)
+        if (cluster_class(dims[b]) < 0) big.push_back((int)b);
+    std::stable_sort(big.begin(), big.end(), [&](int x, int y) { return dims[x] > dims[y]; });
+    return big;
+}
+
+// descriptor bytes: bisection items, one int per block (Householder lists);
+// with large blocks also their scratch offsets and the column-index table of
+// the panel updates
+static size_t big_desc_bytes(const std::vector<int>& dims) {
+    const size_t nb = big_blocks(dims).size();
+    if (nb == 0) return 0;
+    return 8 + nb * sizeof(long) + (size_t)BHH_NB * 4 * BHH_NB * sizeof(int);
+}
 size_t eigh_item_bytes(const std::vector<int>& dims) {
     std::vector<TriItem> items;
     tri_plan(dims, items);
-    return items.size() * sizeof(TriItem) + dims.size() * sizeof(int);
+    return items.size() * sizeof(TriItem) + dims.size() * sizeof(int) + big_desc_bytes(dims);
 }
 
 size_t eigh_gemm_bytes(const std::vector<int>& dims, size_t* tiles_bytes) {
-    if (tiles_bytes) *tiles_bytes = gemm_index_bytes(dims.size());
-    return std::max<size_t>(dims.size(), 1) * sizeof(GemmProblem<double, double, double>);
+    size_t np = dims.size();
+    size_t panels = 0;
+    for (int b : big_blocks(dims)) panels += (size_t)bhh_panels(dims[b]);
+    np = std::max(np, panels);
+    if (tiles_bytes) *tiles_bytes = gemm_index_bytes(np);
+    return std::max<size_t>(np, 1) * sizeof(GemmProblem<double, double, double>);
+}
+
+// The large-block Householder path (see bhh_col_kernel) on stream st.
+// big: the blocks, largest first; d_big / d_boff / d_kidx: their device list,
+// scratch offsets and the panel-update column table (uploaded by the caller).
+static void launch_big(const EighDev& d, const std::vector<int>& dims, const std::vector<long>& moff,
+                       const std::vector<int>& big, const int* d_big, const long* d_boff, const int* d_kidx,
+                       cudaStream_t st) {
+    const int nbig = (int)big.size();
+    std::vector<long> boff(nbig);
+    long o = 2 * BHH_NB;
+    for (int i = 0; i < nbig; ++i) {
+        boff[i] = o;
+        o += bhh_scratch_doubles(dims[big[i]]);
+    }
+    const int nmax = dims[big[0]];
+    // blocks with a reflector in column j: a prefix of the list
+    auto nact = [&](int j) {
+        int c = 0;
+        while (c < nbig && dims[big[c]] - 2 > j) ++c;
+        return c;
+    };
+    BigArgs a{};
+    a.big = d_big;
+    a.boff = d_boff;
+    a.dims = d.dims;
+    a.moff = d.moff;
+    a.eoff = d.eoff;
+    a.A = d.A;
+    a.Zc = d.Zc;
+    a.S = d.S;
+    a.tri = d.tri;
+    double fl = 0.0, by = 0.0;
+    for (int b : big) {
+        const double n = dims[b];
+        fl += 8.0 / 3.0 * n * n * n;
+        by += 16.0 * n * n + 16.0 * n;
+    }
+    ProfRange pr("eigh_blocked_householder", st, fl, by);
+    for (int b : big)
+        PGX_CUDA(cudaMemcpyAsync(d.A + moff[b], d.H + moff[b], (size_t)dims[b] * dims[b] * sizeof(double),
+                                 cudaMemcpyDeviceToDevice, st));
+    {
+        double neg[2 * BHH_NB];
+        for (double& x : neg) x = -1.0;
+        h2d(d.S, neg, sizeof(neg), st);
+    }
+    PGX_CUDA(cudaFuncSetAttribute(bhh_symv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(double) * nmax)));
+    std::vector<GemmProblem<double, double, double>> probs;
+    size_t tiles_cap = 0;
+    const size_t probs_cap = eigh_gemm_bytes(dims, &tiles_cap);
+    // ---- tridiagonalisation
+    for (int k = 0; k < nmax - 2; k += BHH_NB) {
+        a.k = k;
+        const int jend = std::min(k + BHH_NB, nmax - 2);  // columns k .. jend - 1 of the largest block
+        for (int j = k; j < jend; ++j) {
+            a.fin = (j > k) ? j - 1 : -1;
+            a.col = j;
+            a.nact = nact(j > k ? j - 1 : j);
+            bhh_col_kernel<<<(unsigned)a.nact, BHH_COL_THREADS, 0, st>>>(a);
+            check_launch("bhh_col_kernel");
+            a.fin = -1;
+            a.nact = nact(j);
+            long ctas = 0;
+            for (int i = 0; i < a.nact; ++i) ctas += (dims[big[i]] - j - 1 + BHH_SYMV_ROWS - 1) / BHH_SYMV_ROWS;
+            bhh_symv_kernel<<<(unsigned)ctas, BHH_SYMV_THREADS, sizeof(double) * nmax, st>>>(a);
+            check_launch("bhh_symv_kernel");
+        }
+        a.fin = jend - 1;
+        a.col = -1;
+        a.nact = nact(jend - 1);
+        bhh_col_kernel<<<(unsigned)a.nact, BHH_COL_THREADS, 0, st>>>(a);
+        check_launch("bhh_col_kernel");
+        // A(k+p:, k+p:) -= V W^T + W V^T, p = the block's columns in this panel
+        probs.clear();
+        for (int i = 0; i < nact(k); ++i) {
+            const int n = dims[big[i]];
+            const int p = std::min(BHH_NB, n - 2 - k), kp = k + p, m = n - kp;
+            if (m <= 0) continue;
+            double* VW = d.S + boff[i] + kp;
+            GemmProblem<double, double, double> g{};
+            g.A = VW;
+            g.B = VW;
+            g.C = d.A + moff[big[i]] + (long)kp * n + kp;
+            g.M = m;
+            g.N = m;
+            g.K = 2 * p;
+            g.sa_i = 1;
+            g.sa_k = n;
+            g.sb_k = n;
+            g.sb_j = 1;
+            g.sc_i = n;
+            g.sc_j = 1;
+            g.a_kidx = d_kidx + (p - 1) * 4 * BHH_NB;
+            g.b_kidx = g.a_kidx + 2 * BHH_NB;
+            g.kscale = d.S;
+            g.accumulate = 1;
+            probs.push_back(g);
+        }
+        launch_gemm_batch(probs, d.gemm_probs, probs_cap, d.gemm_tiles, tiles_cap, st);
+    }
+    a.nact = nbig;
+    bhh_finish_kernel<<<(unsigned)nbig, 256, 0, st>>>(a);
+    check_launch("bhh_finish_kernel");
+    // ---- Q: Gram matrices and -T of every panel, then the panels from the last
+    probs.clear();
+    long npan_total = 0;
+    long npan_max = 0;
+    for (int i = 0; i < nbig; ++i) {
+        const int n = dims[big[i]];
+        const long np = bhh_panels(n);
+        npan_max = std::max(npan_max, np);
+        npan_total += np;
+        for (long q = 0; q < np; ++q) {
+            const int k = (int)q * BHH_NB, p = std::min(BHH_NB, n - 2 - k), m = n - k - 1;
+            const double* Vp = d.A + moff[big[i]] + (long)(k + 1) * n + k;
+            GemmProblem<double, double, double> g{};
+            g.A = Vp;  // V^T
+            g.B = Vp;
+            g.C = d.S + boff[i] + 2L * BHH_NB * n + 2L * n + q * BHH_NB * BHH_NB;
+            g.M = p;
+            g.N = p;
+            g.K = m;
+            g.sa_i = 1;
+            g.sa_k = n;
+            g.sb_k = n;
+            g.sb_j = 1;
+            g.sc_i = BHH_NB;
+            g.sc_j = 1;
+            probs.push_back(g);
+        }
+    }
+    launch_gemm_batch(probs, d.gemm_probs, probs_cap, d.gemm_tiles, tiles_cap, st);
+    a.nact = nbig;
+    bhh_tfactor_kernel<<<(unsigned)npan_total, 32, 0, st>>>(a);
+    check_launch("bhh_tfactor_kernel");
+    for (long q = npan_max - 1; q >= 0; --q) {
+        const int k = (int)q * BHH_NB;
+        std::vector<GemmProblem<double, double, double>> py, pt, pu;
+        for (int i = 0; i < nact(k); ++i) {
+            const int n = dims[big[i]];
+            const int p = std::min(BHH_NB, n - 2 - k), m = n - k - 1;
+            const double* Vp = d.A + moff[big[i]] + (long)(k + 1) * n + k;
+            double* Qs = d.Zc + moff[big[i]] + (long)(k + 1) * n + (k + 1);
+            double* Y = d.S + boff[i];
+            double* Y2 = Y + (long)BHH_NB * n;
+            const double* nT = d.S + boff[i] + 2L * BHH_NB * n + 2L * n + (bhh_panels(n) + q) * BHH_NB * BHH_NB;
+            GemmProblem<double, double, double> g{};
+            g.A = Vp;  // Y = V^T Q
+            g.sa_i = 1;
+            g.sa_k = n;
+            g.B = Qs;
+            g.sb_k = 1;
+            g.sb_j = n;
+            g.C = Y;
+            g.sc_i = n;
+            g.sc_j = 1;
+            g.M = p;
+            g.N = m;
+            g.K = m;
+            py.push_back(g);
+            GemmProblem<double, double, double> h{};  // Y2 = (-T) Y
+            h.A = nT;
+            h.sa_i = BHH_NB;
+            h.sa_k = 1;
+            h.B = Y;
+            h.sb_k = n;
+            h.sb_j = 1;
+            h.C = Y2;
+            h.sc_i = n;
+            h.sc_j = 1;
+            h.M = p;
+            h.N = m;
+            h.K = p;
+            pt.push_back(h);
+            GemmProblem<double, double, double> u{};  // Q += V Y2
+            u.A = Vp;
+            u.sa_i = n;
+            u.sa_k = 1;
+            u.B = Y2;
+            u.sb_k = n;
+            u.sb_j = 1;
+            u.C = Qs;
+            u.sc_i = 1;
+            u.sc_j = n;
+            u.M = m;
+            u.N = m;
+            u.K = p;
+            u.accumulate = 1;
+            pu.push_back(u);
+        }
+        launch_gemm_batch(py, d.gemm_probs, probs_cap, d.gemm_tiles, tiles_cap, st);
+        launch_gemm_batch(pt, d.gemm_probs, probs_cap, d.gemm_tiles, tiles_cap, st);
+        launch_gemm_batch(pu, d.gemm_probs, probs_cap, d.gemm_tiles, tiles_cap, st);
+    }
 }
 
 // All eigensolver stages on caller-provided device buffers (no allocation),
@@ -877,8 +1195,7 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
         int nclusters = 0;
         if (cudaOccupancyMaxActiveClusters(&nclusters, eigh_cluster_kernel, &cfg) != cudaSuccess || nclusters < 1) {
             cudaGetLastError();
-            hp.global.insert(hp.global.end(), hp.cls[q].begin(), hp.cls[q].end());
-            hp.cls[q].clear();
+            PGX_CHECK(false, PGX_ERR_CUDA, "the eigensolver's thread-block clusters cannot be scheduled on this device");
         }
     }
     std::vector<int> lists(hp.global);
@@ -887,11 +1204,46 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
         cl_off[q] = lists.size();
         lists.insert(lists.end(), hp.cls[q].begin(), hp.cls[q].end());
     }
-    std::vector<char> host(items.size() * sizeof(TriItem) + lists.size() * sizeof(int));
+    // large blocks: scratch offsets (doubles into S) and, per panel width p, the
+    // column gathers of the panel update [V_0..V_p-1 W_0..W_p-1] and [W.. V..]
+    const std::vector<int>& big = hp.global;
+    const size_t lists_end = items.size() * sizeof(TriItem) + lists.size() * sizeof(int);
+    const size_t boff_at = (lists_end + 7) & ~size_t(7);
+    size_t host_bytes = lists_end;
+    std::vector<long> boff;
+    std::vector<int> kidx;
+    if (!big.empty()) {
+        long o = 2 * BHH_NB;
+        for (int b : big) {
+            boff.push_back(o);
+            o += bhh_scratch_doubles(dims[b]);
+        }
+        for (int p = 1; p <= BHH_NB; ++p) {
+            std::vector<int> ia(2 * BHH_NB, 0), ib(2 * BHH_NB, 0);
+            for (int t = 0; t < p; ++t) {
+                ia[t] = t;
+                ia[p + t] = BHH_NB + t;
+                ib[t] = BHH_NB + t;
+                ib[p + t] = t;
+            }
+            kidx.insert(kidx.end(), ia.begin(), ia.end());
+            kidx.insert(kidx.end(), ib.begin(), ib.end());
+        }
+        host_bytes = boff_at + boff.size() * sizeof(long) + kidx.size() * sizeof(int);
+        PGX_CHECK(host_bytes <= eigh_item_bytes(dims), PGX_ERR_ARG, "eigensolver descriptor layout overflow");
+    }
+    std::vector<char> host(host_bytes);
     std::memcpy(host.data(), items.data(), items.size() * sizeof(TriItem));
     std::memcpy(host.data() + items.size() * sizeof(TriItem), lists.data(), lists.size() * sizeof(int));
+    if (!big.empty()) {
+        std::memcpy(host.data() + boff_at, boff.data(), boff.size() * sizeof(long));
+        std::memcpy(host.data() + boff_at + boff.size() * sizeof(long), kidx.data(), kidx.size() * sizeof(int));
+    }
     h2d(d.items, host.data(), host.size(), st);
     const int* d_lists = reinterpret_cast<const int*>(static_cast<const char*>(d.items) + items.size() * sizeof(TriItem));
+    const long* d_boff = reinterpret_cast<const long*>(static_cast<const char*>(d.items) + boff_at);
+    const int* d_kidx = reinterpret_cast<const int*>(static_cast<const char*>(d.items) + boff_at +
+                                                     boff.size() * sizeof(long));
 
     // LAPACK operation counts: tridiagonalisation 4/3 n^3, forming Q 4/3 n^3;
     // minimum DRAM traffic: read H, write Q and the tridiagonal
@@ -910,27 +1262,7 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
         PGX_CUDA(cudaEventRecord(d.fork, st));
         for (int i = 0; i < 3; ++i) PGX_CUDA(cudaStreamWaitEvent(d.aux[i], d.fork, 0));
     }
-    if (!hp.global.empty()) {
-        int gmax = 1;
-        for (int b : hp.global) gmax = std::max(gmax, dims[b]);
-        const size_t smem = 4 * sizeof(double) * (size_t)gmax;
-        PGX_CHECK(smem <= 200 * 1024, PGX_ERR_ARG, "block too large for the single-CTA eigensolver (d > 6400)");
-        PGX_CUDA(cudaFuncSetAttribute(eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        EighArgs a;
-        a.order = d_lists;
-        a.dims = d.dims;
-        a.moff = d.moff;
-        a.eoff = d.eoff;
-        a.H = d.H;
-        a.A = d.A;
-        a.Zc = d.Zc;
-        a.tri = d.tri;
-        double fl, by;
-        hh_work(hp.global, fl, by);
-        ProfRange pr("eigh_kernel", st, fl, by);
-        eigh_kernel<<<(unsigned)hp.global.size(), EIGH_THREADS, smem, st>>>(a);
-        check_launch("eigh_kernel");
-    }
+    if (!big.empty()) launch_big(d, dims, moff, big, d_lists, d_boff, d_kidx, st);
     for (int q = 0; q < 4; ++q) {
         if (hp.cls[q].empty()) continue;
         const cudaStream_t sq = (fork && q > 0) ? d.aux[q - 1] : st;

@@ -78,8 +78,8 @@ def test_eigh_larger_blocks(harness):
 def test_eigh_every_householder_class():
     """One eigensolve whose blocks reach every Householder launch: thread-block
     clusters of 1, 2, 4 and 8 CTAs (blocks whose matrix fits in 8 x 220 KB of
-    distributed shared memory, up to 464 states) and the single-CTA
-    global-memory kernel (larger blocks).
+    distributed shared memory, up to 464 states) and the blocked large-block
+    path (larger blocks).
     Spectra: random, tightly clustered (1e-9 spacings), two-level degenerate."""
     rng = np.random.default_rng(11)
     dims = [150, 200, 256, 300, 401, 464, 465, 514, 640]
@@ -108,6 +108,39 @@ def test_eigh_every_householder_class():
         assert np.abs(h @ u - u * e[None, :]).max() < 1e-10 * scale
         assert np.abs(u.T @ u - np.eye(len(e))).max() < 1e-11
         assert np.abs(e - np.linalg.eigvalsh(h)).max() < 1e-11 * scale
+
+
+def test_eigh_large_blocks():
+    """The blocked large-block path on blocks of 700, 1225 and 2100 states
+    (random, tightly clustered and two-level degenerate spectra), next to
+    small blocks on the cluster path, against LAPACK: residual, orthogonality
+    and eigenvalues at 1e-10 / 1e-11 relative to the spectrum."""
+    rng = np.random.default_rng(12)
+    dims = [2100, 36, 1225, 700, 465]
+    blocks = []
+    for i, d in enumerate(dims):
+        if i % 3 == 0:
+            a = rng.standard_normal((d, d))
+            h = (a + a.T) / 2
+        else:
+            q, _ = np.linalg.qr(rng.standard_normal((d, d)))
+            ev = (np.r_[np.arange(d - 4) * 1e-9, [1.0, 2.0, 3.0, 4.0]] if i % 3 == 1
+                  else np.r_[np.zeros(d // 2), np.ones(d - d // 2)])
+            h = (q * ev) @ q.T
+        blocks.append((h + h.T) / 2)
+    from pomerol_b200.pgx import Engine
+    eng = Engine()
+    eng.set_blocks(dims)
+    eng.set_hamiltonian(blocks)
+    for _ in range(2):  # a second solve on the same context gives the same result
+        eng.eigh()
+        E, U = eng.eigensystem()
+        for h, e, u in zip(blocks, E, U):
+            scale = max(1.0, np.abs(e).max())
+            assert np.all(np.diff(e) >= 0)
+            assert np.abs(h @ u - u * e[None, :]).max() < 1e-10 * scale
+            assert np.abs(u.T @ u - np.eye(len(e))).max() < 1e-11
+            assert np.abs(e - np.linalg.eigvalsh(h)).max() < 1e-11 * scale
 
 
 def test_hamiltonian_ground_energy(harness):
