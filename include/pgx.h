@@ -218,6 +218,39 @@ int pgx_g2_count(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, double 
                  long long* count);
 
 /* ------------------------------------------------------------------------
+ * Batches of independent models.
+ * The reference holds one model per set of objects; for many impurity models
+ * at once (the 64-model batch workload) a context may hold the blocks of
+ * several models, diagonalised by one pgx_eigh, each model weighted at its
+ * own inverse temperature and its pair sums evaluated at its own frequencies.
+ * Per model this is DensityMatrix::compute (DensityMatrix.cpp:38-58) and
+ * GreensFunctionPart / SusceptibilityPart (GreensFunctionPart.cpp:65-110,
+ * SusceptibilityPart.cpp:76-127) as pgx_weights, pgx_gf and pgx_susc do.
+ * ------------------------------------------------------------------------ */
+
+/* Blocks first_block[m] .. first_block[m+1]-1 (first_block[0] = 0,
+ * first_block[nmodels] = the number of blocks) form model m, at inverse
+ * temperature beta[m].  Call after pgx_set_blocks (which forgets models). */
+int pgx_set_models(pgx_ctx* ctx, int32_t nmodels, const int32_t* first_block, const double* beta);
+
+/* Weights of every model on its own states: E0_m = min E, w = exp(-beta_m
+ * (E - E0_m)) / Z_m.  w (sum of dims), E0 and Z (nmodels each) are copied out
+ * when non-NULL.  pgx_g2, pgx_chi3 and pgx_gf_vjp need the weights of a
+ * single model (pgx_weights) and refuse these. */
+int pgx_weights_models(pgx_ctx* ctx, double* w, double* E0, double* Z);
+
+/* pgx_gf / pgx_susc for every model at once: a part belongs to the model of
+ * its blocks; z holds nz frequencies per model (nmodels x nz complex,
+ * model-major) and out the values (same layout); zero_pole (nmodels complex,
+ * or NULL) the zero-pole sums of each model.  The susceptibility's beta is
+ * each model's own. */
+int pgx_gf_models(pgx_ctx* ctx, int32_t op1, int32_t op2, int32_t nparts, const int32_t* outer, const int32_t* inner,
+                  int32_t nz, const double* z, double coef_tol, double* out);
+int pgx_susc_models(pgx_ctx* ctx, int32_t opA, int32_t opB, int32_t nparts, const int32_t* outer,
+                    const int32_t* inner, int32_t nz, const double* z, double pole_res, double coef_tol, double* out,
+                    double* zero_pole);
+
+/* ------------------------------------------------------------------------
  * K6 Three-point fermion-boson susceptibility.
  * Replaces: ThreePointSusceptibility::compute / operator() and
  * ThreePointSusceptibilityPart::computeImpl, addMultiterm and the term

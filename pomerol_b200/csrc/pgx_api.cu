@@ -340,6 +340,7 @@ int pgx_gf_vjp(pgx_ctx* c, int32_t op1, int32_t op2, int32_t nparts, const int32
     return guarded(c, [&] {
         PGX_CHECK(nparts >= 0 && nz >= 0 && (nparts == 0 || (outer && inner)) && (nz == 0 || (z && lambda)) && dterm,
                   PGX_ERR_ARG, "bad arguments");
+        PGX_CHECK(!c->P.w_models, PGX_ERR_STATE, "needs the weights of one model (pgx_weights)");
         pgx::run_gf_vjp(c, op1, op2, nparts, outer, inner, nz, z, lambda, dterm, dE);
     });
 }
@@ -349,7 +350,45 @@ int pgx_chi3(pgx_ctx* c, int32_t channel, int32_t nparts, const pgx_chi3_part* p
     return guarded(c, [&] {
         PGX_CHECK(nparts >= 0 && nfreq >= 0 && (nparts == 0 || parts) && (nfreq == 0 || (z && out)), PGX_ERR_ARG,
                   "bad arguments");
+        PGX_CHECK(!c->P.w_models, PGX_ERR_STATE, "needs the weights of one model (pgx_weights)");
         pgx::run_chi3(c, channel, nparts, parts, nfreq, z, pole_res, out);
+    });
+}
+
+int pgx_set_models(pgx_ctx* c, int32_t nmodels, const int32_t* first_block, const double* beta) {
+    return guarded(c, [&] { pgx::set_models(c->P, nmodels, first_block, beta); });
+}
+
+int pgx_weights_models(pgx_ctx* c, double* w, double* E0, double* Z) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.have_eig, PGX_ERR_STATE, "pgx_eigh first");
+        pgx::launch_weights_models(P, c->stream);
+        P.have_w = true;
+        P.w_models = true;
+        P.retained.assign(P.nblocks, 1);
+        if (w) std::copy(P.w_host.begin(), P.w_host.end(), w);
+        if (E0) std::copy(P.model_E0.begin(), P.model_E0.end(), E0);
+        if (Z) std::copy(P.model_Z.begin(), P.model_Z.end(), Z);
+    });
+}
+
+int pgx_gf_models(pgx_ctx* c, int32_t op1, int32_t op2, int32_t nparts, const int32_t* outer, const int32_t* inner,
+                  int32_t nz, const double* z, double coef_tol, double* out) {
+    return guarded(c, [&] {
+        PGX_CHECK(nparts >= 0 && nz >= 0 && (nz == 0 || (z && out)) && (nparts == 0 || (outer && inner)), PGX_ERR_ARG,
+                  "bad arguments");
+        pgx::run_gf_models(c, op1, op2, nparts, outer, inner, nz, z, coef_tol, out);
+    });
+}
+
+int pgx_susc_models(pgx_ctx* c, int32_t opA, int32_t opB, int32_t nparts, const int32_t* outer,
+                    const int32_t* inner, int32_t nz, const double* z, double pole_res, double coef_tol, double* out,
+                    double* zero_pole) {
+    return guarded(c, [&] {
+        PGX_CHECK(nparts >= 0 && nz >= 0 && (nz == 0 || (z && out)) && (nparts == 0 || (outer && inner)), PGX_ERR_ARG,
+                  "bad arguments");
+        pgx::run_susc_models(c, opA, opB, nparts, outer, inner, nz, z, pole_res, coef_tol, out, zero_pole);
     });
 }
 
@@ -409,6 +448,7 @@ int pgx_weights(pgx_ctx* c, double beta, double* w, double* Z) {
         pgx::launch_weights(P, beta, c->stream);
         P.beta = beta;
         P.have_w = true;
+        P.w_models = false;
         P.retained.assign(P.nblocks, 1);
         if (w) {
             PGX_CUDA(cudaMemcpyAsync(w, P.d_w, P.esize * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -576,6 +616,7 @@ int pgx_g2(pgx_ctx* c, int32_t nparts, const pgx_g2_part* parts, int32_t nfreq, 
     return guarded(c, [&] {
         PGX_CHECK(nparts >= 0 && nfreq >= 0 && (nparts == 0 || parts) && (nfreq == 0 || (z && out)), PGX_ERR_ARG,
                   "bad arguments");
+        PGX_CHECK(!c->P.w_models, PGX_ERR_STATE, "needs the weights of one model (pgx_weights)");
         pgx::run_g2(c, nparts, parts, nfreq, z, pole_res, coef_tol, flags, out);
     });
 }

@@ -102,6 +102,13 @@ struct Problem {
     // complex blocks: real embedding of twice the size and its eigensolver workspace
     DevBuf cx_meta, cx_H, cx_A, cx_Zc, cx_U, cx_E, cx_tri, cx_S, cx_items, cx_gemm;
     std::vector<double> w_host;          // host copy of the weights (set with them)
+    // independent models sharing the context (pgx_set_models): blocks
+    // model_first[m] .. model_first[m+1]-1 form model m, at inverse temperature model_beta[m]
+    int nmodels = 0;
+    std::vector<int> model_first, block_model;
+    std::vector<double> model_beta, model_E0, model_Z;
+    bool w_models = false;               // the weights are per model (pgx_weights_models)
+    DevBuf model_buf;                    // state ranges, inverse temperatures, E0 and Z per model
     int* d_dims = nullptr;
     long* d_moff = nullptr;
     long* d_eoff = nullptr;
@@ -272,6 +279,12 @@ void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq
                      double anchor_tol, double* out);
 void run_chi3(pgx_ctx* c, int channel, int nparts, const pgx_chi3_part* parts, int nfreq, const double* z,
               double pole_res, double* out);
+void set_models(Problem& P, int nmodels, const int32_t* first_block, const double* beta);
+void launch_weights_models(Problem& P, cudaStream_t st);
+void run_gf_models(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,
+                   const double* z, double coef_tol, double* out);
+void run_susc_models(pgx_ctx* c, int opA, int opB, int nparts, const int32_t* outer, const int32_t* inner, int nz,
+                     const double* z, double pole_res, double coef_tol, double* out, double* zero_pole);
 void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_tol, double nz_tol, long long* count);
 
 }  // namespace pgx

@@ -100,6 +100,7 @@ struct PairPart {
     long eo, ei;       // vector offsets of outer / inner blocks
     int d_o, d_i;
     long term0;        // first term slot
+    long model;        // model of the part (0 with a single model): its zero-pole slot
 };
 
 // Residues and poles.  mode 0: G (R = F1 F2 (w_o + w_i)); mode 1: chi
@@ -138,8 +139,8 @@ __global__ void pair_terms_kernel(const PairPart* parts, int nparts, const T* m1
         zx = warp_sum(zx);
         zy = warp_sum(zy);
         if ((threadIdx.x & 31) == 0 && (zx != 0.0 || zy != 0.0)) {
-            atomicAdd(zero, zx);
-            atomicAdd(zero + 1, zy);
+            atomicAdd(zero + 2 * pp.model, zx);
+            atomicAdd(zero + 2 * pp.model + 1, zy);
         }
     }
 }
@@ -170,6 +171,86 @@ __global__ void __launch_bounds__(EVAL_THREADS) pair_eval_kernel(const cd* R, co
     }
     atomicAdd(&out[iz].x, sign * ax);
     atomicAdd(&out[iz].y, sign * ay);
+}
+
+// Independent models: out[m][z] += sign * sum over the terms of model m of
+// R_t / (z_m - P_t).  CTA = (chunk of one model's terms, z tile): the chunks
+// run along x, whose grid limit (2^31 - 1) holds every term list.
+struct EvalChunk {
+    long t0;
+    int cnt, model;
+};
+__global__ void __launch_bounds__(EVAL_THREADS) pair_eval_models_kernel(const cd* R, const double* P,
+                                                                         const EvalChunk* chunks, const cd* z, int nz,
+                                                                         double sign, cd* out) {
+    __shared__ cd sR[EVAL_CHUNK];
+    __shared__ double sP[EVAL_CHUNK];
+    const EvalChunk ch = chunks[blockIdx.x];
+    for (int i = threadIdx.x; i < ch.cnt; i += blockDim.x) {
+        sR[i] = R[ch.t0 + i];
+        sP[i] = P[ch.t0 + i];
+    }
+    __syncthreads();
+    const int iz = blockIdx.y * blockDim.x + threadIdx.x;
+    if (iz >= nz) return;
+    const long o = (long)ch.model * nz + iz;
+    const cd zz = z[o];
+    double ax = 0.0, ay = 0.0;
+    for (int i = 0; i < ch.cnt; ++i) {
+        const cd r = sR[i];
+        if (r.x == 0.0 && r.y == 0.0) continue;
+        const cd q = r * inv(cd{zz.x - sP[i], zz.y});
+        ax += q.x;
+        ay += q.y;
+    }
+    atomicAdd(&out[o].x, sign * ax);
+    atomicAdd(&out[o].y, sign * ay);
+}
+
+// Weights of every model on its own states [s[m], s[m+1]) at its own beta:
+// E0_m = min E, w = exp(-beta_m (E - E0_m)) / Z_m.  One CTA per model (fixed
+// reduction order, as weights_kernel).
+__global__ void __launch_bounds__(1024) weights_models_kernel(const double* E, double* w, const long* s,
+                                                               const double* beta, double* e0z) {
+    __shared__ double red[32];
+    __shared__ double s_e0, s_z;
+    const int m = blockIdx.x, tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const long a = s[m], b = s[m + 1];
+    const double bt = beta[m];
+    double mn = DBL_MAX;
+    for (long i = a + tid; i < b; i += blockDim.x) mn = fmin(mn, E[i]);
+    mn = warp_min(mn);
+    if (lane == 0) red[wid] = mn;
+    __syncthreads();
+    if (wid == 0) {
+        double r = (lane < (int)(blockDim.x >> 5)) ? red[lane] : DBL_MAX;
+        r = warp_min(r);
+        if (lane == 0) s_e0 = r;
+    }
+    __syncthreads();
+    const double e0 = s_e0;
+    double sum = 0.0;
+    for (long i = a + tid; i < b; i += blockDim.x) {
+        const double x = exp(-bt * (E[i] - e0));
+        w[i] = x;
+        sum += x;
+    }
+    sum = warp_sum(sum);
+    __syncthreads();
+    if (lane == 0) red[wid] = sum;
+    __syncthreads();
+    if (wid == 0) {
+        double r = (lane < (int)(blockDim.x >> 5)) ? red[lane] : 0.0;
+        r = warp_sum(r);
+        if (lane == 0) s_z = r;
+    }
+    __syncthreads();
+    const double zs = s_z;
+    for (long i = a + tid; i < b; i += blockDim.x) w[i] /= zs;
+    if (tid == 0) {
+        e0z[2 * m] = e0;
+        e0z[2 * m + 1] = zs;
+    }
 }
 
 template <typename T>
@@ -352,7 +433,7 @@ static void run_pair(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* ou
         const int pa = A.by_left[o], pb = B.by_right[o];
         PGX_CHECK(pa >= 0 && pb >= 0 && A.parts[pa].right == i && B.parts[pb].left == i, PGX_ERR_ARG,
                   "blocks do not form a pair part");
-        PairPart x{A.parts[pa].off, B.parts[pb].off, P.eoff[o], P.eoff[i], P.dims[o], P.dims[i], nterms};
+        PairPart x{A.parts[pa].off, B.parts[pb].off, P.eoff[o], P.eoff[i], P.dims[o], P.dims[i], nterms, 0};
         nterms += (long)x.d_o * x.d_i;
         pp.push_back(x);
     }
@@ -410,6 +491,177 @@ static void run_pair(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* ou
         zero_out[0] = zero.x;
         zero_out[1] = zero.y;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Independent models in one context.
+void set_models(Problem& P, int nmodels, const int32_t* first, const double* beta) {
+    PGX_CHECK(P.nblocks > 0, PGX_ERR_STATE, "pgx_set_blocks first");
+    PGX_CHECK(nmodels >= 1 && first && beta, PGX_ERR_ARG, "bad model description");
+    PGX_CHECK(first[0] == 0 && first[nmodels] == P.nblocks, PGX_ERR_ARG, "models must cover the blocks in order");
+    for (int m = 0; m < nmodels; ++m) {
+        PGX_CHECK(first[m + 1] > first[m], PGX_ERR_ARG, "every model needs at least one block");
+        PGX_CHECK(beta[m] > 0.0, PGX_ERR_ARG, "beta must be positive");
+    }
+    P.nmodels = nmodels;
+    P.model_first.assign(first, first + nmodels + 1);
+    P.model_beta.assign(beta, beta + nmodels);
+    P.block_model.assign(P.nblocks, 0);
+    for (int m = 0; m < nmodels; ++m)
+        for (int b = first[m]; b < first[m + 1]; ++b) P.block_model[b] = m;
+    P.have_w = false;
+}
+
+void launch_weights_models(Problem& P, cudaStream_t st) {
+    PGX_CHECK(P.nmodels > 0, PGX_ERR_STATE, "pgx_set_models first");
+    const int nm = P.nmodels;
+    std::vector<long> s(nm + 1);
+    for (int m = 0; m <= nm; ++m) s[m] = (P.model_first[m] < P.nblocks) ? P.eoff[P.model_first[m]] : P.esize;
+    const size_t b_s = ((nm + 1) * sizeof(long) + 255) & ~size_t(255), b_b = (nm * sizeof(double) + 255) & ~size_t(255);
+    P.model_buf.reserve(b_s + b_b + 2 * nm * sizeof(double));
+    char* base = P.model_buf.as<char>();
+    long* d_s = reinterpret_cast<long*>(base);
+    double* d_beta = reinterpret_cast<double*>(base + b_s);
+    double* d_e0z = reinterpret_cast<double*>(base + b_s + b_b);
+    h2d(d_s, s.data(), (nm + 1) * sizeof(long), st);
+    h2d(d_beta, P.model_beta.data(), nm * sizeof(double), st);
+    {
+        ProfRange pr("weights_models_kernel", st, 0.0, 24.0 * P.esize);
+        weights_models_kernel<<<nm, 1024, 0, st>>>(P.d_E, P.d_w, d_s, d_beta, d_e0z);
+        check_launch("weights_models_kernel");
+    }
+    std::vector<double> h(2 * nm);
+    P.w_host.resize(P.esize);
+    PGX_CUDA(cudaMemcpyAsync(h.data(), d_e0z, 2 * nm * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaMemcpyAsync(P.w_host.data(), P.d_w, P.esize * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaStreamSynchronize(st));
+    P.model_E0.resize(nm);
+    P.model_Z.resize(nm);
+    for (int m = 0; m < nm; ++m) {
+        P.model_E0[m] = h[2 * m];
+        P.model_Z[m] = h[2 * m + 1];
+    }
+}
+
+// The pair sums of run_pair for every model at once: each part belongs to the
+// model of its outer block; z and out are nmodels x nz (model-major), each
+// model summed over its own parts at its own frequencies.
+static void run_pair_models(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner,
+                            int nz, const double* z, double pole_res, double coef_tol, int mode, double sign,
+                            double* out, double* zero_out) {
+    Problem& P = c->P;
+    cudaStream_t st = c->stream;
+    PGX_CHECK(P.nmodels > 0 && P.w_models && P.have_w, PGX_ERR_STATE, "pgx_set_models and pgx_weights_models first");
+    PGX_CHECK(op1 >= 0 && op1 < (int)P.ops.size() && op2 >= 0 && op2 < (int)P.ops.size(), PGX_ERR_ARG,
+              "bad operator id");
+    const Operator& A = P.ops[op1];
+    const Operator& B = P.ops[op2];
+    PGX_CHECK(A.rotated && B.rotated, PGX_ERR_STATE, "operators must be rotated");
+    const int nm = P.nmodels;
+    // parts grouped by model, their terms contiguous
+    std::vector<int> order(nparts);
+    for (int q = 0; q < nparts; ++q) {
+        PGX_CHECK(outer[q] >= 0 && outer[q] < P.nblocks && inner[q] >= 0 && inner[q] < P.nblocks, PGX_ERR_ARG,
+                  "bad block");
+        PGX_CHECK(P.block_model[outer[q]] == P.block_model[inner[q]], PGX_ERR_ARG, "a part joins two models");
+        order[q] = q;
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return P.block_model[outer[x]] < P.block_model[outer[y]]; });
+    std::vector<PairPart> pp;
+    std::vector<EvalChunk> chunks;
+    long nterms = 0;
+    for (int q : order) {
+        const int o = outer[q], i = inner[q];
+        const int pa = A.by_left[o], pb = B.by_right[o];
+        PGX_CHECK(pa >= 0 && pb >= 0 && A.parts[pa].right == i && B.parts[pb].left == i, PGX_ERR_ARG,
+                  "blocks do not form a pair part");
+        const long m = P.block_model[o];
+        PairPart x{A.parts[pa].off, B.parts[pb].off, P.eoff[o], P.eoff[i], P.dims[o], P.dims[i], nterms, m};
+        const long n = (long)x.d_o * x.d_i;
+        for (long t = 0; t < n; t += EVAL_CHUNK)  // chunks never straddle two parts, so never two models
+            chunks.push_back(EvalChunk{nterms + t, (int)std::min<long>(EVAL_CHUNK, n - t), (int)m});
+        nterms += n;
+        pp.push_back(x);
+    }
+    PGX_CHECK(chunks.size() < (1u << 31) && ceil_div(nz, EVAL_THREADS) < 65536, PGX_ERR_ARG,
+              "too many Lehmann terms or frequencies for one call");
+    DevBuf& bR = c->scratch[0];
+    DevBuf& bP = c->scratch[1];
+    DevBuf& bparts = c->scratch[2];
+    DevBuf& bz = c->scratch[3];
+    DevBuf& bout = c->scratch[4];
+    DevBuf& bch = c->scratch[5];
+    const long nzt = (long)nm * nz;
+    bR.reserve(std::max<long>(nterms, 1) * sizeof(cd));
+    bP.reserve(std::max<long>(nterms, 1) * sizeof(double));
+    bparts.reserve(std::max<size_t>(pp.size(), 1) * sizeof(PairPart));
+    bch.reserve(std::max<size_t>(chunks.size(), 1) * sizeof(EvalChunk));
+    bz.reserve(std::max<long>(nzt, 1) * sizeof(cd));
+    bout.reserve((std::max<long>(nzt, 1) + nm) * sizeof(cd));
+    if (!pp.empty()) {
+        h2d(bparts.p, pp.data(), pp.size() * sizeof(PairPart), st);
+        h2d(bch.p, chunks.data(), chunks.size() * sizeof(EvalChunk), st);
+    }
+    if (nzt > 0) h2d(bz.p, z, nzt * sizeof(cd), st);
+    PGX_CUDA(cudaMemsetAsync(bout.p, 0, (nzt + nm) * sizeof(cd), st));
+    cd* d_out = bout.as<cd>();
+    double* d_zero = reinterpret_cast<double*>(d_out + nzt);
+    if (nterms > 0) {
+        long maxn = 1;
+        for (auto& x : pp) maxn = std::max(maxn, (long)x.d_o * x.d_i);
+        dim3 g1(std::min(ceil_div(maxn, 256), 512), (unsigned)pp.size());
+        {
+            ProfRange pr("pair_terms_kernel", st, 0.0, 40.0 * nterms);
+            if (P.is_complex)
+                pair_terms_kernel<cd><<<g1, 256, 0, st>>>(bparts.as<PairPart>(), (int)pp.size(), A.mat.as<cd>(),
+                                                          B.mat.as<cd>(), P.d_E, P.d_w, coef_tol, pole_res, mode,
+                                                          bR.as<cd>(), bP.as<double>(), d_zero);
+            else
+                pair_terms_kernel<double><<<g1, 256, 0, st>>>(bparts.as<PairPart>(), (int)pp.size(),
+                                                              A.mat.as<double>(), B.mat.as<double>(), P.d_E, P.d_w,
+                                                              coef_tol, pole_res, mode, bR.as<cd>(), bP.as<double>(),
+                                                              d_zero);
+            check_launch("pair_terms_kernel");
+        }
+        if (nz > 0) {
+            dim3 g2((unsigned)chunks.size(), ceil_div(nz, EVAL_THREADS));
+            ProfRange pr("pair_eval_models_kernel", st, 12.0 * (double)nterms * nz, 24.0 * nterms);
+            pair_eval_models_kernel<<<g2, EVAL_THREADS, 0, st>>>(bR.as<cd>(), bP.as<double>(), bch.as<EvalChunk>(),
+                                                                 bz.as<cd>(), nz, sign, d_out);
+            check_launch("pair_eval_models_kernel");
+        }
+    }
+    std::vector<cd> h(nzt + nm);
+    PGX_CUDA(cudaMemcpyAsync(h.data(), bout.p, (nzt + nm) * sizeof(cd), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaStreamSynchronize(st));
+    for (int m = 0; m < nm; ++m) {
+        const cd zero = h[nzt + m];
+        for (int k = 0; k < nz; ++k) {
+            const long o = (long)m * nz + k;
+            cd v = h[o];
+            if (mode == 1) {
+                const double az = std::sqrt(z[2 * o] * z[2 * o] + z[2 * o + 1] * z[2 * o + 1]);
+                if (az <= DBL_EPSILON) v = v + zero * P.model_beta[m];
+            }
+            out[2 * o] = v.x;
+            out[2 * o + 1] = v.y;
+        }
+        if (zero_out) {
+            zero_out[2 * m] = zero.x;
+            zero_out[2 * m + 1] = zero.y;
+        }
+    }
+}
+
+void run_gf_models(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,
+                   const double* z, double coef_tol, double* out) {
+    run_pair_models(c, op1, op2, nparts, outer, inner, nz, z, 0.0, coef_tol, 0, 1.0, out, nullptr);
+}
+
+void run_susc_models(pgx_ctx* c, int opA, int opB, int nparts, const int32_t* outer, const int32_t* inner, int nz,
+                     const double* z, double pole_res, double coef_tol, double* out, double* zero_pole) {
+    run_pair_models(c, opA, opB, nparts, outer, inner, nz, z, pole_res, coef_tol, 1, -1.0, out, zero_pole);
 }
 
 void run_gf(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,

@@ -24,7 +24,7 @@ EXPORTS = [
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
-    "pgx_gf_vjp", "pgx_chi3",
+    "pgx_gf_vjp", "pgx_chi3", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
 ]
 
 
@@ -83,6 +83,10 @@ def load():
         lib.pgx_op_release.argtypes = [P, I32]
         lib.pgx_gf_vjp.argtypes = [P, I32, I32, I32, P, P, I32, P, P, P, P]
         lib.pgx_chi3.argtypes = [P, I32, I32, P, I32, P, D, P]
+        lib.pgx_set_models.argtypes = [P, I32, P, P]
+        lib.pgx_weights_models.argtypes = [P, P, P, P]
+        lib.pgx_gf_models.argtypes = [P, I32, I32, I32, P, P, I32, P, D, P]
+        lib.pgx_susc_models.argtypes = [P, I32, I32, I32, P, P, I32, P, D, D, P, P]
         _lib = lib
     return _lib
 
@@ -368,6 +372,53 @@ def _chi3(self, channel, parts, freqs, pole_res=1e-8):
     return out
 
 
+def _set_models(self, first_block, beta):
+    """Independent models in this context: blocks first_block[m] ..
+    first_block[m+1]-1 form model m at inverse temperature beta[m]."""
+    f = np.ascontiguousarray(first_block, dtype=np.int32)
+    b = np.ascontiguousarray(beta, dtype=np.float64)
+    self._ck(self.lib.pgx_set_models(self.h, len(b), _p(f), _p(b)))
+    self.nmodels = len(b)
+
+
+def _weights_models(self):
+    """Per-model weights: (w per block as in weights(), E0[m], Z[m])."""
+    w = np.empty(int(self.eoff[-1]))
+    e0 = np.empty(self.nmodels)
+    z = np.empty(self.nmodels)
+    self._ck(self.lib.pgx_weights_models(self.h, _p(w), _p(e0), _p(z)))
+    return [w[self.eoff[b]:self.eoff[b + 1]] for b in range(len(self.dims))], e0, z
+
+
+def _pair_models(self, fn, op1, op2, outer, inner, z, *tol):
+    z = np.ascontiguousarray(np.asarray(z, dtype=complex))
+    if z.ndim != 2 or z.shape[0] != self.nmodels:
+        raise ValueError("z must be nmodels x nz")
+    o = np.ascontiguousarray(outer, dtype=np.int32)
+    i = np.ascontiguousarray(inner, dtype=np.int32)
+    out = np.zeros(z.shape, dtype=complex)
+    return o, i, z, out
+
+
+def _gf_models(self, op1, op2, outer, inner, z, coef_tol=1e-8):
+    """G of every model at its own frequencies (z: nmodels x nz)."""
+    o, i, z, out = _pair_models(self, None, op1, op2, outer, inner, z)
+    self._ck(self.lib.pgx_gf_models(self.h, int(op1), int(op2), len(o), _p(o), _p(i), z.shape[1],
+                                    _p(z.view(np.float64)), float(coef_tol), _p(out.view(np.float64))))
+    return out
+
+
+def _susc_models(self, opA, opB, outer, inner, z, pole_res=1e-8, coef_tol=1e-8):
+    """chi of every model at its own frequencies (z: nmodels x nz); also the
+    zero-pole sum of each model."""
+    o, i, z, out = _pair_models(self, None, opA, opB, outer, inner, z)
+    zero = np.zeros(self.nmodels, dtype=complex)
+    self._ck(self.lib.pgx_susc_models(self.h, int(opA), int(opB), len(o), _p(o), _p(i), z.shape[1],
+                                      _p(z.view(np.float64)), float(pole_res), float(coef_tol),
+                                      _p(out.view(np.float64)), _p(zero.view(np.float64))))
+    return out, zero
+
+
 def _op_release(self, op_id):
     """Give an operator's device memory back to the context for reuse."""
     self._ck(self.lib.pgx_op_release(self.h, int(op_id)))
@@ -376,6 +427,10 @@ def _op_release(self, op_id):
 Engine.op_release = _op_release
 Engine.gf_vjp = _gf_vjp
 Engine.chi3 = _chi3
+Engine.set_models = _set_models
+Engine.weights_models = _weights_models
+Engine.gf_models = _gf_models
+Engine.susc_models = _susc_models
 Engine.assemble_hamiltonian = _assemble_hamiltonian
 Engine.get_hamiltonian = _get_hamiltonian
 Engine.timer_begin = _timer_begin

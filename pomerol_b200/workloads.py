@@ -7,6 +7,13 @@
              rng = numpy.random.default_rng(0), eps = rng.uniform(-2,2,5) then
              V = rng.uniform(0.2,0.8,5); beta=20, dim 4096
   ring8      8-site Hubbard ring, PBC, t=1, U=4, mu=2, beta=5, dim 65536
+  b64        64 independent Anderson impurities with 3-6 bath sites (dims
+             256-16384): rng = numpy.random.default_rng(1), per model in
+             order nb = rng.integers(3, 7), U = rng.uniform(1, 6),
+             beta = rng.uniform(5, 50), eps = rng.uniform(-2, 2, nb),
+             V = rng.uniform(0.1, 1.0, nb), eps_d = -U/2; G_dn on n = 0..1023
+             and chi_dd (n_d = n_up + n_dn) on m = 0..31, each model at its
+             own beta, all models in one context (BatchRun)
 
 The G2 component is chi_(u0,d0,u0,d0) (c_up c_down c^+_up c^+_down at the
 first site) on the fermionic cube n_k in [-N/2, N/2).  No public dataset is
@@ -147,6 +154,101 @@ def matsubara_square(beta, n):
     k = np.arange(-n // 2, n // 2)
     idx = np.array([(a, b) for a in k for b in k])
     return idx, 1j * np.pi * (2 * idx + 1) / beta
+
+
+def b64_params(seed=1, nmodels=64):
+    """(U, eps_d, eps, V, beta) of each model of the batch workload."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(nmodels):
+        nb = int(rng.integers(3, 7))
+        U = rng.uniform(1, 6)
+        beta = rng.uniform(5, 50)
+        eps = rng.uniform(-2, 2, nb)
+        V = rng.uniform(0.1, 1.0, nb)
+        out.append((U, -U / 2, eps, V, beta))
+    return out
+
+
+def model_inputs(U, eps_d, eps, V, device=0):
+    """One impurity model through the drop-in API: block sizes, block
+    Hamiltonians, and the Fock actions of c^+_dn and n_d = n_up + n_dn
+    (right block, left block, targets, coefficients) per part."""
+    HExpr, imp = anderson_expr(U, eps_d, eps, V)
+    ii = P.MakeIndexClassification(HExpr)
+    hs = P.MakeHilbertSpace(ii, HExpr)
+    hs.compute()
+    S = P.StatesClassification()
+    S.compute(hs)
+    H = P.Hamiltonian(S, device)
+    H.prepare(HExpr, hs)
+    dims = [S.getBlockSize(b) for b in range(S.getNumberOfBlocks())]
+    blocks = [np.array(H.getPart(b).getMatrix()) for b in range(len(dims))]
+    up, dn = ii.getIndex(imp, 0, P.up), ii.getIndex(imp, 0, P.down)
+    cdag = P.CreationOperator(ii, hs, S, H, dn)
+    cdag.prepare(hs)
+    nd = {}
+    for i in (up, dn):
+        n = P.QuadraticOperator(ii, hs, S, H, i, i)
+        n.prepare(hs)
+        for r, l, t, c in n.fockAction():
+            t, c = np.asarray(t), np.asarray(c, dtype=float)
+            acc = nd.setdefault(r, np.zeros(dims[r]))
+            acc += np.where(t >= 0, c, 0.0)
+    ndact = [(b, b, np.where(nd[b] != 0.0, np.arange(dims[b]), -1), nd[b]) for b in sorted(nd)]
+    return dims, blocks, [(r, l, np.asarray(t), np.asarray(c)) for r, l, t, c in cdag.fockAction()], ndact
+
+
+class BatchRun:
+    """The batch workload on one libpgx context: the blocks of every model
+    diagonalised by one eigensolve, per-model weights, one rotation of c^+_dn
+    and of n_d over all models, then G_dn (nG fermionic frequencies) and
+    chi_dd (nchi bosonic frequencies) of every model at its own beta."""
+
+    def __init__(self, params, nG=1024, nchi=32, device=0):
+        from .pgx import Engine
+        self.params = params
+        dims, blocks, cd_parts, nd_parts, first = [], [], [], [], [0]
+        for U, epsd, eps, V, beta in params:
+            d, bl, ca, na = model_inputs(U, epsd, eps, V, device)
+            off = len(dims)
+            dims += d
+            blocks += bl
+            cd_parts += [(r + off, l + off, t, c) for r, l, t, c in ca]
+            nd_parts += [(r + off, l + off, t, c) for r, l, t, c in na]
+            first.append(len(dims))
+        self.dims, self.first = dims, first
+        self.beta = np.array([p[4] for p in params])
+        self.eng = Engine(device)
+        self.eng.set_blocks(dims)
+        self.eng.set_hamiltonian(blocks)
+        self.eng.set_models(first, self.beta)
+        self.h2d_bytes = sum(b.nbytes for b in blocks)
+        self.cdag = self.eng.op_define(cd_parts)
+        self.nd = self.eng.op_define(nd_parts)
+        # G: outer = right block of c^+, inner = its left block; chi: diagonal blocks
+        self.g_outer = np.array([r for r, l, _, _ in cd_parts], dtype=np.int32)
+        self.g_inner = np.array([l for r, l, _, _ in cd_parts], dtype=np.int32)
+        self.x_blocks = np.array([r for r, _, _, _ in nd_parts], dtype=np.int32)
+        n = np.arange(nG)
+        self.zG = 1j * np.pi * (2 * n[None, :] + 1) / self.beta[:, None]
+        m = np.arange(nchi)
+        self.zX = 1j * 2 * np.pi * m[None, :] / self.beta[:, None]
+        self.nterms_G = int(sum(dims[o] * dims[i] for o, i in zip(self.g_outer, self.g_inner)))
+        self.nterms_X = int(sum(dims[b] ** 2 for b in self.x_blocks))
+
+    def step(self):
+        e = self.eng
+        e.eigh()
+        e.weights_models()
+        e.op_rotate(self.cdag)
+        e.op_rotate(self.nd)
+        if getattr(self, "_c", None) is not None:
+            e.op_release(self._c)
+        self._c = e.op_adjoint(self.cdag)
+        G = e.gf_models(self._c, self.cdag, self.g_outer, self.g_inner, self.zG, coef_tol=0.0)
+        X, _ = e.susc_models(self.nd, self.nd, self.x_blocks, self.x_blocks, self.zX, coef_tol=0.0)
+        return G, X
 
 
 class Chi3Run:
