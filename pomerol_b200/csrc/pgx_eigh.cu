@@ -1017,20 +1017,32 @@ static void launch_big(const EighDev& d, const std::vector<int>& dims, const std
             a.fin = (j > k) ? j - 1 : -1;
             a.col = j;
             a.nact = nact(j > k ? j - 1 : j);
-            bhh_col_kernel<<<(unsigned)a.nact, BHH_COL_THREADS, 0, st>>>(a);
-            check_launch("bhh_col_kernel");
+            {
+                ProfRange r1("bhh_col_kernel", st, 0.0, 0.0);
+                bhh_col_kernel<<<(unsigned)a.nact, BHH_COL_THREADS, 0, st>>>(a);
+                check_launch("bhh_col_kernel");
+            }
             a.fin = -1;
             a.nact = nact(j);
             long ctas = 0;
-            for (int i = 0; i < a.nact; ++i) ctas += (dims[big[i]] - j - 1 + BHH_SYMV_ROWS - 1) / BHH_SYMV_ROWS;
+            double bytes = 0.0;
+            for (int i = 0; i < a.nact; ++i) {
+                const long m = dims[big[i]] - j - 1;
+                ctas += (m + BHH_SYMV_ROWS - 1) / BHH_SYMV_ROWS;
+                bytes += 8.0 * m * m;
+            }
+            ProfRange r2("bhh_symv_kernel", st, 0.0, bytes);
             bhh_symv_kernel<<<(unsigned)ctas, BHH_SYMV_THREADS, sizeof(double) * nmax, st>>>(a);
             check_launch("bhh_symv_kernel");
         }
         a.fin = jend - 1;
         a.col = -1;
         a.nact = nact(jend - 1);
-        bhh_col_kernel<<<(unsigned)a.nact, BHH_COL_THREADS, 0, st>>>(a);
-        check_launch("bhh_col_kernel");
+        {
+            ProfRange r1("bhh_col_kernel", st, 0.0, 0.0);
+            bhh_col_kernel<<<(unsigned)a.nact, BHH_COL_THREADS, 0, st>>>(a);
+            check_launch("bhh_col_kernel");
+        }
         // A(k+p:, k+p:) -= V W^T + W V^T, p = the block's columns in this panel
         probs.clear();
         for (int i = 0; i < nact(k); ++i) {

@@ -145,20 +145,21 @@ __global__ void pair_terms_kernel(const PairPart* parts, int nparts, const T* m1
     }
 }
 
-// out[z] += sign * sum_t R_t / (z - P_t).  CTA = (z tile of blockDim, term chunk).
+// out[z] += sign * sum_t R_t / (z - P_t).  CTA = (term chunk, z tile of
+// blockDim): the chunks run along x, whose grid limit holds every term list.
 constexpr int EVAL_THREADS = 128, EVAL_CHUNK = 1024;
 __global__ void __launch_bounds__(EVAL_THREADS) pair_eval_kernel(const cd* R, const double* P, long nterms,
                                                                   const cd* z, int nz, double sign, cd* out) {
     __shared__ cd sR[EVAL_CHUNK];
     __shared__ double sP[EVAL_CHUNK];
-    const long t0 = (long)blockIdx.y * EVAL_CHUNK;
+    const long t0 = (long)blockIdx.x * EVAL_CHUNK;
     const int cnt = (int)min((long)EVAL_CHUNK, nterms - t0);
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
         sR[i] = R[t0 + i];
         sP[i] = P[t0 + i];
     }
     __syncthreads();
-    const int iz = blockIdx.x * blockDim.x + threadIdx.x;
+    const int iz = blockIdx.y * blockDim.x + threadIdx.x;
     if (iz >= nz) return;
     const cd zz = z[iz];
     double ax = 0.0, ay = 0.0;
@@ -467,8 +468,8 @@ static void run_pair(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* ou
                                                           bR.as<cd>(), bP.as<double>(), d_zero);
         check_launch("pair_terms_kernel");
         if (nz > 0) {
-            dim3 g2(ceil_div(nz, EVAL_THREADS), ceil_div(nterms, EVAL_CHUNK));
-            PGX_CHECK(g2.y < 65536u, PGX_ERR_ARG, "too many Lehmann terms for one call");
+            PGX_CHECK(ceil_div(nz, EVAL_THREADS) < 65536, PGX_ERR_ARG, "too many frequencies for one call");
+            dim3 g2((unsigned)((nterms + EVAL_CHUNK - 1) / EVAL_CHUNK), ceil_div(nz, EVAL_THREADS));
             pair_eval_kernel<<<g2, EVAL_THREADS, 0, st>>>(bR.as<cd>(), bP.as<double>(), nterms, bz.as<cd>(), nz, sign,
                                                           d_out);
             check_launch("pair_eval_kernel");

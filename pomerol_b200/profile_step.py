@@ -2,9 +2,13 @@
 ncu captures and stage timing): eigensolve, weights, rotation, G2; with
 --chi3 N the three-point susceptibility chi3_PH(u0, u0, d0, d0) on the
 N x N fermionic square instead of G2; with --batch M the first M models of
-the batch workload (G on 1024 and chi_dd on 32 frequencies per model).
+the batch workload (G on 1024 and chi_dd on 32 frequencies per model); with
+--chain the drop-in chain of a workload stage by stage (Hamiltonian,
+DensityMatrix, field operators, G_u0 on 256 fermionic and chi_zz on 48 bosonic
+frequencies, then G2 on the N x N x N cubes given by --g2-cubes).
 
     python -m pomerol_b200.profile_step [--config a5] [--steps 2] [--chi3 32] [--batch 64]
+    python -m pomerol_b200.profile_step --config ring8 --chain --g2-cubes 2 4
 """
 import argparse
 import time
@@ -19,7 +23,12 @@ def main():
     ap.add_argument("--kernels", action="store_true", help="per-kernel event times of the last step")
     ap.add_argument("--chi3", type=int, default=0, help="chi3 on an N x N square instead of G2")
     ap.add_argument("--batch", type=int, default=0, help="the first M models of the batch workload")
+    ap.add_argument("--chain", action="store_true", help="time the drop-in chain stage by stage")
+    ap.add_argument("--g2-cubes", type=int, nargs="*", default=[], help="cube sides for the G2 stage of --chain")
     a = ap.parse_args()
+    if a.chain:
+        chain(a.config, a.g2_cubes)
+        return
     import torch  # noqa: F401  (CUDA context for the process)
     from .workloads import BatchRun, Chi3Run, EngineRun, Problem, b64_params, matsubara_cube, matsubara_square
     if a.batch:
@@ -61,6 +70,61 @@ def main():
         extra = "" if a.chi3 else f"g2 {run.eng.g2_timing()}, "
         print(f"step {s}: device {ms:.1f} ms, wall {1e3 * (time.perf_counter() - t0):.1f} ms, "
               f"{extra}|v|max {np.abs(v).max():.4e}", flush=True)
+
+
+def chain(config, cubes):
+    import torch  # noqa: F401  (CUDA context for the process)
+    from . import _pomerol as P
+    from .workloads import EngineRun, Problem, matsubara_cube
+    prob = Problem(config)
+    t = time.perf_counter()
+    H = P.Hamiltonian(prob.S)
+    H.prepare(prob.HExpr, prob.hs)
+    H.compute()
+    t1 = time.perf_counter()
+    print(f"Hamiltonian prepare + compute: {t1 - t:.2f} s ({len(prob.dims)} blocks, largest {max(prob.dims)})")
+    rho = P.DensityMatrix(prob.S, H, prob.beta)
+    rho.prepare()
+    rho.compute()
+    if prob.dm_trunc:
+        rho.truncateBlocks(prob.dm_trunc)
+    ops = P.FieldOperatorContainer(prob.ii, prob.hs, prob.S, H, {prob.u0, prob.d0})
+    ops.prepareAll(prob.hs)
+    ops.computeAll()
+    t2 = time.perf_counter()
+    print(f"DensityMatrix + rotation of c+, c (u0, d0): {t2 - t1:.3f} s")
+    G = P.GreensFunction(prob.S, H, ops.getAnnihilationOperator(prob.u0), ops.getCreationOperator(prob.u0), rho)
+    G.prepare()
+    G.compute()
+    g = G.values([1j * np.pi * (2 * n + 1) / prob.beta for n in range(256)])
+    t3 = time.perf_counter()
+    print(f"G_u0 on 256 fermionic frequencies: {t3 - t2:.3f} s, G(0) = {g[0]:.10e}")
+    chi = {}
+    for x in (prob.u0, prob.d0):
+        for y in (prob.u0, prob.d0):
+            nx = P.QuadraticOperator(prob.ii, prob.hs, prob.S, H, x, x)
+            ny = P.QuadraticOperator(prob.ii, prob.hs, prob.S, H, y, y)
+            for n in (nx, ny):
+                n.prepare(prob.hs)
+                n.compute()
+            c = P.Susceptibility(prob.S, H, nx, ny, rho)
+            c.prepare()
+            c.compute()
+            chi[(x, y)] = np.array(c.values([2j * np.pi * m / prob.beta for m in range(48)]))
+    u, d = prob.u0, prob.d0
+    zz = 0.25 * (chi[(u, u)] - chi[(u, d)] - chi[(d, u)] + chi[(d, d)])
+    t4 = time.perf_counter()
+    print(f"chi_zz on 48 bosonic frequencies (4 pair susceptibilities): {t4 - t3:.3f} s, chi_zz(0) = {zz[0]:.10e}")
+    if cubes:
+        run = EngineRun(prob)
+        for n in cubes:
+            _, z = matsubara_cube(prob.beta, n)
+            run.eng.timer_begin()
+            t = time.perf_counter()
+            run.step(z)
+            ms = run.eng.timer_end()
+            print(f"G2 step (eigensolve + weights + rotation + G2) on {len(z)} triples: device {ms:.0f} ms, "
+                  f"wall {time.perf_counter() - t:.1f} s", flush=True)
 
 
 if __name__ == "__main__":
