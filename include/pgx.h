@@ -107,6 +107,14 @@ int pgx_eigh(pgx_ctx* ctx);
  * Either pointer may be NULL. */
 int pgx_get_eigensystem(pgx_ctx* ctx, double* E, double* U);
 
+/* Load an eigensystem saved from pgx_get_eigensystem (same layout: E sum of
+ * dims, ascending inside every block; U packed like H, complex interleaved
+ * for complex blocks) in place of pgx_eigh, so a restart skips the
+ * eigensolve (checkpoint / reload of the eigendata; the reference recomputes
+ * Hamiltonian::compute, Hamiltonian.cpp:69-113, every time).  Call after
+ * pgx_set_blocks with the same blocks; operators must be rotated again. */
+int pgx_set_eigensystem(pgx_ctx* ctx, const double* E, const double* U);
+
 /* Ground energy min_b min E (Hamiltonian::computeGroundEnergy,
  * Hamiltonian.cpp:125-130). */
 int pgx_ground_energy(pgx_ctx* ctx, double* E0);

@@ -429,6 +429,27 @@ int pgx_get_eigensystem(pgx_ctx* c, double* E, double* U) {
     });
 }
 
+int pgx_set_eigensystem(pgx_ctx* c, const double* E, const double* U) {
+    return guarded(c, [&] {
+        pgx::Problem& P = c->P;
+        PGX_CHECK(P.nblocks > 0, PGX_ERR_STATE, "pgx_set_blocks first");
+        PGX_CHECK(E && U, PGX_ERR_ARG, "null eigensystem");
+        const size_t sc = P.is_complex ? 2 : 1;
+        for (long i = 0; i < P.esize; ++i) PGX_CHECK(std::isfinite(E[i]), PGX_ERR_NUMERIC, "non-finite eigenvalue");
+        for (long b = 0; b < P.nblocks; ++b)
+            for (long i = P.eoff[b] + 1; i < P.eoff[b] + P.dims[b]; ++i)
+                PGX_CHECK(E[i - 1] <= E[i], PGX_ERR_ARG, "eigenvalues must ascend inside every block");
+        for (long i = 0; i < P.msize * (long)sc; ++i)
+            PGX_CHECK(std::isfinite(U[i]), PGX_ERR_NUMERIC, "non-finite eigenvector entry");
+        PGX_CUDA(cudaMemcpyAsync(P.d_E, E, P.esize * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        PGX_CUDA(cudaMemcpyAsync(P.d_U, U, P.msize * sc * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+        P.have_eig = true;
+        P.have_w = false;
+        for (auto& op : P.ops) op.rotated = false;
+    });
+}
+
 int pgx_ground_energy(pgx_ctx* c, double* E0) {
     return guarded(c, [&] {
         pgx::Problem& P = c->P;

@@ -4,6 +4,8 @@
 #include <pybind11/complex.h>
 #include <pybind11/numpy.h>
 #include <pybind11/operators.h>
+#include <cmath>
+
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
@@ -131,8 +133,9 @@ PYBIND11_MODULE(_pomerol, m) {
         .def("getEigenValue", &HamiltonianPart::getEigenValue)
         .def("getMinimumEigenvalue", &HamiltonianPart::getMinimumEigenvalue)
         .def("getMatrix", [](HamiltonianPart const& p) {
-            long d = (long)p.getSize();
-            return as_matrix(p.getMatrix(), d, d, p.isComplex());
+            auto m = p.getMatrix();  // the block, or its reduced corner after Hamiltonian::reduce
+            const long d = std::lround(std::sqrt((double)(m.size() / (p.isComplex() ? 2 : 1))));
+            return as_matrix(m, d, d, p.isComplex());
         });
 
     py::class_<Hamiltonian>(m, "Hamiltonian")
@@ -142,6 +145,7 @@ PYBIND11_MODULE(_pomerol, m) {
         .def("prepare", [](Hamiltonian& H, ComplexExpr const& e, HilbertSpace const& hs, int) { H.prepare(e, hs); },
              py::arg("HExpr"), py::arg("HS"), py::arg("comm") = 0)
         .def("compute", [](Hamiltonian& H, int) { H.compute(); }, py::arg("comm") = 0)
+        .def("reduce", &Hamiltonian::reduce, py::arg("Cutoff"))
         .def("getPart", &Hamiltonian::getPart, py::return_value_policy::reference_internal)
         .def("getGroundEnergy", &Hamiltonian::getGroundEnergy)
         .def("getEigenValues", py::overload_cast<>(&Hamiltonian::getEigenValues, py::const_))

@@ -143,6 +143,13 @@ public:
         prepareImpl(HS, comm);
     }
     void compute(MPI_Comm const& comm = MPI_COMM_WORLD);
+    // Hamiltonian::reduce / HamiltonianPart::reduce (Hamiltonian.cpp:115-119,
+    // HamiltonianPart.cpp:151-172): every block keeps its eigenvalues up to
+    // GroundEnergy + Cutoff and the top-left corner of that size of its
+    // eigenvector matrix (a block with none left is kept whole).  The
+    // accessors show the reduced blocks; quantities computed on the device
+    // afterwards still use the full blocks.
+    void reduce(RealType Cutoff);
 
     HamiltonianPart const& getPart(BlockNumber in) const;
     RealType getEigenValue(QuantumState state) const;
@@ -167,6 +174,7 @@ private:
     mutable std::vector<RealType> HPacked;
     std::vector<long> MOff;
     std::vector<std::vector<RealType>> Eigenvalues;
+    std::vector<long> Reduced;  // per block: kept eigenvalues after reduce(), 0 if not reduced
     mutable std::vector<RealType> UPacked;
     std::vector<HamiltonianPart> parts;
     RealType GroundEnergy = 0;

@@ -8,6 +8,7 @@
 // from the terms' Fock action.  Eigensolve, weights and operator rotation run
 // on the GPU through libpgx.
 #include <algorithm>
+#include <cmath>
 #include <numeric>
 #include <unordered_map>
 
@@ -281,8 +282,23 @@ void Hamiltonian::compute(MPI_Comm const&) {
         GroundEnergy = std::min(GroundEnergy, *std::min_element(Eigenvalues[b].begin(), Eigenvalues[b].end()));
     }
     UPacked.clear();
+    Reduced.assign(nb, 0);
     Dev->weights_beta = -1.0;
     setStatus(Computed);
+}
+
+void Hamiltonian::reduce(RealType Cutoff) {
+    if (getStatus() < Computed) throw StatusMismatch("Hamiltonian is not computed yet.");
+    const RealType level = GroundEnergy + Cutoff;
+    for (BlockNumber b = 0; b < (BlockNumber)Eigenvalues.size(); ++b) {
+        auto& e = Eigenvalues[b];
+        long counter = 0;
+        while (counter < (long)e.size() && e[counter] <= level) ++counter;  // ascending
+        if (counter > 0) {
+            e.resize(counter);
+            Reduced[b] = counter;
+        }
+    }
 }
 
 std::vector<RealType> const& Hamiltonian::eigenvectors() const {
@@ -324,12 +340,22 @@ RealType HamiltonianPart::getMinimumEigenvalue() const {
 std::vector<RealType> HamiltonianPart::getMatrix() const {
     const int sc = H->Complex ? 2 : 1;
     auto const& src = (H->getStatus() >= ComputableObject::Computed) ? H->eigenvectors() : H->hostBlocks();
-    return std::vector<RealType>(src.begin() + H->MOff[Block] * sc, src.begin() + H->MOff[Block + 1] * sc);
+    const long r = (H->getStatus() >= ComputableObject::Computed && Block < (BlockNumber)H->Reduced.size())
+                       ? H->Reduced[Block]
+                       : 0;
+    if (r == 0)
+        return std::vector<RealType>(src.begin() + H->MOff[Block] * sc, src.begin() + H->MOff[Block + 1] * sc);
+    // the reduced block: the top-left r x r corner of the eigenvector matrix
+    const long d = (long)getSize();
+    std::vector<RealType> m(r * r * sc);
+    for (long i = 0; i < r; ++i)
+        for (long j = 0; j < r * sc; ++j) m[i * r * sc + j] = src[(H->MOff[Block] + i * d) * sc + j];
+    return m;
 }
 std::vector<RealType> HamiltonianPart::getEigenState(InnerQuantumState state) const {
-    const long d = (long)getSize();
     const int sc = H->Complex ? 2 : 1;
     auto m = getMatrix();
+    const long d = std::lround(std::sqrt((double)(m.size() / sc)));  // the block, or its reduced corner
     std::vector<RealType> v(d * sc);
     for (long i = 0; i < d; ++i)
         for (int c = 0; c < sc; ++c) v[i * sc + c] = m[(i * d + (long)state) * sc + c];

@@ -24,7 +24,7 @@ EXPORTS = [
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
-    "pgx_gf_vjp", "pgx_chi3", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
+    "pgx_gf_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
 ]
 
 
@@ -83,6 +83,7 @@ def load():
         lib.pgx_op_release.argtypes = [P, I32]
         lib.pgx_gf_vjp.argtypes = [P, I32, I32, I32, P, P, I32, P, P, P, P]
         lib.pgx_chi3.argtypes = [P, I32, I32, P, I32, P, D, P]
+        lib.pgx_set_eigensystem.argtypes = [P, P, P]
         lib.pgx_set_models.argtypes = [P, I32, P, P]
         lib.pgx_weights_models.argtypes = [P, P, P, P]
         lib.pgx_gf_models.argtypes = [P, I32, I32, I32, P, P, I32, P, D, P]
@@ -372,6 +373,39 @@ def _chi3(self, channel, parts, freqs, pole_res=1e-8):
     return out
 
 
+def _set_eigensystem(self, E, U):
+    """Load an eigensystem (lists per block, as eigensystem() returns) in
+    place of eigh()."""
+    e = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=np.float64) for x in E]))
+    dt = complex if self.is_complex else np.float64
+    u = np.ascontiguousarray(np.concatenate([np.asarray(x, dtype=dt).ravel() for x in U]))
+    if len(e) != int(sum(self.dims)) or len(u) != int(sum(d * d for d in self.dims)):
+        raise ValueError("eigensystem does not match the blocks")
+    self._ck(self.lib.pgx_set_eigensystem(self.h, _p(e), _p(u.view(np.float64))))
+
+
+def _save_eigensystem(self, path):
+    """Checkpoint the eigensystem and the block sizes to an .npz file."""
+    E, U = self.eigensystem()
+    np.savez(path, dims=np.asarray(self.dims), is_complex=self.is_complex, E=np.concatenate(E),
+             U=np.concatenate([np.asarray(x).ravel() for x in U]))
+
+
+def _load_eigensystem(self, path):
+    """Reload an eigensystem saved by save_eigensystem into a context whose
+    blocks are the same."""
+    f = np.load(path)
+    if list(f["dims"]) != list(self.dims) or bool(f["is_complex"]) != bool(self.is_complex):
+        raise ValueError("the checkpoint's blocks differ from this context's")
+    E, U, oe, ou = [], [], 0, 0
+    for d in self.dims:
+        E.append(f["E"][oe:oe + d])
+        U.append(f["U"][ou:ou + d * d].reshape(d, d))
+        oe += d
+        ou += d * d
+    self.set_eigensystem(E, U)
+
+
 def _set_models(self, first_block, beta):
     """Independent models in this context: blocks first_block[m] ..
     first_block[m+1]-1 form model m at inverse temperature beta[m]."""
@@ -428,6 +462,9 @@ Engine.op_release = _op_release
 Engine.gf_vjp = _gf_vjp
 Engine.chi3 = _chi3
 Engine.set_models = _set_models
+Engine.set_eigensystem = _set_eigensystem
+Engine.save_eigensystem = _save_eigensystem
+Engine.load_eigensystem = _load_eigensystem
 Engine.weights_models = _weights_models
 Engine.gf_models = _gf_models
 Engine.susc_models = _susc_models

@@ -847,3 +847,34 @@ def test_batch_of_models_against_oracle():
             nd[R] = (Lb, sum(mats))
         xref = L.susc_eval(L.susc_terms(ed, nd, nd, rule=False), run.zX[m], beta)
         assert np.abs(X[m] - xref).max() <= 1e-10 * np.abs(xref).max(), m
+
+
+def test_eigensystem_checkpoint_reload(harness, tmp_path):
+    """Eigendata checkpoint: the eigensystem saved from one context and
+    loaded into a fresh one (pgx_set_eigensystem, no eigensolve) gives the
+    same G as the solved context; a checkpoint of other blocks is refused."""
+    from pomerol_b200.pgx import Engine, PgxError
+    m = M.make_model(plaquette_expr())
+    g = harness(m, 10.0)
+    ix = m.info.getIndex("A", 0, M.DOWN)
+    z = L.fermionic(np.arange(32), 10.0)
+    ref = g.gf(g.c(ix), g.cdag(ix), z)
+    path = str(tmp_path / "eig.npz")
+    g.eng.save_eigensystem(path)
+    from tests.pgx_harness import GpuED
+    h = GpuED.__new__(GpuED)
+    h.m, h.beta, h.eng = m, 10.0, Engine()
+    h.eng.set_blocks(m.block_sizes(), m.complex)
+    h.eng.load_eigensystem(path)
+    h.E, h.U = h.eng.eigensystem()
+    h.w, h.Z = h.eng.weights(10.0)
+    h.retained = np.ones(len(m.blocks), dtype=bool)
+    h._cdag, h._c = {}, {}
+    v = h.gf(h.c(ix), h.cdag(ix), z)
+    assert np.abs(v - ref).max() < 1e-15
+    other = Engine()
+    other.set_blocks([3, 5])
+    with pytest.raises(ValueError):
+        other.load_eigensystem(path)
+    with pytest.raises(PgxError):
+        other.set_eigensystem([np.array([2.0, 1.0, 0.0]), np.zeros(5)], [np.eye(3), np.eye(5)])

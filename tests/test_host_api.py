@@ -480,3 +480,29 @@ def test_chi3_3site_reference_case(P, channel):
     assert all(cont.isInContainer(*g) for g in group)
     assert np.abs(np.array(res[group[0]]) - ref).max() < k["tol"]
     assert all(len(res[g]) == 0 for g in group[1:])
+
+
+@pytest.mark.gpu
+def test_hamiltonian_reduce(P):
+    """Hamiltonian::reduce (Hamiltonian.cpp:115-119, HamiltonianPart.cpp:151-172):
+    every block keeps its eigenvalues up to E0 + Cutoff and the top-left
+    corner of its eigenvector matrix of that size; a block left with none
+    stays whole."""
+    L = P.LatticePresets
+    ii, hs, S, H, rho, ops = _setup(P, plaquette(P, L), 10.0)
+    nb = S.getNumberOfBlocks()
+    full_e = [list(H.getPart(b).getEigenValues()) for b in range(nb)]
+    full_u = [np.array(H.getPart(b).getMatrix()) for b in range(nb)]
+    E0, cut = H.getGroundEnergy(), 1.5
+    H.reduce(cut)
+    for b in range(nb):
+        d = S.getBlockSize(b)
+        keep = sum(1 for e in full_e[b] if e <= E0 + cut)
+        e = list(H.getPart(b).getEigenValues())
+        u = np.array(H.getPart(b).getMatrix())
+        if keep == 0:
+            assert e == full_e[b] and np.array_equal(u, full_u[b])
+        else:
+            assert e == full_e[b][:keep]
+            assert np.array_equal(u.reshape(keep, keep), full_u[b].reshape(d, d)[:keep, :keep])
+    assert any(len(H.getPart(b).getEigenValues()) < S.getBlockSize(b) for b in range(nb))
