@@ -236,7 +236,7 @@ int pgx_destroy(pgx_ctx* c) {
     for (auto& b : c->scratch) b.release();
     if (c->ev_begin) cudaEventDestroy(c->ev_begin);
     if (c->ev_end) cudaEventDestroy(c->ev_end);
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < 4; ++i) {
         if (c->aux[i]) cudaStreamDestroy(c->aux[i]);
         if (c->join[i]) cudaEventDestroy(c->join[i]);
     }

@@ -882,14 +882,18 @@ static void tri_plan(const std::vector<int>& dims, std::vector<TriItem>& items, 
             items.push_back(TriItem{b, j0, std::min(dims[b], j0 + BIS_WARPS), 0, 0});
 }
 
-constexpr int CL_SIZES[4] = {1, 2, 4, 8};
+constexpr int CL_NCLS = 5;
+constexpr int CL_SIZES[CL_NCLS] = {1, 2, 4, 8, 16};
 constexpr size_t CL_SMEM_MAX = 220 * 1024;
 
-// the smallest cluster class whose shared memory holds an n x n block, or -1
-// (the block then takes the large-block path)
+// The cluster class of an n x n block, or -1 (the block then takes the
+// large-block path): the smallest cluster whose shared memory holds the
+// block.  16 CTAs (a non-portable cluster size) only where 8 do not suffice
+// (465 to 513 states): at 400 states the per-step cost is set by the cluster
+// barriers, and 16-CTA clusters were measured slower than 8-CTA ones there.
 static int cluster_class(int n) {
     if (n > CL_MAX_DIM) return -1;
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < CL_NCLS; ++i)
         if (cluster_smem_doubles(n, CL_SIZES[i]) * sizeof(double) <= CL_SMEM_MAX) return i;
     return -1;
 }
@@ -910,7 +914,7 @@ size_t eigh_vec_scratch_doubles(const std::vector<int>& dims) {
 // Householder stage plan: the block list of each cluster size (largest
 // blocks first) and the blocks left to the single-CTA global-memory kernel.
 struct HhPlan {
-    std::vector<int> cls[4];
+    std::vector<int> cls[CL_NCLS];
     std::vector<int> global;
 };
 
@@ -1188,11 +1192,12 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     ca.V = d.A;
     ca.Zc = d.Zc;
     ca.tri = d.tri;
-    size_t cl_smem[4] = {0, 0, 0, 0};
-    for (int q = 0; q < 4; ++q) {
+    size_t cl_smem[CL_NCLS] = {0, 0, 0, 0, 0};
+    PGX_CUDA(cudaFuncSetAttribute(eigh_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CL_SMEM_MAX));
+    PGX_CUDA(cudaFuncSetAttribute(eigh_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    for (int q = CL_NCLS - 1; q >= 0; --q) {
         if (hp.cls[q].empty()) continue;
         for (int b : hp.cls[q]) cl_smem[q] = std::max(cl_smem[q], cluster_smem_doubles(dims[b], CL_SIZES[q]) * sizeof(double));
-        PGX_CUDA(cudaFuncSetAttribute(eigh_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CL_SMEM_MAX));
         cudaLaunchConfig_t cfg = {};
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -1207,12 +1212,20 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
         int nclusters = 0;
         if (cudaOccupancyMaxActiveClusters(&nclusters, eigh_cluster_kernel, &cfg) != cudaSuccess || nclusters < 1) {
             cudaGetLastError();
-            PGX_CHECK(false, PGX_ERR_CUDA, "the eigensolver's thread-block clusters cannot be scheduled on this device");
+            // 16-CTA clusters not schedulable: their blocks go to 8-CTA clusters where they fit
+            bool moved = q == 4;
+            for (int b : hp.cls[q])
+                moved = moved && cluster_smem_doubles(dims[b], 8) * sizeof(double) <= CL_SMEM_MAX;
+            PGX_CHECK(moved, PGX_ERR_CUDA, "the eigensolver's thread-block clusters cannot be scheduled on this device");
+            hp.cls[3].insert(hp.cls[3].end(), hp.cls[q].begin(), hp.cls[q].end());
+            std::stable_sort(hp.cls[3].begin(), hp.cls[3].end(), [&](int x, int y) { return dims[x] > dims[y]; });
+            hp.cls[q].clear();
+            cl_smem[q] = 0;
         }
     }
     std::vector<int> lists(hp.global);
-    size_t cl_off[4];
-    for (int q = 0; q < 4; ++q) {
+    size_t cl_off[CL_NCLS];
+    for (int q = 0; q < CL_NCLS; ++q) {
         cl_off[q] = lists.size();
         lists.insert(lists.end(), hp.cls[q].begin(), hp.cls[q].end());
     }
@@ -1269,13 +1282,13 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
     };
     // the launches are independent: with side streams, cluster class q > 0 runs
     // on aux[q - 1] while the main stream runs the global-memory kernel and class 0
-    const bool fork = d.aux[0] && d.aux[1] && d.aux[2] && d.fork;
+    const bool fork = d.aux[0] && d.aux[1] && d.aux[2] && d.aux[3] && d.fork;
     if (fork) {
         PGX_CUDA(cudaEventRecord(d.fork, st));
-        for (int i = 0; i < 3; ++i) PGX_CUDA(cudaStreamWaitEvent(d.aux[i], d.fork, 0));
+        for (int i = 0; i < 4; ++i) PGX_CUDA(cudaStreamWaitEvent(d.aux[i], d.fork, 0));
     }
     if (!big.empty()) launch_big(d, dims, moff, big, d_lists, d_boff, d_kidx, st);
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < CL_NCLS; ++q) {
         if (hp.cls[q].empty()) continue;
         const cudaStream_t sq = (fork && q > 0) ? d.aux[q - 1] : st;
         ca.blocks = d_lists + cl_off[q];
@@ -1293,14 +1306,14 @@ void launch_eigh_raw(const EighDev& d, const std::vector<int>& dims, const std::
         cfg.numAttrs = 1;
         double fl, by;
         hh_work(hp.cls[q], fl, by);
-        static const char* names[4] = {"eigh_cluster_kernel<1>", "eigh_cluster_kernel<2>", "eigh_cluster_kernel<4>",
-                                       "eigh_cluster_kernel<8>"};
+        static const char* names[CL_NCLS] = {"eigh_cluster_kernel<1>", "eigh_cluster_kernel<2>", "eigh_cluster_kernel<4>",
+                                       "eigh_cluster_kernel<8>", "eigh_cluster_kernel<16>"};
         ProfRange pr(names[q], sq, fl, by);
         PGX_CUDA(cudaLaunchKernelEx(&cfg, eigh_cluster_kernel, ca));
         check_launch("eigh_cluster_kernel");
     }
     if (fork) {
-        for (int i = 0; i < 3; ++i) {
+        for (int i = 0; i < 4; ++i) {
             PGX_CUDA(cudaEventRecord(d.join[i], d.aux[i]));
             PGX_CUDA(cudaStreamWaitEvent(st, d.join[i], 0));
         }
@@ -1430,7 +1443,7 @@ static void launch_eigh_complex(pgx_ctx* c) {
     d.U = P.cx_U.as<double>();
     d.E = P.cx_E.as<double>();
     d.status = P.d_status;
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < 4; ++i) {
         d.aux[i] = c->aux[i];
         d.join[i] = c->join[i];
     }
@@ -1454,7 +1467,7 @@ void launch_eigh(pgx_ctx* c) {
     cudaStream_t st = c->stream;
     if (!c->fork) {
         PGX_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
-        for (int i = 0; i < 3; ++i) {
+        for (int i = 0; i < 4; ++i) {
             PGX_CUDA(cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking));
             PGX_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
         }
@@ -1489,7 +1502,7 @@ void launch_eigh(pgx_ctx* c) {
     d.U = P.d_U;
     d.E = P.d_E;
     d.status = P.d_status;
-    for (int i = 0; i < 3; ++i) {
+    for (int i = 0; i < 4; ++i) {
         d.aux[i] = c->aux[i];
         d.join[i] = c->join[i];
     }

@@ -222,8 +222,8 @@ struct pgx_ctx {
     pgx::HostArena arena;
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
     // side streams (and their fork / join events) for independent launches
-    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
     // scratch for G2 and Lehmann kernels
     pgx::DevBuf scratch[12];
 };
@@ -253,8 +253,8 @@ struct EighDev {
     int* status;         // PGX_ERR_NUMERIC when a vector is not finite
     // optional: streams on which independent Householder launches run
     // concurrently with the main stream (all null: everything on one stream)
-    cudaStream_t aux[3] = {nullptr, nullptr, nullptr};
-    cudaEvent_t fork = nullptr, join[3] = {nullptr, nullptr, nullptr};
+    cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 size_t eigh_item_bytes(const std::vector<int>& dims);
 size_t eigh_gemm_bytes(const std::vector<int>& dims, size_t* tiles_bytes);

@@ -77,12 +77,12 @@ def test_eigh_larger_blocks(harness):
 
 def test_eigh_every_householder_class():
     """One eigensolve whose blocks reach every Householder launch: thread-block
-    clusters of 1, 2, 4 and 8 CTAs (blocks whose matrix fits in 8 x 220 KB of
-    distributed shared memory, up to 464 states) and the blocked large-block
-    path (larger blocks).
+    clusters of 1, 2, 4 and 8 CTAs (the smallest that holds the block in
+    distributed shared memory, up to 464 states), of 16 CTAs (465 to 513
+    states) and the blocked large-block path (larger blocks).
     Spectra: random, tightly clustered (1e-9 spacings), two-level degenerate."""
     rng = np.random.default_rng(11)
-    dims = [150, 200, 256, 300, 401, 464, 465, 514, 640]
+    dims = [150, 200, 250, 256, 300, 401, 464, 465, 513, 514, 640]
     blocks = []
     for i, d in enumerate(dims):
         q, _ = np.linalg.qr(rng.standard_normal((d, d)))
