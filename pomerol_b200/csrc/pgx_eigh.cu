@@ -288,13 +288,19 @@ __global__ void bhh_tfactor_kernel(BigArgs g) {
 //
 // The C CTAs of a cluster hold the block's symmetric matrix in distributed
 // shared memory, row r in CTA r mod C (cyclic, so the shrinking trailing
-// matrix stays spread over all CTAs).  Step k of the reduction:
-//   (A) cluster barrier; every CTA reads row k (= the column below the
-//       diagonal) from its owner and forms the Householder vector v, tau;
-//   each CTA computes p = tau B v on its own rows and its share of v.p;
-//   (B) cluster barrier; every CTA gathers all of p and the v.p shares,
-//       forms w = p - (tau/2)(v.p) v and applies B -= v w^T + w v^T to its
-//       own rows.
+// matrix stays spread over all CTAs).  Every CTA also keeps its own copy of
+// the current row k (the column below the diagonal), brought up to date
+// locally, so one cluster barrier per step suffices.  Step k:
+//   every CTA forms the Householder vector v, tau from its copy of row k,
+//   computes p = tau B v on its own rows and its share of v.p (into the
+//   buffers of this step's parity);
+//   cluster barrier;
+//   every CTA gathers all of p and the v.p shares, forms
+//   w = p - (tau/2)(v.p) v, reads row k+1 from its owner (who leaves that
+//   row alone in this step: it leaves the trailing matrix) and updates it
+//   into its copy, and applies B -= v w^T + w v^T to its own rows r >= k+2.
+// A CTA one step ahead writes the other parity's buffers, and cannot get two
+// steps ahead before the others pass the barrier, so no reader is overrun.
 // CTA 0 stores d_k, e_k and sqrt(tau) v (row k of V in global memory).
 // Q = H_0 ... H_{n-3} is then formed from V with the CTAs owning columns
 // j = c (mod C) of Q: a column's update needs only that column, so this
@@ -316,7 +322,7 @@ struct ClusterArgs {
 
 __host__ __device__ inline size_t cluster_smem_doubles(int n, int C) {
     const int R = (n + C - 1) / C;
-    return (size_t)R * n + 2 * (size_t)n + R + 2;
+    return (size_t)R * n + 3 * (size_t)n + 2 * (size_t)R + 2;
 }
 
 __global__ void __launch_bounds__(CL_THREADS) eigh_cluster_kernel(ClusterArgs g) {
@@ -334,8 +340,9 @@ __global__ void __launch_bounds__(CL_THREADS) eigh_cluster_kernel(ClusterArgs g)
     double* slab = sh;                      // R x n rows | later R x n columns of Q
     double* v = sh + (size_t)R * n;         // n
     double* w = v + n;                      // n
-    double* p = w + n;                      // R
-    double* dslot = p + R;                  // 1
+    double* cur = w + n;                    // n: row k, up to date (this CTA's copy)
+    double* pb = cur + n;                   // 2 R: p of the steps of either parity
+    double* dslot = pb + 2 * R;             // 2
     const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5, nw = nt >> 5;
     const double* Hb = g.H + mo;
     double* V = g.V + mo;
@@ -344,19 +351,20 @@ __global__ void __launch_bounds__(CL_THREADS) eigh_cluster_kernel(ClusterArgs g)
         const int lr = (int)(idx / n), j = (int)(idx % n);
         slab[idx] = Hb[(long)(c + C * lr) * n + j];
     }
+    for (int j = tid; j < n; j += nt) cur[j] = Hb[j];  // row 0
+    __syncthreads();
     for (int k = 0; k + 2 < n; ++k) {
         const int m = n - k - 1;
-        cl.sync();  // (A) row k is final; the p slots of the previous step are free
-        const double* rowk = cl.map_shared_rank(slab, k % C) + (size_t)(k / C) * n;
+        double* p = pb + (k & 1) * R;
         double part = 0.0;
         for (int i = tid; i < m; i += nt) {
-            const double x = rowk[k + 1 + i];
+            const double x = cur[k + 1 + i];
             v[i] = x;
             if (i > 0) part += x * x;
         }
         const double sigma = block_sum(part, red);
         const double x0 = v[0];
-        const double dk = rowk[k];
+        const double dk = cur[k];
         double tau = 0.0, alpha = x0, v0 = x0;
         if (sigma != 0.0) {
             const double mu = sqrt(x0 * x0 + sigma);
@@ -372,26 +380,34 @@ __global__ void __launch_bounds__(CL_THREADS) eigh_cluster_kernel(ClusterArgs g)
         double dpart = 0.0;
         for (int lr = lr0 + wid; lr < nrows; lr += nw) {
             const double* row = slab + (size_t)lr * n + (k + 1);
-            double s = 0.0;
-            for (int j = lane; j < m; j += 32) s = fma(row[j], v[j], s);
-            s = warp_sum(s) * tau;
+            double sacc = 0.0;
+            for (int j = lane; j < m; j += 32) sacc = fma(row[j], v[j], sacc);
+            sacc = warp_sum(sacc) * tau;
             if (lane == 0) {
-                p[lr] = s;
-                dpart += v[c + C * lr - (k + 1)] * s;
+                p[lr] = sacc;
+                dpart += v[c + C * lr - (k + 1)] * sacc;
             }
         }
         const double dsum = block_sum(dpart, red);
-        if (tid == 0) dslot[0] = dsum;
-        cl.sync();  // (B) p and the v.p shares of every CTA are complete
+        if (tid == 0) dslot[k & 1] = dsum;
+        cl.sync();  // p and the v.p shares of this step are complete in every CTA
         double dtot = 0.0;
-        for (int q = 0; q < C; ++q) dtot += cl.map_shared_rank(dslot, q)[0];
+        for (int q = 0; q < C; ++q) dtot += cl.map_shared_rank(dslot, q)[k & 1];
         const double K = 0.5 * tau * dtot;
         for (int i = tid; i < m; i += nt) {
             const int r = k + 1 + i;
-            w[i] = cl.map_shared_rank(p, r % C)[r / C] - K * v[i];
+            w[i] = cl.map_shared_rank(pb, r % C)[(k & 1) * R + r / C] - K * v[i];
         }
         __syncthreads();
-        for (int lr = lr0 + wid; lr < nrows; lr += nw) {
+        // row k+1, up to date through step k-1 in its owner's slab, updated into this CTA's copy
+        {
+            const double* nxt = cl.map_shared_rank(slab, (k + 1) % C) + (size_t)((k + 1) / C) * n;
+            const double v1 = v[0], w1 = w[0];
+            for (int i = tid; i < m; i += nt) cur[k + 1 + i] = nxt[k + 1 + i] - (v1 * w[i] + w1 * v[i]);
+        }
+        // own rows r >= k+2 (row k+1 is read by the other CTAs in this step)
+        const int lr2 = (k + 2 - c + C - 1) / C;
+        for (int lr = lr2 + wid; lr < nrows; lr += nw) {
             double* row = slab + (size_t)lr * n + (k + 1);
             const int i = c + C * lr - (k + 1);
             const double vi = v[i], wi = w[i];
@@ -405,13 +421,15 @@ __global__ void __launch_bounds__(CL_THREADS) eigh_cluster_kernel(ClusterArgs g)
             const double st = sqrt(tau);
             for (int i = tid; i < m; i += nt) V[(size_t)k * n + k + 1 + i] = v[i] * st;
         }
+        __syncthreads();  // cur and v are reused by the next step
     }
     cl.sync();
     if (c == 0 && tid == 0) {
         auto elem = [&](int r, int j) { return cl.map_shared_rank(slab, r % C)[(size_t)(r / C) * n + j]; };
+        // row n-2 is this CTA's copy (its owner skipped it in the last step); row n-1 its owner's
         if (n >= 2) {
-            g.tri[2 * eo + n - 2] = elem(n - 2, n - 2);
-            g.tri[2 * eo + n + n - 2] = elem(n - 1, n - 2);
+            g.tri[2 * eo + n - 2] = cur[n - 2];
+            g.tri[2 * eo + n + n - 2] = cur[n - 1];
         }
         g.tri[2 * eo + n - 1] = elem(n - 1, n - 1);
         g.tri[2 * eo + n + n - 1] = 0.0;
@@ -884,7 +902,7 @@ static void tri_plan(const std::vector<int>& dims, std::vector<TriItem>& items, 
 
 constexpr int CL_NCLS = 5;
 constexpr int CL_SIZES[CL_NCLS] = {1, 2, 4, 8, 16};
-constexpr size_t CL_SMEM_MAX = 220 * 1024;
+constexpr size_t CL_SMEM_MAX = 226 * 1024;  // dynamic shared memory per CTA (the static part is 256 bytes)
 
 // The cluster class of an n x n block, or -1 (the block then takes the
 // large-block path): the smallest cluster whose shared memory holds the
