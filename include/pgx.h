@@ -98,6 +98,14 @@ int pgx_get_hamiltonian(pgx_ctx* ctx, double* H);
 int pgx_gf_vjp(pgx_ctx* ctx, int32_t op1, int32_t op2, int32_t nparts, const int32_t* outer, const int32_t* inner,
                int32_t nz, const double* z, const double* lambda, double* dterm, double* dE);
 
+/* The same for a susceptibility: chi(z_n) as pgx_susc evaluates it for the
+ * same (opA, opB, parts, z, pole_res) without coefficient filtering, with
+ * beta the one of the last pgx_weights call (its zero-pole terms act at z = 0
+ * and are differentiated as beta A B w; the disconnected part is not
+ * included, as in pgx_susc).  Outputs as pgx_gf_vjp. */
+int pgx_susc_vjp(pgx_ctx* ctx, int32_t opA, int32_t opB, int32_t nparts, const int32_t* outer, const int32_t* inner,
+                 int32_t nz, const double* z, double pole_res, const double* lambda, double* dterm, double* dE);
+
 /* Diagonalise every block in one launch (FP64).  Eigenvalues ascending per
  * block; eigenvectors are the columns of each block's U.  The uploaded
  * Hamiltonian is kept, so this can be re-run. */

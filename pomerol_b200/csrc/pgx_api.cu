@@ -392,6 +392,16 @@ int pgx_susc_models(pgx_ctx* c, int32_t opA, int32_t opB, int32_t nparts, const 
     });
 }
 
+int pgx_susc_vjp(pgx_ctx* c, int32_t opA, int32_t opB, int32_t nparts, const int32_t* outer, const int32_t* inner,
+                 int32_t nz, const double* z, double pole_res, const double* lambda, double* dterm, double* dE) {
+    return guarded(c, [&] {
+        PGX_CHECK(nparts >= 0 && nz >= 0 && (nparts == 0 || (outer && inner)) && (nz == 0 || (z && lambda)) && dterm,
+                  PGX_ERR_ARG, "bad arguments");
+        PGX_CHECK(!c->P.w_models, PGX_ERR_STATE, "needs the weights of one model (pgx_weights)");
+        pgx::run_susc_vjp(c, opA, opB, nparts, outer, inner, nz, z, pole_res, lambda, dterm, dE);
+    });
+}
+
 int pgx_get_hamiltonian(pgx_ctx* c, double* H) {
     return guarded(c, [&] {
         pgx::Problem& P = c->P;

@@ -266,6 +266,8 @@ void assemble_hamiltonian(pgx_ctx* c, int nterms, const int32_t* ops, const doub
                           const uint64_t* fock, const int32_t* state_block, const int32_t* state_inner);
 void run_gf_vjp(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,
                 const double* z, const double* lambda, double* dterm, double* dE);
+void run_susc_vjp(pgx_ctx* c, int opA, int opB, int nparts, const int32_t* outer, const int32_t* inner, int nz,
+                  const double* z, double pole_res, const double* lambda, double* dterm, double* dE);
 void rotate_operator(Problem& P, Operator& op, cudaStream_t st);
 void adjoint_operator(Problem& P, const Operator& src, Operator& dst, cudaStream_t st);
 void run_gf(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,

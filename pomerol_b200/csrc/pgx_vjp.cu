@@ -1,6 +1,8 @@
-// Reverse-mode derivative of a single-particle Green's function through the
-// exact-diagonalisation chain (pgx_gf_vjp).  The reference computes no
-// derivatives; this follows the forward path of pgx_gf backwards:
+// Reverse-mode derivative of a single-particle Green's function (pgx_gf_vjp)
+// or a susceptibility (pgx_susc_vjp) through the exact-diagonalisation chain.
+// The reference computes no derivatives; this follows the forward path of
+// pgx_gf backwards (for chi the residue is -(w_a - w_b) A B, and a zero-pole
+// pair adds beta A B w_a at z = 0, see pair_vjp_kernel):
 //
 //   G(z_n) = sum_{parts} sum_{a in o, b in i} A_ab B_ba (w_a + w_b) R_ab(n),
 //   R_ab(n) = 1 / (z_n - (E_b - E_a)),  A = U_o^T C1 U_i,  B = U_i^T C2 U_o,
@@ -23,6 +25,7 @@
 // terms cancel).  Finally dL/dc_t = sum over columns j of the terms' Fock
 // action sign * Hbar_sym[o][j], the transpose of the Hamiltonian assembly.
 
+#include <cfloat>
 #include <cmath>
 
 #include "pgx_common.cuh"
@@ -39,18 +42,32 @@ struct VjpPart {
     int d_o, d_i;
 };
 
-// one thread per (a, b) element of a pair part; real operators
+// one thread per (a, b) element of a pair part; real operators.  mode 0: G,
+// residue (w_a + w_b) A B.  mode 1: chi, residue -(w_a - w_b) A B away from
+// the zero pole; a pair with |pole| < pole_res adds beta A B w_a at z = 0
+// only (zre = Re of the sum of lambda over the zero frequencies), as the
+// forward sum does.
 __global__ void pair_vjp_kernel(const VjpPart* parts, const double* m1, const double* m2, const double* E,
                                 const double* w, const cd* z, const cd* lam, int nz, double* g1, double* g2,
-                                double* wbar, double* Ebar) {
+                                double* wbar, double* Ebar, int mode, double pole_res, double beta, double zre) {
     const VjpPart pp = parts[blockIdx.y];
     const long n = (long)pp.d_o * pp.d_i;
     for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
         const int a = (int)(e / pp.d_i), b = (int)(e % pp.d_i);
         const double A = m1[pp.f1 + e], B = m2[pp.f2 + (long)b * pp.d_o + a];
         if (A == 0.0 && B == 0.0) continue;
-        const double wo = w[pp.eo + a], wi = w[pp.ei + b], s = wo + wi;
+        const double wo = w[pp.eo + a], wi = w[pp.ei + b];
         const double pole = E[pp.ei + b] - E[pp.eo + a];
+        if (mode == 1 && fabs(pole) < pole_res) {
+            const double f = beta * zre;
+            if (f != 0.0) {
+                atomicAdd(&g1[pp.f1 + e], B * wo * f);
+                atomicAdd(&g2[pp.f2 + (long)b * pp.d_o + a], A * wo * f);
+                if (A * B != 0.0) atomicAdd(&wbar[pp.eo + a], A * B * f);
+            }
+            continue;
+        }
+        const double s = mode ? -(wo - wi) : wo + wi;
         double Px = 0.0, Qx = 0.0;
         for (int t = 0; t < nz; ++t) {
             const cd R = inv(cd{z[t].x - pole, z[t].y});
@@ -62,7 +79,7 @@ __global__ void pair_vjp_kernel(const VjpPart* parts, const double* m1, const do
         atomicAdd(&g2[pp.f2 + (long)b * pp.d_o + a], A * s * Px);
         const double ab = A * B;
         if (ab != 0.0) {
-            atomicAdd(&wbar[pp.eo + a], ab * Px);
+            atomicAdd(&wbar[pp.eo + a], mode ? -ab * Px : ab * Px);  // d s / d w_a = 1 (G) or -1 (chi)
             atomicAdd(&wbar[pp.ei + b], ab * Px);
             const double de = ab * s * Qx;
             atomicAdd(&Ebar[pp.ei + b], de);
@@ -192,8 +209,9 @@ __global__ void term_grad_kernel(const int* ops, int nterms, const uint64_t* foc
 
 }  // namespace
 
-void run_gf_vjp(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,
-                const double* z, const double* lambda, double* dterm, double* dE) {
+static void run_pair_vjp(pgx_ctx* c, int mode, int op1, int op2, int nparts, const int32_t* outer,
+                         const int32_t* inner, int nz, const double* z, double pole_res, const double* lambda,
+                         double* dterm, double* dE) {
     Problem& P = c->P;
     cudaStream_t st = c->stream;
     PGX_CHECK(!P.is_complex, PGX_ERR_ARG, "pgx_gf_vjp: real Hamiltonians only");
@@ -265,8 +283,12 @@ void run_gf_vjp(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, 
         dim3 g(std::min(ceil_div(maxn, 256), 256), (unsigned)pp.size());
         // per (a, b, z): complex reciprocal (8), lambda R (6), lambda R^2 (6) and two sums
         ProfRange pr("pair_vjp_kernel", st, 22.0 * nel * nz, 56.0 * nel);
+        // chi's zero-pole terms act at z = 0 only (the same test as the forward sum)
+        double zre = 0.0;
+        for (int t = 0; t < nz; ++t)
+            if (std::sqrt(z[2 * t] * z[2 * t] + z[2 * t + 1] * z[2 * t + 1]) <= DBL_EPSILON) zre += lambda[2 * t];
         pair_vjp_kernel<<<g, 256, 0, st>>>(d_pp, A.mat.as<double>(), B.mat.as<double>(), P.d_E, P.d_w, d_z, d_lam, nz,
-                                           g1, g2, wb, Eb);
+                                           g1, g2, wb, Eb, mode, pole_res, P.beta, zre);
         check_launch("pair_vjp_kernel");
     }
     {
@@ -426,6 +448,16 @@ void run_gf_vjp(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, 
     }
     if (dE) PGX_CUDA(cudaMemcpyAsync(dE, Eb, P.esize * sizeof(double), cudaMemcpyDeviceToHost, st));
     PGX_CUDA(cudaStreamSynchronize(st));
+}
+
+void run_gf_vjp(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* outer, const int32_t* inner, int nz,
+                const double* z, const double* lambda, double* dterm, double* dE) {
+    run_pair_vjp(c, 0, op1, op2, nparts, outer, inner, nz, z, 0.0, lambda, dterm, dE);
+}
+
+void run_susc_vjp(pgx_ctx* c, int opA, int opB, int nparts, const int32_t* outer, const int32_t* inner, int nz,
+                  const double* z, double pole_res, const double* lambda, double* dterm, double* dE) {
+    run_pair_vjp(c, 1, opA, opB, nparts, outer, inner, nz, z, pole_res, lambda, dterm, dE);
 }
 
 }  // namespace pgx

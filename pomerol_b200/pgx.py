@@ -24,7 +24,7 @@ EXPORTS = [
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
-    "pgx_gf_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
+    "pgx_gf_vjp", "pgx_susc_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
 ]
 
 
@@ -82,6 +82,7 @@ def load():
         lib.pgx_get_hamiltonian.argtypes = [P, P]
         lib.pgx_op_release.argtypes = [P, I32]
         lib.pgx_gf_vjp.argtypes = [P, I32, I32, I32, P, P, I32, P, P, P, P]
+        lib.pgx_susc_vjp.argtypes = [P, I32, I32, I32, P, P, I32, P, D, P, P, P]
         lib.pgx_chi3.argtypes = [P, I32, I32, P, I32, P, D, P]
         lib.pgx_set_eigensystem.argtypes = [P, P, P]
         lib.pgx_set_models.argtypes = [P, I32, P, P]
@@ -453,6 +454,21 @@ def _susc_models(self, opA, opB, outer, inner, z, pole_res=1e-8, coef_tol=1e-8):
     return out, zero
 
 
+def _susc_vjp(self, opA, opB, outer, inner, z, lam, pole_res=1e-8):
+    """Reverse-mode derivative of susc(opA, opB, outer, inner, z): as gf_vjp."""
+    z = np.ascontiguousarray(np.asarray(z, dtype=complex))
+    lam = np.ascontiguousarray(np.asarray(lam, dtype=complex))
+    if lam.shape != z.shape:
+        raise ValueError("lam needs one entry per frequency")
+    o = np.ascontiguousarray(outer, dtype=np.int32)
+    i = np.ascontiguousarray(inner, dtype=np.int32)
+    dterm = np.zeros(max(getattr(self, "_asm_nterms", 0), 1))
+    dE = np.zeros(int(sum(self.dims)))
+    self._ck(self.lib.pgx_susc_vjp(self.h, int(opA), int(opB), len(o), _p(o), _p(i), len(z), _p(z.view(np.float64)),
+                                   float(pole_res), _p(lam.view(np.float64)), _p(dterm), _p(dE)))
+    return dterm[:getattr(self, "_asm_nterms", 0)], dE
+
+
 def _op_release(self, op_id):
     """Give an operator's device memory back to the context for reuse."""
     self._ck(self.lib.pgx_op_release(self.h, int(op_id)))
@@ -460,6 +476,7 @@ def _op_release(self, op_id):
 
 Engine.op_release = _op_release
 Engine.gf_vjp = _gf_vjp
+Engine.susc_vjp = _susc_vjp
 Engine.chi3 = _chi3
 Engine.set_models = _set_models
 Engine.set_eigensystem = _set_eigensystem

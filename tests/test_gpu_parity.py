@@ -878,3 +878,55 @@ def test_eigensystem_checkpoint_reload(harness, tmp_path):
         other.load_eigensystem(path)
     with pytest.raises(PgxError):
         other.set_eigensystem([np.array([2.0, 1.0, 0.0]), np.zeros(5)], [np.eye(3), np.eye(5)])
+
+
+@pytest.mark.parametrize("same", [True, False])
+def test_susc_vjp_against_finite_differences(same):
+    """pgx_susc_vjp: the gradient of L = Re sum_m lambda_m chi_{n_i n_j}(i Omega_m)
+    on 8 bosonic frequencies (Omega_0 = 0 carries the zero-pole terms) with
+    respect to (U, mu, h, eps_k, V_k), against central differences (step
+    1e-5) of the oracle's exact chi; relative tolerance 1e-6."""
+    from tests.pgx_harness import GpuED
+    beta = 8.0
+    p0 = {"U": 2.0, "mu": 0.9, "h": 0.15, "eps": [-0.6, 0.35], "V": [0.45, 0.3]}
+    m = M.make_model(_anderson_expr(p0))
+    keys = list(m.expr.terms)
+    terms, nmodes, fock, sb, si = _assembly_inputs(m)
+    i = m.info.getIndex("C", 0, M.DOWN)
+    j = i if same else m.info.getIndex("C", 0, M.UP)
+    z = 2j * np.pi * np.arange(8) / beta
+    g = GpuED(m, beta)
+    g.eng.assemble_hamiltonian(terms, nmodes, fock, sb, si)
+    g.eng.eigh()
+    g.E, g.U = g.eng.eigensystem()
+    g.w, g.Z = g.eng.weights(beta)
+    A = g.quadratic(i, i)
+    B = A if same else g.quadratic(j, j)
+    outer, inner = g.pair_parts(A, B)
+
+    def chi_oracle(p):
+        mm = M.make_model(_anderson_expr(p))
+        ed = EDm.ED(mm, beta)
+        return L.susc_eval(L.susc_terms(ed, ed.quadratic(i, i), ed.quadratic(j, j), rule=False), z, beta)
+
+    ref = chi_oracle(p0)
+    X, _ = g.eng.susc(A, B, outer, inner, z, beta, pole_res=1e-8, coef_tol=0.0)
+    assert np.abs(X - ref).max() < 1e-12 * max(1.0, np.abs(ref).max())
+    rng = np.random.default_rng(21)
+    lam = rng.standard_normal(len(z)) + 1j * rng.standard_normal(len(z))
+    dterm, dE = g.eng.susc_vjp(A, B, outer, inner, z, lam, pole_res=1e-8)
+    assert abs(dE.sum()) < 1e-10 * max(1.0, np.abs(dE).max())
+    h = 1e-5
+    for th in [("U",), ("mu",), ("h",), ("eps", 0), ("eps", 1), ("V", 0), ("V", 1)]:
+        qp = {k: (list(v) if isinstance(v, list) else v) for k, v in p0.items()}
+        qm = {k: (list(v) if isinstance(v, list) else v) for k, v in p0.items()}
+        if len(th) == 1:
+            qp[th[0]] += h
+            qm[th[0]] -= h
+        else:
+            qp[th[0]][th[1]] += h
+            qm[th[0]][th[1]] -= h
+        dc = (_term_coefs(qp, keys) - _term_coefs(qm, keys)) / (2 * h)
+        fd = (np.real(lam @ chi_oracle(qp)) - np.real(lam @ chi_oracle(qm))) / (2 * h)
+        got = float(dc @ dterm)
+        assert abs(got - fd) <= 1e-6 * max(1.0, abs(fd)), (th, got, fd)
