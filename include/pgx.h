@@ -234,6 +234,25 @@ int pgx_g2_count(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, double 
                  long long* count);
 
 /* ------------------------------------------------------------------------
+ * CUDA graphs of captured sequences (the reference has no device work to
+ * capture).  Between pgx_graph_begin and pgx_graph_end the context's stream
+ * is captured instead of run: pgx_eigh (real blocks; after one uncaptured
+ * call, which sizes every buffer) and pgx_op_rotate record their device work
+ * into the graph, and every other entry point returns PGX_ERR_STATE.  Host
+ * data they upload is staged in memory the graph keeps.  pgx_graph_replay
+ * runs the graph on the context's current inputs (e.g. new block
+ * Hamiltonians from pgx_set_hamiltonian), waits for it, checks the
+ * eigensolver status and marks the eigensystem and the rotated operators
+ * valid, as the captured calls would.  A graph refuses to replay once any
+ * device buffer of the process was allocated or freed, pgx_set_blocks ran,
+ * or an operator was defined, formed or released after its capture.
+ * ------------------------------------------------------------------------ */
+int pgx_graph_begin(pgx_ctx* ctx);
+int pgx_graph_end(pgx_ctx* ctx, int32_t* graph_id);
+int pgx_graph_replay(pgx_ctx* ctx, int32_t graph_id);
+int pgx_graph_destroy(pgx_ctx* ctx, int32_t graph_id);
+
+/* ------------------------------------------------------------------------
  * Batches of independent models.
  * The reference holds one model per set of objects; for many impurity models
  * at once (the 64-model batch workload) a context may hold the blocks of

@@ -3,8 +3,10 @@
 // exception crosses the ABI.
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <numeric>
+#include <utility>
 
 #include "pgx_common.cuh"
 #include "pgx_internal.h"
@@ -68,6 +70,11 @@ Profiler::~Profiler() {
         cudaEventDestroy(r.b);
     }
     for (auto e : spare) cudaEventDestroy(e);
+}
+
+unsigned long long& alloc_epoch() {
+    static unsigned long long e = 0;
+    return e;
 }
 
 HostArena*& active_arena() {
@@ -147,14 +154,22 @@ __global__ void recip_check_kernel(const double* x, double* y, int n) {
     if (i < n) y[i] = pgx::recip_pos(x[i]);
 }
 
-template <typename F> int guarded(pgx_ctx* c, F&& f) {
+// Runs an entry point: its context's profiler and upload arena (the graph's
+// own arena while a capture is open) are visible to the launch sites, and
+// exceptions become status codes.  While a capture is open only the entry
+// points that may be captured (capture_ok) run.
+template <typename F> int guarded_impl(pgx_ctx* c, bool capture_ok, F&& f) {
     if (!c) return PGX_ERR_ARG;
-    struct Scope {  // the context's profiler and upload arena are visible to launch sites during the call
+    if (c->capturing && !capture_ok) {
+        c->last_error = "this entry point cannot run while a graph is being captured";
+        return PGX_ERR_STATE;
+    }
+    struct Scope {
         pgx::Profiler* saved_p;
         pgx::HostArena* saved_a;
         explicit Scope(pgx_ctx* c) : saved_p(pgx::active_profiler()), saved_a(pgx::active_arena()) {
             pgx::active_profiler() = &c->prof;
-            pgx::active_arena() = &c->arena;
+            pgx::active_arena() = c->capturing ? c->cap.arena.get() : &c->arena;
         }
         ~Scope() {
             pgx::active_profiler() = saved_p;
@@ -164,7 +179,7 @@ template <typename F> int guarded(pgx_ctx* c, F&& f) {
     try {
         PGX_CUDA(cudaSetDevice(c->device));
         f();
-        c->arena.recycle(c->stream);
+        if (!c->capturing) c->arena.recycle(c->stream);
         c->last_error.clear();
         return PGX_OK;
     } catch (const Error& e) {
@@ -178,10 +193,17 @@ template <typename F> int guarded(pgx_ctx* c, F&& f) {
         return PGX_ERR_ARG;
     }
 }
+template <typename F> int guarded(pgx_ctx* c, F&& f) { return guarded_impl(c, false, std::forward<F>(f)); }
+template <typename F> int guarded_cap(pgx_ctx* c, F&& f) { return guarded_impl(c, true, std::forward<F>(f)); }
 
-// A new problem on the context: metadata is reset, device buffers keep their
-// capacity (DevBuf::reserve grows them when needed), so a context reused for
-// problems of similar size allocates and frees nothing.
+void drop_graph(pgx_ctx::Graph& g) {
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g.exec = nullptr;
+    g.graph = nullptr;
+    g.arena.reset();
+}
+
 void reset_problem(pgx::Problem& P) {
     pgx::Problem fresh;
     pgx::DevBuf pgx::Problem::*bufs[] = {&pgx::Problem::H,       &pgx::Problem::work,      &pgx::Problem::work2,
@@ -232,6 +254,15 @@ int pgx_destroy(pgx_ctx* c) {
     if (!c) return PGX_OK;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    if (c->capturing) {
+        cudaGraph_t gr = nullptr;
+        cudaStreamEndCapture(c->stream, &gr);
+        if (gr) cudaGraphDestroy(gr);
+        cudaGetLastError();
+        c->capturing = false;
+    }
+    drop_graph(c->cap);
+    for (auto& g : c->graphs) drop_graph(g);
     reset_problem(c->P);
     for (auto& b : c->scratch) b.release();
     if (c->ev_begin) cudaEventDestroy(c->ev_begin);
@@ -253,6 +284,8 @@ int pgx_set_blocks(pgx_ctx* c, int32_t nblocks, const int32_t* dims, int32_t is_
         PGX_CHECK(nblocks > 0 && dims, PGX_ERR_ARG, "need at least one block");
         for (int b = 0; b < nblocks; ++b) PGX_CHECK(dims[b] > 0, PGX_ERR_ARG, "block sizes must be positive");
         PGX_CUDA(cudaStreamSynchronize(c->stream));
+        ++c->problem_gen;
+        ++c->ops_gen;
         reset_problem(c->P);
         pgx::Problem& P = c->P;
         P.nblocks = nblocks;
@@ -402,6 +435,82 @@ int pgx_susc_vjp(pgx_ctx* c, int32_t opA, int32_t opB, int32_t nparts, const int
     });
 }
 
+int pgx_graph_begin(pgx_ctx* c) {
+    return guarded(c, [&] {
+        PGX_CHECK(!c->prof.on, PGX_ERR_STATE, "stop profiling before capturing a graph");
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+        drop_graph(c->cap);
+        c->cap = pgx_ctx::Graph{};
+        c->cap.arena.reset(new pgx::HostArena());
+        PGX_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+        c->capturing = true;
+    });
+}
+
+int pgx_graph_end(pgx_ctx* c, int32_t* graph_id) {
+    return guarded_cap(c, [&] {
+        PGX_CHECK(c->capturing, PGX_ERR_STATE, "no graph is being captured");
+        PGX_CHECK(graph_id, PGX_ERR_ARG, "null graph id");
+        c->capturing = false;
+        cudaGraph_t gr = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(c->stream, &gr);
+        if (e != cudaSuccess || !gr) {
+            cudaGetLastError();
+            if (gr) cudaGraphDestroy(gr);
+            drop_graph(c->cap);
+            PGX_CHECK(false, PGX_ERR_CUDA, std::string("graph capture failed: ") + cudaGetErrorString(e));
+        }
+        c->cap.graph = gr;
+        if (cudaGraphInstantiate(&c->cap.exec, gr, 0) != cudaSuccess) {
+            cudaGetLastError();
+            drop_graph(c->cap);
+            PGX_CHECK(false, PGX_ERR_CUDA, "graph instantiation failed");
+        }
+        c->cap.epoch = pgx::alloc_epoch();
+        c->cap.problem_gen = c->problem_gen;
+        c->cap.ops_gen = c->ops_gen;
+        size_t slot = 0;
+        while (slot < c->graphs.size() && c->graphs[slot].exec) ++slot;
+        if (slot == c->graphs.size()) c->graphs.emplace_back();
+        c->graphs[slot] = std::move(c->cap);
+        c->cap = pgx_ctx::Graph{};
+        *graph_id = (int32_t)slot;
+    });
+}
+
+int pgx_graph_replay(pgx_ctx* c, int32_t graph_id) {
+    return guarded(c, [&] {
+        PGX_CHECK(graph_id >= 0 && graph_id < (int)c->graphs.size() && c->graphs[graph_id].exec, PGX_ERR_ARG,
+                  "bad graph id");
+        pgx_ctx::Graph& g = c->graphs[graph_id];
+        pgx::Problem& P = c->P;
+        PGX_CHECK(g.epoch == pgx::alloc_epoch() && g.problem_gen == c->problem_gen && g.ops_gen == c->ops_gen,
+                  PGX_ERR_STATE, "device buffers or operators changed since the capture; capture the graph again");
+        PGX_CHECK(!g.eigh || P.have_H, PGX_ERR_STATE, "pgx_set_hamiltonian first");
+        PGX_CHECK(g.eigh || P.have_eig, PGX_ERR_STATE, "pgx_eigh first");
+        PGX_CUDA(cudaGraphLaunch(g.exec, c->stream));
+        int st = 0;
+        if (g.eigh) PGX_CUDA(cudaMemcpyAsync(&st, P.d_status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+        if (g.eigh) {
+            PGX_CHECK(st == 0, PGX_ERR_NUMERIC, "eigensolver did not converge");
+            P.have_eig = true;
+            P.have_w = false;
+            for (auto& op : P.ops) op.rotated = false;
+        }
+        for (int op : g.rotated) P.ops[op].rotated = true;
+    });
+}
+
+int pgx_graph_destroy(pgx_ctx* c, int32_t graph_id) {
+    return guarded(c, [&] {
+        PGX_CHECK(graph_id >= 0 && graph_id < (int)c->graphs.size() && c->graphs[graph_id].exec, PGX_ERR_ARG,
+                  "bad graph id");
+        PGX_CUDA(cudaStreamSynchronize(c->stream));
+        drop_graph(c->graphs[graph_id]);
+    });
+}
+
 int pgx_get_hamiltonian(pgx_ctx* c, double* H) {
     return guarded(c, [&] {
         pgx::Problem& P = c->P;
@@ -413,9 +522,17 @@ int pgx_get_hamiltonian(pgx_ctx* c, double* H) {
 }
 
 int pgx_eigh(pgx_ctx* c) {
-    return guarded(c, [&] {
+    return guarded_cap(c, [&] {
         pgx::Problem& P = c->P;
         PGX_CHECK(P.have_H, PGX_ERR_STATE, "pgx_set_hamiltonian first");
+        if (c->capturing) {  // device work only; the status is read when the graph is replayed
+            PGX_CHECK(!P.is_complex, PGX_ERR_STATE, "complex blocks cannot be captured");
+            PGX_CHECK(c->fork != nullptr, PGX_ERR_STATE, "run pgx_eigh once before capturing it");
+            PGX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int), c->stream));
+            pgx::launch_eigh(c);
+            c->cap.eigh = true;
+            return;
+        }
         PGX_CUDA(cudaMemsetAsync(P.d_status, 0, sizeof(int), c->stream));
         pgx::launch_eigh(c);
         int st = 0;
@@ -507,6 +624,7 @@ int pgx_truncate_blocks(pgx_ctx* c, double tol, int32_t* retained) {
 int pgx_op_define(pgx_ctx* c, int32_t nparts, const int32_t* right_block, const int32_t* left_block,
                   const int32_t* target, const double* coef, int32_t* op_id) {
     return guarded(c, [&] {
+        ++c->ops_gen;
         pgx::Problem& P = c->P;
         PGX_CHECK(P.nblocks > 0, PGX_ERR_STATE, "pgx_set_blocks first");
         PGX_CHECK(nparts >= 0 && op_id && (nparts == 0 || (right_block && left_block && target && coef)),
@@ -555,17 +673,26 @@ int pgx_op_define(pgx_ctx* c, int32_t nparts, const int32_t* right_block, const 
 }
 
 int pgx_op_rotate(pgx_ctx* c, int32_t op_id) {
-    return guarded(c, [&] {
+    return guarded_cap(c, [&] {
         pgx::Problem& P = c->P;
         PGX_CHECK(op_id >= 0 && op_id < (int)P.ops.size(), PGX_ERR_ARG, "bad operator id");
-        PGX_CHECK(P.have_eig, PGX_ERR_STATE, "pgx_eigh first");
+        PGX_CHECK(P.have_eig || (c->capturing && c->cap.eigh), PGX_ERR_STATE, "pgx_eigh first");
         PGX_CHECK(!P.ops[op_id].act_off.empty(), PGX_ERR_ARG, "operator has no Fock action (adjoint?)");
+        if (c->capturing) {  // the rotation happens when the graph is replayed
+            const bool was = P.ops[op_id].rotated;
+            PGX_CHECK(!P.is_complex, PGX_ERR_STATE, "complex operators cannot be captured");
+            pgx::rotate_operator(P, P.ops[op_id], c->stream);
+            P.ops[op_id].rotated = was;
+            c->cap.rotated.push_back(op_id);
+            return;
+        }
         pgx::rotate_operator(P, P.ops[op_id], c->stream);
     });
 }
 
 int pgx_op_adjoint(pgx_ctx* c, int32_t src, int32_t* op_id) {
     return guarded(c, [&] {
+        ++c->ops_gen;
         pgx::Problem& P = c->P;
         PGX_CHECK(src >= 0 && src < (int)P.ops.size() && op_id, PGX_ERR_ARG, "bad operator id");
         PGX_CHECK(P.ops[src].rotated, PGX_ERR_STATE, "rotate the source operator first");
@@ -579,6 +706,7 @@ int pgx_op_adjoint(pgx_ctx* c, int32_t src, int32_t* op_id) {
 
 int pgx_op_release(pgx_ctx* c, int32_t op_id) {
     return guarded(c, [&] {
+        ++c->ops_gen;
         pgx::Problem& P = c->P;
         PGX_CHECK(op_id >= 0 && op_id < (int)P.ops.size(), PGX_ERR_ARG, "bad operator id");
         // work already queued on the context's stream that reads the operator

@@ -5,12 +5,17 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "pgx_common.cuh"
 
 namespace pgx {
+
+// Counts device allocations and frees in the process: a captured CUDA graph
+// records it and refuses to replay once any buffer may have moved.
+unsigned long long& alloc_epoch();
 
 // Device allocation owned by a context.
 struct DevBuf {
@@ -39,6 +44,7 @@ struct DevBuf {
         release();
         if (n == 0) return;
         cudaError_t e = cudaMalloc(&p, n);
+        ++alloc_epoch();
         if (e != cudaSuccess) {
             p = nullptr;
             bytes = 0;
@@ -48,7 +54,10 @@ struct DevBuf {
         bytes = n;
     }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            cudaFree(p);
+            ++alloc_epoch();
+        }
         p = nullptr;
         bytes = 0;
     }
@@ -226,6 +235,21 @@ struct pgx_ctx {
     cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
     // scratch for G2 and Lehmann kernels
     pgx::DevBuf scratch[12];
+    // CUDA graphs of captured entry-point sequences (pgx_graph_begin / end / replay)
+    struct Graph {
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        std::unique_ptr<pgx::HostArena> arena;  // staging of the captured copies, kept with the graph
+        unsigned long long epoch = 0;           // alloc_epoch() at the end of the capture
+        unsigned long problem_gen = 0, ops_gen = 0;
+        bool eigh = false;                      // the sequence contains pgx_eigh
+        std::vector<int> rotated;               // operators the sequence rotates
+    };
+    std::vector<Graph> graphs;
+    bool capturing = false;
+    Graph cap;                                  // the graph being captured
+    unsigned long problem_gen = 0;              // bumped by pgx_set_blocks
+    unsigned long ops_gen = 0;                  // bumped when operators are defined, formed or released
 };
 
 namespace pgx {

@@ -24,7 +24,8 @@ EXPORTS = [
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
-    "pgx_gf_vjp", "pgx_susc_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
+    "pgx_gf_vjp", "pgx_susc_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_graph_begin", "pgx_graph_end",
+    "pgx_graph_replay", "pgx_graph_destroy", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
 ]
 
 
@@ -85,6 +86,10 @@ def load():
         lib.pgx_susc_vjp.argtypes = [P, I32, I32, I32, P, P, I32, P, D, P, P, P]
         lib.pgx_chi3.argtypes = [P, I32, I32, P, I32, P, D, P]
         lib.pgx_set_eigensystem.argtypes = [P, P, P]
+        lib.pgx_graph_begin.argtypes = [P]
+        lib.pgx_graph_end.argtypes = [P, P]
+        lib.pgx_graph_replay.argtypes = [P, I32]
+        lib.pgx_graph_destroy.argtypes = [P, I32]
         lib.pgx_set_models.argtypes = [P, I32, P, P]
         lib.pgx_weights_models.argtypes = [P, P, P, P]
         lib.pgx_gf_models.argtypes = [P, I32, I32, I32, P, P, I32, P, D, P]
@@ -407,6 +412,26 @@ def _load_eigensystem(self, path):
     self.set_eigensystem(E, U)
 
 
+def _graph_begin(self):
+    """Start capturing eigh() / op_rotate() calls into a CUDA graph."""
+    self._ck(self.lib.pgx_graph_begin(self.h))
+
+
+def _graph_end(self):
+    """Finish the capture; returns the graph id."""
+    g = np.zeros(1, dtype=np.int32)
+    self._ck(self.lib.pgx_graph_end(self.h, _p(g)))
+    return int(g[0])
+
+
+def _graph_replay(self, gid):
+    self._ck(self.lib.pgx_graph_replay(self.h, int(gid)))
+
+
+def _graph_destroy(self, gid):
+    self._ck(self.lib.pgx_graph_destroy(self.h, int(gid)))
+
+
 def _set_models(self, first_block, beta):
     """Independent models in this context: blocks first_block[m] ..
     first_block[m+1]-1 form model m at inverse temperature beta[m]."""
@@ -479,6 +504,10 @@ Engine.gf_vjp = _gf_vjp
 Engine.susc_vjp = _susc_vjp
 Engine.chi3 = _chi3
 Engine.set_models = _set_models
+Engine.graph_begin = _graph_begin
+Engine.graph_end = _graph_end
+Engine.graph_replay = _graph_replay
+Engine.graph_destroy = _graph_destroy
 Engine.set_eigensystem = _set_eigensystem
 Engine.save_eigensystem = _save_eigensystem
 Engine.load_eigensystem = _load_eigensystem

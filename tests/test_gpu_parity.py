@@ -930,3 +930,46 @@ def test_susc_vjp_against_finite_differences(same):
         fd = (np.real(lam @ chi_oracle(qp)) - np.real(lam @ chi_oracle(qm))) / (2 * h)
         got = float(dc @ dterm)
         assert abs(got - fd) <= 1e-6 * max(1.0, abs(fd)), (th, got, fd)
+
+
+def test_graph_capture_and_replay(harness):
+    """pgx_graph_begin / end / replay: a captured [eigh, rotate c+] replayed on
+    new block Hamiltonians gives the eigensystem and rotated operator of the
+    direct calls (the same kernels in the same order: equal to 1e-15);
+    entry points that cannot be captured are refused during the capture, and
+    the graph refuses to replay once an operator was defined after it."""
+    from pomerol_b200.pgx import PgxError
+    m = M.make_model(plaquette_expr())
+    g = harness(m, 10.0)
+    ix = m.info.getIndex("A", 0, M.DOWN)
+    op = g.cdag(ix)
+    eng = g.eng
+    eng.graph_begin()
+    eng.eigh()
+    with pytest.raises(PgxError):
+        eng.weights(10.0)
+    eng.op_rotate(op)
+    gid = eng.graph_end()
+    rng = np.random.default_rng(3)
+    blocks2 = []
+    for b in range(len(m.blocks)):
+        h = m.h_block(b)
+        blocks2.append(1.7 * h + 0.2 * np.eye(len(h)) + 1e-3 * (lambda a: a + a.T)(rng.standard_normal(h.shape)))
+    eng.set_hamiltonian(blocks2)
+    eng.graph_replay(gid)
+    E1, U1 = eng.eigensystem()
+    parts1 = [eng.op_read(op, k) for k in range(len(eng.op_info(op)))]
+    for h, e in zip(blocks2, E1):
+        assert np.abs(e - np.linalg.eigvalsh(h)).max() < 1e-12 * max(1.0, np.abs(e).max())
+    eng.eigh()
+    eng.op_rotate(op)
+    E2, U2 = eng.eigensystem()
+    parts2 = [eng.op_read(op, k) for k in range(len(eng.op_info(op)))]
+    assert max(np.abs(a - b).max() for a, b in zip(E1, E2)) < 1e-15
+    assert max(np.abs(a - b).max() for a, b in zip(U1, U2)) < 1e-15
+    assert max(np.abs(a - b).max() for a, b in zip(parts1, parts2)) < 1e-15
+    eng.graph_replay(gid)  # a second replay is fine
+    g.cdag(m.info.getIndex("B", 0, M.UP))  # defines a new operator
+    with pytest.raises(PgxError):
+        eng.graph_replay(gid)
+    eng.graph_destroy(gid)
