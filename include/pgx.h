@@ -234,6 +234,22 @@ int pgx_g2_count(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, double 
                  long long* count);
 
 /* ------------------------------------------------------------------------
+ * GEMM tile-class autotuning (no counterpart in the reference).  Every
+ * batched product of the library runs in one of nine tile classes; by default
+ * the class is the one that pads the product least.  Between
+ * pgx_autotune_begin and pgx_autotune_end (run the workload once in between)
+ * each batch of products a call launches is first timed under the padding
+ * rule and in every class valid for its (M, N) size bucket, outputs
+ * redirected to scratch, before its real launch; results are unchanged and
+ * those calls are slower.  pgx_autotune_end installs per operand-type
+ * combination and bucket the candidate with the least total time.  Later
+ * calls on the context use it.  changed (may be NULL) receives the number of
+ * buckets that left the padding rule.
+ * ------------------------------------------------------------------------ */
+int pgx_autotune_begin(pgx_ctx* ctx);
+int pgx_autotune_end(pgx_ctx* ctx, int32_t* changed);
+
+/* ------------------------------------------------------------------------
  * CUDA graphs of captured sequences (the reference has no device work to
  * capture).  Between pgx_graph_begin and pgx_graph_end the context's stream
  * is captured instead of run: pgx_eigh (real blocks; after one uncaptured

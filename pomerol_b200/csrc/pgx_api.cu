@@ -72,6 +72,19 @@ Profiler::~Profiler() {
     for (auto e : spare) cudaEventDestroy(e);
 }
 
+GemmTune*& active_tune() {
+    static thread_local GemmTune* t = nullptr;
+    return t;
+}
+int& forced_gemm_class() {
+    static thread_local int f = -1;
+    return f;
+}
+TuneRecorder*& active_recorder() {
+    static thread_local TuneRecorder* r = nullptr;
+    return r;
+}
+
 unsigned long long& alloc_epoch() {
     static unsigned long long e = 0;
     return e;
@@ -167,13 +180,21 @@ template <typename F> int guarded_impl(pgx_ctx* c, bool capture_ok, F&& f) {
     struct Scope {
         pgx::Profiler* saved_p;
         pgx::HostArena* saved_a;
-        explicit Scope(pgx_ctx* c) : saved_p(pgx::active_profiler()), saved_a(pgx::active_arena()) {
+        pgx::GemmTune* saved_t;
+        pgx::TuneRecorder* saved_r;
+        explicit Scope(pgx_ctx* c)
+            : saved_p(pgx::active_profiler()), saved_a(pgx::active_arena()), saved_t(pgx::active_tune()),
+              saved_r(pgx::active_recorder()) {
             pgx::active_profiler() = &c->prof;
             pgx::active_arena() = c->capturing ? c->cap.arena.get() : &c->arena;
+            pgx::active_tune() = c->tuned ? &c->tune : nullptr;
+            pgx::active_recorder() = c->capturing ? nullptr : c->recorder.get();
         }
         ~Scope() {
             pgx::active_profiler() = saved_p;
             pgx::active_arena() = saved_a;
+            pgx::active_tune() = saved_t;
+            pgx::active_recorder() = saved_r;
         }
     } scope(c);
     try {
@@ -432,6 +453,23 @@ int pgx_susc_vjp(pgx_ctx* c, int32_t opA, int32_t opB, int32_t nparts, const int
                   PGX_ERR_ARG, "bad arguments");
         PGX_CHECK(!c->P.w_models, PGX_ERR_STATE, "needs the weights of one model (pgx_weights)");
         pgx::run_susc_vjp(c, opA, opB, nparts, outer, inner, nz, z, pole_res, lambda, dterm, dE);
+    });
+}
+
+int pgx_autotune_begin(pgx_ctx* c) {
+    return guarded(c, [&] {
+        c->recorder.reset(new pgx::TuneRecorder());
+        c->tuned = false;  // the recorded run uses the padding rule
+    });
+}
+
+int pgx_autotune_end(pgx_ctx* c, int32_t* changed) {
+    return guarded(c, [&] {
+        PGX_CHECK(c->recorder != nullptr, PGX_ERR_STATE, "pgx_autotune_begin first");
+        std::unique_ptr<pgx::TuneRecorder> rec = std::move(c->recorder);
+        pgx::active_recorder() = nullptr;
+        const int n = pgx::install_tuning(c, *rec);
+        if (changed) *changed = n;
     });
 }
 

@@ -9,6 +9,7 @@
 // (the signed row gather of a fermionic operator).
 #pragma once
 
+#include <cstring>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -301,6 +302,36 @@ template <typename P> inline int gemm_class(const P& p) {
     return best;
 }
 
+// ------------------------------------------------------------ tuned class choice
+// A context's table of measured-fastest tile classes (pgx_autotune), keyed by
+// the operand types and the (M, N) size buckets; -1 keeps the padding rule.
+// The bucket bounds are the narrow classes' limits (4, 16, 32, 48), so a class
+// measured at a bucket's upper bound is valid for every size in the bucket.
+constexpr int GEMM_BUCKET_REP[GEMM_NBUCKET] = {4, 16, 32, 48, 64, 128, 256};
+inline int gemm_bucket(int x) {
+    return x <= 4 ? 0 : x <= 16 ? 1 : x <= 32 ? 2 : x <= 48 ? 3 : x <= 64 ? 4 : x <= 128 ? 5 : 6;
+}
+template <typename T> struct type_code { static constexpr int v = is_cd<T>::value ? 1 : 0; };
+template <typename T> struct type_code<Dressed<T>> { static constexpr int v = 2 + (is_cd<T>::value ? 1 : 0); };
+template <typename TA, typename TB, typename TC> constexpr int gemm_key() {
+    return type_code<TA>::v * 8 + type_code<TB>::v * 2 + type_code<TC>::v;
+}
+
+inline bool gemm_class_valid(int c, int M, int N) {
+    return (GEMM_CLS_M[c] >= 64 || M <= GEMM_CLS_M[c]) && (GEMM_CLS_N[c] >= 64 || N <= GEMM_CLS_N[c]);
+}
+
+template <typename TA, typename TB, typename TC> int gemm_class_for(const GemmProblem<TA, TB, TC>& p) {
+    const int f = forced_gemm_class();
+    if (f >= 0 && gemm_class_valid(f, p.M, p.N)) return f;
+    const GemmTune* t = active_tune();
+    if (t) {
+        const int c = t->cls[gemm_key<TA, TB, TC>()][gemm_bucket(p.M)][gemm_bucket(p.N)];
+        if (c >= 0 && gemm_class_valid(c, p.M, p.N)) return c;
+    }
+    return gemm_class(p);
+}
+
 template <typename TA, typename TB, typename TC, int BM, int BN>
 void launch_gemm_class(const GemmProblem<TA, TB, TC>* dp, const int* d_index, size_t pb, size_t pe, int ntiles,
                        cudaStream_t st) {
@@ -314,8 +345,52 @@ void launch_gemm_class(const GemmProblem<TA, TB, TC>* dp, const int* d_index, si
 // per tile class.  The index needs gemm_index_bytes(probs.size()) bytes.
 template <typename TA, typename TB, typename TC>
 void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* d_probs, size_t probs_cap,
+                       void* d_index, size_t index_cap, cudaStream_t st);
+
+// Measures a batch for the tuner ahead of its real launch: per (M, N) bucket,
+// the bucket's products run in every candidate class with each output
+// redirected to its own stretch of scratch.  The inputs are read where they
+// are, with the contents the real launch reads.
+template <typename TA, typename TB, typename TC>
+void record_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, cudaStream_t st) {
+    TuneRecorder* rec = active_recorder();
+    for (int mb = 0; mb < GEMM_NBUCKET; ++mb)
+        for (int nb = 0; nb < GEMM_NBUCKET; ++nb) {
+            std::vector<GemmProblem<TA, TB, TC>> grp;
+            size_t bytes = 0;
+            bool redirectable = true;
+            for (const auto& g : probs) {
+                if (g.M <= 0 || g.N <= 0 || gemm_bucket(g.M) != mb || gemm_bucket(g.N) != nb) continue;
+                if (g.sc_i < 0 || g.sc_j < 0 || g.bc < 0) redirectable = false;  // not laid out in scratch
+                // the output's extent: last item's last element
+                const long items = std::max(g.nb, 1);
+                const long last = (items - 1) * g.bc + (long)(g.M - 1) * g.sc_i + (long)(g.N - 1) * g.sc_j;
+                grp.push_back(g);
+                grp.back().C = reinterpret_cast<TC*>(bytes);  // offset into the scratch, made a pointer below
+                bytes += ((size_t)(last + 1) * sizeof(TC) + 255) & ~size_t(255);
+            }
+            if (grp.empty() || !redirectable) continue;
+            tune_measure(*rec, gemm_key<TA, TB, TC>(), mb, nb, bytes,
+                         [&grp](int cls, void* scratch, DevBuf& pb, DevBuf& ib, cudaStream_t s2) {
+                             std::vector<GemmProblem<TA, TB, TC>> q = grp;
+                             for (auto& g : q)
+                                 g.C = reinterpret_cast<TC*>(static_cast<char*>(scratch) +
+                                                             reinterpret_cast<size_t>(g.C));
+                             pb.reserve(q.size() * sizeof(q[0]));
+                             ib.reserve(gemm_index_bytes(q.size()));
+                             forced_gemm_class() = cls;
+                             launch_gemm_batch(q, pb.p, pb.bytes, ib.p, ib.bytes, s2);
+                             forced_gemm_class() = -1;
+                         },
+                         st);
+        }
+}
+
+template <typename TA, typename TB, typename TC>
+void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* d_probs, size_t probs_cap,
                        void* d_index, size_t index_cap, cudaStream_t st) {
     if (probs.empty()) return;
+    if (active_recorder()) record_gemm_batch(probs, st);
     std::vector<GemmProblem<TA, TB, TC>> sorted;
     sorted.reserve(probs.size());
     std::vector<int> index;  // per class: prefix over its problems, then the total
@@ -323,7 +398,7 @@ void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* 
     size_t pstart[GEMM_NCLS + 1] = {}, istart[GEMM_NCLS] = {};
     int ntiles[GEMM_NCLS] = {};
     std::vector<int> cls(probs.size());
-    for (size_t q = 0; q < probs.size(); ++q) cls[q] = gemm_class(probs[q]);
+    for (size_t q = 0; q < probs.size(); ++q) cls[q] = gemm_class_for(probs[q]);
     for (int c = 0; c < GEMM_NCLS; ++c) {
         pstart[c] = sorted.size();
         istart[c] = index.size();

@@ -5,13 +5,42 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <cstring>
+#include <functional>
+#include <map>
 #include <memory>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "pgx_common.cuh"
 
 namespace pgx {
+
+// A context's table of measured-fastest GEMM tile classes (pgx_autotune_end),
+// indexed by operand-type key and the (M, N) size buckets; -1 keeps the
+// padding rule (see gemm_class_for).
+constexpr int GEMM_NKEY = 32, GEMM_NBUCKET = 7;
+struct GemmTune {
+    signed char cls[GEMM_NKEY][GEMM_NBUCKET][GEMM_NBUCKET];
+    GemmTune() { std::memset(cls, -1, sizeof(cls)); }
+};
+GemmTune*& active_tune();   // the running context's table (null: untuned)
+int& forced_gemm_class();   // a class imposed while the tuner measures it (-1: none)
+
+// The tuner (pgx_autotune_begin .. end) measures products where they are
+// launched: while a context records, launch_gemm_batch first runs each size
+// bucket's products in every candidate (the padding rule and every valid
+// class), outputs redirected to scratch, and adds the times to the context's
+// TuneRecorder (defined below DevBuf).
+struct TuneRecorder;
+TuneRecorder*& active_recorder();  // non-null while a context records
+struct DevBuf;
+// launch(cls, scratch, probs, index, st): the bucket's products in class cls
+// (-1: the padding rule), outputs in scratch, descriptors in probs and index.
+using TuneLaunch = std::function<void(int cls, void* scratch, DevBuf& probs, DevBuf& index, cudaStream_t st)>;
+void tune_measure(TuneRecorder& rec, int key, int mb, int nb, size_t c_bytes, const TuneLaunch& launch,
+                  cudaStream_t st);
 
 // Counts device allocations and frees in the process: a captured CUDA graph
 // records it and refuses to replay once any buffer may have moved.
@@ -62,6 +91,19 @@ struct DevBuf {
         bytes = 0;
     }
     template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// Times of the products measured since pgx_autotune_begin, per (operand-type
+// key, M bucket, N bucket): index 0 the padding rule, c + 1 tile class c
+// (DBL_MAX where c is not valid for the bucket).
+struct TuneRecorder {
+    std::map<std::tuple<int, int, int>, std::vector<double>> total;
+    DevBuf scratch, probs, index;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    TuneRecorder() = default;
+    TuneRecorder(const TuneRecorder&) = delete;
+    TuneRecorder& operator=(const TuneRecorder&) = delete;
+    ~TuneRecorder();
 };
 
 // One rotated monomial operator.
@@ -250,6 +292,9 @@ struct pgx_ctx {
     Graph cap;                                  // the graph being captured
     unsigned long problem_gen = 0;              // bumped by pgx_set_blocks
     unsigned long ops_gen = 0;                  // bumped when operators are defined, formed or released
+    pgx::GemmTune tune;                         // pgx_autotune_end's measured tile classes
+    bool tuned = false;
+    std::unique_ptr<pgx::TuneRecorder> recorder;  // open between pgx_autotune_begin and end
 };
 
 namespace pgx {
@@ -311,6 +356,7 @@ void run_gf_models(pgx_ctx* c, int op1, int op2, int nparts, const int32_t* oute
                    const double* z, double coef_tol, double* out);
 void run_susc_models(pgx_ctx* c, int opA, int opB, int nparts, const int32_t* outer, const int32_t* inner, int nz,
                      const double* z, double pole_res, double coef_tol, double* out, double* zero_pole);
+int install_tuning(pgx_ctx* c, const TuneRecorder& rec);
 void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_tol, double nz_tol, long long* count);
 
 }  // namespace pgx

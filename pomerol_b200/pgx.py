@@ -24,7 +24,8 @@ EXPORTS = [
     "pgx_ensemble_average", "pgx_g2", "pgx_g2_count", "pgx_g2_last_timing", "pgx_timer_begin", "pgx_timer_end",
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
-    "pgx_gf_vjp", "pgx_susc_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_graph_begin", "pgx_graph_end",
+    "pgx_gf_vjp", "pgx_susc_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_autotune_begin", "pgx_autotune_end",
+    "pgx_graph_begin", "pgx_graph_end",
     "pgx_graph_replay", "pgx_graph_destroy", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
 ]
 
@@ -86,6 +87,8 @@ def load():
         lib.pgx_susc_vjp.argtypes = [P, I32, I32, I32, P, P, I32, P, D, P, P, P]
         lib.pgx_chi3.argtypes = [P, I32, I32, P, I32, P, D, P]
         lib.pgx_set_eigensystem.argtypes = [P, P, P]
+        lib.pgx_autotune_begin.argtypes = [P]
+        lib.pgx_autotune_end.argtypes = [P, P]
         lib.pgx_graph_begin.argtypes = [P]
         lib.pgx_graph_end.argtypes = [P, P]
         lib.pgx_graph_replay.argtypes = [P, I32]
@@ -412,6 +415,19 @@ def _load_eigensystem(self, path):
     self.set_eigensystem(E, U)
 
 
+def _autotune_begin(self):
+    """Record the GEMM products of the following calls for autotune_end()."""
+    self._ck(self.lib.pgx_autotune_begin(self.h))
+
+
+def _autotune_end(self):
+    """Time the recorded products in every tile class and keep the fastest per
+    size bucket; returns the number of buckets that left the padding rule."""
+    n = np.zeros(1, dtype=np.int32)
+    self._ck(self.lib.pgx_autotune_end(self.h, _p(n)))
+    return int(n[0])
+
+
 def _graph_begin(self):
     """Start capturing eigh() / op_rotate() calls into a CUDA graph."""
     self._ck(self.lib.pgx_graph_begin(self.h))
@@ -505,6 +521,8 @@ Engine.susc_vjp = _susc_vjp
 Engine.chi3 = _chi3
 Engine.set_models = _set_models
 Engine.graph_begin = _graph_begin
+Engine.autotune_begin = _autotune_begin
+Engine.autotune_end = _autotune_end
 Engine.graph_end = _graph_end
 Engine.graph_replay = _graph_replay
 Engine.graph_destroy = _graph_destroy

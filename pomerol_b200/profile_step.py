@@ -25,6 +25,8 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="the first M models of the batch workload")
     ap.add_argument("--chain", action="store_true", help="time the drop-in chain stage by stage")
     ap.add_argument("--g2-cubes", type=int, nargs="*", default=[], help="cube sides for the G2 stage of --chain")
+    ap.add_argument("--autotune", action="store_true",
+                    help="measure the GEMM tile classes on one step (after one untimed step) before timing")
     a = ap.parse_args()
     if a.chain:
         chain(a.config, a.g2_cubes)
@@ -33,6 +35,8 @@ def main():
     from .workloads import BatchRun, Chi3Run, EngineRun, Problem, b64_params, matsubara_cube, matsubara_square
     if a.batch:
         run = BatchRun(b64_params()[:a.batch])
+        if a.autotune:
+            autotune(run.eng, run.step)
         for s in range(a.steps):
             last = a.kernels and s == a.steps - 1
             if last:
@@ -55,6 +59,8 @@ def main():
     else:
         _, z = matsubara_cube(prob.beta, prob.nfreq)
         run = EngineRun(prob)
+    if a.autotune:
+        autotune(run.eng, lambda: run.step(z))
     for s in range(a.steps):
         t0 = time.perf_counter()
         last = a.kernels and s == a.steps - 1
@@ -70,6 +76,15 @@ def main():
         extra = "" if a.chi3 else f"g2 {run.eng.g2_timing()}, "
         print(f"step {s}: device {ms:.1f} ms, wall {1e3 * (time.perf_counter() - t0):.1f} ms, "
               f"{extra}|v|max {np.abs(v).max():.4e}", flush=True)
+
+
+def autotune(eng, step):
+    step()  # sizes every buffer
+    eng.autotune_begin()
+    step()
+    t0 = time.perf_counter()
+    n = eng.autotune_end()
+    print(f"autotune: {n} size buckets off the padding rule ({1e3 * (time.perf_counter() - t0):.1f} ms)", flush=True)
 
 
 def chain(config, cubes):

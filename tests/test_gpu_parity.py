@@ -973,3 +973,35 @@ def test_graph_capture_and_replay(harness):
     with pytest.raises(PgxError):
         eng.graph_replay(gid)
     eng.graph_destroy(gid)
+
+
+def test_autotune_keeps_results(harness):
+    """pgx_autotune_begin / end time the GEMM products of an eigensolve and a
+    plaquette G2 in every tile class on this GPU; the G2 measured meanwhile
+    and the tuned
+    context's eigensystem and G2 agree with the untuned ones (different tile
+    shapes change only the summation order: 1e-13)."""
+    beta = 10.0
+    m = M.make_model(M.plaquette())
+    g = harness(m, beta)
+    u, d = m.info.getIndex("A", 0, 1), m.info.getIndex("A", 0, 0)
+    trip = [(a, b, x) for a in range(-2, 2) for b in range(-2, 2) for x in range(-2, 2)]
+    fz = np.array([L.fermionic(np.array(t), beta) for t in trip])
+    v0, _ = g.g2(g.c(u), g.c(d), g.cdag(u), g.cdag(d), fz)
+    E0, U0 = g.eng.eigensystem()
+    g.eng.autotune_begin()
+    g.eng.eigh()
+    g.w, g.Z = g.eng.weights(beta)
+    g._cdag, g._c = {}, {}  # rotated again, under measurement
+    vr, _ = g.g2(g.c(u), g.c(d), g.cdag(u), g.cdag(d), fz)
+    changed = g.eng.autotune_end()
+    assert np.abs(vr - v0).max() < 1e-13 * np.abs(v0).max()  # measuring leaves the real launches alone
+    assert changed >= 0
+    g.eng.eigh()
+    E1, U1 = g.eng.eigensystem()
+    assert max(np.abs(a - b).max() for a, b in zip(E0, E1)) < 1e-13
+    g.E, g.U = E1, U1
+    g.w, g.Z = g.eng.weights(beta)
+    g._cdag, g._c = {}, {}
+    v1, _ = g.g2(g.c(u), g.c(d), g.cdag(u), g.cdag(d), fz)
+    assert np.abs(v1 - v0).max() < 1e-13 * np.abs(v0).max()
