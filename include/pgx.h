@@ -227,6 +227,15 @@ typedef struct pgx_g2_part {
 int pgx_g2(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, int32_t nfreq, const double* z,
            double pole_res, double coef_tol, int32_t flags, double* out);
 
+/* Device workspace limits of pgx_g2's anchored form (0 keeps a default).
+ * batch_bytes: parts are evaluated together while their workspaces fit in it
+ * (default 3 GiB).  chain_bytes: the most one part may take (default half the
+ * free device memory, at most 48 GiB); a part that needs more at the call's
+ * frequency count is evaluated in tiles of the (z1, z3) plane, each with all
+ * of its triples' z2.  Results do not depend on either limit beyond the
+ * summation order. */
+int pgx_set_g2_workspace(pgx_ctx* ctx, int64_t batch_bytes, int64_t chain_bytes);
+
 /* Number of state quadruples the reference enumerates for these parts
  * (TwoParticleGFPart.cpp:210-250): all four rotated elements |x| > nz_tol and
  * w1 + w2 + w3 + w4 > coef_tol.  The work unit of the G2 throughput metric. */

@@ -456,6 +456,14 @@ int pgx_susc_vjp(pgx_ctx* c, int32_t opA, int32_t opB, int32_t nparts, const int
     });
 }
 
+int pgx_set_g2_workspace(pgx_ctx* c, int64_t batch_bytes, int64_t chain_bytes) {
+    return guarded(c, [&] {
+        PGX_CHECK(batch_bytes >= 0 && chain_bytes >= 0, PGX_ERR_ARG, "workspace limits must be >= 0");
+        c->g2_batch_bytes = batch_bytes;
+        c->g2_chain_bytes = chain_bytes;
+    });
+}
+
 int pgx_autotune_begin(pgx_ctx* c) {
     return guarded(c, [&] {
         c->recorder.reset(new pgx::TuneRecorder());

@@ -56,6 +56,7 @@ struct DTerm {
     int va_cplx, vb_cplx; // operand element types
     int va_hstate, vb_hstate;  // h stride applies to the anchor's state index instead of its position
     int use_delta;
+    int nt;               // triples of the plan (work count only)
     double sgn, cdelta, cnum, pref;
 };
 
@@ -188,81 +189,116 @@ __global__ void __launch_bounds__(256) dterm_kernel(const DTerm* terms, const in
     }
 }
 
-struct APlan {
-    std::vector<cd> Z1, Z3;
-    std::vector<int> i1, i3;
-    std::vector<cd> s[4];
-    std::vector<int> gt, goff, gi1, gi3;  // triples grouped by (i1, i3)
-    DevBuf buf;
-    cd *dZ1 = nullptr, *dZ3 = nullptr, *ds[4] = {nullptr, nullptr, nullptr, nullptr};
-    int *di1 = nullptr, *di3 = nullptr;
-    int *dgt = nullptr, *dgoff = nullptr, *dgi1 = nullptr, *dgi3 = nullptr;
-};
+// Frequencies of one permutation of a G2 part: triple t as (z1', z2', z3')
+// = the permuted (z1, z2, -z3), with z1' dressing O1 and z3' dressing O3.
+inline void perm_freqs(const double* z, int t, const int perm[3], cd& a, cd& b, cd& c) {
+    const cd F[3] = {cd{z[6 * t], z[6 * t + 1]}, cd{z[6 * t + 2], z[6 * t + 3]}, cd{-z[6 * t + 4], -z[6 * t + 5]}};
+    a = F[perm[0]];
+    b = F[perm[1]];
+    c = F[perm[2]];
+}
 
 struct KeyC {
     double a, b;
     bool operator<(const KeyC& o) const { return std::tie(a, b) < std::tie(o.a, o.b); }
 };
 
-void build_aplan(APlan& pl, const int perm[3], int nfreq, const double* z, cudaStream_t st) {
-    std::map<KeyC, int> m1, m3;
-    pl.i1.resize(nfreq);
-    pl.i3.resize(nfreq);
-    for (auto& v : pl.s) v.resize(nfreq);
+// Per triple id (every triple of the call), the four frequency sums the
+// contractions use under one permutation: z2', z1'+z2'+z3', z1'+z2', z2'+z3'.
+struct PermSums {
+    DevBuf buf;
+    const cd* ds[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+void build_sums(PermSums& ps, const int perm[3], int nfreq, const double* z, cudaStream_t st) {
+    std::vector<cd> h(4 * (size_t)nfreq);
     for (int t = 0; t < nfreq; ++t) {
-        const cd F[3] = {cd{z[6 * t], z[6 * t + 1]}, cd{z[6 * t + 2], z[6 * t + 3]}, cd{-z[6 * t + 4], -z[6 * t + 5]}};
-        const cd a = F[perm[0]], b = F[perm[1]], c = F[perm[2]];
-        auto x1 = m1.emplace(KeyC{a.x, a.y}, (int)pl.Z1.size());
-        if (x1.second) pl.Z1.push_back(a);
-        auto x3 = m3.emplace(KeyC{c.x, c.y}, (int)pl.Z3.size());
-        if (x3.second) pl.Z3.push_back(c);
-        pl.i1[t] = x1.first->second;
-        pl.i3[t] = x3.first->second;
-        pl.s[0][t] = b;
-        pl.s[1][t] = a + b + c;
-        pl.s[2][t] = a + b;
-        pl.s[3][t] = b + c;
+        cd a, b, c;
+        perm_freqs(z, t, perm, a, b, c);
+        h[t] = b;
+        h[nfreq + t] = a + b + c;
+        h[2 * (size_t)nfreq + t] = a + b;
+        h[3 * (size_t)nfreq + t] = b + c;
     }
-    pl.gt.resize(nfreq);
-    for (int t = 0; t < nfreq; ++t) pl.gt[t] = t;
+    ps.buf.reserve(std::max<size_t>(h.size(), 1) * sizeof(cd));
+    if (!h.empty()) h2d(ps.buf.p, h.data(), h.size() * sizeof(cd), st);
+    for (int k = 0; k < 4; ++k) ps.ds[k] = ps.buf.as<cd>() + (size_t)k * nfreq;
+}
+
+// Distinct z1' and z3' of all triples of a call under one permutation, in
+// order of first appearance, and each triple's index into them.
+struct PermIndex {
+    std::vector<cd> Z1, Z3;
+    std::vector<int> j1, j3;
+};
+
+void index_perm(PermIndex& ix, const int perm[3], int nfreq, const double* z) {
+    std::map<KeyC, int> m1, m3;
+    ix.j1.resize(nfreq);
+    ix.j3.resize(nfreq);
+    for (int t = 0; t < nfreq; ++t) {
+        cd a, b, c;
+        perm_freqs(z, t, perm, a, b, c);
+        auto x1 = m1.emplace(KeyC{a.x, a.y}, (int)ix.Z1.size());
+        if (x1.second) ix.Z1.push_back(a);
+        auto x3 = m3.emplace(KeyC{c.x, c.y}, (int)ix.Z3.size());
+        if (x3.second) ix.Z3.push_back(c);
+        ix.j1[t] = x1.first->second;
+        ix.j3[t] = x3.first->second;
+    }
+}
+
+// The triples of one tile of a permutation's (z1', z3') plane: z1' indices
+// [o1, o1 + n1) and z3' indices [o3, o3 + n3) of its PermIndex, the triples
+// grouped by (z1', z3'), each group one warp's work in the contraction.
+struct APlan {
+    std::vector<cd> Z1, Z3;
+    std::vector<int> gt, goff, gi1, gi3;  // triple ids grouped by (i1, i3)
+    DevBuf buf;
+    cd *dZ1 = nullptr, *dZ3 = nullptr;
+    const cd* ds[4] = {nullptr, nullptr, nullptr, nullptr};  // the permutation's sums
+    int *dgt = nullptr, *dgoff = nullptr, *dgi1 = nullptr, *dgi3 = nullptr;
+};
+
+void build_aplan(APlan& pl, const std::vector<int>& tids, const PermIndex& ix, int o1, int n1, int o3, int n3,
+                 const PermSums& ps, cudaStream_t st) {
+    pl.Z1.assign(ix.Z1.begin() + o1, ix.Z1.begin() + o1 + n1);
+    pl.Z3.assign(ix.Z3.begin() + o3, ix.Z3.begin() + o3 + n3);
+    const size_t nt = tids.size();
+    pl.gt = tids;
     std::stable_sort(pl.gt.begin(), pl.gt.end(), [&](int x, int y) {
-        return std::make_pair(pl.i1[x], pl.i3[x]) < std::make_pair(pl.i1[y], pl.i3[y]);
+        return std::make_pair(ix.j1[x], ix.j3[x]) < std::make_pair(ix.j1[y], ix.j3[y]);
     });
-    for (int q = 0; q < nfreq; ++q) {
+    for (size_t q = 0; q < nt; ++q) {
         const int t = pl.gt[q];
-        if (q == 0 || pl.i1[t] != pl.i1[pl.gt[q - 1]] || pl.i3[t] != pl.i3[pl.gt[q - 1]]) {
-            pl.goff.push_back(q);
-            pl.gi1.push_back(pl.i1[t]);
-            pl.gi3.push_back(pl.i3[t]);
+        if (q == 0 || ix.j1[t] != ix.j1[pl.gt[q - 1]] || ix.j3[t] != ix.j3[pl.gt[q - 1]]) {
+            pl.goff.push_back((int)q);
+            pl.gi1.push_back(ix.j1[t] - o1);
+            pl.gi3.push_back(ix.j3[t] - o3);
         }
     }
-    pl.goff.push_back(nfreq);
-    const size_t n1 = pl.Z1.size(), n3 = pl.Z3.size(), nf = nfreq, ng = pl.gi1.size();
-    pl.buf.reserve((n1 + n3 + 4 * nf) * sizeof(cd) + (3 * nf + 3 * ng + 1) * sizeof(int) + 256);
+    pl.goff.push_back((int)nt);
+    for (int k = 0; k < 4; ++k) pl.ds[k] = ps.ds[k];
+    const size_t ng = pl.gi1.size();
+    pl.buf.reserve((size_t)(n1 + n3) * sizeof(cd) + (nt + 3 * ng + 1) * sizeof(int) + 256);
     char* p = pl.buf.as<char>();
     auto take = [&](size_t b) {
         char* r = p;
         p += (b + 15) & ~size_t(15);
         return r;
     };
-    pl.dZ1 = reinterpret_cast<cd*>(take(n1 * sizeof(cd)));
-    pl.dZ3 = reinterpret_cast<cd*>(take(n3 * sizeof(cd)));
-    for (int k = 0; k < 4; ++k) pl.ds[k] = reinterpret_cast<cd*>(take(nf * sizeof(cd)));
-    pl.di1 = reinterpret_cast<int*>(take(nf * sizeof(int)));
-    pl.di3 = reinterpret_cast<int*>(take(nf * sizeof(int)));
-    pl.dgt = reinterpret_cast<int*>(take(nf * sizeof(int)));
+    pl.dZ1 = reinterpret_cast<cd*>(take((size_t)n1 * sizeof(cd)));
+    pl.dZ3 = reinterpret_cast<cd*>(take((size_t)n3 * sizeof(cd)));
+    pl.dgt = reinterpret_cast<int*>(take(nt * sizeof(int)));
     pl.dgoff = reinterpret_cast<int*>(take((ng + 1) * sizeof(int)));
     pl.dgi1 = reinterpret_cast<int*>(take(ng * sizeof(int)));
     pl.dgi3 = reinterpret_cast<int*>(take(ng * sizeof(int)));
     auto up = [&](void* d, const void* h, size_t b) {
         if (b) h2d(d, h, b, st);
     };
-    up(pl.dZ1, pl.Z1.data(), n1 * sizeof(cd));
-    up(pl.dZ3, pl.Z3.data(), n3 * sizeof(cd));
-    for (int k = 0; k < 4; ++k) up(pl.ds[k], pl.s[k].data(), nf * sizeof(cd));
-    up(pl.di1, pl.i1.data(), nf * sizeof(int));
-    up(pl.di3, pl.i3.data(), nf * sizeof(int));
-    up(pl.dgt, pl.gt.data(), nf * sizeof(int));
+    up(pl.dZ1, pl.Z1.data(), (size_t)n1 * sizeof(cd));
+    up(pl.dZ3, pl.Z3.data(), (size_t)n3 * sizeof(cd));
+    up(pl.dgt, pl.gt.data(), nt * sizeof(int));
     up(pl.dgoff, pl.goff.data(), (ng + 1) * sizeof(int));
     up(pl.dgi1, pl.gi1.data(), ng * sizeof(int));
     up(pl.dgi3, pl.gi3.data(), ng * sizeof(int));
@@ -313,10 +349,10 @@ GemmProblem<TA, TB, cd> gp(const typename src_t<TA>::type* A, long sai, long sak
 }  // namespace
 
 template <typename T>
-static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part* parts, const std::vector<int>& part_plan,
-                      std::vector<APlan>& plans, const std::vector<std::array<int, 4>>& rs,
-                      const std::vector<ChainWs>& wsl, cd* pool, const int* d_hot, const std::vector<long>& hot_off,
-                      double pole_res, int nfreq, cd* d_out) {
+static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector<int>& bplan,
+                      const std::vector<ChainWs>& wsl, const pgx_g2_part* parts, const std::vector<APlan>& plans,
+                      const std::vector<std::array<int, 4>>& rs, cd* pool, const int* d_hot,
+                      const std::vector<long>& hot_off, double pole_res, cd* d_out) {
     Problem& P = c->P;
     cudaStream_t st = c->stream;
     constexpr bool TC = is_cd<T>::value;
@@ -328,10 +364,11 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
     std::vector<GemmProblem<DT, T, cd>> pb;   // dressed x operator
     std::vector<GemmProblem<DT, cd, cd>> pc;  // dressed x stacked anchors (per z1 or z3)
     std::vector<GemmProblem<cd, DT, cd>> pd;  // stacked anchors x dressed
-    for (int q : idx) {
+    for (size_t j = 0; j < idx.size(); ++j) {
+        const int q = idx[j];
         const pgx_g2_part& g = parts[q];
-        const APlan& pl = plans[part_plan[q]];
-        const ChainWs& w = wsl[q];
+        const APlan& pl = plans[bplan[j]];
+        const ChainWs& w = wsl[j];
         const int S1 = g.block[0], S2 = g.block[1], S3 = g.block[2], S4 = g.block[3];
         const int d1 = P.dims[S1], d2 = P.dims[S2], d3 = P.dims[S3], d4 = P.dims[S4];
         const int r1 = rs[q][0], r2 = rs[q][1], r3 = rs[q][2], r4 = rs[q][3];
@@ -390,10 +427,11 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
     launch(pd);
     // ---- contractions per triple
     std::vector<DTerm> dt;
-    for (int q : idx) {
+    for (size_t j = 0; j < idx.size(); ++j) {
+        const int q = idx[j];
         const pgx_g2_part& g = parts[q];
-        const APlan& pl = plans[part_plan[q]];
-        const ChainWs& w = wsl[q];
+        const APlan& pl = plans[bplan[j]];
+        const ChainWs& w = wsl[j];
         const int S[4] = {g.block[0], g.block[1], g.block[2], g.block[3]};
         const int d1 = P.dims[S[0]], d2 = P.dims[S[1]], d3 = P.dims[S[2]], d4 = P.dims[S[3]];
         const int r1 = rs[q][0], r2 = rs[q][1], r3 = rs[q][2], r4 = rs[q][3];
@@ -423,6 +461,7 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
             d.gi1 = pl.dgi1;
             d.gi3 = pl.dgi3;
             d.ng = (int)pl.gi1.size();
+            d.nt = (int)pl.gt.size();
             d.sgn = sgn;
             d.use_delta = use_delta;
             d.cdelta = cd_;
@@ -481,7 +520,7 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const pgx_g2_part
         double elems = 0.0;
         for (size_t q = 0; q < dt.size(); ++q) {
             woff[q + 1] = woff[q] + dt[q].ng;
-            elems += (double)dt[q].nh * dt[q].nk * nfreq;
+            elems += (double)dt[q].nh * dt[q].nk * dt[q].nt;
         }
         DevBuf& bd = c->scratch[3];
         const size_t tb = (dt.size() * sizeof(DTerm) + 255) & ~size_t(255);
@@ -520,55 +559,29 @@ void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq
     DevBuf& bh = c->scratch[11];
     bh.reserve(std::max<size_t>(hot.size(), 1) * sizeof(int));
     if (!hot.empty()) h2d(bh.p, hot.data(), hot.size() * sizeof(int), st);
-    // frequency plans per permutation
+    // permutations of the parts, and the frequency sums of each
     std::map<std::tuple<int, int, int>, int> perm_id;
-    std::vector<APlan> plans;
-    plans.reserve(6);
-    std::vector<int> part_plan(nparts);
+    std::vector<std::array<int, 3>> perms;
+    std::vector<int> part_perm(nparts);
     for (int q = 0; q < nparts; ++q) {
         auto key = std::make_tuple(parts[q].perm[0], parts[q].perm[1], parts[q].perm[2]);
         auto it = perm_id.find(key);
         if (it == perm_id.end()) {
-            it = perm_id.emplace(key, (int)plans.size()).first;
-            plans.emplace_back();
-            const int perm[3] = {parts[q].perm[0], parts[q].perm[1], parts[q].perm[2]};
-            build_aplan(plans.back(), perm, nfreq, z, st);
+            it = perm_id.emplace(key, (int)perms.size()).first;
+            perms.push_back({parts[q].perm[0], parts[q].perm[1], parts[q].perm[2]});
         }
-        part_plan[q] = it->second;
+        part_perm[q] = it->second;
     }
-    // workspace per chain and batching under a memory budget
+    std::vector<PermSums> sums(perms.size());
+    for (size_t p = 0; p < perms.size(); ++p) build_sums(sums[p], perms[p].data(), nfreq, z, st);
+    // anchor counts per part, and the workspace of one chain for N1 x N3 frequencies
     std::vector<std::array<int, 4>> rs(nparts);
-    std::vector<ChainWs> wsl(nparts);
-    const long budget = (long)(3L << 30) / (long)sizeof(cd);
-    DevBuf& pool_b = c->scratch[6];
-    DevBuf& out_b = c->scratch[9];
-    out_b.reserve(std::max(nfreq, 1) * sizeof(cd));
-    PGX_CUDA(cudaMemsetAsync(out_b.p, 0, std::max(nfreq, 1) * sizeof(cd), st));
-    std::vector<int> batch;
-    long used = 0;
-    auto flush = [&]() {
-        if (batch.empty()) return;
-        pool_b.reserve(std::max<long>(used, 1) * sizeof(cd));
-        if (P.is_complex)
-            run_batch<cd>(c, batch, parts, part_plan, plans, rs, wsl, pool_b.as<cd>(), bh.as<int>(), hot_off, pole_res,
-                          nfreq, out_b.as<cd>());
-        else
-            run_batch<double>(c, batch, parts, part_plan, plans, rs, wsl, pool_b.as<cd>(), bh.as<int>(), hot_off,
-                              pole_res, nfreq, out_b.as<cd>());
-        batch.clear();
-        used = 0;
-    };
-    for (int q = 0; q < nparts; ++q) {
-        const pgx_g2_part& g = parts[q];
-        int r[4], d[4];
-        for (int k = 0; k < 4; ++k) {
-            r[k] = nhot[g.block[k]];
-            d[k] = P.dims[g.block[k]];
-        }
-        rs[q] = {r[0], r[1], r[2], r[3]};
-        if (r[0] + r[1] + r[2] + r[3] == 0) continue;
-        const APlan& pl = plans[part_plan[q]];
-        const long N1 = (long)pl.Z1.size(), N3 = (long)pl.Z3.size();
+    for (int q = 0; q < nparts; ++q)
+        for (int k = 0; k < 4; ++k) rs[q][k] = nhot[parts[q].block[k]];
+    auto chain_ws = [&](int q, long N1, long N3) {
+        int d[4];
+        for (int k = 0; k < 4; ++k) d[k] = P.dims[parts[q].block[k]];
+        const auto& r = rs[q];
         ChainWs x{};
         long o = 0;
         auto take = [&](long n) {
@@ -589,14 +602,100 @@ void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq
         x.V2a = take(N3 * N1 * r[0] * d[3]);
         x.V2b = take(N1 * d[0] * N3 * r[3]);
         x.end = o;
-        if (used > 0 && used + x.end > budget) flush();
-        for (long* f : {&x.Lc, &x.Lr, &x.Pr, &x.Pc, &x.Rho, &x.Qc, &x.Rr, &x.Rc, &x.V1a, &x.V1b, &x.V2a,
-                        &x.V2b, &x.end})
-            *f += used;
-        wsl[q] = x;
-        used = x.end;
-        batch.push_back(q);
+        return x;
+    };
+    auto active = [&](int q) { return rs[q][0] + rs[q][1] + rs[q][2] + rs[q][3] > 0; };
+    // Parts are batched up to `budget` of workspace.  One chain may take up to
+    // `tile_budget` (by default half the free device memory, at most 48 GiB); beyond it
+    // the permutation's (z1', z3') plane is cut into tiles, each with all of
+    // its triples' z2'.  The stacked products are per (z1', z3') pair, so
+    // tiling does not repeat them; the per-z1' and per-z3' anchored products
+    // are repeated once per tile row or column.
+    const long budget = (long)((c->g2_batch_bytes > 0 ? c->g2_batch_bytes : (3LL << 30)) / (long long)sizeof(cd));
+    long tile_budget = -1;  // resolved when a chain exceeds the batch budget
+    auto chain_limit = [&]() {
+        if (tile_budget >= 0) return tile_budget;
+        if (c->g2_chain_bytes > 0) {
+            tile_budget = (long)(c->g2_chain_bytes / (long long)sizeof(cd));
+        } else {
+            size_t free_b = 0, total_b = 0;
+            PGX_CUDA(cudaMemGetInfo(&free_b, &total_b));
+            tile_budget = std::max(budget, (long)(std::min<size_t>(free_b / 2, size_t(48) << 30) / sizeof(cd)));
+        }
+        return tile_budget;
+    };
+    std::vector<APlan> plans;
+    std::vector<std::vector<int>> perm_plans(perms.size());
+    for (size_t p = 0; p < perms.size(); ++p) {
+        PermIndex ix;
+        index_perm(ix, perms[p].data(), nfreq, z);
+        const long N1 = (long)ix.Z1.size(), N3 = (long)ix.Z3.size();
+        auto fits = [&](long b) {
+            for (int q = 0; q < nparts; ++q) {
+                if (part_perm[q] != (int)p || !active(q)) continue;
+                const long e = chain_ws(q, std::min(N1, b), std::min(N3, b)).end;
+                if (e > budget && e > chain_limit()) return false;
+            }
+            return true;
+        };
+        long B = std::max<long>(1, std::max(N1, N3));
+        while (B > 1 && !fits(B)) B = std::max<long>(1, std::min(B - 1, B * 3 / 4));
+        const long T1 = ceil_div(std::max<long>(N1, 1), std::min(std::max<long>(N1, 1), B));
+        const long T3 = ceil_div(std::max<long>(N3, 1), std::min(std::max<long>(N3, 1), B));
+        const long b1 = ceil_div(std::max<long>(N1, 1), T1), b3 = ceil_div(std::max<long>(N3, 1), T3);
+        std::vector<std::vector<int>> tiles((size_t)(T1 * T3));
+        if (T1 * T3 == 1) {
+            tiles[0].resize(nfreq);
+            for (int t = 0; t < nfreq; ++t) tiles[0][t] = t;
+        } else {
+            for (int t = 0; t < nfreq; ++t) tiles[(size_t)((ix.j1[t] / b1) * T3 + ix.j3[t] / b3)].push_back(t);
+        }
+        for (long u = 0; u < T1; ++u)
+            for (long v = 0; v < T3; ++v) {
+                const auto& tl = tiles[(size_t)(u * T3 + v)];
+                if (tl.empty()) continue;
+                const int o1 = (int)(u * b1), o3 = (int)(v * b3);
+                const int n1 = (int)std::min(b1, N1 - o1), n3 = (int)std::min(b3, N3 - o3);
+                perm_plans[p].push_back((int)plans.size());
+                plans.emplace_back();
+                build_aplan(plans.back(), tl, ix, o1, n1, o3, n3, sums[p], st);
+            }
     }
+    DevBuf& pool_b = c->scratch[6];
+    DevBuf& out_b = c->scratch[9];
+    out_b.reserve(std::max(nfreq, 1) * sizeof(cd));
+    PGX_CUDA(cudaMemsetAsync(out_b.p, 0, std::max(nfreq, 1) * sizeof(cd), st));
+    std::vector<int> batch, bplan;
+    std::vector<ChainWs> bws;
+    long used = 0;
+    auto flush = [&]() {
+        if (batch.empty()) return;
+        pool_b.reserve(std::max<long>(used, 1) * sizeof(cd));
+        if (P.is_complex)
+            run_batch<cd>(c, batch, bplan, bws, parts, plans, rs, pool_b.as<cd>(), bh.as<int>(), hot_off, pole_res,
+                          out_b.as<cd>());
+        else
+            run_batch<double>(c, batch, bplan, bws, parts, plans, rs, pool_b.as<cd>(), bh.as<int>(), hot_off, pole_res,
+                              out_b.as<cd>());
+        batch.clear();
+        bplan.clear();
+        bws.clear();
+        used = 0;
+    };
+    for (size_t p = 0; p < perms.size(); ++p)
+        for (int pid : perm_plans[p])
+            for (int q = 0; q < nparts; ++q) {
+                if (part_perm[q] != (int)p || !active(q)) continue;
+                ChainWs x = chain_ws(q, (long)plans[pid].Z1.size(), (long)plans[pid].Z3.size());
+                if (used > 0 && used + x.end > budget) flush();
+                for (long* f : {&x.Lc, &x.Lr, &x.Pr, &x.Pc, &x.Rho, &x.Qc, &x.Rr, &x.Rc, &x.V1a, &x.V1b, &x.V2a,
+                                &x.V2b, &x.end})
+                    *f += used;
+                used = x.end;
+                batch.push_back(q);
+                bplan.push_back(pid);
+                bws.push_back(x);
+            }
     flush();
     PGX_CUDA(cudaMemcpyAsync(out, out_b.p, nfreq * sizeof(cd), cudaMemcpyDeviceToHost, st));
     PGX_CUDA(cudaStreamSynchronize(st));

@@ -274,6 +274,7 @@ struct pgx_ctx {
     cudaEvent_t ev_begin = nullptr, ev_end = nullptr;
     // side streams (and their fork / join events) for independent launches
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
+    long long g2_batch_bytes = 0, g2_chain_bytes = 0;  // pgx_set_g2_workspace (0: defaults)
     cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
     // scratch for G2 and Lehmann kernels
     pgx::DevBuf scratch[12];

@@ -25,7 +25,7 @@ EXPORTS = [
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
     "pgx_gf_vjp", "pgx_susc_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_autotune_begin", "pgx_autotune_end",
-    "pgx_graph_begin", "pgx_graph_end",
+    "pgx_set_g2_workspace", "pgx_graph_begin", "pgx_graph_end",
     "pgx_graph_replay", "pgx_graph_destroy", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
 ]
 
@@ -88,6 +88,7 @@ def load():
         lib.pgx_chi3.argtypes = [P, I32, I32, P, I32, P, D, P]
         lib.pgx_set_eigensystem.argtypes = [P, P, P]
         lib.pgx_autotune_begin.argtypes = [P]
+        lib.pgx_set_g2_workspace.argtypes = [P, C.c_int64, C.c_int64]
         lib.pgx_autotune_end.argtypes = [P, P]
         lib.pgx_graph_begin.argtypes = [P]
         lib.pgx_graph_end.argtypes = [P, P]
@@ -415,6 +416,12 @@ def _load_eigensystem(self, path):
     self.set_eigensystem(E, U)
 
 
+def _set_g2_workspace(self, batch_bytes=0, chain_bytes=0):
+    """Workspace limits of the anchored G2 (0 keeps a default); a part whose
+    workspace exceeds chain_bytes is evaluated in (z1, z3) tiles."""
+    self._ck(self.lib.pgx_set_g2_workspace(self.h, int(batch_bytes), int(chain_bytes)))
+
+
 def _autotune_begin(self):
     """Record the GEMM products of the following calls for autotune_end()."""
     self._ck(self.lib.pgx_autotune_begin(self.h))
@@ -521,6 +528,7 @@ Engine.susc_vjp = _susc_vjp
 Engine.chi3 = _chi3
 Engine.set_models = _set_models
 Engine.graph_begin = _graph_begin
+Engine.set_g2_workspace = _set_g2_workspace
 Engine.autotune_begin = _autotune_begin
 Engine.autotune_end = _autotune_end
 Engine.graph_end = _graph_end

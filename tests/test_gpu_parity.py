@@ -313,6 +313,29 @@ def test_anchored_g2_plaquette_matches_exact_oracle(harness, beta):
     assert np.abs(v - g.eng.g2(parts, fz)).max() < 1e-10 * np.abs(v).max()
 
 
+@pytest.mark.parametrize("batch_bytes,chain_bytes", [(1, 1), (0, 1 << 20), (1 << 22, 300 << 10)])
+def test_anchored_g2_tiles_match_untiled(harness, batch_bytes, chain_bytes):
+    """Workspace limits small enough to batch one part at a time and to cut the
+    (z1, z3) plane into tiles (1x1, and about 3x3 with ragged edges) give the
+    untiled result up to the summation order, on an irregular triple list."""
+    beta = 10.0
+    m = M.make_model(M.plaquette())
+    g = harness(m, beta)
+    u, d = m.info.getIndex("A", 0, 1), m.info.getIndex("A", 0, 0)
+    rng = np.random.default_rng(5)
+    trip = [(a, b, x) for a in range(-5, 4) for b in range(-4, 4) for x in range(-3, 4)]
+    trip = [trip[i] for i in sorted(rng.choice(len(trip), 300, replace=False))]
+    fz = np.array([L.fermionic(np.array(t), beta) for t in trip])
+    parts = g.g2_parts(g.c(u), g.c(d), g.cdag(u), g.cdag(d))
+    v0 = _anchored(g, parts, fz)
+    g.eng.set_g2_workspace(batch_bytes, chain_bytes)
+    try:
+        v1 = _anchored(g, parts, fz)
+    finally:
+        g.eng.set_g2_workspace(0, 0)
+    assert np.abs(v1 - v0).max() < 1e-13 * np.abs(v0).max()
+
+
 def test_anchored_g2_anderson_a5_subset(harness):
     """Anderson 1+5 (dim 4096, beta=20): anchored GPU sum vs the exact oracle
     on the largest block chains and a subset of the 16^3 cube."""
