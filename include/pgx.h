@@ -33,6 +33,10 @@ extern "C" {
 #define PGX_G2_REFERENCE_RULE 1  /* apply the reference's weight filter at block level */
 #define PGX_G2_ANCHORED 2        /* weight-anchored sum: each sub-term is restricted to the
                                     states of its weighted index with w > coef_tol */
+#define PGX_G2_SPLIT_I8 4        /* with PGX_G2_ANCHORED: the stacked (z1, z3) products run on
+                                    the int8 tensor cores, operands split into six 7-bit
+                                    slices with power-of-two row/column scales (Ozaki scheme),
+                                    int32-exact partial products summed in FP64 */
 
 typedef struct pgx_ctx pgx_ctx;
 
@@ -235,6 +239,14 @@ int pgx_g2(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, int32_t nfreq
  * of its triples' z2.  Results do not depend on either limit beyond the
  * summation order. */
 int pgx_set_g2_workspace(pgx_ctx* ctx, int64_t batch_bytes, int64_t chain_bytes);
+
+/* Self-check of the int8 split product (no counterpart in the reference):
+ * C = A B for nb items of seeded random complex A (M x K) and B (K x N) with
+ * entries spread over four binary orders of magnitude, once through the split
+ * scheme with `slices` slices and once through the FP64 product.  Returns
+ * max|C_split - C_fp64| / max|C_fp64| and the device time of each (ms). */
+int pgx_split_gemm_check(pgx_ctx* ctx, int32_t M, int32_t N, int32_t K, int32_t nb, int32_t slices, uint64_t seed,
+                         double* max_rel_err, double* ms_split, double* ms_fp64);
 
 /* Number of state quadruples the reference enumerates for these parts
  * (TwoParticleGFPart.cpp:210-250): all four rotated elements |x| > nz_tol and

@@ -18,7 +18,8 @@ LIB = PKG / "lib"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 
-CU_SOURCES = ["pgx_api.cu", "pgx_eigh.cu", "pgx_lehmann.cu", "pgx_g2.cu", "pgx_g2a.cu", "pgx_noalloc.cu", "pgx_assemble.cu", "pgx_vjp.cu", "pgx_chi3.cu", "pgx_tune.cu"]
+CU_SOURCES = ["pgx_api.cu", "pgx_eigh.cu", "pgx_lehmann.cu", "pgx_g2.cu", "pgx_g2a.cu", "pgx_noalloc.cu", "pgx_assemble.cu", "pgx_vjp.cu", "pgx_chi3.cu", "pgx_tune.cu",
+              "pgx_ozaki.cu"]
 
 
 def _run(cmd):

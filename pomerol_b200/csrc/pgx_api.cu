@@ -456,6 +456,14 @@ int pgx_susc_vjp(pgx_ctx* c, int32_t opA, int32_t opB, int32_t nparts, const int
     });
 }
 
+int pgx_split_gemm_check(pgx_ctx* c, int32_t M, int32_t N, int32_t K, int32_t nb, int32_t slices, uint64_t seed,
+                         double* max_rel_err, double* ms_split, double* ms_fp64) {
+    return guarded(c, [&] {
+        PGX_CHECK(max_rel_err && ms_split && ms_fp64, PGX_ERR_ARG, "null output");
+        pgx::run_split_gemm_check(c, M, N, K, nb, slices, seed, max_rel_err, ms_split, ms_fp64);
+    });
+}
+
 int pgx_set_g2_workspace(pgx_ctx* c, int64_t batch_bytes, int64_t chain_bytes) {
     return guarded(c, [&] {
         PGX_CHECK(batch_bytes >= 0 && chain_bytes >= 0, PGX_ERR_ARG, "workspace limits must be >= 0");

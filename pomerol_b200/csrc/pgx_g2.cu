@@ -453,7 +453,14 @@ void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const d
         PGX_CUDA(cudaEventCreate(&a0));
         PGX_CUDA(cudaEventCreate(&a1));
         PGX_CUDA(cudaEventRecord(a0, st));
-        run_g2_anchored(c, nparts, parts, nfreq, z, pole_res, coef_tol, out);
+        const int split = (flags & PGX_G2_SPLIT_I8) ? 6 : 0;
+        if (split && c->oz.err.p) PGX_CUDA(cudaMemsetAsync(c->oz.err.p, 0, sizeof(int), st));
+        run_g2_anchored(c, nparts, parts, nfreq, z, pole_res, coef_tol, split, out);
+        if (split && c->oz.err.p) {
+            int e = 0;
+            PGX_CUDA(cudaMemcpy(&e, c->oz.err.p, sizeof(int), cudaMemcpyDeviceToHost));
+            PGX_CHECK(e == 0, PGX_ERR_TIMEOUT, "split product: a tensor-core wait expired");
+        }
         PGX_CUDA(cudaEventRecord(a1, st));
         PGX_CUDA(cudaEventSynchronize(a1));
         float t = 0.f;

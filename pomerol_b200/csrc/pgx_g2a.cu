@@ -352,7 +352,7 @@ template <typename T>
 static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector<int>& bplan,
                       const std::vector<ChainWs>& wsl, const pgx_g2_part* parts, const std::vector<APlan>& plans,
                       const std::vector<std::array<int, 4>>& rs, cd* pool, const int* d_hot,
-                      const std::vector<long>& hot_off, double pole_res, cd* d_out) {
+                      const std::vector<long>& hot_off, double pole_res, int split, cd* d_out) {
     Problem& P = c->P;
     cudaStream_t st = c->stream;
     constexpr bool TC = is_cd<T>::value;
@@ -420,11 +420,23 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
         if (probs.empty()) return;
         launch_gemm_batch(probs, c->scratch[7].p, c->scratch[7].bytes, c->scratch[8].p, c->scratch[8].bytes, st);
     };
-    // the stacked products read Lc, Pr, rho and Rc written by the first two launches
+    // the stacked products read Lc, Pr, rho and Rc written by the first two
+    // launches; with `split` slices they run on the int8 tensor cores
+    auto launch_stacked = [&](auto& probs) {
+        if (!split) {
+            launch(probs);
+            return;
+        }
+        for (const auto& g : probs) {
+            const double macs = (double)g.M * g.N * g.K * std::max(g.nb, 1);
+            ProfRange pr("oz_split_gemm", st, 8.0 * macs, 0.0);
+            oz_zgemm(g, split, c->oz, st);
+        }
+    };
     launch(pa);
     launch(pb);
-    launch(pc);
-    launch(pd);
+    launch_stacked(pc);
+    launch_stacked(pd);
     // ---- contractions per triple
     std::vector<DTerm> dt;
     for (size_t j = 0; j < idx.size(); ++j) {
@@ -540,7 +552,7 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
 }
 
 void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
-                     double anchor_tol, double* out) {
+                     double anchor_tol, int split, double* out) {
     Problem& P = c->P;
     cudaStream_t st = c->stream;
     // anchor states per block (weights above the threshold)
@@ -673,10 +685,10 @@ void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq
         pool_b.reserve(std::max<long>(used, 1) * sizeof(cd));
         if (P.is_complex)
             run_batch<cd>(c, batch, bplan, bws, parts, plans, rs, pool_b.as<cd>(), bh.as<int>(), hot_off, pole_res,
-                          out_b.as<cd>());
+                          split, out_b.as<cd>());
         else
             run_batch<double>(c, batch, bplan, bws, parts, plans, rs, pool_b.as<cd>(), bh.as<int>(), hot_off, pole_res,
-                              out_b.as<cd>());
+                              split, out_b.as<cd>());
         batch.clear();
         bplan.clear();
         bws.clear();

@@ -448,4 +448,10 @@ void launch_gemm_batch(const std::vector<GemmProblem<TA, TB, TC>>& probs, void* 
     launch_gemm_class<TA, TB, TC, 128, 4>(dp, di + istart[8], pstart[8], pstart[9], ntiles[8], st);
 }
 
+// C = A B through the int8 split scheme (pgx_ozaki.cu): S slices, plain
+// strided operands (one of them may be dressed), items as in launch_gemm_batch.
+struct OzWork;
+template <typename TA, typename TB>
+void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t st);
+
 }  // namespace pgx

@@ -93,6 +93,11 @@ struct DevBuf {
     template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Workspace of the int8 split products (digits, exponents, error flag).
+struct OzWork {
+    DevBuf A, B, ea, fb, err;
+};
+
 // Times of the products measured since pgx_autotune_begin, per (operand-type
 // key, M bucket, N bucket): index 0 the padding rule, c + 1 tile class c
 // (DBL_MAX where c is not valid for the bucket).
@@ -275,6 +280,7 @@ struct pgx_ctx {
     // side streams (and their fork / join events) for independent launches
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
     long long g2_batch_bytes = 0, g2_chain_bytes = 0;  // pgx_set_g2_workspace (0: defaults)
+    pgx::OzWork oz;                                     // int8 split products
     cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
     // scratch for G2 and Lehmann kernels
     pgx::DevBuf scratch[12];
@@ -348,7 +354,9 @@ void run_ensemble_average(pgx_ctx* c, int op, double* out);
 void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
             double coef_tol, int flags, double* out);
 void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const double* z, double pole_res,
-                     double anchor_tol, double* out);
+                     double anchor_tol, int split_slices, double* out);
+void run_split_gemm_check(pgx_ctx* c, int M, int N, int K, int nb, int S, unsigned long long seed, double* err,
+                          double* ms_split, double* ms_fp64);
 void run_chi3(pgx_ctx* c, int channel, int nparts, const pgx_chi3_part* parts, int nfreq, const double* z,
               double pole_res, double* out);
 void set_models(Problem& P, int nmodels, const int32_t* first_block, const double* beta);

@@ -1,0 +1,588 @@
+// Complex FP64 products on the int8 tensor cores (tcgen05, kind::i8): the
+// split ("Ozaki") scheme.  Used by the anchored G2 for its largest products
+// (the stacked (z1, z3) products) when PGX_G2_SPLIT_I8 is set.
+//
+// Each row of A and each column of B is scaled by a power of two so that its
+// largest |Re| or |Im| is below 1, and cut into S signed 7-bit digits:
+//   x * 2^-e = sum_s d_s 2^(-7(s+1)),  d_s integer in [-127, 127]
+// (exact digit extraction in FP64; the truncation left after S digits is
+// below 2^(-7S) of the row's or column's largest element).  The product is
+//   C = diag(2^e) [ sum_{a+b<S} 2^(-7(a+b+2)) A_a B_b ] diag(2^f),
+// each A_a B_b exact in int32, the diagonals a+b = s summed in FP64.  The
+// dropped diagonals (a+b >= S) are bounded by S 2^(-7S) K |A|max |B|max.
+// Complex operands become one real product of twice the depth:
+//   A' = [Re A, Im A] (M x 2K) and, per complex column j of B, two columns
+//   [Re B_j; -Im B_j] (the real part of C_j) and [Im B_j; Re B_j] (its imaginary
+//   part), so C' = A' B' holds Re C and Im C in adjacent columns.
+// Digits are stored K-contiguous per row (A) or per column (B):
+//   A row i: [digits of slice 0 | slice 1 | ... | slice S-1], each K2 = 2K
+//   rounded up to 128 bytes; B column j: [slice S-1 | ... | slice 0].
+// Then diagonal s is one product of depth (s+1) K2 with A from offset 0 and
+// B from offset (S-1-s) K2: both operands are plain strided views.
+//
+// The GEMM kernel: one CTA per 128 x 128 tile of C' (64 complex columns) and
+// batch item; 256 threads stage 128 x 128-byte k-blocks of A' and B' into
+// shared memory with cp.async in the 128-byte-swizzled K-major layout the
+// tensor core reads (4 stages); one thread issues tcgen05.mma (M = N = 128,
+// K = 32 bytes per instruction) into one of two TMEM accumulators (diagonals
+// alternate between them) and commits each stage and each finished diagonal
+// to an mbarrier.  While the next diagonal runs, all eight warps read the
+// finished accumulator (tcgen05.ld, warp w: TMEM lanes 32 (w % 4) ..., 64
+// columns per warp half) and add it, scaled by 2^(-7s), to FP64 registers.
+// Every mbarrier wait is bounded (about 2 s of %globaltimer); on expiry the
+// CTA sets the error flag, stops issuing work, waits (bounded) for its
+// tensor-core work in flight, frees its TMEM and returns.
+
+#include <cstdint>
+#include <vector>
+
+#include "pgx_common.cuh"
+#include "pgx_gemm.cuh"
+#include "pgx_internal.h"
+
+namespace pgx {
+
+namespace {
+
+constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 128;  // tile rows, tile columns, k-block bytes
+constexpr int OZ_STAGES = 4;
+constexpr int OZ_THREADS = 256;
+constexpr int OZ_STAGE_BYTES = (OZ_BM + OZ_BN) * OZ_BK;  // 32 KiB
+constexpr int OZ_SMEM = OZ_STAGES * OZ_STAGE_BYTES + 1024 + 256;
+constexpr int OZ_TMEM_COLS = 2 * OZ_BN;  // two accumulators
+constexpr unsigned long long OZ_WAIT_NS = 2000000000ull;
+
+struct OzArgs {
+    const int8_t* A;  // [item][row][S*K2]
+    long a_item, a_row;
+    const int8_t* B;  // [item][col'][S*K2], col' = 2 * complex column + {0: real part, 1: imaginary part}
+    long b_item, b_row;
+    const int* ea;  // row exponents [item][M]
+    long ea_item;
+    const int* fb;  // complex-column exponents [item][N]
+    long fb_item;
+    int M, N;  // rows, complex columns
+    int K2, S;
+    cd* C;
+    long c_item, sc_i, sc_j;
+    int* err;
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for phase `parity` of an mbarrier by a full warp; false (for
+// the whole warp) when any lane's wait expired.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    const unsigned long long t0 = gtimer();
+    bool done = false;
+    while (true) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) {
+            done = true;
+            break;
+        }
+        if (gtimer() - t0 > OZ_WAIT_NS) break;
+    }
+    return __all_sync(0xffffffffu, done);
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (the layout written by oz_load_stage).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);  // start address
+    d |= (uint64_t)1 << 16;                    // leading byte offset (unused with this swizzle)
+    d |= (uint64_t)(1024 >> 4) << 32;          // stride byte offset: 8 rows x 128 bytes
+    d |= (uint64_t)1 << 46;                    // descriptor version
+    d |= (uint64_t)2 << 61;                    // 128-byte swizzle
+    return d;
+}
+
+// Instruction descriptor: s32 accumulator, signed 8-bit A and B, both
+// K-major, N = 128, M = 128.
+constexpr uint32_t OZ_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
+                              ((uint32_t)(OZ_BM >> 4) << 24);
+
+// One k-block of A' rows [i0, i0+128) and B' columns [j0, j0+128) into a stage:
+// row r, 16-byte chunk c lands at (r/8)*1024 + (r%8)*128 + ((c ^ (r%8)) * 16).
+// Rows beyond the matrix read as zero.
+__device__ __forceinline__ void oz_load_stage(char* st, const int8_t* Ab, long a_row, int arows, const int8_t* Bb,
+                                              long b_row, int brows, long koffA, long koffB, int tid) {
+#pragma unroll
+    for (int q = 0; q < (OZ_BM + OZ_BN) * (OZ_BK / 16) / OZ_THREADS; ++q) {
+        const int idx = tid + q * OZ_THREADS;  // 0 .. 2047
+        const bool isB = idx >= OZ_BM * (OZ_BK / 16);
+        const int li = isB ? idx - OZ_BM * (OZ_BK / 16) : idx;
+        const int r = li >> 3, c = li & 7;
+        const int8_t* src;
+        int bytes;
+        if (!isB) {
+            bytes = r < arows ? 16 : 0;
+            src = bytes ? Ab + (long)r * a_row + koffA + c * 16 : Ab;
+        } else {
+            bytes = r < brows ? 16 : 0;
+            src = bytes ? Bb + (long)r * b_row + koffB + c * 16 : Bb;
+        }
+        char* dst = st + (isB ? OZ_BM * OZ_BK : 0) + (r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(bytes)
+                     : "memory");
+    }
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];\n"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+
+__global__ void __launch_bounds__(OZ_THREADS, 1) oz_gemm_kernel(OzArgs p) {
+    extern __shared__ char oz_raw[];
+    char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(oz_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + OZ_STAGES * OZ_STAGE_BYTES);  // [STAGES] stage, [2] accumulator
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + OZ_STAGES + 2);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int item = blockIdx.z;
+    const int i0 = blockIdx.y * OZ_BM, j0 = blockIdx.x * OZ_BN;  // j0: column of C' (2 per complex column)
+    const int arows = min(OZ_BM, p.M - i0), brows = min(OZ_BN, 2 * p.N - j0);
+    const int8_t* Ab = p.A + item * p.a_item + (long)i0 * p.a_row;
+    const int8_t* Bb = p.B + item * p.b_item + (long)j0 * p.b_row;
+
+    if (tid == 0) {
+        for (int s = 0; s < OZ_STAGES + 2; ++s)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[s])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(s_tmem)),
+                     "r"(OZ_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *s_tmem;
+
+    // k-block sequence: diagonal s has (s+1) K2 / BK blocks
+    const int kbd = p.K2 / OZ_BK;
+    int total = 0;
+    for (int s = 0; s < p.S; ++s) total += (s + 1) * kbd;
+    auto block_of = [&](int it, int& s, int& kb) {
+        s = 0;
+        while (it >= (s + 1) * kbd) {
+            it -= (s + 1) * kbd;
+            ++s;
+        }
+        kb = it;
+    };
+    auto issue_load = [&](int it) {
+        int s, kb;
+        block_of(it, s, kb);
+        char* st = smem + (it % OZ_STAGES) * OZ_STAGE_BYTES;
+        oz_load_stage(st, Ab, p.a_row, arows, Bb, p.b_row, brows, (long)kb * OZ_BK,
+                      (long)(p.S - 1 - s) * p.K2 + (long)kb * OZ_BK, tid);
+    };
+
+    double acc[64];
+#pragma unroll
+    for (int q = 0; q < 64; ++q) acc[q] = 0.0;
+    const int lane_base = 32 * (warp & 3), col_base = 64 * (warp >> 2);
+    // adds the accumulator of diagonal s, times 2^(-7s), to acc; false when the wait expired
+    auto drain = [&](int s) {
+        const uint32_t bar = smem_u32(&bars[OZ_STAGES + (s & 1)]);
+        if (!mbar_wait(bar, (uint32_t)((s >> 1) & 1))) return false;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        const double sc = ldexp(1.0, -7 * s);
+        const uint32_t base = tmem + ((uint32_t)lane_base << 16) + (uint32_t)((s & 1) * OZ_BN + col_base);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t v[16];
+            tmem_ld16(base + 16 * q, v);
+            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+            for (int e = 0; e < 16; ++e) acc[16 * q + e] = fma((double)(int)v[e], sc, acc[16 * q + e]);
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+        return true;
+    };
+
+    for (int it = 0; it < OZ_STAGES - 1 && it < total; ++it) issue_load(it);
+    int s_cur = 0, kb_end = kbd;  // diagonal of iteration it and the iteration that ends it
+    int issued_to = -1;           // last iteration whose tensor-core work was issued
+    int my_fail = 0;              // this thread saw a wait expire
+    bool failed = false;          // some thread did (uniform across the CTA)
+    for (int it = 0; it < total; ++it) {
+        if (it == kb_end) {  // iteration it starts diagonal s_cur + 1
+            ++s_cur;
+            kb_end += (s_cur + 1) * kbd;
+        }
+        // this stage's bytes have landed (all but the newest STAGES-2 groups)
+        if (it + OZ_STAGES - 1 <= total) asm volatile("cp.async.wait_group %0;\n" ::"n"(OZ_STAGES - 2) : "memory");
+        else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        if (__syncthreads_or(my_fail)) {
+            failed = true;
+            break;
+        }
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t sa = smem_u32(smem + (it % OZ_STAGES) * OZ_STAGE_BYTES);
+            const uint32_t sb = sa + OZ_BM * OZ_BK;
+            const uint32_t dt = tmem + (uint32_t)((s_cur & 1) * OZ_BN);
+            const int first = (it == kb_end - (s_cur + 1) * kbd);  // first k-block of the diagonal
+#pragma unroll
+            for (int k = 0; k < OZ_BK / 32; ++k) {
+                const uint64_t da = sw128_desc(sa + 32 * k), db = sw128_desc(sb + 32 * k);
+                const uint32_t accum = (first && k == 0) ? 0u : 1u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(dt), "l"(da), "l"(db), "r"(OZ_IDESC), "r"(accum)
+                    : "memory");
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                             smem_u32(&bars[it % OZ_STAGES]))
+                         : "memory");
+            if (it == kb_end - 1)
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                                 smem_u32(&bars[OZ_STAGES + (s_cur & 1)]))
+                             : "memory");
+        }
+        issued_to = it;
+        // refill the stage of iteration it - 1 once its tensor-core reads are done
+        const int nxt = it + OZ_STAGES - 1;
+        if (nxt < total) {
+            bool ready = true;
+            if (it >= 1) {
+                const int prev = it - 1;
+                ready = mbar_wait(smem_u32(&bars[prev % OZ_STAGES]), (uint32_t)((prev / OZ_STAGES) & 1));
+            }
+            if (ready) issue_load(nxt);
+            else my_fail = 1;
+        }
+        // the previous diagonal is complete once this one has started
+        if (!my_fail && it == kb_end - (s_cur + 1) * kbd && s_cur >= 1 && !drain(s_cur - 1)) my_fail = 1;
+    }
+    if (!failed && !my_fail && !drain(p.S - 1)) my_fail = 1;
+    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+    // all tensor-core work of this CTA has finished before TMEM is freed
+    if (issued_to >= 0 && !mbar_wait(smem_u32(&bars[issued_to % OZ_STAGES]), (uint32_t)((issued_to / OZ_STAGES) & 1)))
+        my_fail = 1;
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    const bool ok = !__syncthreads_or(my_fail) && !failed;
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(OZ_TMEM_COLS)
+                     : "memory");
+    }
+    if (!ok) {
+        if (tid == 0) atomicExch(p.err, 1);
+        return;
+    }
+    // C(i, j) = 2^(e_i + f_j - 14) acc, real and imaginary parts in adjacent columns
+    const int r = lane_base + lane;
+    const int i = i0 + r;
+    if (i >= p.M) return;
+    const int ei = p.ea[item * p.ea_item + i];
+    cd* crow = p.C + item * p.c_item + (long)i * p.sc_i;
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+        const int jc = (j0 + col_base) / 2 + q;
+        if (jc < p.N) {
+            const double sc = ldexp(1.0, ei + p.fb[item * p.fb_item + jc] - 14);
+            crow[(long)jc * p.sc_j] = cd{acc[2 * q] * sc, acc[2 * q + 1] * sc};
+        }
+    }
+}
+
+// Digits of an operand.  Output row r (a row of A', or a complex column of B
+// giving rows 2r and 2r+1 of B'), reduction index k < K:
+//   x(r, k) = X[r*s_r + k*s_k] (+ item*s_item), dressed when Er/Ek are set:
+//   x / (z - (Er[r] - Ek[k])) if rk_order, else x / (z - (Ek[k] - Er[r])) -- the
+//   dress() convention with (row energy, column energy) of the dressed matrix.
+struct OzSrc {
+    const void* X;
+    int cplx;
+    long s_r, s_k, s_item;
+    const double *Er, *Ek;
+    int rk_order;  // 1: dressed matrix has rows r, columns k; 0: rows k, columns r
+    const cd* zs;
+};
+
+__device__ __forceinline__ cd oz_value(const OzSrc& q, int item, int r, int k) {
+    const long off = item * q.s_item + (long)r * q.s_r + (long)k * q.s_k;
+    const cd x = q.cplx ? static_cast<const cd*>(q.X)[off] : cd{static_cast<const double*>(q.X)[off], 0.0};
+    if (!q.Er) return x;
+    const cd z = q.zs[item];
+    return q.rk_order ? dress(x, q.Er[r], q.Ek[k], z) : dress(x, q.Ek[k], q.Er[r], z);
+}
+
+// One warp per output row r; is_b selects the B' layout (two rows per complex
+// column, slices in reverse order).
+__global__ void oz_prep_kernel(OzSrc q, int R, int K, int K2, int S, int is_b, int8_t* out, long out_item, int* ex,
+                               long ex_item) {
+    const int warp = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+    const int item = blockIdx.y;
+    if (warp >= R) return;
+    const int r = warp;
+    double m = 0.0;
+    for (int k = lane; k < K; k += 32) {
+        const cd v = oz_value(q, item, r, k);
+        m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);  // m = f 2^e, f in [0.5, 1): every |x| 2^-e < 1
+    if (lane == 0) ex[item * ex_item + r] = e;
+    const long row_bytes = (long)S * K2;
+    int8_t* o0 = out + item * out_item + (long)(is_b ? 2 * r : r) * row_bytes;
+    int8_t* o1 = o0 + row_bytes;  // B' only: the imaginary-part row
+    for (int k = lane; k < K2 / 2; k += 32) {
+        double vr = 0.0, vi = 0.0;
+        if (k < K) {
+            const cd v = oz_value(q, item, r, k);
+            vr = ldexp(v.x, -e);
+            vi = ldexp(v.y, -e);
+        }
+        for (int s = 0; s < S; ++s) {
+            vr *= 128.0;
+            vi *= 128.0;
+            const double dr = trunc(vr), di = trunc(vi);
+            vr -= dr;
+            vi -= di;
+            const long base = (long)(is_b ? S - 1 - s : s) * K2;
+            // the first K2/2 positions pair with Re of the other side, the rest with Im
+            if (!is_b) {
+                o0[base + k] = (int8_t)dr;               // A' = [Re A, Im A]
+                o0[base + K2 / 2 + k] = (int8_t)di;
+            } else {
+                o0[base + k] = (int8_t)dr;               // real-part column: [Re B; -Im B]
+                o0[base + K2 / 2 + k] = (int8_t)(-di);
+                o1[base + k] = (int8_t)di;               // imaginary-part column: [Im B; Re B]
+                o1[base + K2 / 2 + k] = (int8_t)dr;
+            }
+        }
+    }
+}
+
+}  // namespace
+
+bool oz_supported(int M, int N, int K) { return M > 0 && N > 0 && K > 0 && 2L * K <= (1L << 20); }
+
+// C (+ item strides) = A B for the nb items of g, through the split scheme.
+template <typename TA, typename TB>
+void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t st) {
+    static_assert(!is_dressed<TA>::value || !is_dressed<TB>::value, "one dressed operand at most");
+    const int M = g.M, N = g.N, K = g.K, nb = std::max(g.nb, 1);
+    PGX_CHECK(!g.accumulate && !g.a_kidx && !g.b_kidx && !g.kscale && !g.a_iidx && !g.b_jidx && !g.conj_a,
+              PGX_ERR_ARG, "split product: plain strided operands only");
+    PGX_CHECK(S >= 1 && S <= 8, PGX_ERR_ARG, "split product: 1..8 slices");
+    const int K2 = (int)(ceil_div(2L * K, OZ_BK) * OZ_BK);
+    const long row_bytes = (long)S * K2;
+    // an operand changes per item when it is dressed (per-item frequency) or strided over items
+    const bool a_item = is_dressed<TA>::value || g.ba != 0;
+    const bool b_item = is_dressed<TB>::value || g.bb != 0;
+    // int32 accumulation: depth (S) K2 with |digit| <= 127 stays below 2^31
+    PGX_CHECK((double)S * K2 * 127.0 * 127.0 < 2147483647.0, PGX_ERR_ARG, "split product too deep for int32");
+    const long a_bytes = (long)M * row_bytes, b_bytes = 2L * N * row_bytes;
+    // items per chunk under about 4 GiB of digits
+    const long per_item = (a_item ? a_bytes : 0) + (b_item ? b_bytes : 0);
+    int chunk = nb;
+    if (per_item > 0) chunk = (int)std::max<long>(1, std::min<long>(nb, (4L << 30) / per_item));
+    const long ac = a_item ? chunk : 1, bc = b_item ? chunk : 1;
+    w.A.reserve(ac * a_bytes);
+    w.B.reserve(bc * b_bytes);
+    w.ea.reserve(ac * M * sizeof(int));
+    w.fb.reserve(bc * N * sizeof(int));
+    if (!w.err.p) {
+        w.err.reserve(sizeof(int));
+        PGX_CUDA(cudaMemsetAsync(w.err.p, 0, sizeof(int), st));
+    }
+    static bool attr = false;
+    if (!attr) {
+        PGX_CUDA(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM));
+        attr = true;
+    }
+    using SA = typename src_t<TA>::type;
+    using SB = typename src_t<TB>::type;
+    for (int b0 = 0; b0 < nb; b0 += chunk) {
+        const int cn = std::min(chunk, nb - b0);
+        // A rows: A(i, k) = A[i sa_i + k sa_k]; dressed as dress(x, dEa[i], dEb[k], z)
+        if (a_item || b0 == 0) {
+            OzSrc q{};
+            q.X = g.A + (a_item ? b0 * g.ba : 0);
+            q.cplx = is_cd<SA>::value;
+            q.s_r = g.sa_i;
+            q.s_k = g.sa_k;
+            q.s_item = g.ba;
+            if (is_dressed<TA>::value) {
+                q.Er = g.dEa;
+                q.Ek = g.dEb;
+                q.rk_order = 1;
+                q.zs = g.dzs + b0;
+            }
+            const int items = a_item ? cn : 1;
+            dim3 grid((unsigned)ceil_div((long)M * 32, 256), (unsigned)items);
+            oz_prep_kernel<<<grid, 256, 0, st>>>(q, M, K, K2, S, 0, w.A.as<int8_t>(), a_bytes, w.ea.as<int>(), M);
+            check_launch("oz_prep_kernel");
+        }
+        // B columns: B(k, j) = B[k sb_k + j sb_j]; dressed as dress(x, dEa[k], dEb[j], z)
+        if (b_item || b0 == 0) {
+            OzSrc q{};
+            q.X = g.B + (b_item ? b0 * g.bb : 0);
+            q.cplx = is_cd<SB>::value;
+            q.s_r = g.sb_j;
+            q.s_k = g.sb_k;
+            q.s_item = g.bb;
+            if (is_dressed<TB>::value) {
+                q.Er = g.dEb;
+                q.Ek = g.dEa;
+                q.rk_order = 0;
+                q.zs = g.dzs + b0;
+            }
+            const int items = b_item ? cn : 1;
+            dim3 grid((unsigned)ceil_div((long)N * 32, 256), (unsigned)items);
+            oz_prep_kernel<<<grid, 256, 0, st>>>(q, N, K, K2, S, 1, w.B.as<int8_t>(), b_bytes, w.fb.as<int>(), N);
+            check_launch("oz_prep_kernel");
+        }
+        OzArgs a{};
+        a.A = w.A.as<int8_t>();
+        a.a_item = a_item ? a_bytes : 0;
+        a.a_row = row_bytes;
+        a.B = w.B.as<int8_t>();
+        a.b_item = b_item ? b_bytes : 0;
+        a.b_row = row_bytes;
+        a.ea = w.ea.as<int>();
+        a.ea_item = a_item ? M : 0;
+        a.fb = w.fb.as<int>();
+        a.fb_item = b_item ? N : 0;
+        a.M = M;
+        a.N = N;
+        a.K2 = K2;
+        a.S = S;
+        a.C = g.C + (long)b0 * g.bc;
+        a.c_item = g.bc;
+        a.sc_i = g.sc_i;
+        a.sc_j = g.sc_j;
+        a.err = w.err.as<int>();
+        dim3 grid((unsigned)ceil_div(2L * N, OZ_BN), (unsigned)ceil_div((long)M, OZ_BM), (unsigned)cn);
+        oz_gemm_kernel<<<grid, OZ_THREADS, OZ_SMEM, st>>>(a);
+        check_launch("oz_gemm_kernel");
+    }
+}
+
+template void oz_zgemm<Dressed<double>, cd>(const GemmProblem<Dressed<double>, cd, cd>&, int, OzWork&, cudaStream_t);
+template void oz_zgemm<Dressed<cd>, cd>(const GemmProblem<Dressed<cd>, cd, cd>&, int, OzWork&, cudaStream_t);
+template void oz_zgemm<cd, Dressed<double>>(const GemmProblem<cd, Dressed<double>, cd>&, int, OzWork&, cudaStream_t);
+template void oz_zgemm<cd, Dressed<cd>>(const GemmProblem<cd, Dressed<cd>, cd>&, int, OzWork&, cudaStream_t);
+template void oz_zgemm<cd, cd>(const GemmProblem<cd, cd, cd>&, int, OzWork&, cudaStream_t);
+
+}  // namespace pgx
+
+namespace pgx {
+
+namespace {
+// Seeded uniform values in [-1, 1) times 2^-(h mod 4) (SplitMix64 hash of the index).
+__global__ void oz_fill_kernel(cd* x, long n, unsigned long long seed) {
+    const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    unsigned long long h = seed + 0x9E3779B97F4A7C15ull * (unsigned long long)(i + 1);
+    auto mix = [](unsigned long long z) {
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+    };
+    const unsigned long long a = mix(h), b = mix(h ^ 0x5555555555555555ull);
+    const double sc = ldexp(1.0, -(int)(a & 3));
+    x[i] = cd{(((a >> 11) * 0x1.0p-53) * 2.0 - 1.0) * sc, (((b >> 11) * 0x1.0p-53) * 2.0 - 1.0) * sc};
+}
+}  // namespace
+
+void run_split_gemm_check(pgx_ctx* c, int M, int N, int K, int nb, int S, unsigned long long seed, double* err,
+                          double* ms_split, double* ms_fp64) {
+    PGX_CHECK(M > 0 && N > 0 && K > 0 && nb > 0 && (long)M * K * nb < (1L << 31) && (long)K * N < (1L << 31),
+              PGX_ERR_ARG, "split check: sizes out of range");
+    cudaStream_t st = c->stream;
+    DevBuf A, B, C1, C2;
+    const long na = (long)nb * M * K, nbb = (long)K * N, nc = (long)nb * M * N;
+    A.reserve(na * sizeof(cd));
+    B.reserve(nbb * sizeof(cd));
+    C1.reserve(nc * sizeof(cd));
+    C2.reserve(nc * sizeof(cd));
+    oz_fill_kernel<<<(unsigned)ceil_div(na, 256L), 256, 0, st>>>(A.as<cd>(), na, seed);
+    oz_fill_kernel<<<(unsigned)ceil_div(nbb, 256L), 256, 0, st>>>(B.as<cd>(), nbb, seed ^ 0xABCDEFull);
+    check_launch("oz_fill_kernel");
+    GemmProblem<cd, cd, cd> g{};
+    g.A = A.as<cd>();
+    g.B = B.as<cd>();
+    g.M = M;
+    g.N = N;
+    g.K = K;
+    g.sa_i = K;
+    g.sa_k = 1;
+    g.sb_k = N;
+    g.sb_j = 1;
+    g.sc_i = N;
+    g.sc_j = 1;
+    g.nb = nb;
+    g.ba = (long)M * K;
+    g.bb = 0;
+    g.bc = (long)M * N;
+    cudaEvent_t e0, e1, e2;
+    PGX_CUDA(cudaEventCreate(&e0));
+    PGX_CUDA(cudaEventCreate(&e1));
+    PGX_CUDA(cudaEventCreate(&e2));
+    if (c->oz.err.p) PGX_CUDA(cudaMemsetAsync(c->oz.err.p, 0, sizeof(int), st));
+    g.C = C1.as<cd>();
+    PGX_CUDA(cudaEventRecord(e0, st));
+    oz_zgemm(g, S, c->oz, st);
+    PGX_CUDA(cudaEventRecord(e1, st));
+    g.C = C2.as<cd>();
+    std::vector<GemmProblem<cd, cd, cd>> probs{g};
+    DevBuf pb, ib;
+    pb.reserve(sizeof(g));
+    ib.reserve(gemm_index_bytes(1));
+    launch_gemm_batch(probs, pb.p, pb.bytes, ib.p, ib.bytes, st);
+    PGX_CUDA(cudaEventRecord(e2, st));
+    PGX_CUDA(cudaEventSynchronize(e2));
+    float t1 = 0.f, t2 = 0.f;
+    PGX_CUDA(cudaEventElapsedTime(&t1, e0, e1));
+    PGX_CUDA(cudaEventElapsedTime(&t2, e1, e2));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaEventDestroy(e2);
+    int flag = 0;
+    PGX_CUDA(cudaMemcpy(&flag, c->oz.err.p, sizeof(int), cudaMemcpyDeviceToHost));
+    PGX_CHECK(flag == 0, PGX_ERR_TIMEOUT, "split product: a tensor-core wait expired");
+    std::vector<cd> h1(nc), h2(nc);
+    PGX_CUDA(cudaMemcpy(h1.data(), C1.p, nc * sizeof(cd), cudaMemcpyDeviceToHost));
+    PGX_CUDA(cudaMemcpy(h2.data(), C2.p, nc * sizeof(cd), cudaMemcpyDeviceToHost));
+    double dmax = 0.0, cmax = 0.0;
+    for (long i = 0; i < nc; ++i) {
+        dmax = std::max(dmax, std::hypot(h1[i].x - h2[i].x, h1[i].y - h2[i].y));
+        cmax = std::max(cmax, std::hypot(h2[i].x, h2[i].y));
+    }
+    *err = cmax > 0.0 ? dmax / cmax : dmax;
+    *ms_split = t1;
+    *ms_fp64 = t2;
+}
+
+}  // namespace pgx

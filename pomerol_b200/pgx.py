@@ -15,7 +15,7 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().parent / "lib" / "libpgx.so"
 
 PGX_OK, PGX_ERR_ARG, PGX_ERR_OOM, PGX_ERR_CUDA, PGX_ERR_TIMEOUT, PGX_ERR_NUMERIC, PGX_ERR_STATE, PGX_ERR_NODEV = range(8)
-PGX_G2_EXACT, PGX_G2_REFERENCE_RULE, PGX_G2_ANCHORED = 0, 1, 2
+PGX_G2_EXACT, PGX_G2_REFERENCE_RULE, PGX_G2_ANCHORED, PGX_G2_SPLIT_I8 = 0, 1, 2, 4
 
 EXPORTS = [
     "pgx_version", "pgx_create", "pgx_destroy", "pgx_last_error", "pgx_set_blocks", "pgx_set_hamiltonian",
@@ -25,7 +25,7 @@ EXPORTS = [
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
     "pgx_gf_vjp", "pgx_susc_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_autotune_begin", "pgx_autotune_end",
-    "pgx_set_g2_workspace", "pgx_graph_begin", "pgx_graph_end",
+    "pgx_set_g2_workspace", "pgx_split_gemm_check", "pgx_graph_begin", "pgx_graph_end",
     "pgx_graph_replay", "pgx_graph_destroy", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
 ]
 
@@ -89,6 +89,8 @@ def load():
         lib.pgx_set_eigensystem.argtypes = [P, P, P]
         lib.pgx_autotune_begin.argtypes = [P]
         lib.pgx_set_g2_workspace.argtypes = [P, C.c_int64, C.c_int64]
+        lib.pgx_split_gemm_check.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
+                                             P, P, P]
         lib.pgx_autotune_end.argtypes = [P, P]
         lib.pgx_graph_begin.argtypes = [P]
         lib.pgx_graph_end.argtypes = [P, P]
@@ -422,6 +424,14 @@ def _set_g2_workspace(self, batch_bytes=0, chain_bytes=0):
     self._ck(self.lib.pgx_set_g2_workspace(self.h, int(batch_bytes), int(chain_bytes)))
 
 
+def _split_gemm_check(self, M, N, K, nb=1, slices=6, seed=1):
+    """int8 split product vs FP64 on seeded random complex matrices:
+    (max relative error, split ms, FP64 ms)."""
+    r = np.zeros(3, dtype=np.float64)
+    self._ck(self.lib.pgx_split_gemm_check(self.h, M, N, K, nb, slices, seed, _p(r[0:1]), _p(r[1:2]), _p(r[2:3])))
+    return float(r[0]), float(r[1]), float(r[2])
+
+
 def _autotune_begin(self):
     """Record the GEMM products of the following calls for autotune_end()."""
     self._ck(self.lib.pgx_autotune_begin(self.h))
@@ -529,6 +539,7 @@ Engine.chi3 = _chi3
 Engine.set_models = _set_models
 Engine.graph_begin = _graph_begin
 Engine.set_g2_workspace = _set_g2_workspace
+Engine.split_gemm_check = _split_gemm_check
 Engine.autotune_begin = _autotune_begin
 Engine.autotune_end = _autotune_end
 Engine.graph_end = _graph_end

@@ -29,7 +29,7 @@ def main():
                     help="measure the GEMM tile classes on one step (after one untimed step) before timing")
     a = ap.parse_args()
     if a.chain:
-        chain(a.config, a.g2_cubes)
+        chain(a.config, a.g2_cubes, a.kernels)
         return
     import torch  # noqa: F401  (CUDA context for the process)
     from .workloads import BatchRun, Chi3Run, EngineRun, Problem, b64_params, matsubara_cube, matsubara_square
@@ -87,7 +87,7 @@ def autotune(eng, step):
     print(f"autotune: {n} size buckets off the padding rule ({1e3 * (time.perf_counter() - t0):.1f} ms)", flush=True)
 
 
-def chain(config, cubes):
+def chain(config, cubes, kernels=False):
     import torch  # noqa: F401  (CUDA context for the process)
     from . import _pomerol as P
     from .workloads import EngineRun, Problem, matsubara_cube
@@ -132,14 +132,21 @@ def chain(config, cubes):
     print(f"chi_zz on 48 bosonic frequencies (4 pair susceptibilities): {t4 - t3:.3f} s, chi_zz(0) = {zz[0]:.10e}")
     if cubes:
         run = EngineRun(prob)
-        for n in cubes:
+        for i, n in enumerate(cubes):
             _, z = matsubara_cube(prob.beta, n)
+            prof = kernels and i == len(cubes) - 1
+            if prof:
+                run.eng.profile_begin()
             run.eng.timer_begin()
             t = time.perf_counter()
             run.step(z)
             ms = run.eng.timer_end()
             print(f"G2 step (eigensolve + weights + rotation + G2) on {len(z)} triples: device {ms:.0f} ms, "
-                  f"wall {time.perf_counter() - t:.1f} s", flush=True)
+                  f"wall {time.perf_counter() - t:.1f} s, g2 {run.eng.g2_timing()['total_ms'] / 1e3:.1f} s", flush=True)
+            if prof:
+                for k in run.eng.profile_end()[:10]:
+                    print(f"  {k['name']:48s} x{k['launches']:<5d} {k['ms'] / 1e3:8.2f} s  "
+                          f"{k['flops'] / max(k['ms'], 1e-9) / 1e9:7.2f} TFLOP/s", flush=True)
 
 
 if __name__ == "__main__":

@@ -336,6 +336,37 @@ def test_anchored_g2_tiles_match_untiled(harness, batch_bytes, chain_bytes):
     assert np.abs(v1 - v0).max() < 1e-13 * np.abs(v0).max()
 
 
+@pytest.mark.parametrize("M,N,K,nb", [(128, 64, 64, 1), (200, 150, 300, 2), (1000, 900, 2000, 3)])
+def test_split_gemm_matches_fp64(M, N, K, nb):
+    """int8 tensor-core split product (six 7-bit slices) against the FP64
+    product on seeded random complex matrices spread over four binary orders of
+    magnitude, ragged tile edges included: max error 1e-11 of max|C|.  Three
+    slices leave about 2^-21 of it, which shows that every slice is used."""
+    from pomerol_b200.pgx import Engine
+    eng = Engine()
+    err6, _, _ = eng.split_gemm_check(M, N, K, nb, slices=6, seed=3)
+    assert err6 < 1e-11
+    err3, _, _ = eng.split_gemm_check(M, N, K, nb, slices=3, seed=3)
+    assert 1e-9 < err3 < 1e-4
+
+
+def test_anchored_g2_split_i8_anderson_a5(harness):
+    """Anderson 1+5 (dim 4096, beta=20) on the 16^3 cube: the anchored G2 with
+    its stacked products on the int8 tensor cores (PGX_G2_SPLIT_I8) against the
+    FP64 anchored G2, within 1e-9 of max|G2|."""
+    from pomerol_b200.pgx import PGX_G2_ANCHORED, PGX_G2_SPLIT_I8
+    U, epsd, eps, V, beta = M.anderson_a5_params(0)
+    m = M.make_model(M.anderson(U, epsd, eps, V))
+    g = harness(m, beta)
+    u, d = m.info.getIndex("C", 0, 1), m.info.getIndex("C", 0, 0)
+    n = np.arange(-8, 8)
+    fz = L.fermionic(np.array([(a, b, x) for a in n for b in n for x in n]), beta)
+    parts = g.g2_parts(g.c(u), g.c(d), g.cdag(u), g.cdag(d))
+    v = _anchored(g, parts, fz)
+    vs = g.eng.g2(parts, fz, pole_res=1e-8, coef_tol=1e-16, flags=PGX_G2_ANCHORED | PGX_G2_SPLIT_I8)
+    assert np.abs(vs - v).max() < 1e-9 * np.abs(v).max()
+
+
 def test_anchored_g2_anderson_a5_subset(harness):
     """Anderson 1+5 (dim 4096, beta=20): anchored GPU sum vs the exact oracle
     on the largest block chains and a subset of the 16^3 cube."""
