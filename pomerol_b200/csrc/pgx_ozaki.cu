@@ -21,17 +21,15 @@
 // B from offset (S-1-s) K2: both operands are plain strided views.
 //
 // The GEMM kernel: one CTA per 128 x 128 tile of C' (64 complex columns) and
-// batch item; 256 threads stage 128 x 128-byte k-blocks of A' and B' into
-// shared memory with cp.async in the 128-byte-swizzled K-major layout the
-// tensor core reads (4 stages); one thread issues tcgen05.mma (M = N = 128,
-// K = 32 bytes per instruction) into one of two TMEM accumulators (diagonals
-// alternate between them) and commits each stage and each finished diagonal
-// to an mbarrier.  While the next diagonal runs, all eight warps read the
-// finished accumulator (tcgen05.ld, warp w: TMEM lanes 32 (w % 4) ..., 64
-// columns per warp half) and add it, scaled by 2^(-7s), to FP64 registers.
-// Every mbarrier wait is bounded (about 2 s of %globaltimer); on expiry the
-// CTA sets the error flag, stops issuing work, waits (bounded) for its
-// tensor-core work in flight, frees its TMEM and returns.
+// batch item; tcgen05.mma with M = N = 128 and K = 32 bytes per instruction,
+// into one of two TMEM accumulators (diagonals alternate between them), so
+// one diagonal is summed into FP64 while the next runs.  Every mbarrier wait
+// is bounded (about 2 s of %globaltimer); on expiry the CTA sets the error
+// flag, stops issuing work, waits (bounded) for its copies and tensor-core
+// work in flight, frees its TMEM and returns.
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
 
 #include <cstdint>
 #include <vector>
@@ -46,27 +44,10 @@ namespace {
 
 constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 128;  // tile rows, tile columns, k-block bytes
 constexpr int OZ_STAGES = 4;
-constexpr int OZ_THREADS = 256;
 constexpr int OZ_STAGE_BYTES = (OZ_BM + OZ_BN) * OZ_BK;  // 32 KiB
 constexpr int OZ_SMEM = OZ_STAGES * OZ_STAGE_BYTES + 1024 + 256;
 constexpr int OZ_TMEM_COLS = 2 * OZ_BN;  // two accumulators
 constexpr unsigned long long OZ_WAIT_NS = 2000000000ull;
-
-struct OzArgs {
-    const int8_t* A;  // [item][row][S*K2]
-    long a_item, a_row;
-    const int8_t* B;  // [item][col'][S*K2], col' = 2 * complex column + {0: real part, 1: imaginary part}
-    long b_item, b_row;
-    const int* ea;  // row exponents [item][M]
-    long ea_item;
-    const int* fb;  // complex-column exponents [item][N]
-    long fb_item;
-    int M, N;  // rows, complex columns
-    int K2, S;
-    cd* C;
-    long c_item, sc_i, sc_j;
-    int* err;
-};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -116,33 +97,6 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
 constexpr uint32_t OZ_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
                               ((uint32_t)(OZ_BM >> 4) << 24);
 
-// One k-block of A' rows [i0, i0+128) and B' columns [j0, j0+128) into a stage:
-// row r, 16-byte chunk c lands at (r/8)*1024 + (r%8)*128 + ((c ^ (r%8)) * 16).
-// Rows beyond the matrix read as zero.
-__device__ __forceinline__ void oz_load_stage(char* st, const int8_t* Ab, long a_row, int arows, const int8_t* Bb,
-                                              long b_row, int brows, long koffA, long koffB, int tid) {
-#pragma unroll
-    for (int q = 0; q < (OZ_BM + OZ_BN) * (OZ_BK / 16) / OZ_THREADS; ++q) {
-        const int idx = tid + q * OZ_THREADS;  // 0 .. 2047
-        const bool isB = idx >= OZ_BM * (OZ_BK / 16);
-        const int li = isB ? idx - OZ_BM * (OZ_BK / 16) : idx;
-        const int r = li >> 3, c = li & 7;
-        const int8_t* src;
-        int bytes;
-        if (!isB) {
-            bytes = r < arows ? 16 : 0;
-            src = bytes ? Ab + (long)r * a_row + koffA + c * 16 : Ab;
-        } else {
-            bytes = r < brows ? 16 : 0;
-            src = bytes ? Bb + (long)r * b_row + koffB + c * 16 : Bb;
-        }
-        char* dst = st + (isB ? OZ_BM * OZ_BK : 0) + (r >> 3) * 1024 + (r & 7) * 128 + ((c ^ (r & 7)) << 4);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(bytes)
-                     : "memory");
-    }
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-}
-
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -152,21 +106,59 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
         : "r"(taddr));
 }
 
-__global__ void __launch_bounds__(OZ_THREADS, 1) oz_gemm_kernel(OzArgs p) {
+// The product kernel, with specialised warps (384 threads): warp 8 lane 0
+// loads each k-block of A' and B' with the tensor-memory accelerator (3-D
+// tensor maps over [item][row][S*K2], 128 x 128-byte boxes, 128-byte swizzle;
+// rows past the matrix read as zero) into a 4-stage ring; warp 9 lane 0
+// issues the MMAs as soon as a stage is full and releases it with
+// tcgen05.commit; warps 0-7 (TMEM lanes 32 (w % 4) ..., 64 columns per warp
+// half) read each finished diagonal's accumulator with tcgen05.ld, add it,
+// scaled by 2^(-7s), to FP64 registers and release it.  Barriers: full and
+// empty per stage; per accumulator "finished" (commit) and "drained" (one
+// arrival per drain warp).
+struct OzArgs2 {
+    int a_items, b_items;  // 0: the operand is shared by all items
+    const int* ea;
+    long ea_item;
+    const int* fb;
+    long fb_item;
+    int M, N, K2, S;
+    cd* C;
+    long c_item, sc_i, sc_j;
+    int* err;
+};
+
+__device__ __forceinline__ void tma_load3(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];\n"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+
+__global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_constant__ CUtensorMap tmA,
+                                                             const __grid_constant__ CUtensorMap tmB, OzArgs2 p) {
     extern __shared__ char oz_raw[];
     char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(oz_raw) + 1023) & ~uintptr_t(1023));
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + OZ_STAGES * OZ_STAGE_BYTES);  // [STAGES] stage, [2] accumulator
-    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(bars + OZ_STAGES + 2);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + OZ_STAGES * OZ_STAGE_BYTES);
+    uint64_t* empty = full + OZ_STAGES;
+    uint64_t* accf = empty + OZ_STAGES;  // [2]
+    uint64_t* acce = accf + 2;           // [2]
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(acce + 2);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(s_tmem + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int item = blockIdx.z;
-    const int i0 = blockIdx.y * OZ_BM, j0 = blockIdx.x * OZ_BN;  // j0: column of C' (2 per complex column)
-    const int arows = min(OZ_BM, p.M - i0), brows = min(OZ_BN, 2 * p.N - j0);
-    const int8_t* Ab = p.A + item * p.a_item + (long)i0 * p.a_row;
-    const int8_t* Bb = p.B + item * p.b_item + (long)j0 * p.b_row;
+    const int i0 = blockIdx.y * OZ_BM, j0 = blockIdx.x * OZ_BN;
 
     if (tid == 0) {
-        for (int s = 0; s < OZ_STAGES + 2; ++s)
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&bars[s])) : "memory");
+        for (int q = 0; q < OZ_STAGES; ++q) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[q])) : "memory");
+        }
+        for (int q = 0; q < 2; ++q) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&accf[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 8;\n" ::"r"(smem_u32(&acce[q])) : "memory");
+        }
+        *s_fail = 0;
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     if (warp == 0) {
@@ -179,78 +171,61 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) oz_gemm_kernel(OzArgs p) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     const uint32_t tmem = *s_tmem;
-
-    // k-block sequence: diagonal s has (s+1) K2 / BK blocks
     const int kbd = p.K2 / OZ_BK;
     int total = 0;
     for (int s = 0; s < p.S; ++s) total += (s + 1) * kbd;
-    auto block_of = [&](int it, int& s, int& kb) {
-        s = 0;
-        while (it >= (s + 1) * kbd) {
-            it -= (s + 1) * kbd;
-            ++s;
+
+    // single-thread bounded wait (the roles below run on one lane)
+    auto wait1 = [&](uint32_t bar, uint32_t parity) {
+        const unsigned long long t0 = gtimer();
+        while (true) {
+            uint32_t ok;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(ok)
+                : "r"(bar), "r"(parity)
+                : "memory");
+            if (ok) return true;
+            if (*s_fail || gtimer() - t0 > OZ_WAIT_NS) {
+                *s_fail = 1;
+                return false;
+            }
         }
-        kb = it;
-    };
-    auto issue_load = [&](int it) {
-        int s, kb;
-        block_of(it, s, kb);
-        char* st = smem + (it % OZ_STAGES) * OZ_STAGE_BYTES;
-        oz_load_stage(st, Ab, p.a_row, arows, Bb, p.b_row, brows, (long)kb * OZ_BK,
-                      (long)(p.S - 1 - s) * p.K2 + (long)kb * OZ_BK, tid);
     };
 
-    double acc[64];
-#pragma unroll
-    for (int q = 0; q < 64; ++q) acc[q] = 0.0;
-    const int lane_base = 32 * (warp & 3), col_base = 64 * (warp >> 2);
-    // adds the accumulator of diagonal s, times 2^(-7s), to acc; false when the wait expired
-    auto drain = [&](int s) {
-        const uint32_t bar = smem_u32(&bars[OZ_STAGES + (s & 1)]);
-        if (!mbar_wait(bar, (uint32_t)((s >> 1) & 1))) return false;
-        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-        const double sc = ldexp(1.0, -7 * s);
-        const uint32_t base = tmem + ((uint32_t)lane_base << 16) + (uint32_t)((s & 1) * OZ_BN + col_base);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            uint32_t v[16];
-            tmem_ld16(base + 16 * q, v);
-            asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-            for (int e = 0; e < 16; ++e) acc[16 * q + e] = fma((double)(int)v[e], sc, acc[16 * q + e]);
+    int issued = 0;                // producer: k-blocks whose loads were issued
+    if (warp == 8 && lane == 0) {  // producer
+        int s = 0, kb = 0;
+        for (int it = 0; it < total; ++it) {
+            const int st = it % OZ_STAGES, use = it / OZ_STAGES;
+            if (use >= 1 && !wait1(smem_u32(&empty[st]), (uint32_t)((use - 1) & 1))) break;
+            const uint32_t fb = smem_u32(&full[st]);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(OZ_STAGE_BYTES)
+                         : "memory");
+            const uint32_t dst = smem_u32(smem + st * OZ_STAGE_BYTES);
+            tma_load3(dst, &tmA, kb * OZ_BK, i0, p.a_items ? item : 0, fb);
+            tma_load3(dst + OZ_BM * OZ_BK, &tmB, (p.S - 1 - s) * p.K2 + kb * OZ_BK, j0, p.b_items ? item : 0, fb);
+            issued = it + 1;
+            if (++kb == (s + 1) * kbd) {
+                kb = 0;
+                ++s;
+            }
         }
-        asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-        return true;
-    };
-
-    for (int it = 0; it < OZ_STAGES - 1 && it < total; ++it) issue_load(it);
-    int s_cur = 0, kb_end = kbd;  // diagonal of iteration it and the iteration that ends it
-    int issued_to = -1;           // last iteration whose tensor-core work was issued
-    int my_fail = 0;              // this thread saw a wait expire
-    bool failed = false;          // some thread did (uniform across the CTA)
-    for (int it = 0; it < total; ++it) {
-        if (it == kb_end) {  // iteration it starts diagonal s_cur + 1
-            ++s_cur;
-            kb_end += (s_cur + 1) * kbd;
-        }
-        // this stage's bytes have landed (all but the newest STAGES-2 groups)
-        if (it + OZ_STAGES - 1 <= total) asm volatile("cp.async.wait_group %0;\n" ::"n"(OZ_STAGES - 2) : "memory");
-        else asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        if (__syncthreads_or(my_fail)) {
-            failed = true;
-            break;
-        }
-        if (tid == 0) {
+    } else if (warp == 9 && lane == 0) {  // MMA issuer
+        int s = 0, kb = 0, last = -1;
+        for (int it = 0; it < total; ++it) {
+            const int st = it % OZ_STAGES, use = it / OZ_STAGES;
+            if (kb == 0 && s >= 2 && !wait1(smem_u32(&acce[s & 1]), (uint32_t)(((s >> 1) - 1) & 1))) break;
+            if (!wait1(smem_u32(&full[st]), (uint32_t)(use & 1))) break;
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const uint32_t sa = smem_u32(smem + (it % OZ_STAGES) * OZ_STAGE_BYTES);
-            const uint32_t sb = sa + OZ_BM * OZ_BK;
-            const uint32_t dt = tmem + (uint32_t)((s_cur & 1) * OZ_BN);
-            const int first = (it == kb_end - (s_cur + 1) * kbd);  // first k-block of the diagonal
+            const uint32_t sa = smem_u32(smem + st * OZ_STAGE_BYTES), sb = sa + OZ_BM * OZ_BK;
+            const uint32_t dt = tmem + (uint32_t)((s & 1) * OZ_BN);
 #pragma unroll
             for (int k = 0; k < OZ_BK / 32; ++k) {
                 const uint64_t da = sw128_desc(sa + 32 * k), db = sw128_desc(sb + 32 * k);
-                const uint32_t accum = (first && k == 0) ? 0u : 1u;
+                const uint32_t accum = (kb == 0 && k == 0) ? 0u : 1u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
                     "setp.ne.b32 p, %4, 0;\n\t"
@@ -259,35 +234,85 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) oz_gemm_kernel(OzArgs p) {
                     : "memory");
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                             smem_u32(&bars[it % OZ_STAGES]))
+                             smem_u32(&empty[st]))
                          : "memory");
-            if (it == kb_end - 1)
+            last = it;
+            if (++kb == (s + 1) * kbd) {
                 asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-                                 smem_u32(&bars[OZ_STAGES + (s_cur & 1)]))
+                                 smem_u32(&accf[s & 1]))
                              : "memory");
-        }
-        issued_to = it;
-        // refill the stage of iteration it - 1 once its tensor-core reads are done
-        const int nxt = it + OZ_STAGES - 1;
-        if (nxt < total) {
-            bool ready = true;
-            if (it >= 1) {
-                const int prev = it - 1;
-                ready = mbar_wait(smem_u32(&bars[prev % OZ_STAGES]), (uint32_t)((prev / OZ_STAGES) & 1));
+                kb = 0;
+                ++s;
             }
-            if (ready) issue_load(nxt);
-            else my_fail = 1;
         }
-        // the previous diagonal is complete once this one has started
-        if (!my_fail && it == kb_end - (s_cur + 1) * kbd && s_cur >= 1 && !drain(s_cur - 1)) my_fail = 1;
+        // the tensor core has finished every issued MMA before TMEM is freed
+        if (last >= 0) {
+            const unsigned long long t0 = gtimer();
+            while (true) {
+                uint32_t ok;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}"
+                    : "=r"(ok)
+                    : "r"(smem_u32(&empty[last % OZ_STAGES])), "r"((uint32_t)((last / OZ_STAGES) & 1))
+                    : "memory");
+                if (ok) break;
+                if (gtimer() - t0 > OZ_WAIT_NS) {
+                    *s_fail = 1;
+                    break;
+                }
+            }
+        }
     }
-    if (!failed && !my_fail && !drain(p.S - 1)) my_fail = 1;
-    asm volatile("cp.async.wait_group 0;\n" ::: "memory");
-    // all tensor-core work of this CTA has finished before TMEM is freed
-    if (issued_to >= 0 && !mbar_wait(smem_u32(&bars[issued_to % OZ_STAGES]), (uint32_t)((issued_to / OZ_STAGES) & 1)))
-        my_fail = 1;
+    double acc[64];
+#pragma unroll
+    for (int q = 0; q < 64; ++q) acc[q] = 0.0;
+    const int lane_base = 32 * (warp & 3), col_base = 64 * ((warp >> 2) & 1);
+    if (warp < 8) {  // drain
+        for (int s = 0; s < p.S; ++s) {
+            if (!mbar_wait(smem_u32(&accf[s & 1]), (uint32_t)((s >> 1) & 1))) {
+                *s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const double sc = ldexp(1.0, -7 * s);
+            const uint32_t base = tmem + ((uint32_t)lane_base << 16) + (uint32_t)((s & 1) * OZ_BN + col_base);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                uint32_t v[16];
+                tmem_ld16(base + 16 * q, v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+                for (int e = 0; e < 16; ++e) acc[16 * q + e] = fma((double)(int)v[e], sc, acc[16 * q + e]);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(&acce[s & 1])) : "memory");
+        }
+    }
     asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    const bool ok = !__syncthreads_or(my_fail) && !failed;
+    __syncthreads();
+    // after a failure, loads issued but never consumed land before the CTA
+    // exits: the latest use of each stage completes its phase (bounded waits)
+    if (warp == 8 && lane == 0 && *s_fail) {
+        for (int it = max(0, issued - OZ_STAGES); it < issued; ++it) {
+            const unsigned long long t0 = gtimer();
+            while (true) {
+                uint32_t ok;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                    "selp.u32 %0, 1, 0, p;\n\t}"
+                    : "=r"(ok)
+                    : "r"(smem_u32(&full[it % OZ_STAGES])), "r"((uint32_t)((it / OZ_STAGES) & 1))
+                    : "memory");
+                if (ok || gtimer() - t0 > OZ_WAIT_NS) break;
+            }
+        }
+    }
+    __syncthreads();
+    const bool ok = !*s_fail;
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(OZ_TMEM_COLS)
@@ -297,9 +322,8 @@ __global__ void __launch_bounds__(OZ_THREADS, 1) oz_gemm_kernel(OzArgs p) {
         if (tid == 0) atomicExch(p.err, 1);
         return;
     }
-    // C(i, j) = 2^(e_i + f_j - 14) acc, real and imaginary parts in adjacent columns
-    const int r = lane_base + lane;
-    const int i = i0 + r;
+    if (warp >= 8) return;
+    const int i = i0 + lane_base + lane;
     if (i >= p.M) return;
     const int ei = p.ea[item * p.ea_item + i];
     cd* crow = p.C + item * p.c_item + (long)i * p.sc_i;
@@ -383,6 +407,37 @@ __global__ void oz_prep_kernel(OzSrc q, int R, int K, int K2, int S, int is_b, i
     }
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+    static PFN_cuTensorMapEncodeTiled_v12000 f = nullptr;
+    if (!f) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        PGX_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+        PGX_CHECK(fn && q == cudaDriverEntryPointSuccess, PGX_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+        f = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    return f;
+}
+
+// Tensor map over digits [items][rows][row_bytes] (bytes): 128-byte x 128-row
+// boxes, 128-byte swizzle, zero fill past the rows.
+CUtensorMap digit_map(const void* base, long row_bytes, long rows, long items) {
+    PGX_CHECK(reinterpret_cast<uintptr_t>(base) % 16 == 0 && row_bytes % 16 == 0, PGX_ERR_ARG,
+              "split product: unaligned digit buffer");
+    CUtensorMap m;
+    const cuuint64_t dims[3] = {(cuuint64_t)row_bytes, (cuuint64_t)rows, (cuuint64_t)items};
+    const cuuint64_t strides[2] = {(cuuint64_t)row_bytes, (cuuint64_t)(row_bytes * rows)};
+    const cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)OZ_BM, 1u};
+    const cuuint32_t es[3] = {1u, 1u, 1u};
+    const CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims,
+                                            strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                                            CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    PGX_CHECK(r == CUDA_SUCCESS, PGX_ERR_CUDA, "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")");
+    return m;
+}
+
 }  // namespace
 
 bool oz_supported(int M, int N, int K) { return M > 0 && N > 0 && K > 0 && 2L * K <= (1L << 20); }
@@ -418,7 +473,7 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
     }
     static bool attr = false;
     if (!attr) {
-        PGX_CUDA(cudaFuncSetAttribute(oz_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM));
+        PGX_CUDA(cudaFuncSetAttribute(oz_gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM));
         attr = true;
     }
     using SA = typename src_t<TA>::type;
@@ -463,13 +518,11 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
             oz_prep_kernel<<<grid, 256, 0, st>>>(q, N, K, K2, S, 1, w.B.as<int8_t>(), b_bytes, w.fb.as<int>(), N);
             check_launch("oz_prep_kernel");
         }
-        OzArgs a{};
-        a.A = w.A.as<int8_t>();
-        a.a_item = a_item ? a_bytes : 0;
-        a.a_row = row_bytes;
-        a.B = w.B.as<int8_t>();
-        a.b_item = b_item ? b_bytes : 0;
-        a.b_row = row_bytes;
+        const CUtensorMap tmA = digit_map(w.A.p, row_bytes, M, a_item ? cn : 1);
+        const CUtensorMap tmB = digit_map(w.B.p, row_bytes, 2L * N, b_item ? cn : 1);
+        OzArgs2 a{};
+        a.a_items = a_item;
+        a.b_items = b_item;
         a.ea = w.ea.as<int>();
         a.ea_item = a_item ? M : 0;
         a.fb = w.fb.as<int>();
@@ -484,8 +537,8 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
         a.sc_j = g.sc_j;
         a.err = w.err.as<int>();
         dim3 grid((unsigned)ceil_div(2L * N, OZ_BN), (unsigned)ceil_div((long)M, OZ_BM), (unsigned)cn);
-        oz_gemm_kernel<<<grid, OZ_THREADS, OZ_SMEM, st>>>(a);
-        check_launch("oz_gemm_kernel");
+        oz_gemm_tma_kernel<<<grid, 384, OZ_SMEM, st>>>(tmA, tmB, a);
+        check_launch("oz_gemm_tma_kernel");
     }
 }
 

@@ -281,6 +281,7 @@ PYBIND11_MODULE(_pomerol, m) {
         .def_readwrite("CoefficientTolerance", &TwoParticleGF::CoefficientTolerance)
         .def_readwrite("AnchorTolerance", &TwoParticleGF::AnchorTolerance)
         .def_readwrite("ExactSum", &TwoParticleGF::ExactSum)
+        .def_readwrite("SplitProducts", &TwoParticleGF::SplitProducts)
         .def("prepare", &TwoParticleGF::prepare)
         .def("compute",
              [](TwoParticleGF& g, bool clear, std::vector<std::tuple<C, C, C>> const& f, int) {
@@ -311,6 +312,7 @@ PYBIND11_MODULE(_pomerol, m) {
              py::keep_alive<1, 3>(), py::keep_alive<1, 4>(), py::keep_alive<1, 5>(), py::keep_alive<1, 6>())
         .def_readwrite("PoleResolution", &TwoParticleGFContainer::PoleResolution)
         .def_readwrite("CoefficientTolerance", &TwoParticleGFContainer::CoefficientTolerance)
+        .def_readwrite("SplitProducts", &TwoParticleGFContainer::SplitProducts)
         .def("prepareAll",
              [](TwoParticleGFContainer& g, std::vector<std::array<ParticleIndex, 4>> const& idx) {
                  std::set<IndexCombination4> s;

@@ -152,6 +152,10 @@ public:
     // AnchorTolerance); ExactSum = true sums every state quadruple instead.
     RealType AnchorTolerance = 1e-15;
     bool ExactSum = false;
+    // SplitProducts = true runs the anchored sum's largest products on the int8
+    // tensor cores (six 7-bit slices per operand, FP64 recombination; about
+    // 1e-11 relative error of G2).  Ignored with ExactSum.
+    bool SplitProducts = false;
 
     TwoParticleGF(StatesClassification const& S, Hamiltonian const& H, AnnihilationOperator const& C1,
                   AnnihilationOperator const& C2, CreationOperator const& CX3, CreationOperator const& CX4,
@@ -200,6 +204,7 @@ class TwoParticleGFContainer : public Thermal {
 public:
     RealType PoleResolution = 1e-8;
     RealType CoefficientTolerance = 1e-16;
+    bool SplitProducts = false;  // passed to every element (TwoParticleGF::SplitProducts)
 
     TwoParticleGFContainer(IndexClassification const& IndexInfo, StatesClassification const& S, Hamiltonian const& H,
                            DensityMatrix const& DM, FieldOperatorContainer const& Ops);

@@ -274,7 +274,8 @@ std::vector<ComplexType> TwoParticleGF::values(FreqVec3 const& freqs) const {
     // ExactSum evaluates every state quadruple.
     const double anchor = std::min(CoefficientTolerance, AnchorTolerance);
     dev.check(pgx_g2(dev.ctx(), (int32_t)parts.size(), parts.data(), (int32_t)freqs.size(), z.data(), PoleResolution,
-                     ExactSum ? 0.0 : anchor, ExactSum ? PGX_G2_EXACT : PGX_G2_ANCHORED,
+                     ExactSum ? 0.0 : anchor,
+                     ExactSum ? PGX_G2_EXACT : (PGX_G2_ANCHORED | (SplitProducts ? PGX_G2_SPLIT_I8 : 0)),
                      reinterpret_cast<double*>(out.data())),
               "pgx_g2");
     return out;
@@ -372,6 +373,7 @@ void TwoParticleGFContainer::prepareAll(std::set<IndexCombination4> const& Indic
         TwoParticleGF& g = kv.second.element();
         g.PoleResolution = PoleResolution;
         g.CoefficientTolerance = CoefficientTolerance;
+        g.SplitProducts = SplitProducts;
         g.prepare();
     }
 }
@@ -381,6 +383,7 @@ std::map<IndexCombination4, std::vector<ComplexType>> TwoParticleGFContainer::co
                                                                                          MPI_Comm const& comm,
                                                                                          bool split) {
     std::map<IndexCombination4, std::vector<ComplexType>> out;
+    for (auto& kv : NonTrivialElements) kv.second->SplitProducts = SplitProducts;
     if (split) {
         for (auto& kv : NonTrivialElements) out[kv.first] = kv.second->compute(clearTerms, freqs, comm);
     } else {
@@ -395,6 +398,7 @@ ElementWithPermFreq<TwoParticleGF>& TwoParticleGFContainer::operator()(IndexComb
     auto& e = create(I);
     e.element().PoleResolution = PoleResolution;
     e.element().CoefficientTolerance = CoefficientTolerance;
+    e.element().SplitProducts = SplitProducts;
     e.element().prepare();
     return e;
 }

@@ -25,11 +25,14 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="the first M models of the batch workload")
     ap.add_argument("--chain", action="store_true", help="time the drop-in chain stage by stage")
     ap.add_argument("--g2-cubes", type=int, nargs="*", default=[], help="cube sides for the G2 stage of --chain")
+    ap.add_argument("--split", action="store_true",
+                    help="anchored G2 with its stacked products on the int8 tensor cores (PGX_G2_SPLIT_I8); "
+                         "with --chain each cube also runs in FP64 for the error")
     ap.add_argument("--autotune", action="store_true",
                     help="measure the GEMM tile classes on one step (after one untimed step) before timing")
     a = ap.parse_args()
     if a.chain:
-        chain(a.config, a.g2_cubes, a.kernels)
+        chain(a.config, a.g2_cubes, a.kernels, a.split)
         return
     import torch  # noqa: F401  (CUDA context for the process)
     from .workloads import BatchRun, Chi3Run, EngineRun, Problem, b64_params, matsubara_cube, matsubara_square
@@ -58,7 +61,7 @@ def main():
         run = Chi3Run(prob)
     else:
         _, z = matsubara_cube(prob.beta, prob.nfreq)
-        run = EngineRun(prob)
+        run = EngineRun(prob, split=a.split)
     if a.autotune:
         autotune(run.eng, lambda: run.step(z))
     for s in range(a.steps):
@@ -87,7 +90,7 @@ def autotune(eng, step):
     print(f"autotune: {n} size buckets off the padding rule ({1e3 * (time.perf_counter() - t0):.1f} ms)", flush=True)
 
 
-def chain(config, cubes, kernels=False):
+def chain(config, cubes, kernels=False, split=False):
     import torch  # noqa: F401  (CUDA context for the process)
     from . import _pomerol as P
     from .workloads import EngineRun, Problem, matsubara_cube
@@ -131,22 +134,30 @@ def chain(config, cubes, kernels=False):
     t4 = time.perf_counter()
     print(f"chi_zz on 48 bosonic frequencies (4 pair susceptibilities): {t4 - t3:.3f} s, chi_zz(0) = {zz[0]:.10e}")
     if cubes:
-        run = EngineRun(prob)
+        runs = [("fp64", EngineRun(prob))] + ([("split-i8", EngineRun(prob, split=True))] if split else [])
         for i, n in enumerate(cubes):
             _, z = matsubara_cube(prob.beta, n)
-            prof = kernels and i == len(cubes) - 1
-            if prof:
-                run.eng.profile_begin()
-            run.eng.timer_begin()
-            t = time.perf_counter()
-            run.step(z)
-            ms = run.eng.timer_end()
-            print(f"G2 step (eigensolve + weights + rotation + G2) on {len(z)} triples: device {ms:.0f} ms, "
-                  f"wall {time.perf_counter() - t:.1f} s, g2 {run.eng.g2_timing()['total_ms'] / 1e3:.1f} s", flush=True)
-            if prof:
-                for k in run.eng.profile_end()[:10]:
-                    print(f"  {k['name']:48s} x{k['launches']:<5d} {k['ms'] / 1e3:8.2f} s  "
-                          f"{k['flops'] / max(k['ms'], 1e-9) / 1e9:7.2f} TFLOP/s", flush=True)
+            ref = None
+            for label, run in runs:
+                prof = kernels and i == len(cubes) - 1
+                if prof:
+                    run.eng.profile_begin()
+                run.eng.timer_begin()
+                t = time.perf_counter()
+                v = run.step(z)
+                ms = run.eng.timer_end()
+                extra = ""
+                if ref is None:
+                    ref = v
+                else:
+                    extra = f", max|diff| / max|G2| vs fp64 {np.abs(v - ref).max() / np.abs(ref).max():.2e}"
+                print(f"G2 step [{label}] (eigensolve + weights + rotation + G2) on {len(z)} triples: device {ms:.0f} "
+                      f"ms, wall {time.perf_counter() - t:.1f} s, g2 {run.eng.g2_timing()['total_ms'] / 1e3:.1f} s"
+                      f"{extra}", flush=True)
+                if prof:
+                    for k in run.eng.profile_end()[:10]:
+                        print(f"  {k['name']:48s} x{k['launches']:<5d} {k['ms'] / 1e3:8.2f} s  "
+                              f"{k['flops'] / max(k['ms'], 1e-9) / 1e9:7.2f} TFLOP/s", flush=True)
 
 
 if __name__ == "__main__":

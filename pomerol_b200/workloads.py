@@ -311,9 +311,11 @@ class EngineRun:
     """The G2 stage chain on one libpgx context with the Hamiltonian resident
     in HBM: eigensolve, weights, rotation of c^+ and c, G2 on the triples."""
 
-    def __init__(self, prob: Problem, device=0, anchored=True, anchor_tol=1e-16):
-        from .pgx import PGX_G2_ANCHORED, PGX_G2_EXACT, Engine
+    def __init__(self, prob: Problem, device=0, anchored=True, anchor_tol=1e-16, split=False):
+        from .pgx import PGX_G2_ANCHORED, PGX_G2_EXACT, PGX_G2_SPLIT_I8, Engine
         self.flags = PGX_G2_ANCHORED if anchored else PGX_G2_EXACT
+        if split and anchored:
+            self.flags |= PGX_G2_SPLIT_I8  # stacked products on the int8 tensor cores
         self.anchor_tol = anchor_tol if anchored else 0.0
         self.prob = prob
         blocks, self.actions, self.chains = prob.engine_inputs()

@@ -287,8 +287,10 @@ def test_vertex4_reference_case(P):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("split", [True, False])
-def test_anderson2pgf_reference_case(P, split):
+@pytest.mark.parametrize("split,products", [(True, False), (False, False), (True, True)])
+def test_anderson2pgf_reference_case(P, split, products):
+    """Anderson2PGFTest's golden chi values through the container; products=True
+    also runs the stacked products on the int8 tensor cores (SplitProducts)."""
     L = P.LatticePresets
     k = KATS["anderson2pgf"]
     HExpr = L.CoulombS("C", k["U"], -k["mu"])
@@ -313,6 +315,7 @@ def test_anderson2pgf_reference_case(P, split):
     Chi4 = P.TwoParticleGFContainer(ii, S, H, rho, ops)
     Chi4.PoleResolution = k["pole_resolution"]
     Chi4.CoefficientTolerance = k["coefficient_tolerance"]
+    Chi4.SplitProducts = products
     Chi4.prepareAll([(u0, u0, u0, u0), (u0, d0, u0, d0), (d0, d0, d0, d0)])
     Om, om = 1j * 2 * np.pi / beta, 1j * np.pi / beta
     freqs = [(om + Om, 1j * (2 * i + 1) * np.pi / beta, om) for i in range(10)]
