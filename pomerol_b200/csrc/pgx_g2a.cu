@@ -422,21 +422,35 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
     };
     // the stacked products read Lc, Pr, rho and Rc written by the first two
     // launches; with `split` slices they run on the int8 tensor cores
-    auto launch_stacked = [&](auto& probs) {
+    // products of at least 1e8 complex multiply-adds go to the tensor cores
+    // (smaller ones do not repay the digit preparation and tile padding);
+    // complex Hamiltonians keep the anchored products in FP64
+    auto launch_split = [&](auto& probs) {
         if (!split) {
             launch(probs);
             return;
         }
+        std::remove_reference_t<decltype(probs)> rest;
         for (const auto& g : probs) {
             const double macs = (double)g.M * g.N * g.K * std::max(g.nb, 1);
+            if (macs < 1e8) {
+                rest.push_back(g);
+                continue;
+            }
             ProfRange pr("oz_split_gemm", st, 8.0 * macs, 0.0);
             oz_zgemm(g, split, c->oz, st);
         }
+        launch(rest);
     };
-    launch(pa);
-    launch(pb);
-    launch_stacked(pc);
-    launch_stacked(pd);
+    if constexpr (TC) {
+        launch(pa);
+        launch(pb);
+    } else {
+        launch_split(pa);
+        launch_split(pb);
+    }
+    launch_split(pc);
+    launch_split(pd);
     // ---- contractions per triple
     std::vector<DTerm> dt;
     for (size_t j = 0; j < idx.size(); ++j) {

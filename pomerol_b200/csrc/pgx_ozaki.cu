@@ -345,6 +345,7 @@ __global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_consta
 struct OzSrc {
     const void* X;
     int cplx;
+    const int* ridx;  // output row r reads source row ridx[r] (nullable), energies included
     long s_r, s_k, s_item;
     const double *Er, *Ek;
     int rk_order;  // 1: dressed matrix has rows r, columns k; 0: rows k, columns r
@@ -352,6 +353,7 @@ struct OzSrc {
 };
 
 __device__ __forceinline__ cd oz_value(const OzSrc& q, int item, int r, int k) {
+    if (q.ridx) r = q.ridx[r];
     const long off = item * q.s_item + (long)r * q.s_r + (long)k * q.s_k;
     const cd x = q.cplx ? static_cast<const cd*>(q.X)[off] : cd{static_cast<const double*>(q.X)[off], 0.0};
     if (!q.Er) return x;
@@ -447,8 +449,8 @@ template <typename TA, typename TB>
 void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t st) {
     static_assert(!is_dressed<TA>::value || !is_dressed<TB>::value, "one dressed operand at most");
     const int M = g.M, N = g.N, K = g.K, nb = std::max(g.nb, 1);
-    PGX_CHECK(!g.accumulate && !g.a_kidx && !g.b_kidx && !g.kscale && !g.a_iidx && !g.b_jidx && !g.conj_a,
-              PGX_ERR_ARG, "split product: plain strided operands only");
+    PGX_CHECK(!g.accumulate && !g.a_kidx && !g.b_kidx && !g.kscale && !g.conj_a, PGX_ERR_ARG,
+              "split product: strided operands with row / column gathers only");
     PGX_CHECK(S >= 1 && S <= 8, PGX_ERR_ARG, "split product: 1..8 slices");
     const int K2 = (int)(ceil_div(2L * K, OZ_BK) * OZ_BK);
     const long row_bytes = (long)S * K2;
@@ -485,6 +487,7 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
             OzSrc q{};
             q.X = g.A + (a_item ? b0 * g.ba : 0);
             q.cplx = is_cd<SA>::value;
+            q.ridx = g.a_iidx;
             q.s_r = g.sa_i;
             q.s_k = g.sa_k;
             q.s_item = g.ba;
@@ -504,6 +507,7 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
             OzSrc q{};
             q.X = g.B + (b_item ? b0 * g.bb : 0);
             q.cplx = is_cd<SB>::value;
+            q.ridx = g.b_jidx;
             q.s_r = g.sb_j;
             q.s_k = g.sb_k;
             q.s_item = g.bb;
@@ -547,6 +551,10 @@ template void oz_zgemm<Dressed<cd>, cd>(const GemmProblem<Dressed<cd>, cd, cd>&,
 template void oz_zgemm<cd, Dressed<double>>(const GemmProblem<cd, Dressed<double>, cd>&, int, OzWork&, cudaStream_t);
 template void oz_zgemm<cd, Dressed<cd>>(const GemmProblem<cd, Dressed<cd>, cd>&, int, OzWork&, cudaStream_t);
 template void oz_zgemm<cd, cd>(const GemmProblem<cd, cd, cd>&, int, OzWork&, cudaStream_t);
+template void oz_zgemm<double, Dressed<double>>(const GemmProblem<double, Dressed<double>, cd>&, int, OzWork&,
+                                                cudaStream_t);
+template void oz_zgemm<Dressed<double>, double>(const GemmProblem<Dressed<double>, double, cd>&, int, OzWork&,
+                                                cudaStream_t);
 
 }  // namespace pgx
 
