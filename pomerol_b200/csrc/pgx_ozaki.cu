@@ -44,6 +44,7 @@ namespace {
 
 constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 128;  // tile rows, tile columns, k-block bytes
 constexpr int OZ_STAGES = 4;
+constexpr int OZ_GROUP_M = 8;
 constexpr int OZ_STAGE_BYTES = (OZ_BM + OZ_BN) * OZ_BK;  // 32 KiB
 constexpr int OZ_SMEM = OZ_STAGES * OZ_STAGE_BYTES + 1024 + 256;
 constexpr int OZ_TMEM_COLS = 2 * OZ_BN;  // two accumulators
@@ -117,6 +118,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 // empty per stage; per accumulator "finished" (commit) and "drained" (one
 // arrival per drain warp).
 struct OzArgs2 {
+    int tiles_m, tiles_n;  // tile counts of C' (blockIdx.x enumerates both, grouped by OZ_GROUP_M row tiles)
     int a_items, b_items;  // 0: the operand is shared by all items
     const int* ea;
     long ea_item;
@@ -147,7 +149,12 @@ __global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_consta
     volatile int* s_fail = reinterpret_cast<volatile int*>(s_tmem + 1);
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int item = blockIdx.z;
-    const int i0 = blockIdx.y * OZ_BM, j0 = blockIdx.x * OZ_BN;
+    // tiles in groups of OZ_GROUP_M row tiles, columns within a group: the
+    // CTAs resident together share few A and B panels, which then stay in L2
+    const int lin = blockIdx.x, per_group = OZ_GROUP_M * p.tiles_n;
+    const int first_m = (lin / per_group) * OZ_GROUP_M, gsz = min(p.tiles_m - first_m, OZ_GROUP_M);
+    const int tm = first_m + (lin % per_group) % gsz, tn = (lin % per_group) / gsz;
+    const int i0 = tm * OZ_BM, j0 = tn * OZ_BN;
 
     if (tid == 0) {
         for (int q = 0; q < OZ_STAGES; ++q) {
@@ -540,7 +547,10 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
         a.sc_i = g.sc_i;
         a.sc_j = g.sc_j;
         a.err = w.err.as<int>();
-        dim3 grid((unsigned)ceil_div(2L * N, OZ_BN), (unsigned)ceil_div((long)M, OZ_BM), (unsigned)cn);
+        a.tiles_m = (int)ceil_div((long)M, OZ_BM);
+        a.tiles_n = (int)ceil_div(2L * N, OZ_BN);
+        PGX_CHECK((long)a.tiles_m * a.tiles_n < (1L << 31), PGX_ERR_ARG, "split product: too many tiles");
+        dim3 grid((unsigned)((long)a.tiles_m * a.tiles_n), 1u, (unsigned)cn);
         oz_gemm_tma_kernel<<<grid, 384, OZ_SMEM, st>>>(tmA, tmB, a);
         check_launch("oz_gemm_tma_kernel");
     }
