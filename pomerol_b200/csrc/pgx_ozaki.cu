@@ -20,10 +20,11 @@
 // Then diagonal s is one product of depth (s+1) K2 with A from offset 0 and
 // B from offset (S-1-s) K2: both operands are plain strided views.
 //
-// The GEMM kernel: one CTA per 128 x 128 tile of C' (64 complex columns) and
-// batch item; tcgen05.mma with M = N = 128 and K = 32 bytes per instruction,
-// into one of two TMEM accumulators (diagonals alternate between them), so
-// one diagonal is summed into FP64 while the next runs.  Every mbarrier wait
+// The GEMM kernel: one CTA per 128 x 256 tile of C' (128 complex columns) and
+// batch item; tcgen05.mma with M = 128, N = 256 and K = 32 bytes per
+// instruction, into one of two TMEM accumulators (diagonals alternate between
+// them, 2 x 256 = all 512 columns), so one diagonal is added into C while the
+// next runs.  Every mbarrier wait
 // is bounded (about 2 s of %globaltimer); on expiry the CTA sets the error
 // flag, stops issuing work, waits (bounded) for its copies and tensor-core
 // work in flight, frees its TMEM and returns.
@@ -42,12 +43,12 @@ namespace pgx {
 
 namespace {
 
-constexpr int OZ_BM = 128, OZ_BN = 128, OZ_BK = 128;  // tile rows, tile columns, k-block bytes
+constexpr int OZ_BM = 128, OZ_BN = 256, OZ_BK = 128;  // tile rows, tile columns, k-block bytes
 constexpr int OZ_STAGES = 4;
 constexpr int OZ_GROUP_M = 8;
-constexpr int OZ_STAGE_BYTES = (OZ_BM + OZ_BN) * OZ_BK;  // 32 KiB
+constexpr int OZ_STAGE_BYTES = (OZ_BM + OZ_BN) * OZ_BK;  // 48 KiB
 constexpr int OZ_SMEM = OZ_STAGES * OZ_STAGE_BYTES + 1024 + 256;
-constexpr int OZ_TMEM_COLS = 2 * OZ_BN;  // two accumulators
+constexpr int OZ_TMEM_COLS = 2 * OZ_BN;  // two accumulators: all 512 columns
 constexpr unsigned long long OZ_WAIT_NS = 2000000000ull;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -109,12 +110,14 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 
 // The product kernel, with specialised warps (384 threads): warp 8 lane 0
 // loads each k-block of A' and B' with the tensor-memory accelerator (3-D
-// tensor maps over [item][row][S*K2], 128 x 128-byte boxes, 128-byte swizzle;
-// rows past the matrix read as zero) into a 4-stage ring; warp 9 lane 0
+// tensor maps over [item][row][S*K2], 128-byte boxes of 128 (A) or 256 (B)
+// rows, 128-byte swizzle; rows past the matrix read as zero) into a 4-stage
+// ring; warp 9 lane 0
 // issues the MMAs as soon as a stage is full and releases it with
-// tcgen05.commit; warps 0-7 (TMEM lanes 32 (w % 4) ..., 64 columns per warp
+// tcgen05.commit; warps 0-7 (TMEM lanes 32 (w % 4) ..., 128 columns per warp
 // half) read each finished diagonal's accumulator with tcgen05.ld, add it,
-// scaled by 2^(-7s), to FP64 registers and release it.  Barriers: full and
+// scaled by 2^(e_i + f_j - 14 - 7s), into C (stored by the first diagonal,
+// read and added by the others; the tile stays in L2) and release it.  Barriers: full and
 // empty per stage; per accumulator "finished" (commit) and "drained" (one
 // arrival per drain warp).
 struct OzArgs2 {
@@ -272,26 +275,39 @@ __global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_consta
             }
         }
     }
-    double acc[64];
-#pragma unroll
-    for (int q = 0; q < 64; ++q) acc[q] = 0.0;
-    const int lane_base = 32 * (warp & 3), col_base = 64 * ((warp >> 2) & 1);
-    if (warp < 8) {  // drain
+    // drain: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its rows) and the
+    // 128 accumulator columns of half w / 4, and adds them, scaled, to C
+    const int lane_base = 32 * (warp & 3), col_base = 128 * ((warp >> 2) & 1);
+    if (warp < 8) {
+        const int i = i0 + lane_base + lane;
+        const bool row_ok = i < p.M;
+        const int ei = row_ok ? p.ea[item * p.ea_item + i] : 0;
+        cd* crow = p.C + item * p.c_item + (long)(row_ok ? i : 0) * p.sc_i;
+        const int* fbi = p.fb + item * p.fb_item;
         for (int s = 0; s < p.S; ++s) {
             if (!mbar_wait(smem_u32(&accf[s & 1]), (uint32_t)((s >> 1) & 1))) {
                 *s_fail = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-            const double sc = ldexp(1.0, -7 * s);
             const uint32_t base = tmem + ((uint32_t)lane_base << 16) + (uint32_t)((s & 1) * OZ_BN + col_base);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
+#pragma unroll 1
+            for (int q = 0; q < 8; ++q) {
                 uint32_t v[16];
                 tmem_ld16(base + 16 * q, v);
                 asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                if (row_ok) {
 #pragma unroll
-                for (int e = 0; e < 16; ++e) acc[16 * q + e] = fma((double)(int)v[e], sc, acc[16 * q + e]);
+                    for (int e = 0; e < 8; ++e) {
+                        const int jc = (j0 + col_base) / 2 + 8 * q + e;
+                        if (jc < p.N) {
+                            const double sc = ldexp(1.0, ei + fbi[jc] - 14 - 7 * s);
+                            const cd add{(double)(int)v[2 * e] * sc, (double)(int)v[2 * e + 1] * sc};
+                            cd& dst = crow[(long)jc * p.sc_j];
+                            dst = s == 0 ? add : cd{dst.x + add.x, dst.y + add.y};
+                        }
+                    }
+                }
             }
             asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
             __syncwarp();
@@ -325,23 +341,7 @@ __global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_consta
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(OZ_TMEM_COLS)
                      : "memory");
     }
-    if (!ok) {
-        if (tid == 0) atomicExch(p.err, 1);
-        return;
-    }
-    if (warp >= 8) return;
-    const int i = i0 + lane_base + lane;
-    if (i >= p.M) return;
-    const int ei = p.ea[item * p.ea_item + i];
-    cd* crow = p.C + item * p.c_item + (long)i * p.sc_i;
-#pragma unroll
-    for (int q = 0; q < 32; ++q) {
-        const int jc = (j0 + col_base) / 2 + q;
-        if (jc < p.N) {
-            const double sc = ldexp(1.0, ei + p.fb[item * p.fb_item + jc] - 14);
-            crow[(long)jc * p.sc_j] = cd{acc[2 * q] * sc, acc[2 * q + 1] * sc};
-        }
-    }
+    if (!ok && tid == 0) atomicExch(p.err, 1);
 }
 
 // Digits of an operand.  Output row r (a row of A', or a complex column of B
@@ -429,15 +429,15 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
     return f;
 }
 
-// Tensor map over digits [items][rows][row_bytes] (bytes): 128-byte x 128-row
+// Tensor map over digits [items][rows][row_bytes] (bytes): 128-byte x box_rows
 // boxes, 128-byte swizzle, zero fill past the rows.
-CUtensorMap digit_map(const void* base, long row_bytes, long rows, long items) {
+CUtensorMap digit_map(const void* base, long row_bytes, long rows, long items, int box_rows) {
     PGX_CHECK(reinterpret_cast<uintptr_t>(base) % 16 == 0 && row_bytes % 16 == 0, PGX_ERR_ARG,
               "split product: unaligned digit buffer");
     CUtensorMap m;
     const cuuint64_t dims[3] = {(cuuint64_t)row_bytes, (cuuint64_t)rows, (cuuint64_t)items};
     const cuuint64_t strides[2] = {(cuuint64_t)row_bytes, (cuuint64_t)(row_bytes * rows)};
-    const cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)OZ_BM, 1u};
+    const cuuint32_t box[3] = {(cuuint32_t)OZ_BK, (cuuint32_t)box_rows, 1u};
     const cuuint32_t es[3] = {1u, 1u, 1u};
     const CUresult r = tensor_map_encoder()(&m, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims,
                                             strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
@@ -529,8 +529,8 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
             oz_prep_kernel<<<grid, 256, 0, st>>>(q, N, K, K2, S, 1, w.B.as<int8_t>(), b_bytes, w.fb.as<int>(), N);
             check_launch("oz_prep_kernel");
         }
-        const CUtensorMap tmA = digit_map(w.A.p, row_bytes, M, a_item ? cn : 1);
-        const CUtensorMap tmB = digit_map(w.B.p, row_bytes, 2L * N, b_item ? cn : 1);
+        const CUtensorMap tmA = digit_map(w.A.p, row_bytes, M, a_item ? cn : 1, OZ_BM);
+        const CUtensorMap tmB = digit_map(w.B.p, row_bytes, 2L * N, b_item ? cn : 1, OZ_BN);
         OzArgs2 a{};
         a.a_items = a_item;
         a.b_items = b_item;
