@@ -322,7 +322,7 @@ struct Dress {
 template <typename TA, typename TB>
 GemmProblem<TA, TB, cd> gp(const typename src_t<TA>::type* A, long sai, long sak, const typename src_t<TB>::type* B,
                            long sbk, long sbj, cd* C, long sci, int M, int N, int K, const int* aii, const int* bjj,
-                           Dress dr, int nb, long bc) {
+                           Dress dr, int nb, long bc, long scj = 1) {
     GemmProblem<TA, TB, cd> g{};
     g.A = A;
     g.B = B;
@@ -335,7 +335,7 @@ GemmProblem<TA, TB, cd> gp(const typename src_t<TA>::type* A, long sai, long sak
     g.sb_k = sbk;
     g.sb_j = sbj;
     g.sc_i = sci;
-    g.sc_j = 1;
+    g.sc_j = scj;
     g.a_iidx = aii;
     g.b_jidx = bjj;
     g.dEa = dr.Ea;
@@ -384,31 +384,32 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
         const Dress A1{E1, E2, pl.dZ1};  // A1(z1) = O1 dressed with z1: d1 x d2, row-major
         const Dress C3{E3, E4, pl.dZ3};  // C3(z3) = O3 dressed with z3: d3 x d4, row-major
         // anchored products, one item per z1 (or z3)
-        if (r2) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lc, (long)N1 * r2, d4, r2, d1, nullptr, H2, A1, N1,
-                                       r2));                                              // Lc = X4 A1[:,H2]
+        // outputs that the contractions read along k are stored k-contiguous
+        if (r2) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lc, 1, d4, r2, d1, nullptr, H2, A1, N1,
+                                       (long)r2 * d4, d4));                               // Lc = X4 A1[:,H2]: [(i1,h)][k]
         if (r4) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lr, d2, r4, d2, d1, H4, nullptr, A1, N1,
                                        (long)r4 * d2));                                   // Lr = X4[H4,:] A1
         if (r1) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pr, d3, r1, d3, d2, H1, nullptr, A1, N1,
                                        (long)r1 * d3));                                   // Pr = A1[H1,:] O2
-        if (r3) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pc, r3, d1, r3, d2, nullptr, H3, A1, N1,
-                                       (long)d1 * r3));                                   // Pc = A1 O2[:,H3]
+        if (r3) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pc, 1, d1, r3, d2, nullptr, H3, A1, N1,
+                                       (long)d1 * r3, d1));                               // Pc = A1 O2[:,H3]: [i1][h][k]
         if (r3) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Rho, d1, r3, d1, d4, H3, nullptr, C3, N3,
                                        (long)r3 * d1));                                   // rho = C3[H3,:] X4
-        if (r1) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Qc, r1, d3, r1, d4, nullptr, H1, C3, N3,
-                                       (long)d3 * r1));                                   // Qc = C3 X4[:,H1]
+        if (r1) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Qc, 1, d3, r1, d4, nullptr, H1, C3, N3,
+                                       (long)d3 * r1, d3));                               // Qc = C3 X4[:,H1]: [i3][h][k]
         if (r2) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rr, d4, r2, d4, d3, H2, nullptr, C3, N3,
                                        (long)r2 * d4));                                   // Rr = O2[H2,:] C3
-        if (r4) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rc, (long)N3 * r4, d2, r4, d3, nullptr, H4, C3,
-                                       N3, r4));                                          // Rc = O2 C3[:,H4]
+        if (r4) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rc, 1, d2, r4, d3, nullptr, H4, C3, N3,
+                                       (long)r4 * d2, d2));                               // Rc = O2 C3[:,H4]: [(i3,h)][k]
         // products over (z1, z3): anchors of all frequencies stacked as columns / rows
-        if (r2) pc.push_back(gp<DT, cd>(O3, d4, 1, pool + w.Lc, (long)N1 * r2, 1, pool + w.V1a, (long)N1 * r2, d3, N1 * r2,
-                                        d4, nullptr, nullptr, C3, N3, (long)d3 * N1 * r2));   // V1a = C3 LcAll
+        if (r2) pc.push_back(gp<DT, cd>(O3, d4, 1, pool + w.Lc, 1, d4, pool + w.V1a, 1, d3, N1 * r2, d4, nullptr,
+                                        nullptr, C3, N3, (long)d3 * N1 * r2, d3));  // V1a = C3 LcAll: [i3][(i1,h)][k]
         if (r1) pd.push_back(gp<cd, DT>(pool + w.Pr, d3, 1, O3, d4, 1, pool + w.V2a, d4, N1 * r1, d4, d3, nullptr, nullptr,
                                         C3, N3, (long)N1 * r1 * d4));                         // V2a = PrAll C3
         if (r3) pd.push_back(gp<cd, DT>(pool + w.Rho, d1, 1, O1, d2, 1, pool + w.V1b, d2, N3 * r3, d2, d1, nullptr, nullptr,
                                         A1, N1, (long)N3 * r3 * d2));                         // V1b = rhoAll A1
-        if (r4) pc.push_back(gp<DT, cd>(O1, d2, 1, pool + w.Rc, (long)N3 * r4, 1, pool + w.V2b, (long)N3 * r4, d1, N3 * r4,
-                                        d2, nullptr, nullptr, A1, N1, (long)d1 * N3 * r4));   // V2b = A1 RcAll
+        if (r4) pc.push_back(gp<DT, cd>(O1, d2, 1, pool + w.Rc, 1, d2, pool + w.V2b, 1, d1, N3 * r4, d2, nullptr,
+                                        nullptr, A1, N1, (long)d1 * N3 * r4, d1));  // V2b = A1 RcAll: [i1][(i3,h)][k]
     }
     // descriptor buffers sized once for the largest list, before any launch
     {
@@ -496,15 +497,15 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
             return d;
         };
         const int opc = TC ? 1 : 0;
-        if (r2) {  // T1a: va = O2[h,k] (state h), vb = V1a[i3][k][(i1,h)]
+        if (r2) {  // T1a: va = O2[h,k] (state h), vb = V1a[i3][(i1,h)][k]
             DTerm d = base(1, r2, d3, 2, +1.0, 0, 0, 0.0, 1.0, -sign);
             d.VA = O2; d.va_cplx = opc; d.va_hstate = 1; d.ah = d3; d.ak = 1;
-            d.VB = pool + w.V1a; d.vb_cplx = 1; d.b3 = (long)d3 * N1 * r2; d.bk = N1 * r2; d.b1 = r2; d.bh = 1;
+            d.VB = pool + w.V1a; d.vb_cplx = 1; d.b3 = (long)d3 * N1 * r2; d.bk = 1; d.b1 = (long)r2 * d3; d.bh = d3;
             dt.push_back(d);
-            // T4a: va = Rr[i3][h][k], vb = LcAll[k][(i1,h)]
+            // T4a: va = Rr[i3][h][k], vb = Lc[(i1,h)][k]
             DTerm e = base(1, r2, d4, 3, +1.0, 3, 1, -1.0, 1.0, sign);
             e.VA = pool + w.Rr; e.va_cplx = 1; e.a3 = (long)r2 * d4; e.ah = d4; e.ak = 1;
-            e.VB = pool + w.Lc; e.vb_cplx = 1; e.bk = N1 * r2; e.b1 = r2; e.bh = 1;
+            e.VB = pool + w.Lc; e.vb_cplx = 1; e.bk = 1; e.b1 = (long)r2 * d4; e.bh = d4;
             dt.push_back(e);
         }
         if (r3) {  // T1b: va = O2[k,h] (state h), vb = V1b[i1][(i3,h)][k]
@@ -512,9 +513,9 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
             d.VA = O2; d.va_cplx = opc; d.va_hstate = 1; d.ah = 1; d.ak = d3;
             d.VB = pool + w.V1b; d.vb_cplx = 1; d.b1 = N3 * r3 * d2; d.b3 = (long)r3 * d2; d.bh = d2; d.bk = 1;
             dt.push_back(d);
-            // T3b: va = Pc[i1][k][h], vb = rho[(i3,h)][k]
+            // T3b: va = Pc[i1][h][k], vb = rho[(i3,h)][k]
             DTerm e = base(2, r3, d1, 0, -1.0, 2, 1, 0.0, 1.0, sign);
-            e.VA = pool + w.Pc; e.va_cplx = 1; e.a1 = (long)d1 * r3; e.ak = r3; e.ah = 1;
+            e.VA = pool + w.Pc; e.va_cplx = 1; e.a1 = (long)d1 * r3; e.ak = 1; e.ah = d1;
             e.VB = pool + w.Rho; e.vb_cplx = 1; e.b3 = (long)r3 * d1; e.bh = d1; e.bk = 1;
             dt.push_back(e);
         }
@@ -523,20 +524,20 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
             d.VA = X4; d.va_cplx = opc; d.va_hstate = 1; d.ah = 1; d.ak = d1;
             d.VB = pool + w.V2a; d.vb_cplx = 1; d.b3 = N1 * r1 * d4; d.b1 = (long)r1 * d4; d.bh = d4; d.bk = 1;
             dt.push_back(d);
-            // T3a: va = PrAll[(i1,h)][k], vb = Qc[i3][k][h]
+            // T3a: va = PrAll[(i1,h)][k], vb = Qc[i3][h][k]
             DTerm e = base(0, r1, d3, 2, +1.0, 2, 1, 1.0, -1.0, sign);
             e.VA = pool + w.Pr; e.va_cplx = 1; e.a1 = (long)r1 * d3; e.ah = d3; e.ak = 1;
-            e.VB = pool + w.Qc; e.vb_cplx = 1; e.b3 = (long)d3 * r1; e.bk = r1; e.bh = 1;
+            e.VB = pool + w.Qc; e.vb_cplx = 1; e.b3 = (long)d3 * r1; e.bk = 1; e.bh = d3;
             dt.push_back(e);
         }
-        if (r4) {  // T2b: va = X4[h,k] (state h), vb = V2b[i1][k][(i3,h)]
+        if (r4) {  // T2b: va = X4[h,k] (state h), vb = V2b[i1][(i3,h)][k]
             DTerm d = base(3, r4, d1, 0, -1.0, 1, 0, 0.0, 1.0, sign);
             d.VA = X4; d.va_cplx = opc; d.va_hstate = 1; d.ah = d1; d.ak = 1;
-            d.VB = pool + w.V2b; d.vb_cplx = 1; d.b1 = (long)d1 * N3 * r4; d.bk = N3 * r4; d.b3 = r4; d.bh = 1;
+            d.VB = pool + w.V2b; d.vb_cplx = 1; d.b1 = (long)d1 * N3 * r4; d.bk = 1; d.b3 = (long)r4 * d1; d.bh = d1;
             dt.push_back(d);
-            // T4b: va = RcAll[k][(i3,h)], vb = Lr[i1][h][k]
+            // T4b: va = Rc[(i3,h)][k], vb = Lr[i1][h][k]
             DTerm e = base(3, r4, d2, 1, -1.0, 3, 1, 0.0, -1.0, sign);
-            e.VA = pool + w.Rc; e.va_cplx = 1; e.ak = N3 * r4; e.a3 = r4; e.ah = 1;
+            e.VA = pool + w.Rc; e.va_cplx = 1; e.ak = 1; e.a3 = (long)r4 * d2; e.ah = d2;
             e.VB = pool + w.Lr; e.vb_cplx = 1; e.b1 = (long)r4 * d2; e.bh = d2; e.bk = 1;
             dt.push_back(e);
         }
