@@ -240,6 +240,11 @@ int pgx_g2(pgx_ctx* ctx, int32_t nparts, const pgx_g2_part* parts, int32_t nfreq
  * summation order. */
 int pgx_set_g2_workspace(pgx_ctx* ctx, int64_t batch_bytes, int64_t chain_bytes);
 
+/* With PGX_G2_SPLIT_I8: products of at least min_macs complex multiply-adds
+ * run on the int8 tensor cores, smaller ones on the FP64 tiles (default 1e9;
+ * 0 sends every stacked and anchored product to the tensor cores). */
+int pgx_set_g2_split_threshold(pgx_ctx* ctx, double min_macs);
+
 /* Self-check of the int8 split product (no counterpart in the reference):
  * C = A B for nb items of seeded random complex A (M x K) and B (K x N) with
  * entries spread over four binary orders of magnitude, once through the split

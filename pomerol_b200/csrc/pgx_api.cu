@@ -464,6 +464,13 @@ int pgx_split_gemm_check(pgx_ctx* c, int32_t M, int32_t N, int32_t K, int32_t nb
     });
 }
 
+int pgx_set_g2_split_threshold(pgx_ctx* c, double min_macs) {
+    return guarded(c, [&] {
+        PGX_CHECK(min_macs >= 0.0, PGX_ERR_ARG, "threshold must be >= 0");
+        c->g2_split_min_macs = min_macs;
+    });
+}
+
 int pgx_set_g2_workspace(pgx_ctx* c, int64_t batch_bytes, int64_t chain_bytes) {
     return guarded(c, [&] {
         PGX_CHECK(batch_bytes >= 0 && chain_bytes >= 0, PGX_ERR_ARG, "workspace limits must be >= 0");

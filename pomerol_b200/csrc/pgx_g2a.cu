@@ -423,9 +423,11 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
     };
     // the stacked products read Lc, Pr, rho and Rc written by the first two
     // launches; with `split` slices they run on the int8 tensor cores
-    // products of at least 1e8 complex multiply-adds go to the tensor cores
-    // (smaller ones do not repay the digit preparation and tile padding);
-    // complex Hamiltonians keep the anchored products in FP64
+    // products of at least g2_split_min_macs complex multiply-adds (default
+    // 1e9) go to the tensor cores: smaller ones, such as every product of a
+    // 400-state block, run faster on the FP64 tiles than their digit
+    // preparation and 128 x 256 tile padding allow.  Complex Hamiltonians keep
+    // the anchored products in FP64.
     auto launch_split = [&](auto& probs) {
         if (!split) {
             launch(probs);
@@ -434,7 +436,7 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
         std::remove_reference_t<decltype(probs)> rest;
         for (const auto& g : probs) {
             const double macs = (double)g.M * g.N * g.K * std::max(g.nb, 1);
-            if (macs < 1e8) {
+            if (macs < c->g2_split_min_macs) {
                 rest.push_back(g);
                 continue;
             }

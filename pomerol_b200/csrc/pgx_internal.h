@@ -280,6 +280,7 @@ struct pgx_ctx {
     // side streams (and their fork / join events) for independent launches
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
     long long g2_batch_bytes = 0, g2_chain_bytes = 0;  // pgx_set_g2_workspace (0: defaults)
+    double g2_split_min_macs = 1e9;                     // pgx_set_g2_split_threshold
     pgx::OzWork oz;                                     // int8 split products
     cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
     // scratch for G2 and Lehmann kernels

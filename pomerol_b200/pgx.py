@@ -25,7 +25,7 @@ EXPORTS = [
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
     "pgx_gf_vjp", "pgx_susc_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_autotune_begin", "pgx_autotune_end",
-    "pgx_set_g2_workspace", "pgx_split_gemm_check", "pgx_graph_begin", "pgx_graph_end",
+    "pgx_set_g2_workspace", "pgx_set_g2_split_threshold", "pgx_split_gemm_check", "pgx_graph_begin", "pgx_graph_end",
     "pgx_graph_replay", "pgx_graph_destroy", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
 ]
 
@@ -89,6 +89,7 @@ def load():
         lib.pgx_set_eigensystem.argtypes = [P, P, P]
         lib.pgx_autotune_begin.argtypes = [P]
         lib.pgx_set_g2_workspace.argtypes = [P, C.c_int64, C.c_int64]
+        lib.pgx_set_g2_split_threshold.argtypes = [P, C.c_double]
         lib.pgx_split_gemm_check.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
                                              P, P, P]
         lib.pgx_autotune_end.argtypes = [P, P]
@@ -424,6 +425,12 @@ def _set_g2_workspace(self, batch_bytes=0, chain_bytes=0):
     self._ck(self.lib.pgx_set_g2_workspace(self.h, int(batch_bytes), int(chain_bytes)))
 
 
+def _set_g2_split_threshold(self, min_macs=1e9):
+    """Products of at least min_macs complex multiply-adds use the int8
+    tensor cores under PGX_G2_SPLIT_I8."""
+    self._ck(self.lib.pgx_set_g2_split_threshold(self.h, float(min_macs)))
+
+
 def _split_gemm_check(self, M, N, K, nb=1, slices=6, seed=1):
     """int8 split product vs FP64 on seeded random complex matrices:
     (max relative error, split ms, FP64 ms)."""
@@ -540,6 +547,7 @@ Engine.set_models = _set_models
 Engine.graph_begin = _graph_begin
 Engine.set_g2_workspace = _set_g2_workspace
 Engine.split_gemm_check = _split_gemm_check
+Engine.set_g2_split_threshold = _set_g2_split_threshold
 Engine.autotune_begin = _autotune_begin
 Engine.autotune_end = _autotune_end
 Engine.graph_end = _graph_end

@@ -352,8 +352,9 @@ def test_split_gemm_matches_fp64(M, N, K, nb):
 
 def test_anchored_g2_split_i8_anderson_a5(harness):
     """Anderson 1+5 (dim 4096, beta=20) on the 16^3 cube: the anchored G2 with
-    its stacked products on the int8 tensor cores (PGX_G2_SPLIT_I8) against the
-    FP64 anchored G2, within 1e-9 of max|G2|."""
+    every stacked and anchored product on the int8 tensor cores
+    (PGX_G2_SPLIT_I8, threshold 0) against the FP64 anchored G2, within 1e-9
+    of max|G2|."""
     from pomerol_b200.pgx import PGX_G2_ANCHORED, PGX_G2_SPLIT_I8
     U, epsd, eps, V, beta = M.anderson_a5_params(0)
     m = M.make_model(M.anderson(U, epsd, eps, V))
@@ -363,7 +364,11 @@ def test_anchored_g2_split_i8_anderson_a5(harness):
     fz = L.fermionic(np.array([(a, b, x) for a in n for b in n for x in n]), beta)
     parts = g.g2_parts(g.c(u), g.c(d), g.cdag(u), g.cdag(d))
     v = _anchored(g, parts, fz)
-    vs = g.eng.g2(parts, fz, pole_res=1e-8, coef_tol=1e-16, flags=PGX_G2_ANCHORED | PGX_G2_SPLIT_I8)
+    g.eng.set_g2_split_threshold(0.0)  # every stacked and anchored product on the tensor cores
+    try:
+        vs = g.eng.g2(parts, fz, pole_res=1e-8, coef_tol=1e-16, flags=PGX_G2_ANCHORED | PGX_G2_SPLIT_I8)
+    finally:
+        g.eng.set_g2_split_threshold(1e9)
     assert np.abs(vs - v).max() < 1e-9 * np.abs(v).max()
 
 
