@@ -57,6 +57,7 @@ struct DTerm {
     int va_hstate, vb_hstate;  // h stride applies to the anchor's state index instead of its position
     int use_delta;
     int nt;               // triples of the plan (work count only)
+    int hc, nhc;          // anchors per work item and items per group: heavy groups split by anchor range
     double sgn, cdelta, cnum, pref;
 };
 
@@ -69,7 +70,7 @@ __device__ __forceinline__ cd load_v(const void* p, int cplx, long idx) {
 constexpr int DG = 8;  // the batch inversion below is written out for eight
 
 template <bool DELTA>
-__device__ void dterm_group(const DTerm& d, int g, double beta, double tol2, cd* out, int lane) {
+__device__ void dterm_group(const DTerm& d, int g, int h0, int h1, double beta, double tol2, cd* out, int lane) {
     const int i1 = d.gi1[g], i3 = d.gi3[g];
     const int tb = d.goff[g], te = d.goff[g + 1];
     for (int t0 = tb; t0 < te; t0 += DG) {
@@ -86,7 +87,7 @@ __device__ void dterm_group(const DTerm& d, int g, double beta, double tol2, cd*
             ax[q] = 0.0;
             ay[q] = 0.0;
         }
-        for (int h = 0; h < d.nh; ++h) {
+        for (int h = h0; h < h1; ++h) {
             const int hs = d.hot[h];
             const double eh = d.Eh[hs], w = d.wh[hs];
             const double cw = d.cnum * w, cdl = d.cdelta * beta * w;
@@ -168,8 +169,8 @@ __device__ void dterm_group(const DTerm& d, int g, double beta, double tol2, cd*
     }
 }
 
-// One warp per (sub-term, (z1, z3) group); lanes over the summed index k.
-// woff[q] = first work item of term q (prefix sum of the group counts).
+// One warp per (sub-term, (z1, z3) group, anchor range); lanes over the summed
+// index k.  woff[q] = first work item of term q (prefix sum of groups x ranges).
 __global__ void __launch_bounds__(256) dterm_kernel(const DTerm* terms, const int* woff, int nterms, double beta,
                                                     double tol2, cd* out) {
     const int lane = threadIdx.x & 31;
@@ -183,9 +184,9 @@ __global__ void __launch_bounds__(256) dterm_kernel(const DTerm* terms, const in
             else hi = mid - 1;
         }
         const DTerm& d = terms[lo];
-        const int g = wk - woff[lo];
-        if (d.use_delta) dterm_group<true>(d, g, beta, tol2, out, lane);
-        else dterm_group<false>(d, g, beta, tol2, out, lane);
+        const int u = wk - woff[lo], g = u / d.nhc, h0 = (u % d.nhc) * d.hc, h1 = min(d.nh, h0 + d.hc);
+        if (d.use_delta) dterm_group<true>(d, g, h0, h1, beta, tol2, out, lane);
+        else dterm_group<false>(d, g, h0, h1, beta, tol2, out, lane);
     }
 }
 
@@ -545,11 +546,19 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
         }
     }
     if (!dt.empty()) {
+        // a work item covers at most about 2^17 (anchor, state) pairs per pass
+        // over its triples, so that no single warp sets the kernel's duration
         std::vector<int> woff(dt.size() + 1, 0);
         double elems = 0.0;
+        long items = 0;
         for (size_t q = 0; q < dt.size(); ++q) {
-            woff[q + 1] = woff[q] + dt[q].ng;
-            elems += (double)dt[q].nh * dt[q].nk * dt[q].nt;
+            DTerm& d = dt[q];
+            d.hc = std::max(1, std::min(std::max(d.nh, 1), (1 << 17) / std::max(d.nk, 1)));
+            d.nhc = std::max(1, (int)ceil_div((long)d.nh, (long)d.hc));
+            items += (long)d.ng * d.nhc;
+            PGX_CHECK(items < (1L << 31), PGX_ERR_ARG, "G2 contraction: too many work items");
+            woff[q + 1] = (int)items;
+            elems += (double)d.nh * d.nk * d.nt;
         }
         DevBuf& bd = c->scratch[3];
         const size_t tb = (dt.size() * sizeof(DTerm) + 255) & ~size_t(255);
