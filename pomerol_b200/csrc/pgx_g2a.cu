@@ -67,7 +67,9 @@ __device__ __forceinline__ cd load_v(const void* p, int cplx, long idx) {
 
 // Triples of one (z1, z3) group handled together: the operand product
 // VA * VB does not depend on z2, so it is loaded once for DG triples.
-constexpr int DG = 8;  // the batch inversion below is written out for eight
+// Four per pass: 128 registers and two 256-thread CTAs per SM (eight triples
+// per pass needed 211 registers and left one CTA per SM; 17% slower).
+constexpr int DG = 4;  // the batch inversion below is written out for four
 
 template <bool DELTA>
 __device__ void dterm_group(const DTerm& d, int g, int h0, int h1, double beta, double tol2, cd* out, int lane) {
@@ -121,24 +123,18 @@ __device__ void dterm_group(const DTerm& d, int g, int h0, int h1, double beta, 
                     in_range = in_range && recip_in_range(m2[q]);
                 }
                 if (in_range) {
-                    // Montgomery's batch inversion in tree form: the eight
-                    // reciprocals from one division of the product of all eight
-                    // (pairwise products up, then each subtree's reciprocal times
-                    // its sibling's product down; depth 3 each way).  With every
-                    // value in [1e-30, 1e30] the product stays inside the double range.
-                    const double p01 = m2[0] * m2[1], p23 = m2[2] * m2[3], p45 = m2[4] * m2[5], p67 = m2[6] * m2[7];
-                    const double p03 = p01 * p23, p47 = p45 * p67;
-                    const double inv = 1.0 / (p03 * p47);
-                    const double i03 = inv * p47, i47 = inv * p03;
-                    const double i01 = i03 * p23, i23 = i03 * p01, i45 = i47 * p67, i67 = i47 * p45;
+                    // Montgomery's batch inversion: the four reciprocals from one
+                    // division of the product of all four (pairwise products up,
+                    // then each pair's reciprocal times its sibling's product
+                    // down).  With every value in [1e-30, 1e30] the product stays
+                    // inside the double range.
+                    const double p01 = m2[0] * m2[1], p23 = m2[2] * m2[3];
+                    const double inv = 1.0 / (p01 * p23);
+                    const double i01 = inv * p23, i23 = inv * p01;
                     rc[0] = i01 * m2[1];
                     rc[1] = i01 * m2[0];
                     rc[2] = i23 * m2[3];
                     rc[3] = i23 * m2[2];
-                    rc[4] = i45 * m2[5];
-                    rc[5] = i45 * m2[4];
-                    rc[6] = i67 * m2[7];
-                    rc[7] = i67 * m2[6];
                 } else {
 #pragma unroll
                     for (int q = 0; q < DG; ++q) rc[q] = 1.0 / m2[q];
@@ -171,7 +167,7 @@ __device__ void dterm_group(const DTerm& d, int g, int h0, int h1, double beta, 
 
 // One warp per (sub-term, (z1, z3) group, anchor range); lanes over the summed
 // index k.  woff[q] = first work item of term q (prefix sum of groups x ranges).
-__global__ void __launch_bounds__(256) dterm_kernel(const DTerm* terms, const int* woff, int nterms, double beta,
+__global__ void __launch_bounds__(256, 2) dterm_kernel(const DTerm* terms, const int* woff, int nterms, double beta,
                                                     double tol2, cd* out) {
     const int lane = threadIdx.x & 31;
     const int nwork = woff[nterms];
