@@ -1480,16 +1480,19 @@ static void launch_eigh_complex(pgx_ctx* c) {
     check_launch("cx_extract_kernel");
 }
 
+void ensure_side_streams(pgx_ctx* c) {
+    if (c->fork) return;
+    PGX_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
+    for (int i = 0; i < 4; ++i) {
+        PGX_CUDA(cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking));
+        PGX_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
+    }
+}
+
 void launch_eigh(pgx_ctx* c) {
     Problem& P = c->P;
     cudaStream_t st = c->stream;
-    if (!c->fork) {
-        PGX_CUDA(cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming));
-        for (int i = 0; i < 4; ++i) {
-            PGX_CUDA(cudaStreamCreateWithFlags(&c->aux[i], cudaStreamNonBlocking));
-            PGX_CUDA(cudaEventCreateWithFlags(&c->join[i], cudaEventDisableTiming));
-        }
-    }
+    ensure_side_streams(c);
     if (P.is_complex) {
         launch_eigh_complex(c);
         return;

@@ -408,28 +408,26 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
         if (r4) pc.push_back(gp<DT, cd>(O1, d2, 1, pool + w.Rc, 1, d2, pool + w.V2b, 1, d1, N3 * r4, d2, nullptr,
                                         nullptr, A1, N1, (long)d1 * N3 * r4, d1));  // V2b = A1 RcAll: [i1][(i3,h)][k]
     }
-    // descriptor buffers sized once for the largest list, before any launch
-    {
-        const long nprob = (long)std::max({pa.size(), pb.size(), pc.size(), pd.size()});
-        c->scratch[7].reserve(std::max<long>(nprob, 1) * sizeof(GemmProblem<cd, cd, cd>));
-        c->scratch[8].reserve(gemm_index_bytes(nprob));
-    }
-    auto launch = [&](auto& probs) {
+    // descriptor buffers: one region per product list, sized once for the
+    // largest list before any launch, so that lists on different streams do
+    // not share one
+    const long nprob = std::max<long>(1, (long)std::max({pa.size(), pb.size(), pc.size(), pd.size()}));
+    const size_t preg = ((size_t)nprob * sizeof(GemmProblem<cd, cd, cd>) + 255) & ~size_t(255);
+    const size_t ireg = (gemm_index_bytes(nprob) + 255) & ~size_t(255);
+    c->scratch[7].reserve(4 * preg);
+    c->scratch[8].reserve(4 * ireg);
+    auto launch_on = [&](auto& probs, int region, cudaStream_t s2) {
         if (probs.empty()) return;
-        launch_gemm_batch(probs, c->scratch[7].p, c->scratch[7].bytes, c->scratch[8].p, c->scratch[8].bytes, st);
+        launch_gemm_batch(probs, c->scratch[7].as<char>() + region * preg, preg, c->scratch[8].as<char>() + region * ireg,
+                          ireg, s2);
     };
-    // the stacked products read Lc, Pr, rho and Rc written by the first two
-    // launches; with `split` slices they run on the int8 tensor cores
-    // products of at least g2_split_min_macs complex multiply-adds (default
-    // 1e9) go to the tensor cores: smaller ones, such as every product of a
-    // 400-state block, run faster on the FP64 tiles than their digit
-    // preparation and 128 x 256 tile padding allow.  Complex Hamiltonians keep
-    // the anchored products in FP64.
-    auto launch_split = [&](auto& probs) {
-        if (!split) {
-            launch(probs);
-            return;
-        }
+    // The stacked products read Lc, Pr, rho and Rc written by the first two
+    // lists.  With `split` slices, products of at least g2_split_min_macs
+    // complex multiply-adds (default 1e9) go to the int8 tensor cores: smaller
+    // ones, such as every product of a 400-state block, run faster on the FP64
+    // tiles than their digit preparation and 128 x 256 tile padding allow.
+    // Complex Hamiltonians keep the anchored products in FP64.
+    auto launch_split = [&](auto& probs, int region) {
         std::remove_reference_t<decltype(probs)> rest;
         for (const auto& g : probs) {
             const double macs = (double)g.M * g.N * g.K * std::max(g.nb, 1);
@@ -440,17 +438,39 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
             ProfRange pr("oz_split_gemm", st, 8.0 * macs, 0.0);
             oz_zgemm(g, split, c->oz, st);
         }
-        launch(rest);
+        launch_on(rest, region, st);
     };
-    if constexpr (TC) {
-        launch(pa);
-        launch(pb);
+    if (split) {  // the split products share one workspace: one stream
+        if constexpr (TC) {
+            launch_on(pa, 0, st);
+            launch_on(pb, 1, st);
+        } else {
+            launch_split(pa, 0);
+            launch_split(pb, 1);
+        }
+        launch_split(pc, 2);
+        launch_split(pd, 3);
     } else {
-        launch_split(pa);
-        launch_split(pb);
+        // pa and pb are independent, and so are pc and pd (each needs both of
+        // the first pair): each pair runs on two side streams at once
+        ensure_side_streams(c);
+        cudaStream_t s0 = c->aux[0], s1 = c->aux[1];
+        PGX_CUDA(cudaEventRecord(c->fork, st));
+        PGX_CUDA(cudaStreamWaitEvent(s0, c->fork, 0));
+        PGX_CUDA(cudaStreamWaitEvent(s1, c->fork, 0));
+        launch_on(pa, 0, s0);
+        launch_on(pb, 1, s1);
+        PGX_CUDA(cudaEventRecord(c->join[0], s0));
+        PGX_CUDA(cudaEventRecord(c->join[1], s1));
+        PGX_CUDA(cudaStreamWaitEvent(s0, c->join[1], 0));
+        PGX_CUDA(cudaStreamWaitEvent(s1, c->join[0], 0));
+        launch_on(pc, 2, s0);
+        launch_on(pd, 3, s1);
+        PGX_CUDA(cudaEventRecord(c->join[0], s0));
+        PGX_CUDA(cudaEventRecord(c->join[1], s1));
+        PGX_CUDA(cudaStreamWaitEvent(st, c->join[0], 0));
+        PGX_CUDA(cudaStreamWaitEvent(st, c->join[1], 0));
     }
-    launch_split(pc);
-    launch_split(pd);
     // ---- contractions per triple
     std::vector<DTerm> dt;
     for (size_t j = 0; j < idx.size(); ++j) {

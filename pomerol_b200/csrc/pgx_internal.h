@@ -308,6 +308,7 @@ struct pgx_ctx {
 namespace pgx {
 
 void launch_eigh(pgx_ctx* c);
+void ensure_side_streams(pgx_ctx* c);  // the context's four side streams and their events
 
 // Device buffers of one eigensolve (any number of blocks), all caller-owned.
 struct EighDev {
