@@ -1,20 +1,39 @@
-"""Benchmark of the G2 path on B200: full two-particle Green's function
-(block eigensolve + operator rotation + Lehmann sum) of the Anderson 1+5
-impurity (dim 4096, chi_(u0,d0,u0,d0) on the 16^3 fermionic cube, beta=20).
+"""Benchmark of the G2 path on B200.
 
-Metric: G2 Lehmann term*freq evaluations per second = N_quad * N_freq / step
-time, where N_quad counts the state quadruples the reference enumerates
-(all four rotated elements non-zero, w1+w2+w3+w4 > 1e-16) and N_freq the
-frequency triples.
+Default workload (ring8): the 8-site Hubbard ring (periodic, t=1, U=4, mu=2,
+beta=5, truncateBlocks(1e-12); dim 65536 in 81 blocks up to 4900 states),
+G2 = chi_(u0,d0,u0,d0) on the full 24^3 fermionic grid (13 824 triples).
+With --config a5: the Anderson impurity with 5 bath sites (dim 4096, 16^3
+cube, beta=20).
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+Metric: G2 Lehmann term*freq evaluations per second = N_quad * N_freq / time,
+N_quad counting the state quadruples the reference enumerates (all four
+rotated elements non-zero, |x| > 1e-20 as its sparseView(1e-8) keeps, and
+w1+w2+w3+w4 > 1e-16) and N_freq the frequency triples.
 
-Our arm, per step (value): eigensolve, weights, rotation of c^+/c and the G2
-sum on one libpgx context with the block Hamiltonians resident in HBM.  e2e:
-the same through the drop-in API from the Hamiltonian expression, with every
-host<->device copy inside the timed region.  Multi-GPU: one process per GPU,
-each rank computes its own frequency slab (weak scaling, no collective in the
-data path), time = max over ranks.
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference] [--config ring8|a5]
+
+ring8, our arm.  One step is one batch of block chains (the 304 chains of
+TwoParticleGF::prepare split into 20 batches of about equal cost) over the
+whole 24^3 grid on one libpgx context: anchored sum, products of at least 1e9
+multiply-adds on the int8 tensor cores, anchor threshold 1e-13.  Step k runs
+batch k mod 20, so 20 steps are one full G2.  The eigensolve, weights and
+rotation run once before the steps and are reported as stages; full_g2_s is
+their time plus one pass over all batches (device time).  The plain FP64 form
+(FP64 products, same sum) runs on two of the batches for the mixed / FP64
+ratio.  e2e: one full run through the drop-in API (Hamiltonian expression ->
+TwoParticleGFContainer.computeAll) with every host<->device copy in the timed
+region.  Multi-GPU: rank r runs batches r, r+N, ...; the partial G2s of the
+first pass are summed by one NCCL all-reduce (the reference's Allreduce over
+parts, TwoParticleGF.cpp:183); time = max over ranks.
+
+a5, our arm.  One step is eigensolve + weights + rotation + G2 over the cube.
+
+Reference arm (--impl reference): the reference's algorithm restated in C++
+(oracle/g2_oracle.cpp: chase enumeration, weight filter, TermList merging,
+OpenMP frequency loop) on a fixed bounded sample of the same workload, all
+host threads; rank 0 only.  The cpu_baseline of our arm times the same sample.
+This arm imports nothing from pomerol_b200.
 """
 from __future__ import annotations
 
@@ -32,20 +51,34 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-CONFIG = "a5"
-NZ_TOL = 1e-12
+CONFIG = "ring8"
+NZ_TOL = 1e-20   # the reference's sparseView(Tolerance=1e-8) keeps |x| > 1e-8 * 1e-12
 COEF_TOL = 1e-16
+POLE_RES = 1e-8
+SETTINGS = {
+    "ring8": dict(beta=5.0, nfreq=24, dm_trunc=1e-12, site="S0", anchor_tol=1e-13, split=True, nbatch=20,
+                  workload="hubbard_ring8_dim65536_chi_u0d0u0d0_24cube_beta5"),
+    "a5": dict(beta=20.0, nfreq=16, dm_trunc=None, site="C", anchor_tol=1e-16, split=False, nbatch=1,
+               workload="anderson_1+5_dim4096_chi_u0d0u0d0_16cube_beta20"),
+}
 
 
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default=CONFIG)
+    ap.add_argument("--config", default=CONFIG, choices=sorted(SETTINGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
+
+
+def matsubara_cube(beta, n):
+    k = np.arange(-n // 2, n // 2)
+    idx = np.array([(a, b, c) for a in k for b in k for c in k])
+    return idx, 1j * np.pi * (2 * idx + 1) / beta
 
 
 # ------------------------------------------------------------------ helpers
@@ -94,11 +127,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(self.rows)}
 
 
-def flush_l2(buf):
-    if buf is not None:
-        buf.add_(1.0)
-
-
 def fp64_peak_tflops(torch):
     """Measured FP64 reference: cuBLAS DGEMM 8192^3 via torch.matmul (best of 3)."""
     n = 8192
@@ -119,51 +147,69 @@ def fp64_peak_tflops(torch):
     return 2.0 * n ** 3 / best / 1e12
 
 
+def measured_peaks():
+    try:
+        return json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        return {}
+
+
 # ------------------------------------------------------------------ CPU side
-def cpu_sample(config, seconds_target=12.0, nthreads=0):
-    """The reference's algorithm (oracle/g2_oracle.cpp restatement: chase
-    enumeration, TermList merging, OpenMP frequency loop) on a bounded sample
-    of the workload: rows of index1 of the largest block chain, all triples.
-    Returns (rate term*freq/s, seconds, description, threads)."""
-    from oracle import ed as EDm
+def sample_spec(config, dims_of_parts):
+    """The bounded sample both CPU legs time: (part index, row step, col
+    step).  a5: the chain with the most quadruples, every 60th index1, every
+    index3.  ring8: the chain with the most (index1, index3) pairs among
+    those with d2*d4 <= 40000 quadruples per pair, index1 rows 0 and d1/2,
+    index3 row 0 (two pairs, every index2 and index4 chased)."""
+    if config == "a5":
+        k = int(np.argmax([np.prod(d) for d in dims_of_parts]))
+        return k, 60, 1
+    best = None
+    for k, d in enumerate(dims_of_parts):
+        if d[1] * d[3] <= 40000 and (best is None or d[0] * d[2] > best[1]):
+            best = (k, d[0] * d[2])
+    k = best[0]
+    d = dims_of_parts[k]
+    return k, max(1, d[0] // 2), d[2]
+
+
+def cpu_run(ed_like, parts, z, spec, threads):
+    """One timed run of the reference algorithm on the sample."""
     from oracle import g2c
+    k, rs, cs = spec
+    d1 = len(ed_like.E[parts[k]["b"][0]])
+    t0 = time.perf_counter()
+    _, nq, terms = g2c.evaluate(ed_like, parts, z, pole_res=POLE_RES, coef_tol=COEF_TOL, rule=True, nz_tol=NZ_TOL,
+                                rows=(k, 0, d1, rs, cs), nthreads=threads)
+    dt = time.perf_counter() - t0
+    return nq * len(z) / dt, dt, nq, int(terms.sum())
+
+
+def describe_sample(config, parts, ed_like, spec, nq, terms, nz, dt, threads):
+    k, rs, cs = spec
+    dims = [len(ed_like.E[b]) for b in parts[k]["b"]]
+    return (f"reference algorithm restated (oracle/g2_oracle.cpp, rule=1): block chain {k} of {len(parts)} "
+            f"(blocks {dims}), index1 every {rs}-th, index3 every {min(cs, dims[2])}-th, {nq} quadruples, "
+            f"{terms} merged terms, {nz} triples, {dt:.2f} s on {threads} threads")
+
+
+def oracle_problem(config):
+    """The workload built by the oracle alone (numpy ED, rotation, chains)."""
+    from oracle import ed as EDm
     from oracle import lehmann as L
     from oracle import model as M
-    from pomerol_b200.workloads import CONFIGS, a5_params, matsubara_cube
-
-    cfg = CONFIGS[config]
+    cfg = SETTINGS[config]
     if config == "a5":
-        U, epsd, eps, V, beta = a5_params(0)
+        U, epsd, eps, V, _ = M.anderson_a5_params(0)
         mdl = M.make_model(M.anderson(U, epsd, eps, V))
-        site = "C"
-    elif config == "plaquette":
-        mdl, beta, site = M.make_model(M.plaquette()), cfg["beta"], "A"
     else:
-        raise ValueError(config)
-    ed = EDm.ED(mdl, beta)
-    u, d = mdl.info.getIndex(site, 0, 1), mdl.info.getIndex(site, 0, 0)
+        mdl = M.make_model(M.hubbard_ring())
+    ed = EDm.ED(mdl, cfg["beta"])
+    if cfg["dm_trunc"]:
+        ed.truncate_blocks(cfg["dm_trunc"])
+    u, d = mdl.info.getIndex(cfg["site"], 0, 1), mdl.info.getIndex(cfg["site"], 0, 0)
     parts = L.g2_parts(ed, ed.c(u), ed.c(d), ed.cdag(u), ed.cdag(d))
-    sizes = [np.prod([len(mdl.blocks[b]) for b in p["b"]]) for p in parts]
-    k = int(np.argmax(sizes))
-    _, z = matsubara_cube(beta, cfg["nfreq"])
-    d1 = len(mdl.blocks[parts[k]["b"][0]])
-    threads = nthreads or g2c.lib().g2o_max_threads()
-    # index1 rows strided across the whole block (eigenvalues ascend, so the
-    # hot low-energy rows and the cold ones are both represented)
-    nrows = 2
-    while True:
-        step = max(1, d1 // nrows)
-        t0 = time.perf_counter()
-        _, nq, terms = g2c.evaluate(ed, parts, z, rows=(k, 0, d1, step), nthreads=threads)
-        dt = time.perf_counter() - t0
-        if dt > seconds_target / 3 or step == 1:
-            break
-        nrows = min(d1, max(nrows + 1, int(nrows * min(8.0, seconds_target / 3 / max(dt, 1e-3)))))
-    rate = nq * len(z) / dt
-    desc = (f"reference algorithm restated (oracle/g2_oracle.cpp): block chain {k} of {len(parts)} "
-            f"(blocks {[len(mdl.blocks[b]) for b in parts[k]['b']]}), every {step}-th index1 row of {d1}, "
-            f"{nq} quadruples, {int(terms.sum())} merged terms, {len(z)} triples, {dt:.2f} s on {threads} threads")
-    return rate, dt, desc, threads, (k, step)
+    return ed, parts
 
 
 def run_reference(args, rank, world):
@@ -176,74 +222,287 @@ def run_reference(args, rank, world):
     except Exception as e:  # pragma: no cover
         print(json.dumps({"impl": "reference", "unavailable": f"oracle build failed: {e}"}))
         return
-    rate, dt, desc, threads, (k, step) = cpu_sample(args.config, seconds_target=8.0)
-    times, rates = [], []
+    cfg = SETTINGS[args.config]
+    ed, parts = oracle_problem(args.config)
+    _, z = matsubara_cube(cfg["beta"], cfg["nfreq"])
+    spec = sample_spec(args.config, [[len(ed.E[b]) for b in p["b"]] for p in parts])
+    threads = g2c.lib().g2o_max_threads()
+    rates, times = [], []
     for i in range(args.warmup + args.steps):
-        r, t, _, _, _ = cpu_sample_fixed(args.config, k, step, threads)
+        r, t, nq, terms = cpu_run(ed, parts, z, spec, threads)
         if i >= args.warmup:
             rates.append(r)
-        if i >= args.warmup:
             times.append(t)
-    ms = 1e3 * float(np.mean(times))
     value = float(np.mean(rates))
+    desc = describe_sample(args.config, parts, ed, spec, nq, terms, len(z), float(np.mean(times)), threads)
     line = {"metric": "G2 Lehmann term*freq evals/s", "value": value, "unit": unit, "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "anderson_1+5_dim4096_chi_u0d0u0d0_16cube_beta20", "sample": desc},
+            "config": {"workload": cfg["workload"], "sample": desc},
             "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port", "sample": desc},
             "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-_CPU_CACHE = {}
+def cpu_baseline_from_engine(config, run, z):
+    """The reference-arm sample, timed once on this process's host threads,
+    with the chain's rotated matrices and weights read back from the engine."""
+    from types import SimpleNamespace
 
-
-def cpu_sample_fixed(config, k, step, threads):
-    from oracle import ed as EDm
     from oracle import g2c
-    from oracle import lehmann as L
-    from oracle import model as M
-    from pomerol_b200.workloads import CONFIGS, a5_params, matsubara_cube
-    if config not in _CPU_CACHE:
-        cfg = CONFIGS[config]
-        if config == "a5":
-            U, epsd, eps, V, beta = a5_params(0)
-            mdl, site = M.make_model(M.anderson(U, epsd, eps, V)), "C"
-        else:
-            mdl, beta, site = M.make_model(M.plaquette()), cfg["beta"], "A"
-        ed = EDm.ED(mdl, beta)
-        u, d = mdl.info.getIndex(site, 0, 1), mdl.info.getIndex(site, 0, 0)
-        parts = L.g2_parts(ed, ed.c(u), ed.c(d), ed.cdag(u), ed.cdag(d))
-        _, z = matsubara_cube(beta, cfg["nfreq"])
-        _CPU_CACHE[config] = (ed, parts, z)
-    ed, parts, z = _CPU_CACHE[config]
-    t0 = time.perf_counter()
-    d1 = len(ed.E[parts[k]["b"][0]])
-    _, nq, _ = g2c.evaluate(ed, parts, z, rows=(k, 0, d1, step), nthreads=threads)
-    dt = time.perf_counter() - t0
-    return nq * len(z) / dt, dt, None, threads, None
+    eng = run.eng
+    E, _ = eng.eigensystem()
+    w, _ = eng.weights(SETTINGS[config]["beta"])
+    if SETTINGS[config]["dm_trunc"]:
+        eng.truncate_blocks(SETTINGS[config]["dm_trunc"])
+    dims_of_parts = [[eng.dims[b] for b in p[1]] for p in run.parts]
+    spec = sample_spec(config, dims_of_parts)
+    ops, blocks, perm, sign = run.parts[spec[0]]
+
+    def mat(op, left):
+        info = eng.op_info(op)
+        return eng.op_read(op, next(i for i, (r, lb) in enumerate(info) if lb == left))
+
+    one = dict(b=blocks, O1=mat(ops[0], blocks[0]), O2=mat(ops[1], blocks[1]), O3=mat(ops[2], blocks[2]),
+               CX4=mat(ops[3], blocks[3]), perm=perm, sign=sign)
+    parts = [dict(b=p[1]) for p in run.parts]
+    parts[spec[0]] = one
+    host = SimpleNamespace(E=E, w=w, beta=SETTINGS[config]["beta"])
+    threads = g2c.lib().g2o_max_threads()
+    rate, dt, nq, terms = cpu_run(host, parts, z, spec, threads)
+    return {"value": rate, "unit": "term*freq/s", "cores": threads, "kind": "port",
+            "sample": describe_sample(config, parts, host, spec, nq, terms, len(z), dt, threads)}
 
 
 # ------------------------------------------------------------------ GPU side
-def run_ours(args, rank, world, local_rank):
+def roofline_entry(top, steps, torch, config):
+    """Dominant kernel of the timed steps: algorithmic work per launch over its
+    average event-timed duration, against the peak of the pipe it runs on."""
+    if not top or top["ms"] <= 0:
+        return None
+    per_launch_s = top["ms"] / top["launches"] / 1e3
+    name = top["name"]
+    peaks = measured_peaks()
+    traffic = None
+    tf = ROOT / "profiles" / "roofline_traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get(config, {}).get(name)
+        except Exception:
+            traffic = None
+    if name.startswith("oz_split_gemm"):
+        # int8 tensor-core split products: 84 int8 multiply-adds (21 slice
+        # products x 4 real products) per complex multiply-add; flops were
+        # recorded as 8 per complex multiply-add
+        int8_ops = top["flops"] / 8.0 * 84.0 * 2.0 / top["launches"]
+        peak = 2.0 * peaks["bf16_tflops"] if peaks.get("bf16_tflops") else 2.0 * 1590.0
+        achieved = int8_ops / per_launch_s / 1e12
+        return {"kernel": name, "bound": "int8-tensor", "achieved": achieved, "peak": peak, "unit": "TOPS",
+                "frac": achieved / peak, "traffic": traffic,
+                "peak_source": ("2 x MEASURED_PEAKS.json bf16_tflops (dense int8 runs at twice the bf16 rate on "
+                                "the B200 tensor cores)" if peaks.get("bf16_tflops") else "2 x fallback bf16 1590"),
+                "fp64_equivalent_tflops": top["flops"] / top["launches"] / per_launch_s / 1e12,
+                "launches_per_step": top["launches"] / steps, "ms_per_launch": per_launch_s * 1e3,
+                "algorithmic_ops_per_launch": int8_ops}
+    peak = fp64_peak_tflops(torch)
+    achieved = top["flops"] / top["launches"] / per_launch_s / 1e12
+    return {"kernel": name, "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak, "traffic": traffic,
+            "peak_source": "measured live: cuBLAS FP64 DGEMM 8192^3 (torch.matmul float64); MEASURED_PEAKS.json "
+                           "has no FP64 figure",
+            "launches_per_step": top["launches"] / steps, "ms_per_launch": per_launch_s * 1e3,
+            "flops_per_launch": top["flops"] / top["launches"]}
+
+
+def run_ours_ring8(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
     from pomerol_b200 import pgx
-    from pomerol_b200.workloads import EngineRun, Problem, matsubara_cube
+    from pomerol_b200.pgx import PGX_G2_ANCHORED, PGX_G2_SPLIT_I8
+    from pomerol_b200.workloads import EngineRun, Problem, chain_cost, lpt_batches
+    cfg = SETTINGS["ring8"]
+    NB = cfg["nbatch"]
+    prob = Problem("ring8", device=local_rank)
+    run = EngineRun(prob, device=local_rank, split=cfg["split"], anchor_tol=cfg["anchor_tol"])
+    _, z = matsubara_cube(prob.beta, prob.nfreq)
+    nfreq = len(z)
+    eng = run.eng
+    run.prepare()  # sizes every buffer
+    torch.cuda.synchronize()
+    eng.timer_begin()
+    parts = run.prepare()
+    setup_ms = eng.timer_end()
+    w, _ = eng.weights(prob.beta)
+    if prob.dm_trunc:
+        eng.truncate_blocks(prob.dm_trunc)
+    anchors = [int((wb > cfg["anchor_tol"]).sum()) for wb in w]
+    dropped_w = float(sum(wb[wb <= cfg["anchor_tol"]].sum() for wb in w))
+    costs = [chain_cost([prob.dims[b] for b in p[1]], [anchors[b] for b in p[1]], prob.nfreq) for p in parts]
+    batches = lpt_batches(costs, NB)
+    bparts = [[parts[k] for k in b] for b in batches]
+    nq_b = [eng.g2_count(bp, COEF_TOL, NZ_TOL) for bp in bparts]
+    nquad = int(sum(nq_b))
+    l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
+    acc = np.zeros(nfreq, dtype=complex)
+    seen = set()
+    batch_ms = {}
 
-    prob = Problem(args.config, device=local_rank)
-    # weak scaling: rank r owns the slab shifted by r * nfreq along n1
-    idx, z = matsubara_cube(prob.beta, prob.nfreq)
+    def step(i):
+        b = (i * world + rank) % NB
+        v = run.g2(bparts[b], z)
+        if b not in seen:
+            seen.add(b)
+            acc[:] += v
+        return b
+
+    eng.profile_begin()
+    for i in range(args.warmup):
+        step(i)
+    eng.profile_end()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    times, units = [], 0.0
+    launches0 = pgx.launch_count()
+    eng.profile_begin()
+    with ClockSampler(local_rank) as clk:
+        for i in range(args.steps):
+            l2buf.add_(1.0)
+            torch.cuda.synchronize()
+            eng.timer_begin()
+            b = step(args.warmup + i)
+            ms = eng.timer_end()
+            times.append(ms)
+            batch_ms.setdefault(b, ms)
+            units += float(nq_b[b]) * nfreq
+    launches = pgx.launch_count() - launches0
+    kstats = eng.profile_end()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    t_sum = float(np.sum(times))
+    t_max = t_sum
+    if world > 1:
+        t = torch.tensor([t_sum, units], device="cuda", dtype=torch.float64)
+        tt = t.clone()
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.SUM)
+        t_max, units = float(t[0].item()), float(tt[1].item())
+    value = units / (t_max / 1e3)
+    # batches no timed step covered: one untimed pass so the G2 is complete
+    for b in range(rank, NB, world):
+        if b not in batch_ms:
+            eng.timer_begin()
+            v = run.g2(bparts[b], z)
+            batch_ms[b] = eng.timer_end()
+            if b not in seen:
+                seen.add(b)
+                acc[:] += v
+    g2_ms = float(sum(batch_ms.values()))
+    if world > 1:
+        t = torch.tensor(acc.view(np.float64), device="cuda")
+        torch.distributed.all_reduce(t)  # the partial G2 of every rank's chains, summed
+        acc = t.cpu().numpy().view(complex)
+        t = torch.tensor([g2_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        g2_ms = float(t.item())
+    full_g2_s = (setup_ms + g2_ms) / 1e3
+
+    # the plain FP64 form (FP64 products, same anchored sum) on two batches
+    fp64 = None
+    if rank == 0:
+        sel = [0, NB // 2]
+        t_fp, t_mx, err = 0.0, 0.0, 0.0
+        for b in sel:
+            eng.timer_begin()
+            v64 = run.g2(bparts[b], z, flags=PGX_G2_ANCHORED)
+            t_fp += eng.timer_end()
+            eng.timer_begin()
+            vmx = run.g2(bparts[b], z, flags=PGX_G2_ANCHORED | PGX_G2_SPLIT_I8)
+            t_mx += eng.timer_end()
+            err = max(err, float(np.abs(vmx - v64).max() / max(np.abs(v64).max(), 1e-300)))
+        ratio = t_fp / t_mx
+        fp64 = {"batches_measured": sel, "fp64_ms": t_fp, "mixed_ms": t_mx, "g2_ratio_fp64_over_mixed": ratio,
+                "max_rel_diff_mixed_vs_fp64": err,
+                "fp64_form_full_g2_s_estimate": (setup_ms + g2_ms * ratio) / 1e3,
+                "note": "FP64 form timed on 2 of the 20 batches (same chains, same anchored sum); its full-G2 "
+                        "time is the setup plus the mixed G2 time scaled by the measured ratio"}
+
+    # e2e: the drop-in API from the Hamiltonian expression, whole job
+    e2e = None
+    if not args.no_e2e:
+        triples = [tuple(x) for x in z]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        v = prob.run_api(triples, split=cfg["split"], anchor_tol=cfg["anchor_tol"])
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        agree = float(np.abs(v - acc).max() / max(np.abs(acc).max(), 1e-300))
+        h2d = int(sum(int(d) * int(d) * 8 for d in prob.dims) + z.nbytes)
+        e2e = {"value": float(nquad) * nfreq * world / e2e_s, "unit": "term*freq/s", "h2d_bytes_per_step": h2d,
+               "d2h_bytes_per_step": int(nfreq * 16), "seconds_per_step": e2e_s,
+               "path": "drop-in API from the Hamiltonian expression (Hamiltonian.compute, DensityMatrix, "
+                       "FieldOperatorContainer.computeAll, TwoParticleGFContainer.computeAll on all 13824 "
+                       "triples), one whole job per step, wall clock with device syncs",
+               "max_rel_diff_vs_value_leg": agree}
+    if rank != 0:
+        return
+    top = kstats[0] if kstats else None
+    roof = roofline_entry(top, args.steps, torch, "ring8")
+    if roof is not None:
+        roof["kernels_ms_per_step"] = {k["name"]: round(k["ms"] / args.steps, 3) for k in kstats}
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_from_engine("ring8", run, z)
+            cpu["full_g2_extrapolated_s"] = float(nquad) * nfreq / cpu["value"]
+            cpu["note"] = "did not finish: the full G2 in the reference algorithm is extrapolated from N_quad / rate"
+        except Exception as e:
+            cpu = {"value": None, "unit": "term*freq/s", "cores": None, "kind": "port", "sample": f"failed: {e}"}
+    line = {
+        "metric": "G2 Lehmann term*freq evals/s", "value": value, "unit": "term*freq/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": cfg["workload"], "n_quad": nquad, "n_freq": nfreq, "blocks": len(prob.dims),
+                   "max_block": max(prob.dims), "g2_parts": len(parts), "batches": NB,
+                   "step": "one batch of block chains over the whole 24^3 grid; 20 steps = one full G2",
+                   "anchor_tol": cfg["anchor_tol"], "anchor_states": int(sum(anchors)),
+                   "anchor_dropped_weight": dropped_w,
+                   "products": "int8 tensor-core split (Ozaki, 6 slices) for products >= 1e9 multiply-adds",
+                   "l2": "flushed (256 MB write) between timed steps; working set of a step is several GB",
+                   "pole_resolution": POLE_RES, "nz_tol": NZ_TOL, "coef_tol": COEF_TOL},
+        "stages": {"eigh_weights_rotation_ms": setup_ms, "g2_all_batches_ms": g2_ms, "full_g2_s": full_g2_s},
+        "fp64_form": fp64,
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "e2e": e2e,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours_a5(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    from pomerol_b200 import pgx
+    from pomerol_b200.workloads import EngineRun, Problem
+    cfg = SETTINGS["a5"]
+    prob = Problem("a5", device=local_rank)
+    # weak scaling: rank r owns the cube shifted by r * nfreq along n1
+    _, z = matsubara_cube(prob.beta, prob.nfreq)
     z = z.copy()
     z[:, 0] += 1j * 2 * np.pi * rank * prob.nfreq / prob.beta
     run = EngineRun(prob, device=local_rank)
     run.step(z)
     nquad = run.eng.g2_count(run.parts, COEF_TOL, NZ_TOL)
     nfreq = len(z)
-    l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
-    # per-kernel CUDA-event ranges stay on through warm-up (their events are
-    # created there) and the timed steps; the timed steps' stats give the roofline
+    l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
     run.eng.profile_begin()
     for _ in range(args.warmup):
         run.step(z)
@@ -256,7 +515,7 @@ def run_ours(args, rank, world, local_rank):
     run.eng.profile_begin()
     with ClockSampler(local_rank) as clk:
         for _ in range(args.steps):
-            flush_l2(l2buf)
+            l2buf.add_(1.0)
             torch.cuda.synchronize()
             run.eng.timer_begin()
             out = run.step(z)
@@ -266,82 +525,58 @@ def run_ours(args, rank, world, local_rank):
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
-    ms = float(np.mean(times))
-    t_max = ms
+    t_max = float(np.mean(times))
     if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        t = torch.tensor([t_max], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         t_max = float(t.item())
-    units = float(nquad) * nfreq * world
-    value = units / (t_max / 1e3)
-
-    # e2e through the drop-in API from the Hamiltonian expression
-    e2e_times = []
-    triples = [tuple(x) for x in z]  # the caller's input, in host memory before the timed region
-    # untimed calls first: the drop-in objects of one call live until the next
-    # call replaces them, so the first two calls each set up a GPU context
-    e2e_warm = max(2, args.warmup)
-    for i in range(max(2, args.steps // 2) + e2e_warm):
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        v = prob.run_api(triples)
-        torch.cuda.synchronize()
-        if i >= e2e_warm:
-            e2e_times.append(time.perf_counter() - t0)
-    e2e_s = float(np.mean(e2e_times))
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_s = float(t.item())
-    agree = float(np.abs(v - out).max() / max(np.abs(out).max(), 1e-300))
-
+    value = float(nquad) * nfreq * world / (t_max / 1e3)
+    e2e = None
+    if not args.no_e2e:
+        triples = [tuple(x) for x in z]
+        e2e_times = []
+        for i in range(max(2, args.steps // 2) + 2):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            v = prob.run_api(triples)
+            torch.cuda.synchronize()
+            if i >= 2:
+                e2e_times.append(time.perf_counter() - t0)
+        e2e_s = float(np.mean(e2e_times))
+        if world > 1:
+            t = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            e2e_s = float(t.item())
+        e2e = {"value": float(nquad) * nfreq * world / e2e_s, "unit": "term*freq/s",
+               "h2d_bytes_per_step": int(run.h2d_bytes + z.nbytes), "d2h_bytes_per_step": int(out.nbytes),
+               "seconds_per_step": e2e_s,
+               "path": "drop-in API (Hamiltonian..TwoParticleGFContainer.computeAll) from the expression",
+               "max_rel_diff_vs_value_leg": float(np.abs(v - out).max() / max(np.abs(out).max(), 1e-300))}
     if rank != 0:
         return
-    # dominant kernel of the timed steps: algorithmic FLOPs per launch over its
-    # average event-timed duration, against the measured FP64 GEMM peak
     top = kstats[0] if kstats else None
-    peak = fp64_peak_tflops(torch)
-    achieved = None
-    if top and top["ms"] > 0 and top["flops"] > 0:
-        achieved = (top["flops"] / top["launches"]) / (top["ms"] / top["launches"] / 1e3) / 1e12
-    traffic = None
-    tf = ROOT / "profiles" / "roofline_traffic.json"
-    if tf.exists() and top:
-        try:
-            traffic = json.loads(tf.read_text()).get(args.config, {}).get(top["name"])
-        except Exception:
-            traffic = None
+    roof = roofline_entry(top, args.steps, torch, "a5")
+    if roof is not None:
+        roof["kernels_ms_per_step"] = {k["name"]: round(k["ms"] / args.steps, 4) for k in kstats}
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         try:
-            rate, dt, desc, threads, _ = cpu_sample(args.config)
-            cpu = {"value": rate, "unit": "term*freq/s", "cores": threads, "kind": "port", "sample": desc}
+            cpu = cpu_baseline_from_engine("a5", run, z)
         except Exception as e:
             cpu = {"value": None, "unit": "term*freq/s", "cores": None, "kind": "port", "sample": f"failed: {e}"}
     line = {
         "metric": "G2 Lehmann term*freq evals/s", "value": value, "unit": "term*freq/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_max, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "anderson_1+5_dim4096_chi_u0d0u0d0_16cube_beta20", "n_quad": nquad,
-                   "n_freq_per_rank": nfreq, "blocks": len(prob.dims), "max_block": max(prob.dims),
-                   "g2_parts": len(run.parts), "l2": "flushed (256 MB write) between timed steps; working set > L2",
-                   "stages_in_step": "eigh+weights+rotate(c+,c)+G2", "pole_resolution": 1e-8},
+        "config": {"workload": cfg["workload"], "n_quad": nquad, "n_freq_per_rank": nfreq,
+                   "blocks": len(prob.dims), "max_block": max(prob.dims), "g2_parts": len(run.parts),
+                   "l2": "flushed (256 MB write) between timed steps; working set > L2",
+                   "stages_in_step": "eigh+weights+rotate(c+,c)+G2", "pole_resolution": POLE_RES,
+                   "nz_tol": NZ_TOL, "coef_tol": COEF_TOL},
         "gpu_launches": launches // max(1, args.steps) * args.steps,
         "clocks": clk.summary(),
-        "e2e": {"value": float(nquad) * nfreq * world / e2e_s, "unit": "term*freq/s",
-                "h2d_bytes_per_step": int(run.h2d_bytes + z.nbytes),
-                "d2h_bytes_per_step": int(out.nbytes), "seconds_per_step": e2e_s,
-                "path": "drop-in API (Hamiltonian..TwoParticleGFContainer.computeAll) from the expression",
-                "max_rel_diff_vs_value_leg": agree},
-        "roofline": {"kernel": top["name"] if top else None,
-                     "bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": (achieved / peak) if (achieved and peak) else None, "traffic": traffic,
-                     "peak_source": "measured live: cuBLAS FP64 DGEMM 8192^3 (torch.matmul float64); "
-                                    "MEASURED_PEAKS.json has no FP64 figure (FP64 arithmetic, CUDA-core FMA pipe)",
-                     "launches_per_step": (top["launches"] / args.steps) if top else None,
-                     "ms_per_launch": (top["ms"] / top["launches"]) if top else None,
-                     "flops_per_launch": (top["flops"] / top["launches"]) if top else None,
-                     "kernels_ms_per_step": {k["name"]: round(k["ms"] / args.steps, 4) for k in kstats}},
+        "e2e": e2e,
+        "roofline": roof,
         "cpu_baseline": cpu,
     }
     print(json.dumps(line), flush=True)
@@ -360,10 +595,13 @@ def main():
 
         import torch
         torch.cuda.set_device(local_rank)
-        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
                                              device_id=torch.device("cuda", local_rank))
     try:
-        run_ours(args, rank, world, local_rank)
+        if args.config == "ring8":
+            run_ours_ring8(args, rank, world, local_rank)
+        else:
+            run_ours_a5(args, rank, world, local_rank)
     finally:
         if world > 1:
             import torch

@@ -18,8 +18,10 @@
 //   NonResonantTerm / ResonantTerm::operator()  TwoParticleGFPart.hpp:475-495
 //   TwoParticleGFPart::operator()    TwoParticleGFPart.cpp:309-322
 //   the OpenMP loop over frequencies TwoParticleGF.cpp:136-144.
-// "Non-zero" matrix elements are |x| > nz_tol (the reference's sparseView
-// keeps |x| > Tolerance * 1e-12).
+// "Non-zero" matrix elements are |x| > nz_tol: the reference's
+// sparseView(Tolerance) (MonomialOperatorPart.cpp:87) keeps |x| > Tolerance *
+// 1e-12 (Eigen's default dummy precision), i.e. |x| > 1e-20 at the default
+// Tolerance 1e-8.
 #include <omp.h>
 
 #include <cmath>
@@ -88,7 +90,9 @@ struct TermList {
 
 extern "C" {
 
-// Count quadruples passing the reference's enumeration filter.
+// Count quadruples passing the reference's enumeration filter: all four
+// elements non-zero and w1 + w2 + w3 + w4 > coef_tol, summed in that order
+// (TwoParticleGFPart.cpp:241).
 long long g2o_count(int d1, int d2, int d3, int d4, const double* O1, const double* O2, const double* O3,
                     const double* X4, const double* w1, const double* w2, const double* w3, const double* w4,
                     double coef_tol, double nz_tol) {
@@ -104,13 +108,13 @@ long long g2o_count(int d1, int d2, int d3, int d4, const double* O1, const doub
             if (l2.empty()) continue;
             for (int i4 = 0; i4 < d4; ++i4)
                 if (std::fabs(O3[(long)i3 * d4 + i4]) > nz_tol && std::fabs(X4[(long)i4 * d1 + i1]) > nz_tol) l4.push_back(i4);
-            const double a = w1[i1] + w3[i3];
-            if (a > coef_tol) {
+            // a rounded sum of non-negative weights only grows as terms are added
+            if (w1[i1] + w3[i3] > coef_tol) {
                 n += (long long)l2.size() * (long long)l4.size();
                 continue;
             }
             for (int i2 : l2)
-                for (int i4 : l4) n += (a + w2[i2] + w4[i4] > coef_tol);
+                for (int i4 : l4) n += (w1[i1] + w2[i2] + w3[i3] + w4[i4] > coef_tol);
         }
     }
     return n;
@@ -118,13 +122,16 @@ long long g2o_count(int d1, int d2, int d3, int d4, const double* O1, const doub
 
 // Reference-rule (rule=1) or exact (rule=0) evaluation of one part.
 // z: nfreq triples (re,im)x3 BEFORE the part's permutation; out += values.
-// row_begin/row_end restrict index1 (bounded samples); returns the number of
+// row_begin/row_end/row_step restrict index1 and col_step strides index3
+// (bounded samples: every quadruple of the sampled (index1, index3) pairs is
+// enumerated and evaluated as the reference does); returns the number of
 // quadruples enumerated; terms_out[0..1] = non-resonant / resonant terms kept.
 long long g2o_part(int d1, int d2, int d3, int d4, const double* O1, const double* O2, const double* O3,
                    const double* X4, const double* E1, const double* E2, const double* E3, const double* E4,
                    const double* w1, const double* w2, const double* w3, const double* w4, const int* perm, int sign,
                    double beta, double pole_res, double coef_tol, double nz_tol, int rule, int nfreq, const double* z,
-                   int row_begin, int row_end, int row_step, double* out, long long* terms_out, int nthreads) {
+                   int row_begin, int row_end, int row_step, int col_step, double* out, long long* terms_out,
+                   int nthreads) {
     TermList NR{pole_res, coef_tol, {}}, RS{pole_res, coef_tol, {}};
     std::vector<Term> nr_plain, rs_plain;  // exact mode keeps every term
     std::vector<int> flags_nr, flags_rs;
@@ -132,7 +139,7 @@ long long g2o_part(int d1, int d2, int d3, int d4, const double* O1, const doubl
     std::vector<int> l4;
     const double ctol = rule ? coef_tol : -1.0;
     for (int i1 = row_begin; i1 < row_end; i1 += std::max(row_step, 1)) {
-        for (int i3 = 0; i3 < d3; ++i3) {
+        for (int i3 = 0; i3 < d3; i3 += std::max(col_step, 1)) {
             l4.clear();
             for (int i4 = 0; i4 < d4; ++i4)
                 if (std::fabs(O3[(long)i3 * d4 + i4]) > nz_tol && std::fabs(X4[(long)i4 * d1 + i1]) > nz_tol)

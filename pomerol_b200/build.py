@@ -9,6 +9,7 @@ from __future__ import annotations
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -40,15 +41,18 @@ def build_pgx(verbose_ptxas: bool = False) -> Path:
     deps = [CSRC / s for s in CU_SOURCES] + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [ROOT / "include/pgx.h"]
     if not _stale(out, deps):
         return out
-    objs = []
+    objs, cmds = [], []
     for s in CU_SOURCES:
         o = LIB / (Path(s).stem + ".o")
         cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-I", ROOT / "include",
                "-c", CSRC / s, "-o", o]
         if verbose_ptxas:
             cmd[1:1] = ["-Xptxas", "-v"]
-        _run(cmd)
+        cmds.append(cmd)
         objs.append(o)
+    # translation units compile independently: one nvcc per core
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        list(ex.map(_run, cmds))
     _run([NVCC, *ARCH, "-shared", "-o", out, *objs, "-lcudart"])
     for o in objs:
         o.unlink()

@@ -149,10 +149,12 @@ __global__ void __launch_bounds__(CT_THREADS) contract_kernel(ContractArgs g) {
 
 // Number of state quadruples of one chain that the reference enumerates
 // (TwoParticleGFPart.cpp:210-250): all four rotated elements non-zero
-// (|x| > nz) and w1 + w2 + w3 + w4 > tol.  One thread per (i1, i3).  When
-// w1 + w3 > tol every (i2, i4) of the pair counts; otherwise a pair only
-// fails when all four weights are below tol, and the cold (i2, i4) pairs are
-// enumerated only for i2 close enough to the threshold to matter.
+// (|x| > nz) and w1 + w2 + w3 + w4 > tol, summed in that order as the
+// reference does (:241).  One thread per (i1, i3).  When w1 + w3 > tol every
+// (i2, i4) of the pair counts (the rounded sum only grows when a non-negative
+// weight is added); otherwise a pair only fails when all four weights are
+// below tol, and the cold (i2, i4) pairs are enumerated only for i2 close
+// enough to the threshold to matter.
 template <typename T>
 __global__ void count_kernel(const T* O1, const T* O2, const T* O3, const T* X4, int d1, int d2, int d3, int d4,
                              const double* w1, const double* w2, const double* w3, const double* w4, double tol,
@@ -161,7 +163,7 @@ __global__ void count_kernel(const T* O1, const T* O2, const T* O3, const T* X4,
     unsigned long long cnt = 0;
     if (idx < (long)d1 * d3) {
         const int i1 = (int)(idx / d3), i3 = (int)(idx % d3);
-        const double a = w1[i1] + w3[i3];
+        const double x1 = w1[i1], x3 = w3[i3];
         long n2 = 0, n4 = 0, n2c = 0, n4c = 0;
         for (int i2 = 0; i2 < d2; ++i2) {
             const bool v = sqrt(abs2(tocd(O1[(long)i1 * d2 + i2]))) > nz && sqrt(abs2(tocd(O2[(long)i2 * d3 + i3]))) > nz;
@@ -173,25 +175,70 @@ __global__ void count_kernel(const T* O1, const T* O2, const T* O3, const T* X4,
             n4 += v;
             n4c += v && !(w4[i4] > tol);
         }
-        if (a > tol) {
+        if (x1 + x3 > tol) {
             cnt = (unsigned long long)(n2 * n4);
         } else {
             cnt = (unsigned long long)(n2 * n4 - n2c * n4c);
-            const double t = tol - a;
             for (int i2 = 0; i2 < d2; ++i2) {
-                if (w2[i2] > tol || !(w2[i2] + cold_max4 > t)) continue;
+                if (w2[i2] > tol) continue;
+                const double s = (x1 + w2[i2]) + x3;
+                if (!(s + cold_max4 > tol)) continue;
                 if (!(sqrt(abs2(tocd(O1[(long)i1 * d2 + i2]))) > nz && sqrt(abs2(tocd(O2[(long)i2 * d3 + i3]))) > nz)) continue;
                 for (int i4 = 0; i4 < d4; ++i4) {
                     if (w4[i4] > tol) continue;
                     const bool v =
                         sqrt(abs2(tocd(O3[(long)i3 * d4 + i4]))) > nz && sqrt(abs2(tocd(X4[(long)i4 * d1 + i1]))) > nz;
-                    cnt += v && (w2[i2] + w4[i4] > t);
+                    cnt += v && (s + w4[i4] > tol);
                 }
             }
         }
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
+// Entries of one rotated operator part with |x| <= nz (absent from the
+// reference's sparse matrices after sparseView).
+template <typename T>
+__global__ void zero_count_kernel(const T* a, long n, double nz, unsigned long long* out) {
+    unsigned long long cnt = 0;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x)
+        cnt += !(sqrt(abs2(tocd(a[i]))) > nz);
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
+// Quadruples of one chain whose four rotated elements are all non-zero but
+// which fail the weight filter: ((w1 + w2) + w3) + w4 <= tol.  Only states
+// with w <= tol can take part ("cold" states; c1 .. c4 their weights, c2 and
+// c4 sorted descending).  One thread per cold (i1, i3): of the n2 x n4 cold
+// (i2, i4) pairs it subtracts those that pass, found per i2 by a binary
+// search over c4 (the rounded sum is monotone in each weight); i2 stops at
+// the first that cannot pass with the largest w4.
+__global__ void cold_fail_kernel(const double* c1, int n1, const double* c3, int n3, const double* c2, int n2,
+                                 const double* c4, int n4, double tol, unsigned long long* out) {
+    const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    unsigned long long fail = 0;
+    if (idx < (long)n1 * n3 && n2 > 0 && n4 > 0) {
+        const double x1 = c1[idx / n3], x3 = c3[idx % n3];
+        if (!(x1 + x3 > tol)) {
+            unsigned long long pass = 0;
+            for (int q = 0; q < n2; ++q) {
+                const double s = (x1 + c2[q]) + x3;
+                if (!(s + c4[0] > tol)) break;
+                int lo = 1, hi = n4;  // c4[0 .. lo) pass; find the first index that fails
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s + c4[mid] > tol) lo = mid + 1;
+                    else hi = mid;
+                }
+                pass += (unsigned long long)lo;
+            }
+            fail = (unsigned long long)n2 * (unsigned long long)n4 - pass;
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) fail += __shfl_xor_sync(0xffffffffu, fail, o);
+    if ((threadIdx.x & 31) == 0 && fail) atomicAdd(out, fail);
 }
 
 // Frequency plan of one permutation: distinct z1, z3, distinct (z1, z3)
@@ -449,9 +496,8 @@ void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const d
     }
     if (flags & PGX_G2_ANCHORED) {
         PGX_CHECK(coef_tol >= 0.0, PGX_ERR_ARG, "anchor threshold must be non-negative");
-        cudaEvent_t a0, a1;
-        PGX_CUDA(cudaEventCreate(&a0));
-        PGX_CUDA(cudaEventCreate(&a1));
+        ScopedEvents ev(2);
+        const cudaEvent_t a0 = ev[0], a1 = ev[1];
         PGX_CUDA(cudaEventRecord(a0, st));
         const int split = (flags & PGX_G2_SPLIT_I8) ? 6 : 0;
         if (split && c->oz.err.p) PGX_CUDA(cudaMemsetAsync(c->oz.err.p, 0, sizeof(int), st));
@@ -468,15 +514,10 @@ void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const d
         c->g2t.total_ms = t;
         c->g2t.gemm_ms = 0.0;
         c->g2t.gemm_flops = 0.0;
-        cudaEventDestroy(a0);
-        cudaEventDestroy(a1);
         return;
     }
-    cudaEvent_t e0, e1, ea, eb;
-    PGX_CUDA(cudaEventCreate(&e0));
-    PGX_CUDA(cudaEventCreate(&e1));
-    PGX_CUDA(cudaEventCreate(&ea));
-    PGX_CUDA(cudaEventCreate(&eb));
+    ScopedEvents ev(4);
+    const cudaEvent_t e0 = ev[0], e1 = ev[1], ea = ev[2], eb = ev[3];
     PGX_CUDA(cudaEventRecord(ea, st));
     // one frequency plan per distinct permutation
     std::map<std::tuple<int, int, int>, int> perm_id;
@@ -567,10 +608,6 @@ void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const d
     c->g2t.total_ms = tot;
     c->g2t.gemm_ms = gemm_ms;
     c->g2t.gemm_flops = gemm_flops;
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    cudaEventDestroy(ea);
-    cudaEventDestroy(eb);
 }
 
 }  // namespace pgx
@@ -582,12 +619,6 @@ void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_
     Problem& P = c->P;
     cudaStream_t st = c->stream;
     PGX_CHECK(P.have_w, PGX_ERR_STATE, "weights must be computed before counting");
-    DevBuf& b = c->scratch[10];
-    b.reserve(sizeof(unsigned long long));
-    PGX_CUDA(cudaMemsetAsync(b.p, 0, sizeof(unsigned long long), st));
-    std::vector<double> w(P.esize);
-    PGX_CUDA(cudaMemcpyAsync(w.data(), P.d_w, P.esize * sizeof(double), cudaMemcpyDeviceToHost, st));
-    PGX_CUDA(cudaStreamSynchronize(st));
     for (int q = 0; q < nparts; ++q) {
         const pgx_g2_part& gp = parts[q];
         for (int k = 0; k < 4; ++k) {
@@ -598,8 +629,78 @@ void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_
             PGX_CHECK(o.rotated && pi >= 0 && o.parts[pi].right == gp.block[(k + 1) % 4], PGX_ERR_ARG,
                       "G2 part is not a block chain of rotated operators");
         }
+    }
+    // zero entries (|x| <= nz) of every operator part the chains use: a chain
+    // whose four parts have none is counted in closed form
+    std::map<std::pair<int, int>, int> zslot;
+    for (int q = 0; q < nparts; ++q)
+        for (int k = 0; k < 4; ++k) {
+            const int pi = P.ops[parts[q].op[k]].by_left[parts[q].block[k]];
+            zslot.emplace(std::make_pair(parts[q].op[k], pi), (int)zslot.size());
+        }
+    DevBuf& b = c->scratch[10];
+    // slot 0: quadruples counted by count_kernel; slot 1: quadruples of the dense
+    // chains that fail the weight filter; then one zero count per operator part
+    b.reserve((2 + zslot.size()) * sizeof(unsigned long long));
+    PGX_CUDA(cudaMemsetAsync(b.p, 0, (2 + zslot.size()) * sizeof(unsigned long long), st));
+    unsigned long long* d_cnt = b.as<unsigned long long>();
+    for (const auto& kv : zslot) {
+        const Operator& o = P.ops[kv.first.first];
+        const OpPart& op = o.parts[kv.first.second];
+        const long n = (long)op.dl * op.dr;
+        const int blocks = (int)std::max<long>(1, std::min<long>(ceil_div(n, 256), 148L * 8));
+        if (o.is_complex)
+            zero_count_kernel<cd><<<blocks, 256, 0, st>>>(o.mat.as<cd>() + op.off, n, nz_tol, d_cnt + 2 + kv.second);
+        else
+            zero_count_kernel<double><<<blocks, 256, 0, st>>>(o.mat.as<double>() + op.off, n, nz_tol,
+                                                              d_cnt + 2 + kv.second);
+        check_launch("zero_count_kernel");
+    }
+    std::vector<unsigned long long> zeros(zslot.size());
+    if (!zeros.empty())
+        PGX_CUDA(cudaMemcpyAsync(zeros.data(), d_cnt + 2, zeros.size() * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, st));
+    std::vector<double> w(P.esize);
+    PGX_CUDA(cudaMemcpyAsync(w.data(), P.d_w, P.esize * sizeof(double), cudaMemcpyDeviceToHost, st));
+    PGX_CUDA(cudaStreamSynchronize(st));
+    // cold weights (w <= tol) of every block, sorted descending
+    std::vector<double> cold;
+    std::vector<long> cold_off(P.nblocks + 1, 0);
+    for (int bl = 0; bl < P.nblocks; ++bl) {
+        cold_off[bl] = (long)cold.size();
+        for (int i = 0; i < P.dims[bl]; ++i) {
+            const double x = w[P.eoff[bl] + i];
+            if (!(x > coef_tol)) cold.push_back(x);
+        }
+        std::sort(cold.begin() + cold_off[bl], cold.end(), [](double x, double y) { return x > y; });
+    }
+    cold_off[P.nblocks] = (long)cold.size();
+    DevBuf& cb = c->scratch[11];
+    cb.reserve(std::max<size_t>(cold.size(), 1) * sizeof(double));
+    if (!cold.empty()) h2d(cb.p, cold.data(), cold.size() * sizeof(double), st);
+    const double* d_cold = cb.as<double>();
+    unsigned long long dense_total = 0;  // closed-form chains: d1 d2 d3 d4 each
+    for (int q = 0; q < nparts; ++q) {
+        const pgx_g2_part& gp = parts[q];
         const int S1 = gp.block[0], S2 = gp.block[1], S3 = gp.block[2], S4 = gp.block[3];
         const int d1 = P.dims[S1], d2 = P.dims[S2], d3 = P.dims[S3], d4 = P.dims[S4];
+        bool dense = true;
+        for (int k = 0; k < 4; ++k)
+            dense = dense && zeros[zslot.at({gp.op[k], P.ops[gp.op[k]].by_left[gp.block[k]]})] == 0;
+        if (dense) {
+            // every (i1, i2, i3, i4) is enumerated; subtract those failing the weight filter
+            dense_total += (unsigned long long)d1 * d2 * d3 * d4;
+            const int n1 = (int)(cold_off[S1 + 1] - cold_off[S1]), n3 = (int)(cold_off[S3 + 1] - cold_off[S3]);
+            const int n2 = (int)(cold_off[S2 + 1] - cold_off[S2]), n4 = (int)(cold_off[S4 + 1] - cold_off[S4]);
+            const long n = (long)n1 * n3;
+            if (n > 0 && n2 > 0 && n4 > 0) {
+                cold_fail_kernel<<<(int)ceil_div(n, 256), 256, 0, st>>>(
+                    d_cold + cold_off[S1], n1, d_cold + cold_off[S3], n3, d_cold + cold_off[S2], n2,
+                    d_cold + cold_off[S4], n4, coef_tol, d_cnt + 1);
+                check_launch("cold_fail_kernel");
+            }
+            continue;
+        }
         double cold4 = 0.0;
         for (int i = 0; i < d4; ++i) {
             const double x = w[P.eoff[S4] + i];
@@ -612,19 +713,19 @@ void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_
             count_kernel<cd><<<ceil_div(n, 256), 256, 0, st>>>(
                 o1.mat.as<cd>() + o1.parts[o1.by_left[S1]].off, o2.mat.as<cd>() + o2.parts[o2.by_left[S2]].off,
                 o3.mat.as<cd>() + o3.parts[o3.by_left[S3]].off, o4.mat.as<cd>() + o4.parts[o4.by_left[S4]].off, d1, d2,
-                d3, d4, w1, w2, w3, w4, coef_tol, nz_tol, cold4, b.as<unsigned long long>());
+                d3, d4, w1, w2, w3, w4, coef_tol, nz_tol, cold4, d_cnt);
         } else {
             count_kernel<double><<<ceil_div(n, 256), 256, 0, st>>>(
                 o1.mat.as<double>() + o1.parts[o1.by_left[S1]].off, o2.mat.as<double>() + o2.parts[o2.by_left[S2]].off,
                 o3.mat.as<double>() + o3.parts[o3.by_left[S3]].off, o4.mat.as<double>() + o4.parts[o4.by_left[S4]].off,
-                d1, d2, d3, d4, w1, w2, w3, w4, coef_tol, nz_tol, cold4, b.as<unsigned long long>());
+                d1, d2, d3, d4, w1, w2, w3, w4, coef_tol, nz_tol, cold4, d_cnt);
         }
         check_launch("count_kernel");
     }
-    unsigned long long h = 0;
-    PGX_CUDA(cudaMemcpyAsync(&h, b.p, sizeof(h), cudaMemcpyDeviceToHost, st));
+    unsigned long long h[2] = {0, 0};
+    PGX_CUDA(cudaMemcpyAsync(h, d_cnt, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     PGX_CUDA(cudaStreamSynchronize(st));
-    *count = (long long)h;
+    *count = (long long)(h[0] + dense_total - h[1]);
 }
 
 }  // namespace pgx

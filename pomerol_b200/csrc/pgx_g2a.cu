@@ -46,143 +46,230 @@ struct DTerm {
     long b1, b3, bh, bk;
     const double *Ek, *Eh, *wh;
     const int* hot;       // anchor states (inner indices) of the anchor block
-    const cd* ts;         // per triple: s of this sub-term
-    const int* gt;        // triples grouped by (z1, z3): triple ids
-    const int* goff;      // group g holds gt[goff[g] .. goff[g+1])
     const int* gi1;       // per group: index of z1 in the plan
     const int* gi3;       // per group: index of z3 in the plan
-    int ng;
     int nh, nk;
     int va_cplx, vb_cplx; // operand element types
     int va_hstate, vb_hstate;  // h stride applies to the anchor's state index instead of its position
     int use_delta;
-    int nt;               // triples of the plan (work count only)
-    int hc, nhc;          // anchors per work item and items per group: heavy groups split by anchor range
     double sgn, cdelta, cnum, pref;
+    // host side only: the plan and the frequency sum (0: z2, 1: z1+z2+z3,
+    // 2: z1+z2, 3: z2+z3) of the sub-term
+    int plan, sidx;
 };
 
 __device__ __forceinline__ cd load_v(const void* p, int cplx, long idx) {
     return cplx ? static_cast<const cd*>(p)[idx] : cd{static_cast<const double*>(p)[idx], 0.0};
 }
 
-// Triples of one (z1, z3) group handled together: the operand product
-// VA * VB does not depend on z2, so it is loaded once for DG triples.
-// Four per pass: 128 registers and two 256-thread CTAs per SM (eight triples
-// per pass needed 211 registers and left one CTA per SM; 17% slower).
-constexpr int DG = 4;  // the batch inversion below is written out for four
+// ---- contractions as products
+// For one sub-term, the (z1, z3) groups of a plan whose triples carry the same
+// list of frequency sums s_j form a class.  Over a class the contraction is a
+// complex product
+//   out[t(g, j)] += pref * sum_{h, k} AB[g, (h, k)] K[(h, k), j]
+// with AB[g, (h, k)] = VA(g, h, k) VB(g, h, k) (the two anchored operand
+// arrays, multiplied as the tile is loaded) and the Lehmann kernel
+//   K[(h, k), j] = delta ? cdelta beta w_h : cnum w_h / (s_j - sgn (E_k - E_h)),
+// delta = |s_j - sgn (E_k - E_h)| <= PoleResolution (FP64, the reference's
+// rule for resonant terms).  K is formed once per tile element and used by
+// every row of the tile; the rows of a T1 class are all (z1, z3) groups, those
+// of T2, T3, T4 classes the groups with equal z1 + z3, z1 or z3.  A work item
+// is one tile of rows of a class over a range of anchors; items of the same
+// outputs add their results with atomics.
+struct CClass {
+    int term;          // index into the DTerm list
+    int nrows, ncols;  // rows (groups) and columns (frequency sums) of the class
+    const cd* s;       // ncols frequency sums
+    const int* rows;   // nrows group indices
+    const int* slots;  // nrows x ncols triple ids (row-major), -1 where absent
+};
+struct CItem {
+    int cls, row0, h0, h1;
+};
 
-template <bool DELTA>
-__device__ void dterm_group(const DTerm& d, int g, int h0, int h1, double beta, double tol2, cd* out, int lane) {
-    const int i1 = d.gi1[g], i3 = d.gi3[g];
-    const int tb = d.goff[g], te = d.goff[g + 1];
-    for (int t0 = tb; t0 < te; t0 += DG) {
-        const int cnt = min(DG, te - t0);
-        double sx[DG], sy[DG], ax[DG], ay[DG];
-        int tt[DG];
-#pragma unroll
-        for (int q = 0; q < DG; ++q) {
-            const int t = d.gt[t0 + min(q, cnt - 1)];  // a short group repeats its last triple
-            const cd sv = d.ts[t];
-            tt[q] = t;
-            sx[q] = sv.x;
-            sy[q] = sv.y;
-            ax[q] = 0.0;
-            ay[q] = 0.0;
+constexpr int CG_NX = 8;
+// rows per thread: 4 in 64-row tiles (16 thread rows), BM / 8 below (8 thread rows)
+__host__ __device__ constexpr int cg_tm(int bm) { return bm >= 64 ? 4 : bm / 8; }
+
+// One CTA per work item: BM rows x BN columns, (BM / TM) x CG_NX threads,
+// each a TM x (BN / CG_NX) block of complex accumulators.  The next k-tile's
+// operand loads are issued into registers before the current tile's products.
+template <int BM, int BN>
+__global__ void __launch_bounds__((BM / cg_tm(BM)) * CG_NX)
+    contract_gemm_kernel(const DTerm* __restrict__ terms, const CClass* __restrict__ classes,
+                         const CItem* __restrict__ items, double beta, double tol2, cd* __restrict__ out) {
+    constexpr int CG_TM = cg_tm(BM);
+    constexpr int NY = BM / CG_TM, NT = NY * CG_NX, TN = BN / CG_NX;
+    // k-tile depth: 16, or 8 where two 16-deep buffers would pass 48 KB
+    constexpr int CG_BK = (BM * BN > 64 * 24) ? 8 : 16;
+    constexpr int LA = (BM * CG_BK + NT - 1) / NT, LB = (BN * CG_BK + NT - 1) / NT;
+    __shared__ cd As[2][CG_BK][BM + 1];
+    __shared__ cd Bs[2][CG_BK][BN + 1];
+    __shared__ cd s_s[BN];
+    __shared__ long s_oa[BM], s_ob[BM];
+    const CItem it = items[blockIdx.x];
+    const CClass cc = classes[it.cls];
+    const DTerm& d = terms[cc.term];
+    const int tid = threadIdx.x, tx = tid % CG_NX, ty = tid / CG_NX;
+    const int nrows = min(BM, cc.nrows - it.row0);
+    for (int j = tid; j < BN; j += NT) s_s[j] = j < cc.ncols ? cc.s[j] : cd{0.0, 0.0};
+    for (int r = tid; r < BM; r += NT) {
+        long oa = 0, ob = 0;
+        if (r < nrows) {
+            const int g = cc.rows[it.row0 + r];
+            const long i1 = d.gi1[g], i3 = d.gi3[g];
+            oa = i1 * d.a1 + i3 * d.a3;
+            ob = i1 * d.b1 + i3 * d.b3;
         }
-        for (int h = h0; h < h1; ++h) {
-            const int hs = d.hot[h];
-            const double eh = d.Eh[hs], w = d.wh[hs];
-            const double cw = d.cnum * w, cdl = d.cdelta * beta * w;
-            const long oa = i1 * d.a1 + i3 * d.a3 + (long)(d.va_hstate ? hs : h) * d.ah;
-            const long ob = i1 * d.b1 + i3 * d.b3 + (long)(d.vb_hstate ? hs : h) * d.bh;
-            // operands of the next k are loaded while the current one is computed
-            cd nva{0.0, 0.0}, nvb{0.0, 0.0};
-            double nek = 0.0;
-            if (lane < d.nk) {
-                nva = load_v(d.VA, d.va_cplx, oa + lane * d.ak);
-                nvb = load_v(d.VB, d.vb_cplx, ob + lane * d.bk);
-                nek = d.Ek[lane];
-            }
-            for (int k = lane; k < d.nk; k += 32) {
-                const cd ab = nva * nvb;
-                const double de = d.sgn * (nek - eh);
-                if (k + 32 < d.nk) {
-                    nva = load_v(d.VA, d.va_cplx, oa + (k + 32) * d.ak);
-                    nvb = load_v(d.VB, d.vb_cplx, ob + (k + 32) * d.bk);
-                    nek = d.Ek[k + 32];
-                }
-                double Dx[DG], m2[DG], rc[DG];
-                bool dl[DG];
-                bool in_range = true;
+        s_oa[r] = oa;
+        s_ob[r] = ob;
+    }
+    cd acc[CG_TM][TN];
 #pragma unroll
-                for (int q = 0; q < DG; ++q) {
-                    Dx[q] = sx[q] - de;
-                    const double mq = fma(Dx[q], Dx[q], sy[q] * sy[q]);
-                    dl[q] = DELTA && mq <= tol2;
-                    m2[q] = dl[q] ? 1.0 : mq;  // resonant: the kernel value does not use it
-                    in_range = in_range && recip_in_range(m2[q]);
-                }
-                if (in_range) {
-                    // Montgomery's batch inversion: the four reciprocals from one
-                    // division of the product of all four (pairwise products up,
-                    // then each pair's reciprocal times its sibling's product
-                    // down).  With every value in [1e-30, 1e30] the product stays
-                    // inside the double range.
-                    const double p01 = m2[0] * m2[1], p23 = m2[2] * m2[3];
-                    const double inv = 1.0 / (p01 * p23);
-                    const double i01 = inv * p23, i23 = inv * p01;
-                    rc[0] = i01 * m2[1];
-                    rc[1] = i01 * m2[0];
-                    rc[2] = i23 * m2[3];
-                    rc[3] = i23 * m2[2];
-                } else {
+    for (int a = 0; a < CG_TM; ++a)
 #pragma unroll
-                    for (int q = 0; q < DG; ++q) rc[q] = 1.0 / m2[q];
-                }
+        for (int b = 0; b < TN; ++b) acc[a][b] = cd{0.0, 0.0};
+    __syncthreads();
+
+    const int nk = d.nk;
+    const int ktiles = (nk + CG_BK - 1) / CG_BK;
+    const long nsteps = (long)(it.h1 - it.h0) * ktiles;
+    cd ra[LA], rb[LB];
+    // operands of step q (anchor h0 + q / ktiles, k-tile q % ktiles) into registers
+    auto load = [&](long q) {
+        const int h = it.h0 + (int)(q / ktiles), k0 = (int)(q % ktiles) * CG_BK;
+        const int hs = d.hot[h];
+        const long oah = (long)(d.va_hstate ? hs : h) * d.ah, obh = (long)(d.vb_hstate ? hs : h) * d.bh;
 #pragma unroll
-                for (int q = 0; q < DG; ++q) {
-                    const double r = cw * rc[q];
-                    const bool delta = dl[q];
-                    const double Kx = delta ? cdl : Dx[q] * r;
-                    const double Ky = delta ? 0.0 : -sy[q] * r;
-                    ax[q] = fma(ab.x, Kx, fma(-ab.y, Ky, ax[q]));
-                    ay[q] = fma(ab.x, Ky, fma(ab.y, Kx, ay[q]));
+        for (int u = 0; u < LA; ++u) {
+            const int l = tid + u * NT;
+            cd v{0.0, 0.0};
+            if (l < BM * CG_BK) {
+                const int r = l / CG_BK, kk = l % CG_BK, k = k0 + kk;
+                if (r < nrows && k < nk) {
+                    const cd x = load_v(d.VA, d.va_cplx, s_oa[r] + oah + (long)k * d.ak);
+                    const cd y = load_v(d.VB, d.vb_cplx, s_ob[r] + obh + (long)k * d.bk);
+                    v = x * y;
                 }
             }
+            ra[u] = v;
+        }
+        const double eh = d.Eh[hs], w = d.wh[hs];
+        const double cw = d.cnum * w, cdl = d.cdelta * beta * w;
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            const int l = tid + u * NT;
+            cd v{0.0, 0.0};
+            if (l < BN * CG_BK) {
+                const int kk = l / BN, j = l % BN, k = k0 + kk;
+                if (k < nk && j < cc.ncols) {
+                    const cd sv = s_s[j];
+                    const double dx = sv.x - d.sgn * (d.Ek[k] - eh);
+                    const double m2 = fma(dx, dx, sv.y * sv.y);
+                    if (d.use_delta && m2 <= tol2) {
+                        v = cd{cdl, 0.0};
+                    } else {
+                        const double rr = cw * recip_pos(m2);
+                        v = cd{dx * rr, -sv.y * rr};
+                    }
+                }
+            }
+            rb[u] = v;
+        }
+    };
+    auto store = [&](int buf) {
+#pragma unroll
+        for (int u = 0; u < LA; ++u) {
+            const int l = tid + u * NT;
+            if (l < BM * CG_BK) As[buf][l % CG_BK][l / CG_BK] = ra[u];
         }
 #pragma unroll
-        for (int q = 0; q < DG; ++q) {
-            double x = ax[q], y = ay[q];
-            for (int o = 16; o > 0; o >>= 1) {
-                x += __shfl_xor_sync(0xffffffffu, x, o);
-                y += __shfl_xor_sync(0xffffffffu, y, o);
-            }
-            if (lane == 0 && q < cnt && (x != 0.0 || y != 0.0)) {
-                atomicAdd(&out[tt[q]].x, d.pref * x);
-                atomicAdd(&out[tt[q]].y, d.pref * y);
+        for (int u = 0; u < LB; ++u) {
+            const int l = tid + u * NT;
+            if (l < BN * CG_BK) Bs[buf][l / BN][l % BN] = rb[u];
+        }
+    };
+    if (nsteps > 0) {
+        load(0);
+        store(0);
+    }
+    __syncthreads();
+    int buf = 0;
+    for (long q = 0; q < nsteps; ++q) {
+        const bool more = q + 1 < nsteps;
+        if (more) load(q + 1);
+#pragma unroll
+        for (int kk = 0; kk < CG_BK; ++kk) {
+            cd a[CG_TM], b[TN];
+#pragma unroll
+            for (int u = 0; u < CG_TM; ++u) a[u] = As[buf][kk][ty + NY * u];
+#pragma unroll
+            for (int u = 0; u < TN; ++u) b[u] = Bs[buf][kk][tx + CG_NX * u];
+#pragma unroll
+            for (int qa = 0; qa < CG_TM; ++qa)
+#pragma unroll
+                for (int qb = 0; qb < TN; ++qb) {
+                    acc[qa][qb].x = fma(a[qa].x, b[qb].x, acc[qa][qb].x);
+                    acc[qa][qb].x = fma(-a[qa].y, b[qb].y, acc[qa][qb].x);
+                    acc[qa][qb].y = fma(a[qa].x, b[qb].y, acc[qa][qb].y);
+                    acc[qa][qb].y = fma(a[qa].y, b[qb].x, acc[qa][qb].y);
+                }
+        }
+        if (more) store(buf ^ 1);
+        __syncthreads();
+        buf ^= 1;
+    }
+#pragma unroll
+    for (int qa = 0; qa < CG_TM; ++qa) {
+        const int r = ty + NY * qa;
+        if (r >= nrows) continue;
+#pragma unroll
+        for (int qb = 0; qb < TN; ++qb) {
+            const int j = tx + CG_NX * qb;
+            if (j >= cc.ncols) continue;
+            const int t = cc.slots[(long)(it.row0 + r) * cc.ncols + j];
+            const double x = acc[qa][qb].x, y = acc[qa][qb].y;
+            if (t >= 0 && (x != 0.0 || y != 0.0)) {
+                atomicAdd(&out[t].x, d.pref * x);
+                atomicAdd(&out[t].y, d.pref * y);
             }
         }
     }
 }
 
-// One warp per (sub-term, (z1, z3) group, anchor range); lanes over the summed
-// index k.  woff[q] = first work item of term q (prefix sum of groups x ranges).
-__global__ void __launch_bounds__(256, 2) dterm_kernel(const DTerm* terms, const int* woff, int nterms, double beta,
-                                                    double tol2, cd* out) {
-    const int lane = threadIdx.x & 31;
-    const int nwork = woff[nterms];
-    for (int wk = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5); wk < nwork;
-         wk += (int)(((long)gridDim.x * blockDim.x) >> 5)) {
-        int lo = 0, hi = nterms - 1;  // last q with woff[q] <= wk
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (woff[mid] <= wk) lo = mid;
-            else hi = mid - 1;
-        }
-        const DTerm& d = terms[lo];
-        const int u = wk - woff[lo], g = u / d.nhc, h0 = (u % d.nhc) * d.hc, h1 = min(d.nh, h0 + d.hc);
-        if (d.use_delta) dterm_group<true>(d, g, h0, h1, beta, tol2, out, lane);
-        else dterm_group<false>(d, g, h0, h1, beta, tol2, out, lane);
+// Column widths of the contraction tiles; a class with more columns is split
+// into column chunks of at most CG_BN_MAX.
+constexpr int CG_NBN = 4, CG_BN_MAX = 32;
+constexpr int CG_BNS[CG_NBN] = {8, 16, 24, 32};
+
+template <int BM, int BN>
+void launch_contract_t(unsigned n, cudaStream_t st, const DTerm* t, const CClass* c, const CItem* i, double beta,
+                       double tol2, cd* out) {
+    contract_gemm_kernel<BM, BN><<<n, (BM / cg_tm(BM)) * CG_NX, 0, st>>>(t, c, i, beta, tol2, out);
+}
+
+template <int BM>
+void launch_contract_m(int BN, unsigned n, cudaStream_t st, const DTerm* t, const CClass* c, const CItem* i,
+                       double beta, double tol2, cd* out) {
+    if (BN == 8) launch_contract_t<BM, 8>(n, st, t, c, i, beta, tol2, out);
+    else if (BN == 16) launch_contract_t<BM, 16>(n, st, t, c, i, beta, tol2, out);
+    else if (BN == 24) launch_contract_t<BM, 24>(n, st, t, c, i, beta, tol2, out);
+    else launch_contract_t<BM, 32>(n, st, t, c, i, beta, tol2, out);
+}
+
+// Row-tile heights of the contraction (a class takes the smallest that holds
+// its rows, 64-row tiles above 32 rows).
+constexpr int CG_NBM = 5;
+constexpr int CG_BMS[CG_NBM] = {8, 16, 24, 32, 64};
+
+void launch_contract(int BM, int BN, unsigned n, cudaStream_t st, const DTerm* t, const CClass* c, const CItem* i,
+                     double beta, double tol2, cd* out) {
+    switch (BM) {
+        case 8: launch_contract_m<8>(BN, n, st, t, c, i, beta, tol2, out); break;
+        case 16: launch_contract_m<16>(BN, n, st, t, c, i, beta, tol2, out); break;
+        case 24: launch_contract_m<24>(BN, n, st, t, c, i, beta, tol2, out); break;
+        case 32: launch_contract_m<32>(BN, n, st, t, c, i, beta, tol2, out); break;
+        default: launch_contract_m<64>(BN, n, st, t, c, i, beta, tol2, out); break;
     }
 }
 
@@ -204,6 +291,8 @@ struct KeyC {
 // contractions use under one permutation: z2', z1'+z2'+z3', z1'+z2', z2'+z3'.
 struct PermSums {
     DevBuf buf;
+    std::vector<cd> h;  // host copy: sum k of triple t at h[k * nfreq + t]
+    int nfreq = 0;
     const cd* ds[4] = {nullptr, nullptr, nullptr, nullptr};
 };
 
@@ -220,6 +309,8 @@ void build_sums(PermSums& ps, const int perm[3], int nfreq, const double* z, cud
     ps.buf.reserve(std::max<size_t>(h.size(), 1) * sizeof(cd));
     if (!h.empty()) h2d(ps.buf.p, h.data(), h.size() * sizeof(cd), st);
     for (int k = 0; k < 4; ++k) ps.ds[k] = ps.buf.as<cd>() + (size_t)k * nfreq;
+    ps.h = std::move(h);
+    ps.nfreq = nfreq;
 }
 
 // Distinct z1' and z3' of all triples of a call under one permutation, in
@@ -255,7 +346,96 @@ struct APlan {
     cd *dZ1 = nullptr, *dZ3 = nullptr;
     const cd* ds[4] = {nullptr, nullptr, nullptr, nullptr};  // the permutation's sums
     int *dgt = nullptr, *dgoff = nullptr, *dgi1 = nullptr, *dgi3 = nullptr;
+    const PermSums* sums = nullptr;
+    // contraction classes per frequency sum (built on first use), device
+    // pointers in `cls` (term unset), storage in cbuf
+    bool have_cls[4] = {false, false, false, false};
+    std::vector<CClass> cls[4];
+    DevBuf cbuf[4];
 };
+
+// Contraction classes of one plan for frequency sum k: the (z1, z3) groups
+// whose triples carry the same sums (compared after rounding to 2^-46 of the
+// largest |s|, so sums equal up to rounding share a class; the class uses its
+// first group's values), columns ordered by sum, split into chunks of at most
+// CG_BN_MAX columns.
+void build_classes(APlan& pl, int k, cudaStream_t st) {
+    if (pl.have_cls[k]) return;
+    const PermSums& ps = *pl.sums;
+    const cd* sv = ps.h.data() + (size_t)k * ps.nfreq;
+    double smax = 0.0;
+    for (int t : pl.gt) smax = std::max(smax, std::max(std::fabs(sv[t].x), std::fabs(sv[t].y)));
+    const double q = smax > 0.0 ? std::ldexp(smax, -46) : 1.0;
+    using Key = std::vector<std::pair<long long, long long>>;
+    struct HC {
+        std::vector<cd> s;
+        std::vector<int> rows, slots;
+    };
+    std::map<Key, int> idx;
+    std::vector<HC> hc;
+    const int ng = (int)pl.gi1.size();
+    std::vector<std::tuple<long long, long long, int>> el;
+    for (int g = 0; g < ng; ++g) {
+        el.clear();
+        for (int u = pl.goff[g]; u < pl.goff[g + 1]; ++u) {
+            const int t = pl.gt[u];
+            el.emplace_back(std::llround(sv[t].x / q), std::llround(sv[t].y / q), t);
+        }
+        std::sort(el.begin(), el.end());
+        Key key;
+        key.reserve(el.size());
+        for (auto& e : el) key.emplace_back(std::get<0>(e), std::get<1>(e));
+        auto it = idx.find(key);
+        if (it == idx.end()) {
+            it = idx.emplace(std::move(key), (int)hc.size()).first;
+            hc.emplace_back();
+            for (auto& e : el) hc.back().s.push_back(sv[std::get<2>(e)]);
+        }
+        HC& c = hc[it->second];
+        c.rows.push_back(g);
+        for (auto& e : el) c.slots.push_back(std::get<2>(e));
+    }
+    // column chunks, then one device buffer for every class of this sum
+    std::vector<HC> fin;
+    for (HC& c : hc) {
+        const int nc = (int)c.s.size(), nr = (int)c.rows.size();
+        for (int j0 = 0; j0 < nc; j0 += CG_BN_MAX) {
+            const int w = std::min(CG_BN_MAX, nc - j0);
+            HC f;
+            f.s.assign(c.s.begin() + j0, c.s.begin() + j0 + w);
+            f.rows = c.rows;
+            f.slots.resize((size_t)nr * w);
+            for (int r = 0; r < nr; ++r)
+                for (int j = 0; j < w; ++j) f.slots[(size_t)r * w + j] = c.slots[(size_t)r * nc + j0 + j];
+            fin.push_back(std::move(f));
+        }
+    }
+    auto al = [](size_t b) { return (b + 15) & ~size_t(15); };
+    size_t bytes = 0;
+    for (const HC& f : fin) bytes += al(f.s.size() * sizeof(cd)) + al(f.rows.size() * sizeof(int)) + al(f.slots.size() * sizeof(int));
+    pl.cbuf[k].reserve(std::max<size_t>(bytes, 16));
+    std::vector<char> host(std::max<size_t>(bytes, 16));
+    char* dev = pl.cbuf[k].as<char>();
+    size_t o = 0;
+    for (const HC& f : fin) {
+        CClass c{};
+        c.term = -1;
+        c.nrows = (int)f.rows.size();
+        c.ncols = (int)f.s.size();
+        std::memcpy(host.data() + o, f.s.data(), f.s.size() * sizeof(cd));
+        c.s = reinterpret_cast<const cd*>(dev + o);
+        o += al(f.s.size() * sizeof(cd));
+        std::memcpy(host.data() + o, f.rows.data(), f.rows.size() * sizeof(int));
+        c.rows = reinterpret_cast<const int*>(dev + o);
+        o += al(f.rows.size() * sizeof(int));
+        std::memcpy(host.data() + o, f.slots.data(), f.slots.size() * sizeof(int));
+        c.slots = reinterpret_cast<const int*>(dev + o);
+        o += al(f.slots.size() * sizeof(int));
+        pl.cls[k].push_back(c);
+    }
+    if (bytes) h2d(dev, host.data(), bytes, st);
+    pl.have_cls[k] = true;
+}
 
 void build_aplan(APlan& pl, const std::vector<int>& tids, const PermIndex& ix, int o1, int n1, int o3, int n3,
                  const PermSums& ps, cudaStream_t st) {
@@ -276,6 +456,7 @@ void build_aplan(APlan& pl, const std::vector<int>& tids, const PermIndex& ix, i
     }
     pl.goff.push_back((int)nt);
     for (int k = 0; k < 4; ++k) pl.ds[k] = ps.ds[k];
+    pl.sums = &ps;
     const size_t ng = pl.gi1.size();
     pl.buf.reserve((size_t)(n1 + n3) * sizeof(cd) + (nt + 3 * ng + 1) * sizeof(int) + 256);
     char* p = pl.buf.as<char>();
@@ -347,7 +528,7 @@ GemmProblem<TA, TB, cd> gp(const typename src_t<TA>::type* A, long sai, long sak
 
 template <typename T>
 static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector<int>& bplan,
-                      const std::vector<ChainWs>& wsl, const pgx_g2_part* parts, const std::vector<APlan>& plans,
+                      const std::vector<ChainWs>& wsl, const pgx_g2_part* parts, std::vector<APlan>& plans,
                       const std::vector<std::array<int, 4>>& rs, cd* pool, const int* d_hot,
                       const std::vector<long>& hot_off, double pole_res, int split, cd* d_out) {
     Problem& P = c->P;
@@ -458,6 +639,7 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
         PGX_CUDA(cudaEventRecord(c->fork, st));
         PGX_CUDA(cudaStreamWaitEvent(s0, c->fork, 0));
         PGX_CUDA(cudaStreamWaitEvent(s1, c->fork, 0));
+        SideJoin join(c, st, 2);  // st waits for both side streams on every exit
         launch_on(pa, 0, s0);
         launch_on(pb, 1, s1);
         PGX_CUDA(cudaEventRecord(c->join[0], s0));
@@ -466,10 +648,6 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
         PGX_CUDA(cudaStreamWaitEvent(s1, c->join[0], 0));
         launch_on(pc, 2, s0);
         launch_on(pd, 3, s1);
-        PGX_CUDA(cudaEventRecord(c->join[0], s0));
-        PGX_CUDA(cudaEventRecord(c->join[1], s1));
-        PGX_CUDA(cudaStreamWaitEvent(st, c->join[0], 0));
-        PGX_CUDA(cudaStreamWaitEvent(st, c->join[1], 0));
     }
     // ---- contractions per triple
     std::vector<DTerm> dt;
@@ -501,13 +679,10 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
             d.hot = d_hot + hot_off[S[anchor]];
             d.nh = nh;
             d.nk = nk;
-            d.ts = pl.ds[sidx];
-            d.gt = pl.dgt;
-            d.goff = pl.dgoff;
             d.gi1 = pl.dgi1;
             d.gi3 = pl.dgi3;
-            d.ng = (int)pl.gi1.size();
-            d.nt = (int)pl.gt.size();
+            d.plan = bplan[j];
+            d.sidx = sidx;
             d.sgn = sgn;
             d.use_delta = use_delta;
             d.cdelta = cd_;
@@ -562,33 +737,60 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
         }
     }
     if (!dt.empty()) {
-        // a work item covers at most about 2^17 (anchor, state) pairs per pass
-        // over its triples, so that no single warp sets the kernel's duration
-        std::vector<int> woff(dt.size() + 1, 0);
-        double elems = 0.0;
-        long items = 0;
+        // classes of every sub-term, grouped by tile shape (BM 32 or 64 rows,
+        // BN 8 / 16 / 24 / 32 columns); a work item is one row tile of a class
+        // over a range of anchors, about 2^22 complex multiply-adds
+        std::vector<CClass> cls[CG_NBM][CG_NBN];
+        std::vector<CItem> its[CG_NBM][CG_NBN];
+        double macs = 0.0;
         for (size_t q = 0; q < dt.size(); ++q) {
-            DTerm& d = dt[q];
-            d.hc = std::max(1, std::min(std::max(d.nh, 1), (1 << 17) / std::max(d.nk, 1)));
-            d.nhc = std::max(1, (int)ceil_div((long)d.nh, (long)d.hc));
-            items += (long)d.ng * d.nhc;
-            PGX_CHECK(items < (1L << 31), PGX_ERR_ARG, "G2 contraction: too many work items");
-            woff[q + 1] = (int)items;
-            elems += (double)d.nh * d.nk * d.nt;
+            const DTerm& d = dt[q];
+            APlan& pl = plans[d.plan];
+            build_classes(pl, d.sidx, st);
+            for (const CClass& c0 : pl.cls[d.sidx]) {
+                int bm = 0, bn = 0;
+                while (bm < CG_NBM - 1 && CG_BMS[bm] < c0.nrows) ++bm;
+                while (CG_BNS[bn] < c0.ncols) ++bn;
+                const int BM = CG_BMS[bm], BN = CG_BNS[bn];
+                CClass c = c0;
+                c.term = (int)q;
+                const int ci = (int)cls[bm][bn].size();
+                cls[bm][bn].push_back(c);
+                const int hc = (int)std::max<long>(1, (1L << 22) / ((long)BM * BN * std::max(d.nk, 1)));
+                for (int r0 = 0; r0 < c.nrows; r0 += BM)
+                    for (int h0 = 0; h0 < d.nh; h0 += hc) its[bm][bn].push_back(CItem{ci, r0, h0, std::min(d.nh, h0 + hc)});
+                macs += (double)c.nrows * c.ncols * d.nh * d.nk;
+            }
         }
+        size_t bytes = ((dt.size() * sizeof(DTerm) + 255) & ~size_t(255));
+        for (int a = 0; a < CG_NBM; ++a)
+            for (int b = 0; b < CG_NBN; ++b)
+                bytes += ((cls[a][b].size() * sizeof(CClass) + 255) & ~size_t(255)) +
+                         ((its[a][b].size() * sizeof(CItem) + 255) & ~size_t(255));
         DevBuf& bd = c->scratch[3];
-        const size_t tb = (dt.size() * sizeof(DTerm) + 255) & ~size_t(255);
-        bd.reserve(tb + woff.size() * sizeof(int));
-        h2d(bd.p, dt.data(), dt.size() * sizeof(DTerm), st);
-        h2d(bd.as<char>() + tb, woff.data(), woff.size() * sizeof(int), st);
-        const long warps = woff.back();
-        const int blocks = (int)std::max<long>(1, std::min<long>(ceil_div(warps * 32, 256), 148L * 16));
-        // 24 FP64 operations per (h, k, triple) element: two complex products,
-        // the denominator, its squared modulus, the kernel value, accumulation
-        ProfRange pr("dterm_kernel", st, 24.0 * elems, 0.0);
-        dterm_kernel<<<blocks, 256, 0, st>>>(bd.as<DTerm>(), reinterpret_cast<const int*>(bd.as<char>() + tb),
-                                             (int)dt.size(), P.beta, pole_res * pole_res, d_out);
-        check_launch("dterm_kernel");
+        bd.reserve(bytes);
+        char* base_p = bd.as<char>();
+        size_t o = 0;
+        auto put = [&](const void* h, size_t n) {
+            char* d = base_p + o;
+            if (n) h2d(d, h, n, st);
+            o += (n + 255) & ~size_t(255);
+            return d;
+        };
+        const DTerm* d_terms = reinterpret_cast<const DTerm*>(put(dt.data(), dt.size() * sizeof(DTerm)));
+        // 8 FP64 operations per complex multiply-add of (h, k, triple)
+        ProfRange pr("contract_gemm_kernel", st, 8.0 * macs, 0.0);
+        const double tol2 = pole_res * pole_res;
+        for (int a = 0; a < CG_NBM; ++a)
+            for (int b = 0; b < CG_NBN; ++b) {
+                if (its[a][b].empty()) continue;
+                PGX_CHECK(its[a][b].size() < (1u << 31), PGX_ERR_ARG, "G2 contraction: too many work items");
+                const CClass* dc = reinterpret_cast<const CClass*>(put(cls[a][b].data(), cls[a][b].size() * sizeof(CClass)));
+                const CItem* di = reinterpret_cast<const CItem*>(put(its[a][b].data(), its[a][b].size() * sizeof(CItem)));
+                const unsigned n = (unsigned)its[a][b].size();
+                launch_contract(CG_BMS[a], CG_BNS[b], n, st, d_terms, dc, di, P.beta, tol2, d_out);
+            }
+        check_launch("contract_gemm_kernel");
     }
     // the next batch reuses the device descriptor buffers in stream order
 }

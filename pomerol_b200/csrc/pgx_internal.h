@@ -196,6 +196,33 @@ inline Operator take_operator(Problem& P) {
     return op;
 }
 
+// Events owned by one call, destroyed on every exit from it (a throw included).
+struct ScopedEvents {
+    cudaEvent_t e[4] = {nullptr, nullptr, nullptr, nullptr};
+    explicit ScopedEvents(int n) {
+        for (int i = 0; i < n && i < 4; ++i) {
+            const cudaError_t r = cudaEventCreate(&e[i]);
+            if (r != cudaSuccess) {
+                e[i] = nullptr;
+                release();
+                throw Error{PGX_ERR_CUDA, std::string("cudaEventCreate: ") + cudaGetErrorString(r)};
+            }
+        }
+    }
+    ~ScopedEvents() { release(); }
+    ScopedEvents(const ScopedEvents&) = delete;
+    ScopedEvents& operator=(const ScopedEvents&) = delete;
+    cudaEvent_t operator[](int i) const { return e[i]; }
+
+  private:
+    void release() {
+        for (auto& x : e) {
+            if (x) cudaEventDestroy(x);
+            x = nullptr;
+        }
+    }
+};
+
 struct G2Timing {
     double total_ms = 0, gemm_ms = 0, gemm_flops = 0;
 };
@@ -309,6 +336,24 @@ namespace pgx {
 
 void launch_eigh(pgx_ctx* c);
 void ensure_side_streams(pgx_ctx* c);  // the context's four side streams and their events
+
+// Makes stream st wait for the context's first n side streams when the scope
+// ends, on a throw too: work issued there before the throw then completes
+// before st's later work and before the host staging is recycled.
+struct SideJoin {
+    pgx_ctx* c;
+    cudaStream_t st;
+    int n;
+    SideJoin(pgx_ctx* c_, cudaStream_t st_, int n_) : c(c_), st(st_), n(n_) {}
+    ~SideJoin() {
+        for (int k = 0; k < n; ++k) {
+            cudaEventRecord(c->join[k], c->aux[k]);
+            cudaStreamWaitEvent(st, c->join[k], 0);
+        }
+    }
+    SideJoin(const SideJoin&) = delete;
+    SideJoin& operator=(const SideJoin&) = delete;
+};
 
 // Device buffers of one eigensolve (any number of blocks), all caller-owned.
 struct EighDev {

@@ -313,6 +313,7 @@ PYBIND11_MODULE(_pomerol, m) {
         .def_readwrite("PoleResolution", &TwoParticleGFContainer::PoleResolution)
         .def_readwrite("CoefficientTolerance", &TwoParticleGFContainer::CoefficientTolerance)
         .def_readwrite("SplitProducts", &TwoParticleGFContainer::SplitProducts)
+        .def_readwrite("AnchorTolerance", &TwoParticleGFContainer::AnchorTolerance)
         .def("prepareAll",
              [](TwoParticleGFContainer& g, std::vector<std::array<ParticleIndex, 4>> const& idx) {
                  std::set<IndexCombination4> s;

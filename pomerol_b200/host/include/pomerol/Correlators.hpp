@@ -148,9 +148,11 @@ class TwoParticleGF : public Thermal, public ComputableObject {
 public:
     RealType PoleResolution = 1e-8;
     RealType CoefficientTolerance = 1e-16;
-    // Sub-terms are anchored on states with weight > min(CoefficientTolerance,
-    // AnchorTolerance); ExactSum = true sums every state quadruple instead.
-    RealType AnchorTolerance = 1e-15;
+    // Sub-terms are anchored on states with weight > AnchorTolerance (a
+    // negative value, the default, takes CoefficientTolerance).  The part it
+    // drops is bounded by (beta/pi)^3 times the Boltzmann weight of the
+    // dropped states.  ExactSum = true sums every state quadruple instead.
+    RealType AnchorTolerance = -1;
     bool ExactSum = false;
     // SplitProducts = true runs the anchored sum's largest products on the int8
     // tensor cores (six 7-bit slices per operand, FP64 recombination; about
@@ -205,6 +207,7 @@ public:
     RealType PoleResolution = 1e-8;
     RealType CoefficientTolerance = 1e-16;
     bool SplitProducts = false;  // passed to every element (TwoParticleGF::SplitProducts)
+    RealType AnchorTolerance = -1;  // passed to every element (TwoParticleGF::AnchorTolerance)
 
     TwoParticleGFContainer(IndexClassification const& IndexInfo, StatesClassification const& S, Hamiltonian const& H,
                            DensityMatrix const& DM, FieldOperatorContainer const& Ops);

@@ -272,7 +272,7 @@ std::vector<ComplexType> TwoParticleGF::values(FreqVec3 const& freqs) const {
     // anchored sum: sub-terms whose Boltzmann weight is below the anchor
     // threshold are skipped (the same order as the coefficient filter);
     // ExactSum evaluates every state quadruple.
-    const double anchor = std::min(CoefficientTolerance, AnchorTolerance);
+    const double anchor = AnchorTolerance < 0 ? CoefficientTolerance : AnchorTolerance;
     dev.check(pgx_g2(dev.ctx(), (int32_t)parts.size(), parts.data(), (int32_t)freqs.size(), z.data(), PoleResolution,
                      ExactSum ? 0.0 : anchor,
                      ExactSum ? PGX_G2_EXACT : (PGX_G2_ANCHORED | (SplitProducts ? PGX_G2_SPLIT_I8 : 0)),
@@ -374,6 +374,7 @@ void TwoParticleGFContainer::prepareAll(std::set<IndexCombination4> const& Indic
         g.PoleResolution = PoleResolution;
         g.CoefficientTolerance = CoefficientTolerance;
         g.SplitProducts = SplitProducts;
+        g.AnchorTolerance = AnchorTolerance;
         g.prepare();
     }
 }
@@ -383,7 +384,10 @@ std::map<IndexCombination4, std::vector<ComplexType>> TwoParticleGFContainer::co
                                                                                          MPI_Comm const& comm,
                                                                                          bool split) {
     std::map<IndexCombination4, std::vector<ComplexType>> out;
-    for (auto& kv : NonTrivialElements) kv.second->SplitProducts = SplitProducts;
+    for (auto& kv : NonTrivialElements) {
+        kv.second->SplitProducts = SplitProducts;
+        kv.second->AnchorTolerance = AnchorTolerance;
+    }
     if (split) {
         for (auto& kv : NonTrivialElements) out[kv.first] = kv.second->compute(clearTerms, freqs, comm);
     } else {
@@ -399,6 +403,7 @@ ElementWithPermFreq<TwoParticleGF>& TwoParticleGFContainer::operator()(IndexComb
     e.element().PoleResolution = PoleResolution;
     e.element().CoefficientTolerance = CoefficientTolerance;
     e.element().SplitProducts = SplitProducts;
+    e.element().AnchorTolerance = AnchorTolerance;
     e.element().prepare();
     return e;
 }

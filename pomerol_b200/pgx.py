@@ -264,7 +264,7 @@ class Engine:
             arr[k].sign = int(sign)
         return arr
 
-    def g2_count(self, parts, coef_tol=1e-16, nz_tol=1e-12):
+    def g2_count(self, parts, coef_tol=1e-16, nz_tol=1e-20):
         arr = self._parts_array(parts)
         out = np.zeros(1, dtype=np.int64)
         self._ck(self.lib.pgx_g2_count(self.h, len(parts), C.cast(arr, C.c_void_p), float(coef_tol), float(nz_tol),

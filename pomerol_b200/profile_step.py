@@ -28,6 +28,8 @@ def main():
     ap.add_argument("--split", action="store_true",
                     help="anchored G2 with its stacked products on the int8 tensor cores (PGX_G2_SPLIT_I8); "
                          "with --chain each cube also runs in FP64 for the error")
+    ap.add_argument("--anchor-tol", type=float, default=1e-16, help="anchor weight threshold of the G2 sum")
+    ap.add_argument("--fp64", action="store_true", help="with --split: also run the plain FP64 form (same sum)")
     ap.add_argument("--autotune", action="store_true",
                     help="measure the GEMM tile classes on one step (after one untimed step) before timing")
     a = ap.parse_args()
@@ -61,7 +63,7 @@ def main():
         run = Chi3Run(prob)
     else:
         _, z = matsubara_cube(prob.beta, prob.nfreq)
-        run = EngineRun(prob, split=a.split)
+        run = EngineRun(prob, split=a.split, anchor_tol=a.anchor_tol)
     if a.autotune:
         autotune(run.eng, lambda: run.step(z))
     for s in range(a.steps):
@@ -79,6 +81,17 @@ def main():
         extra = "" if a.chi3 else f"g2 {run.eng.g2_timing()}, "
         print(f"step {s}: device {ms:.1f} ms, wall {1e3 * (time.perf_counter() - t0):.1f} ms, "
               f"{extra}|v|max {np.abs(v).max():.4e}", flush=True)
+    if a.fp64 and a.split and not a.chi3:
+        from .pgx import PGX_G2_ANCHORED
+        run.eng.profile_begin()
+        run.eng.timer_begin()
+        v64 = run.g2(run.parts, z, flags=PGX_G2_ANCHORED)
+        ms = run.eng.timer_end()
+        for k in run.eng.profile_end()[:6]:
+            print(f"  {k['name']:40s} x{k['launches']:<3d} {k['ms']:9.3f} ms  "
+                  f"{k['flops'] / max(k['ms'], 1e-9) / 1e9:9.3f} TFLOP/s", flush=True)
+        print(f"plain FP64 form (G2 only, same anchored sum): device {ms:.1f} ms; split vs FP64: max|diff| / max|G2| "
+              f"{np.abs(v - v64).max() / np.abs(v64).max():.2e}", flush=True)
 
 
 def autotune(eng, step):

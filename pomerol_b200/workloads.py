@@ -105,10 +105,11 @@ class Problem:
         self.dims = [self.S.getBlockSize(b) for b in range(self.S.getNumberOfBlocks())]
         self.device = device
 
-    def run_api(self, freqs):
+    def run_api(self, freqs, split=False, anchor_tol=None):
         """Full drop-in sequence from the Hamiltonian expression: Hamiltonian
         (eigensolve), DensityMatrix, FieldOperatorContainer (rotation),
-        TwoParticleGFContainer.computeAll on the triples.  Returns the values."""
+        TwoParticleGFContainer.computeAll on the triples (SplitProducts =
+        split; AnchorTolerance = anchor_tol when given).  Returns the values."""
         H = P.Hamiltonian(self.S, self.device)
         H.prepare(self.HExpr, self.hs)
         H.compute()
@@ -121,6 +122,9 @@ class Problem:
         ops.prepareAll(self.hs)
         ops.computeAll()
         chi = P.TwoParticleGFContainer(self.ii, self.S, H, rho, ops)
+        chi.SplitProducts = bool(split)
+        if anchor_tol is not None:
+            chi.AnchorTolerance = float(anchor_tol)
         key = (self.u0, self.d0, self.u0, self.d0)
         chi.prepareAll([key])
         out = chi.computeAll(True, [tuple(t) for t in freqs])
@@ -326,7 +330,9 @@ class EngineRun:
         self.cdag = {i: self.eng.op_define([(r, l, np.asarray(t), np.asarray(c)) for r, l, t, c in a])
                      for i, a in self.actions.items()}
 
-    def step(self, triples):
+    def prepare(self):
+        """Eigensolve, weights, block truncation, rotation of c^+ and c; sets
+        self.parts (the block chains of chi_(u0,d0,u0,d0) on this context)."""
         e = self.eng
         e.eigh()
         e.weights(self.prob.beta)
@@ -340,7 +346,42 @@ class EngineRun:
         c = {i: e.op_adjoint(self.cdag[i]) for i in (u, d)}
         self._adjoints = tuple(c.values())
         slots = (c[u], c[d], self.cdag[u])  # C1, C2, CX3 of chi_(u0,d0,u0,d0)
-        parts = [((slots[p[0]], slots[p[1]], slots[p[2]], self.cdag[d]), tuple(b), tuple(p), s)
-                 for b, p, s in self.chains]
-        self.parts = parts
-        return e.g2(parts, triples, pole_res=1e-8, coef_tol=self.anchor_tol, flags=self.flags)
+        self.parts = [((slots[p[0]], slots[p[1]], slots[p[2]], self.cdag[d]), tuple(b), tuple(p), s)
+                      for b, p, s in self.chains]
+        return self.parts
+
+    def g2(self, parts, triples, flags=None):
+        """G2 of a list of block chains at the triples (one pgx_g2 call)."""
+        return self.eng.g2(parts, triples, pole_res=1e-8, coef_tol=self.anchor_tol,
+                           flags=self.flags if flags is None else flags)
+
+    def step(self, triples):
+        self.prepare()
+        return self.g2(self.parts, triples)
+
+
+def chain_cost(dims, anchors, nfreq):
+    """Relative cost of one block chain's anchored G2 on an nfreq^3 cube:
+    complex multiply-adds of its products over (z1, z3) pairs (those of at
+    least 1e9 run about five times faster, on the int8 tensor cores) plus its
+    contractions over the triples."""
+    d1, d2, d3, d4 = dims
+    r1, r2, r3, r4 = anchors
+    n2 = float(nfreq) ** 2
+    prods = [n2 * d3 * d4 * r2, n2 * r1 * d3 * d4, n2 * r3 * d1 * d2, n2 * d1 * d2 * r4]
+    cost = sum(m / 5.0 if m >= 1e9 else m for m in prods)
+    cost += float(nfreq) ** 3 * (r2 * (d3 + d4) + r3 * (d2 + d1) + r1 * (d4 + d3) + r4 * (d1 + d2)) / 2.0
+    return cost
+
+
+def lpt_batches(costs, nbatch):
+    """Chains split into nbatch lists of about equal cost: largest first, each
+    to the list with the least cost so far.  Lists keep the chains' order."""
+    order = sorted(range(len(costs)), key=lambda k: -costs[k])
+    load = [0.0] * nbatch
+    out = [[] for _ in range(nbatch)]
+    for k in order:
+        b = min(range(nbatch), key=lambda i: load[i])
+        out[b].append(k)
+        load[b] += costs[k]
+    return [sorted(b) for b in out]

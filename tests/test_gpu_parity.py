@@ -388,11 +388,103 @@ def test_anchored_g2_anderson_a5_subset(harness):
     # dense GPU sum over every quadruple (exact mode) on the full cube
     vx = g.eng.g2(parts, fz)
     assert np.abs(v - vx).max() < 1e-9 * np.abs(vx).max()
-    # exact oracle on a few triples, all chains
+    # exact oracle on a few triples, all chains: two ordinary ones, and two
+    # resonant ones (n1 + n2 = -1 and n1 = n3; n2 = n3)
     oparts = L.g2_parts(ed, ed.c(u), ed.c(d), ed.cdag(u), ed.cdag(d))
-    sel = [0, 777, 2048, 4095]
+    pick = [(-8, -8, -8), (7, 0, -3), (-1, 0, -1), (3, 5, 5)]
+    sel = [int(np.flatnonzero((trip == np.array(t)).all(1))[0]) for t in pick]
     ref = L.g2_exact(ed, oparts, [tuple(fz[t]) for t in sel])
     assert np.abs(vx[sel] - ref).max() < 1e-9 * np.abs(ref).max()
+
+
+def test_anchored_g2_anderson_a5_vs_anchored_oracle(harness):
+    """Anderson 1+5 (dim 4096, beta=20), all 216 block chains, 64 triples
+    (n1, n2, n3) in {-8, -1, 0, 7}^3, which hold every resonant case
+    (n1 + n2 = -1, n1 = n3, n2 = n3) and the cube's extreme frequencies: the
+    anchored GPU sum (FP64 products, and int8 split products) against the
+    numpy anchored oracle at the same anchor threshold (1e-16): 1e-12 and
+    1e-9 of max|G2|."""
+    from oracle import g2_anchored as GA
+    from pomerol_b200.pgx import PGX_G2_ANCHORED, PGX_G2_SPLIT_I8
+    U, epsd, eps, V, beta = M.anderson_a5_params(0)
+    m = M.make_model(M.anderson(U, epsd, eps, V))
+    g = harness(m, beta)
+    ed = EDm.ED(m, beta)
+    u, d = m.info.getIndex("C", 0, 1), m.info.getIndex("C", 0, 0)
+    S = (-8, -1, 0, 7)
+    fz = L.fermionic(np.array([(a, b, x) for a in S for b in S for x in S]), beta)
+    parts = g.g2_parts(g.c(u), g.c(d), g.cdag(u), g.cdag(d))
+    oparts = L.g2_parts(ed, ed.c(u), ed.c(d), ed.cdag(u), ed.cdag(d))
+    assert len(parts) == len(oparts) == 216
+    ref = GA.g2_anchored(ed, oparts, fz, res=1e-8, anchor_tol=1e-16)
+    v = _anchored(g, parts, fz)
+    assert np.abs(v - ref).max() < 1e-12 * np.abs(ref).max()
+    g.eng.set_g2_split_threshold(0.0)
+    try:
+        vs = g.eng.g2(parts, fz, pole_res=1e-8, coef_tol=1e-16, flags=PGX_G2_ANCHORED | PGX_G2_SPLIT_I8)
+    finally:
+        g.eng.set_g2_split_threshold(1e9)
+    assert np.abs(vs - ref).max() < 1e-9 * np.abs(ref).max()
+
+
+def test_g2_reference_rule_anderson_a5_small_chains(harness):
+    """Anderson 1+5: the reference's own algorithm (oracle/g2_oracle.cpp,
+    rule=1: sparse chase, weight filter at CoefficientTolerance 1e-16,
+    sub-term filters, TermList pole merging at PoleResolution 1e-8) on the 40
+    block chains with the fewest state quadruples, against the GPU's
+    anchored sum of the same chains at 8 triples including resonant ones.
+    Merging averages poles that agree within 1e-8, so the two agree to
+    about 1e-8 of max|G2| (stated tolerance 1e-7)."""
+    from oracle import g2c
+    U, epsd, eps, V, beta = M.anderson_a5_params(0)
+    m = M.make_model(M.anderson(U, epsd, eps, V))
+    g = harness(m, beta)
+    ed = EDm.ED(m, beta)
+    u, d = m.info.getIndex("C", 0, 1), m.info.getIndex("C", 0, 0)
+    parts = g.g2_parts(g.c(u), g.c(d), g.cdag(u), g.cdag(d))
+    oparts = L.g2_parts(ed, ed.c(u), ed.c(d), ed.cdag(u), ed.cdag(d))
+    size = [int(np.prod([len(ed.E[b]) for b in p["b"]])) for p in oparts]
+    keep = [int(k) for k in np.argsort(size, kind="stable")[:40]]
+    fz = L.fermionic(np.array([(-1, 0, -1), (3, -4, 2), (0, 0, 5), (-8, 7, 7), (5, 2, -6), (-3, 2, 4),
+                               (1, 1, 1), (6, -7, -2)]), beta)
+    ref, nq, _ = g2c.evaluate(ed, [oparts[k] for k in keep], fz, pole_res=1e-8, coef_tol=1e-16, rule=True)
+    assert nq > 0
+    v = _anchored(g, [parts[k] for k in keep], fz)
+    assert np.abs(v - ref).max() < 1e-7 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("model", ["plaquette", "anderson3"])
+@pytest.mark.parametrize("coef_tol,nz_tol", [(1e-16, 1e-20), (1e-16, 1e-12), (1e-4, 1e-20), (1e-3, 1e-12)])
+def test_g2_count_matches_oracle(harness, model, coef_tol, nz_tol):
+    """N_quad, the work unit of the G2 metric (pgx_g2_count: the closed form
+    for chains without zero elements, the per-(i1, i3) kernel otherwise)
+    against the oracle's enumeration of the reference's filter
+    (TwoParticleGFPart.cpp:210-250) on the same rotated matrices and weights
+    (read back from the device, since the count depends on the eigenbasis
+    chosen inside degenerate subspaces): equal counts."""
+    from types import SimpleNamespace
+
+    from oracle import g2c
+    if model == "plaquette":
+        mdl, beta, site = M.make_model(M.plaquette()), 10.0, "A"
+    else:
+        U, epsd, eps, V, beta = M.anderson_a5_params(0)
+        mdl, site = M.make_model(M.anderson(U, epsd, eps[:3], V[:3])), "C"
+    g = harness(mdl, beta)
+    u, d = mdl.info.getIndex(site, 0, 1), mdl.info.getIndex(site, 0, 0)
+    parts = g.g2_parts(g.c(u), g.c(d), g.cdag(u), g.cdag(d))
+
+    def mat(op, left):
+        info = g.eng.op_info(op)
+        k = next(i for i, (r, lb) in enumerate(info) if lb == left)
+        return g.eng.op_read(op, k)
+
+    oparts = [dict(b=b, O1=mat(ops[0], b[0]), O2=mat(ops[1], b[1]), O3=mat(ops[2], b[2]), CX4=mat(ops[3], b[3]),
+                   perm=perm, sign=sign) for ops, b, perm, sign in parts]
+    host = SimpleNamespace(E=g.E, w=g.w)
+    n_gpu = g.eng.g2_count(parts, coef_tol, nz_tol)
+    n_ref = g2c.count(host, oparts, coef_tol, nz_tol)
+    assert n_gpu == n_ref > 0
 
 
 def test_plaquette_g2_matches_oracle(harness):
@@ -880,14 +972,14 @@ def test_chi3_anderson5_workload_sample(harness):
 
 def test_batch_of_models_against_oracle():
     """The batch workload's engine path (one context, blocks of every model
-    in one eigensolve, per-model weights and frequencies) on the first eight
-    models of the 64-model draw (3-6 bath sites, dims 256-16384, beta 6-50):
+    in one eigensolve, per-model weights and frequencies) on all 64 models of
+    the draw (3-6 bath sites, dims 256-16384, beta 5-50):
     G_dn on 64 fermionic and chi_dd on 8 bosonic frequencies of every model
     against the oracle's exact sums (1e-11 / 1e-10 relative); a second step
     on the same context reproduces the first up to the order of the
     evaluation's atomic accumulation (1e-13 relative)."""
     from pomerol_b200.workloads import BatchRun, b64_params
-    params = b64_params()[:8]
+    params = b64_params()
     run = BatchRun(params, nG=64, nchi=8)
     G, X = run.step()
     G2, X2 = run.step()

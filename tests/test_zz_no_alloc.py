@@ -43,12 +43,19 @@ def test_eigh_noalloc_matches_pgx_eigh(n):
     Ed = torch.empty(n, dtype=torch.float64, device="cuda")
     Ud = torch.empty((n, n), dtype=torch.float64, device="cuda")
     scale = max(1.0, float(np.abs(E0).max()))
-    for _ in range(2):
+    for call in range(2):
         Ed.fill_(float("nan"))
         Ud.fill_(float("nan"))
         torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
         rc = lib.pgx_eigh_noalloc(_ptr(Hd), n, _ptr(Ed), _ptr(Ud), None)
+        torch.cuda.synchronize()
+        free1 = torch.cuda.mem_get_info()[0]
         assert rc == pgx.PGX_OK
+        if call == 1:
+            # the first call may load the library's kernels; from then on the
+            # entry point leaves the device's free memory exactly as it was
+            assert free1 == free0
         E1, U1 = Ed.cpu().numpy(), Ud.cpu().numpy()
         assert np.abs(E1 - E0).max() <= 1e-12 * scale
         # same eigenvectors up to sign: |U1^T U0| is the identity
