@@ -320,7 +320,8 @@ def run_ours_ring8(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     from pomerol_b200 import pgx
     from pomerol_b200.pgx import PGX_G2_ANCHORED, PGX_G2_SPLIT_I8
-    from pomerol_b200.workloads import EngineRun, Problem, chain_cost, lpt_batches
+    from pomerol_b200.shard import ChainShards, allreduce_sum
+    from pomerol_b200.workloads import EngineRun, Problem, chain_cost
     cfg = SETTINGS["ring8"]
     NB = cfg["nbatch"]
     prob = Problem("ring8", device=local_rank)
@@ -339,20 +340,18 @@ def run_ours_ring8(args, rank, world, local_rank):
     anchors = [int((wb > cfg["anchor_tol"]).sum()) for wb in w]
     dropped_w = float(sum(wb[wb <= cfg["anchor_tol"]].sum() for wb in w))
     costs = [chain_cost([prob.dims[b] for b in p[1]], [anchors[b] for b in p[1]], prob.nfreq) for p in parts]
-    batches = lpt_batches(costs, NB)
-    bparts = [[parts[k] for k in b] for b in batches]
+    shards = ChainShards(costs, NB, rank, world)
+    bparts = [[parts[k] for k in b] for b in shards.batches]
     nq_b = [eng.g2_count(bp, COEF_TOL, NZ_TOL) for bp in bparts]
     nquad = int(sum(nq_b))
     l2buf = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")  # 256 MB > 126 MB L2
     acc = np.zeros(nfreq, dtype=complex)
-    seen = set()
     batch_ms = {}
 
     def step(i):
-        b = (i * world + rank) % NB
+        b = shards.batch_of(i)
         v = run.g2(bparts[b], z)
-        if b not in seen:
-            seen.add(b)
+        if shards.first_visit(b):
             acc[:] += v
         return b
 
@@ -391,19 +390,17 @@ def run_ours_ring8(args, rank, world, local_rank):
         t_max, units = float(t[0].item()), float(tt[1].item())
     value = units / (t_max / 1e3)
     # batches no timed step covered: one untimed pass so the G2 is complete
-    for b in range(rank, NB, world):
-        if b not in batch_ms:
+    for b in shards.own_batches():
+        if b not in batch_ms:  # not reached by a timed step (maybe by a warm-up step)
             eng.timer_begin()
             v = run.g2(bparts[b], z)
             batch_ms[b] = eng.timer_end()
-            if b not in seen:
-                seen.add(b)
+            if shards.first_visit(b):
                 acc[:] += v
-    g2_ms = float(sum(batch_ms.values()))
+    # full-G2 time of this rank: one evaluation of each batch it owns
+    g2_ms = float(sum(batch_ms[b] for b in shards.own_batches()))
     if world > 1:
-        t = torch.tensor(acc.view(np.float64), device="cuda")
-        torch.distributed.all_reduce(t)  # the partial G2 of every rank's chains, summed
-        acc = t.cpu().numpy().view(complex)
+        acc = allreduce_sum(acc)  # the partial G2 of every rank's chains, summed (NCCL)
         t = torch.tensor([g2_ms], device="cuda", dtype=torch.float64)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         g2_ms = float(t.item())

@@ -245,6 +245,18 @@ int pgx_set_g2_workspace(pgx_ctx* ctx, int64_t batch_bytes, int64_t chain_bytes)
  * 0 sends every stacked and anchored product to the tensor cores). */
 int pgx_set_g2_split_threshold(pgx_ctx* ctx, double min_macs);
 
+/* With PGX_G2_SPLIT_I8: digits (7-bit slices) per operand element, 1..8
+ * (default 6).  The products keep the slice pairs a + b < slices; the error
+ * left is below about slices * 2^(-7 slices) * K of |A|max |B|max per element
+ * (no counterpart in the reference, which computes in FP64 only). */
+int pgx_set_g2_split_slices(pgx_ctx* ctx, int32_t slices);
+
+/* Tile shape of the int8 split products (no counterpart in the reference):
+ * 1 (default) runs 256 x 256 tiles on pairs of CTAs (tcgen05 cta_group::2,
+ * each SM loading half of the tile's operands), 0 runs 128 x 256 tiles on
+ * single CTAs.  Results are identical. */
+int pgx_set_split_cta_pair(pgx_ctx* ctx, int32_t cta_pair);
+
 /* Self-check of the int8 split product (no counterpart in the reference):
  * C = A B for nb items of seeded random complex A (M x K) and B (K x N) with
  * entries spread over four binary orders of magnitude, once through the split

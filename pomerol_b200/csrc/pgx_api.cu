@@ -309,6 +309,14 @@ int pgx_set_blocks(pgx_ctx* c, int32_t nblocks, const int32_t* dims, int32_t is_
         ++c->ops_gen;
         reset_problem(c->P);
         pgx::Problem& P = c->P;
+        // a failed allocation below leaves no half-declared problem behind
+        struct Undo {
+            pgx::Problem& P;
+            bool armed = true;
+            ~Undo() {
+                if (armed) reset_problem(P);
+            }
+        } undo{P};
         P.nblocks = nblocks;
         P.is_complex = is_complex != 0;
         P.dims.assign(dims, dims + nblocks);
@@ -355,6 +363,7 @@ int pgx_set_blocks(pgx_ctx* c, int32_t nblocks, const int32_t* dims, int32_t is_
         PGX_CUDA(cudaMemcpy(P.d_eoff, P.eoff.data(), nblocks * sizeof(long), cudaMemcpyHostToDevice));
         PGX_CUDA(cudaMemcpy(P.d_order, order.data(), nblocks * sizeof(int), cudaMemcpyHostToDevice));
         PGX_CUDA(cudaMemset(P.d_status, 0, 64));
+        undo.armed = false;
     });
 }
 
@@ -364,6 +373,9 @@ int pgx_set_hamiltonian(pgx_ctx* c, const double* H) {
         PGX_CHECK(P.nblocks > 0, PGX_ERR_STATE, "pgx_set_blocks first");
         PGX_CHECK(H, PGX_ERR_ARG, "null Hamiltonian");
         const size_t sc = P.is_complex ? 2 : 1;
+        // a NaN or infinity would only surface after the eigensolve: refuse it here
+        for (size_t i = 0; i < P.msize * sc; ++i)
+            PGX_CHECK(std::isfinite(H[i]), PGX_ERR_NUMERIC, "non-finite Hamiltonian entry " + std::to_string(i));
         PGX_CUDA(cudaMemcpyAsync(P.d_H, H, P.msize * sc * sizeof(double), cudaMemcpyHostToDevice, c->stream));
         PGX_CUDA(cudaStreamSynchronize(c->stream));
         P.have_H = true;
@@ -468,6 +480,20 @@ int pgx_set_g2_split_threshold(pgx_ctx* c, double min_macs) {
     return guarded(c, [&] {
         PGX_CHECK(min_macs >= 0.0, PGX_ERR_ARG, "threshold must be >= 0");
         c->g2_split_min_macs = min_macs;
+    });
+}
+
+int pgx_set_split_cta_pair(pgx_ctx* c, int32_t cta_pair) {
+    return guarded(c, [&] {
+        PGX_CHECK(cta_pair == 0 || cta_pair == 1, PGX_ERR_ARG, "cta_pair must be 0 or 1");
+        c->oz.cta_pair = cta_pair;
+    });
+}
+
+int pgx_set_g2_split_slices(pgx_ctx* c, int32_t slices) {
+    return guarded(c, [&] {
+        PGX_CHECK(slices >= 1 && slices <= 8, PGX_ERR_ARG, "split slices must be 1..8");
+        c->g2_split_slices = slices;
     });
 }
 

@@ -499,7 +499,7 @@ void run_g2(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq, const d
         ScopedEvents ev(2);
         const cudaEvent_t a0 = ev[0], a1 = ev[1];
         PGX_CUDA(cudaEventRecord(a0, st));
-        const int split = (flags & PGX_G2_SPLIT_I8) ? 6 : 0;
+        const int split = (flags & PGX_G2_SPLIT_I8) ? c->g2_split_slices : 0;
         if (split && c->oz.err.p) PGX_CUDA(cudaMemsetAsync(c->oz.err.p, 0, sizeof(int), st));
         run_g2_anchored(c, nparts, parts, nfreq, z, pole_res, coef_tol, split, out);
         if (split && c->oz.err.p) {

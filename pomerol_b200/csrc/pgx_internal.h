@@ -96,6 +96,7 @@ struct DevBuf {
 // Workspace of the int8 split products (digits, exponents, error flag).
 struct OzWork {
     DevBuf A, B, ea, fb, err;
+    int cta_pair = 1;  // 1: 256 x 256 tiles on CTA pairs (cta_group::2); 0: 128 x 256 tiles on single CTAs
 };
 
 // Times of the products measured since pgx_autotune_begin, per (operand-type
@@ -308,6 +309,7 @@ struct pgx_ctx {
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
     long long g2_batch_bytes = 0, g2_chain_bytes = 0;  // pgx_set_g2_workspace (0: defaults)
     double g2_split_min_macs = 1e9;                     // pgx_set_g2_split_threshold
+    int g2_split_slices = 6;                            // pgx_set_g2_split_slices
     pgx::OzWork oz;                                     // int8 split products
     cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};
     // scratch for G2 and Lehmann kernels

@@ -344,6 +344,261 @@ __global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_consta
     if (!ok && tid == 0) atomicExch(p.err, 1);
 }
 
+// ---- the same product on CTA pairs (tcgen05 cta_group::2): one 256 x 256
+// tile of C' per pair of CTAs in a cluster of two.  CTA r of the pair loads
+// rows 128 r .. 128 r + 127 of the tile's A' rows and of its B' rows (real
+// columns of C') into its own shared memory; the even CTA issues
+// tcgen05.mma.cta_group::2 with M = 256, N = 256, which reads both CTAs'
+// operands and writes rows 128 r .. of the accumulator into CTA r's tensor
+// memory.  Per SM, a k-block moves 32 KiB of operands for 128 x 256 x 128
+// multiply-adds instead of 48 KiB: the operand traffic from L2, which bounds
+// the single-CTA kernel, drops by a third.  Loads are plain (no multicast).
+// Barriers: both CTAs' loads complete on the even CTA's "full" barrier (its
+// producer posts the expected bytes of both); the even CTA's MMA thread
+// commits each stage to the "empty" barrier and each finished diagonal to the
+// "finished" barrier of both CTAs (one commit per CTA); the drain warps of
+// both CTAs arrive on the even CTA's "drained" barrier (16 arrivals).  Every
+// wait is bounded as in oz_gemm_tma_kernel; both CTAs always reach the final
+// cluster barrier, so neither leaves while its partner may touch its memory.
+constexpr int OZ2_HALF = 128;                                  // rows of A' / B' per CTA
+constexpr int OZ2_STAGES = 6;
+constexpr int OZ2_STAGE_BYTES = 2 * OZ2_HALF * OZ_BK;          // 32 KiB per CTA
+constexpr int OZ2_SMEM = OZ2_STAGES * OZ2_STAGE_BYTES + 1024 + 256;
+constexpr uint32_t OZ2_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
+                               ((uint32_t)(256 >> 4) << 24);
+
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t local, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;\n" : "=r"(r) : "r"(local), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void tma_load3_pair(uint32_t dst, const CUtensorMap* map, int x, int y, int z,
+                                               uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, "
+        "%4}], [%5];\n" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void commit_pair(uint32_t bar_cluster) {
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar_cluster)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.aligned;\n" ::: "memory");
+    asm volatile("barrier.cluster.wait.aligned;\n" ::: "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(384, 1)
+    oz_gemm_pair_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, OzArgs2 p) {
+    extern __shared__ char oz_raw[];
+    char* smem = reinterpret_cast<char*>((reinterpret_cast<uintptr_t>(oz_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + OZ2_STAGES * OZ2_STAGE_BYTES);
+    uint64_t* empty = full + OZ2_STAGES;
+    uint64_t* accf = empty + OZ2_STAGES;  // [2]
+    uint64_t* acce = accf + 2;            // [2]
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(acce + 2);
+    volatile int* s_fail = reinterpret_cast<volatile int*>(s_tmem + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint32_t rank;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;\n" : "=r"(rank));
+    const bool lead = rank == 0;
+    const int item = blockIdx.z;
+    // tiles of 256 x 256 in groups of OZ_GROUP_M row tiles, one per CTA pair
+    const int pair = blockIdx.x >> 1, per_group = OZ_GROUP_M * p.tiles_n;
+    const int first_m = (pair / per_group) * OZ_GROUP_M, gsz = min(p.tiles_m - first_m, OZ_GROUP_M);
+    const int tm = first_m + (pair % per_group) % gsz, tn = (pair % per_group) / gsz;
+    const int i0 = tm * 2 * OZ2_HALF + OZ2_HALF * (int)rank;  // this CTA's rows of A' and of the accumulator
+    const int jb = tn * 2 * OZ2_HALF + OZ2_HALF * (int)rank;  // this CTA's rows of B'
+    const int j0 = tn * 2 * OZ2_HALF;                         // the pair's first real column of C'
+
+    if (tid == 0) {
+        for (int q = 0; q < OZ2_STAGES; ++q) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&full[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&empty[q])) : "memory");
+        }
+        for (int q = 0; q < 2; ++q) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(smem_u32(&accf[q])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 16;\n" ::"r"(smem_u32(&acce[q])) : "memory");
+        }
+        *s_fail = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(smem_u32(s_tmem)),
+                     "r"(OZ_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;\n" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    cluster_sync_all();  // both CTAs' barriers exist before either signals the other's
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    const uint32_t tmem = *s_tmem;
+    const int kbd = p.K2 / OZ_BK;
+    int total = 0;
+    for (int s = 0; s < p.S; ++s) total += (s + 1) * kbd;
+
+    auto wait1 = [&](uint32_t bar, uint32_t parity) {
+        const unsigned long long t0 = gtimer();
+        while (true) {
+            uint32_t ok;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}"
+                : "=r"(ok)
+                : "r"(bar), "r"(parity)
+                : "memory");
+            if (ok) return true;
+            if (*s_fail || gtimer() - t0 > OZ_WAIT_NS) {
+                *s_fail = 1;
+                return false;
+            }
+        }
+    };
+
+    int issued = 0;
+    if (warp == 8 && lane == 0) {  // producer (both CTAs): loads complete on the even CTA's full barrier
+        int s = 0, kb = 0;
+        for (int it = 0; it < total; ++it) {
+            const int st = it % OZ2_STAGES, use = it / OZ2_STAGES;
+            if (use >= 1 && !wait1(smem_u32(&empty[st]), (uint32_t)((use - 1) & 1))) break;
+            const uint32_t fb_local = smem_u32(&full[st]);
+            if (lead)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb_local),
+                             "r"(2 * OZ2_STAGE_BYTES)
+                             : "memory");
+            const uint32_t fb = cluster_addr(fb_local, 0);
+            const uint32_t dst = smem_u32(smem + st * OZ2_STAGE_BYTES);
+            tma_load3_pair(dst, &tmA, kb * OZ_BK, i0, p.a_items ? item : 0, fb);
+            tma_load3_pair(dst + OZ2_HALF * OZ_BK, &tmB, (p.S - 1 - s) * p.K2 + kb * OZ_BK, jb, p.b_items ? item : 0,
+                           fb);
+            issued = it + 1;
+            if (++kb == (s + 1) * kbd) {
+                kb = 0;
+                ++s;
+            }
+        }
+    } else if (warp == 9 && lane == 0 && lead) {  // MMA issuer (even CTA only)
+        int s = 0, kb = 0, last = -1;
+        for (int it = 0; it < total; ++it) {
+            const int st = it % OZ2_STAGES, use = it / OZ2_STAGES;
+            if (kb == 0 && s >= 2 && !wait1(smem_u32(&acce[s & 1]), (uint32_t)(((s >> 1) - 1) & 1))) break;
+            if (!wait1(smem_u32(&full[st]), (uint32_t)(use & 1))) break;
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t sa = smem_u32(smem + st * OZ2_STAGE_BYTES), sb = sa + OZ2_HALF * OZ_BK;
+            const uint32_t dt = tmem + (uint32_t)((s & 1) * OZ_BN);
+#pragma unroll
+            for (int k = 0; k < OZ_BK / 32; ++k) {
+                const uint64_t da = sw128_desc(sa + 32 * k), db = sw128_desc(sb + 32 * k);
+                const uint32_t accum = (kb == 0 && k == 0) ? 0u : 1u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::2.kind::i8 [%0], %1, %2, %3, p;\n\t}"
+                    ::"r"(dt), "l"(da), "l"(db), "r"(OZ2_IDESC), "r"(accum)
+                    : "memory");
+            }
+            const uint32_t eb = smem_u32(&empty[st]);
+            commit_pair(cluster_addr(eb, 0));
+            commit_pair(cluster_addr(eb, 1));
+            last = it;
+            if (++kb == (s + 1) * kbd) {
+                const uint32_t ab = smem_u32(&accf[s & 1]);
+                commit_pair(cluster_addr(ab, 0));
+                commit_pair(cluster_addr(ab, 1));
+                kb = 0;
+                ++s;
+            }
+        }
+        // the tensor cores have finished every issued MMA before TMEM is freed
+        if (last >= 0 && !wait1(smem_u32(&empty[last % OZ2_STAGES]), (uint32_t)((last / OZ2_STAGES) & 1))) {
+            *s_fail = 1;
+        }
+    }
+    // drain (both CTAs): warp w reads TMEM lanes 32 (w % 4) .. + 31 (its rows) and
+    // the 128 accumulator columns of half w / 4, and adds them, scaled, to C
+    const int lane_base = 32 * (warp & 3), col_base = 128 * ((warp >> 2) & 1);
+    if (warp < 8) {
+        const int i = i0 + lane_base + lane;
+        const bool row_ok = i < p.M;
+        const int ei = row_ok ? p.ea[item * p.ea_item + i] : 0;
+        cd* crow = p.C + item * p.c_item + (long)(row_ok ? i : 0) * p.sc_i;
+        const int* fbi = p.fb + item * p.fb_item;
+        for (int s = 0; s < p.S; ++s) {
+            if (!mbar_wait(smem_u32(&accf[s & 1]), (uint32_t)((s >> 1) & 1))) {
+                *s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const uint32_t base = tmem + ((uint32_t)lane_base << 16) + (uint32_t)((s & 1) * OZ_BN + col_base);
+#pragma unroll 1
+            for (int q = 0; q < 8; ++q) {
+                uint32_t v[16];
+                tmem_ld16(base + 16 * q, v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+                if (row_ok) {
+#pragma unroll
+                    for (int e = 0; e < 8; ++e) {
+                        const int jc = (j0 + col_base) / 2 + 8 * q + e;
+                        if (jc < p.N) {
+                            const double sc = ldexp(1.0, ei + fbi[jc] - 14 - 7 * s);
+                            const cd add{(double)(int)v[2 * e] * sc, (double)(int)v[2 * e + 1] * sc};
+                            cd& dst = crow[(long)jc * p.sc_j];
+                            dst = s == 0 ? add : cd{dst.x + add.x, dst.y + add.y};
+                        }
+                    }
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];\n" ::"r"(
+                                 cluster_addr(smem_u32(&acce[s & 1]), 0))
+                             : "memory");
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    // after a failure, the even CTA waits (bounded) for the loads it can see
+    // complete; a short pause covers loads of its partner that were issued
+    // for phases it never posted, so nothing lands in freed shared memory
+    if (warp == 8 && lane == 0 && *s_fail) {
+        if (lead) {
+            for (int it = max(0, issued - OZ2_STAGES); it < issued; ++it) {
+                const unsigned long long t0 = gtimer();
+                while (true) {
+                    uint32_t ok;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                        "selp.u32 %0, 1, 0, p;\n\t}"
+                        : "=r"(ok)
+                        : "r"(smem_u32(&full[it % OZ2_STAGES])), "r"((uint32_t)((it / OZ2_STAGES) & 1))
+                        : "memory");
+                    if (ok || gtimer() - t0 > OZ_WAIT_NS) break;
+                }
+            }
+        }
+        const unsigned long long t0 = gtimer();
+        while (gtimer() - t0 < 2000000ull) {
+        }
+    }
+    __syncthreads();
+    cluster_sync_all();  // neither CTA leaves while its partner may still use its memory
+    const bool ok = !*s_fail;
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(OZ_TMEM_COLS)
+                     : "memory");
+    }
+    if (!ok && tid == 0) atomicExch(p.err, 1);
+}
+
 // Digits of an operand.  Output row r (a row of A', or a complex column of B
 // giving rows 2r and 2r+1 of B'), reduction index k < K:
 //   x(r, k) = X[r*s_r + k*s_k] (+ item*s_item), dressed when Er/Ek are set:
@@ -483,6 +738,7 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
     static bool attr = false;
     if (!attr) {
         PGX_CUDA(cudaFuncSetAttribute(oz_gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM));
+        PGX_CUDA(cudaFuncSetAttribute(oz_gemm_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ2_SMEM));
         attr = true;
     }
     using SA = typename src_t<TA>::type;
@@ -529,8 +785,9 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
             oz_prep_kernel<<<grid, 256, 0, st>>>(q, N, K, K2, S, 1, w.B.as<int8_t>(), b_bytes, w.fb.as<int>(), N);
             check_launch("oz_prep_kernel");
         }
-        const CUtensorMap tmA = digit_map(w.A.p, row_bytes, M, a_item ? cn : 1, OZ_BM);
-        const CUtensorMap tmB = digit_map(w.B.p, row_bytes, 2L * N, b_item ? cn : 1, OZ_BN);
+        const bool pair = w.cta_pair != 0;
+        const CUtensorMap tmA = digit_map(w.A.p, row_bytes, M, a_item ? cn : 1, pair ? OZ2_HALF : OZ_BM);
+        const CUtensorMap tmB = digit_map(w.B.p, row_bytes, 2L * N, b_item ? cn : 1, pair ? OZ2_HALF : OZ_BN);
         OzArgs2 a{};
         a.a_items = a_item;
         a.b_items = b_item;
@@ -547,12 +804,21 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
         a.sc_i = g.sc_i;
         a.sc_j = g.sc_j;
         a.err = w.err.as<int>();
-        a.tiles_m = (int)ceil_div((long)M, OZ_BM);
-        a.tiles_n = (int)ceil_div(2L * N, OZ_BN);
-        PGX_CHECK((long)a.tiles_m * a.tiles_n < (1L << 31), PGX_ERR_ARG, "split product: too many tiles");
-        dim3 grid((unsigned)((long)a.tiles_m * a.tiles_n), 1u, (unsigned)cn);
-        oz_gemm_tma_kernel<<<grid, 384, OZ_SMEM, st>>>(tmA, tmB, a);
-        check_launch("oz_gemm_tma_kernel");
+        if (pair) {  // 256 x 256 tiles, one per CTA pair
+            a.tiles_m = (int)ceil_div((long)M, 2L * OZ2_HALF);
+            a.tiles_n = (int)ceil_div(2L * N, 2L * OZ2_HALF);
+            PGX_CHECK((long)a.tiles_m * a.tiles_n < (1L << 30), PGX_ERR_ARG, "split product: too many tiles");
+            dim3 grid((unsigned)(2L * a.tiles_m * a.tiles_n), 1u, (unsigned)cn);
+            oz_gemm_pair_kernel<<<grid, 384, OZ2_SMEM, st>>>(tmA, tmB, a);
+            check_launch("oz_gemm_pair_kernel");
+        } else {
+            a.tiles_m = (int)ceil_div((long)M, OZ_BM);
+            a.tiles_n = (int)ceil_div(2L * N, OZ_BN);
+            PGX_CHECK((long)a.tiles_m * a.tiles_n < (1L << 31), PGX_ERR_ARG, "split product: too many tiles");
+            dim3 grid((unsigned)((long)a.tiles_m * a.tiles_n), 1u, (unsigned)cn);
+            oz_gemm_tma_kernel<<<grid, 384, OZ_SMEM, st>>>(tmA, tmB, a);
+            check_launch("oz_gemm_tma_kernel");
+        }
     }
 }
 

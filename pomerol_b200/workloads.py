@@ -315,7 +315,7 @@ class EngineRun:
     """The G2 stage chain on one libpgx context with the Hamiltonian resident
     in HBM: eigensolve, weights, rotation of c^+ and c, G2 on the triples."""
 
-    def __init__(self, prob: Problem, device=0, anchored=True, anchor_tol=1e-16, split=False):
+    def __init__(self, prob: Problem, device=0, anchored=True, anchor_tol=1e-16, split=False, slices=6):
         from .pgx import PGX_G2_ANCHORED, PGX_G2_EXACT, PGX_G2_SPLIT_I8, Engine
         self.flags = PGX_G2_ANCHORED if anchored else PGX_G2_EXACT
         if split and anchored:
@@ -326,6 +326,7 @@ class EngineRun:
         self.eng = Engine(device)
         self.eng.set_blocks(prob.dims)
         self.eng.set_hamiltonian(blocks)
+        self.eng.set_g2_split_slices(slices)
         self.h2d_bytes = sum(b.nbytes for b in blocks)
         self.cdag = {i: self.eng.op_define([(r, l, np.asarray(t), np.asarray(c)) for r, l, t, c in a])
                      for i, a in self.actions.items()}
@@ -372,16 +373,3 @@ def chain_cost(dims, anchors, nfreq):
     cost = sum(m / 5.0 if m >= 1e9 else m for m in prods)
     cost += float(nfreq) ** 3 * (r2 * (d3 + d4) + r3 * (d2 + d1) + r1 * (d4 + d3) + r4 * (d1 + d2)) / 2.0
     return cost
-
-
-def lpt_batches(costs, nbatch):
-    """Chains split into nbatch lists of about equal cost: largest first, each
-    to the list with the least cost so far.  Lists keep the chains' order."""
-    order = sorted(range(len(costs)), key=lambda k: -costs[k])
-    load = [0.0] * nbatch
-    out = [[] for _ in range(nbatch)]
-    for k in order:
-        b = min(range(nbatch), key=lambda i: load[i])
-        out[b].append(k)
-        load[b] += costs[k]
-    return [sorted(b) for b in out]
