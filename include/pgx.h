@@ -252,8 +252,8 @@ int pgx_set_g2_split_threshold(pgx_ctx* ctx, double min_macs);
 int pgx_set_g2_split_slices(pgx_ctx* ctx, int32_t slices);
 
 /* Tile shape of the int8 split products (no counterpart in the reference):
- * 1 runs 256 x 256 tiles on pairs of CTAs (tcgen05 cta_group::2,
- * each SM loading half of the tile's operands), 0 (default) runs 128 x 256 tiles on
+ * 1 (default) runs 256 x 256 tiles on pairs of CTAs (tcgen05 cta_group::2,
+ * each SM loading half of the tile's operands), 0 runs 128 x 256 tiles on
  * single CTAs.  Results are identical. */
 int pgx_set_split_cta_pair(pgx_ctx* ctx, int32_t cta_pair);
 

@@ -107,10 +107,13 @@ __global__ void __launch_bounds__((BM / cg_tm(BM)) * CG_NX)
     __shared__ cd Bs[2][CG_BK][BN + 1];
     __shared__ cd s_s[BN];
     __shared__ long s_oa[BM], s_ob[BM];
+    __shared__ DTerm s_term;  // the sub-term's descriptor, read once per CTA
     const CItem it = items[blockIdx.x];
     const CClass cc = classes[it.cls];
-    const DTerm& d = terms[cc.term];
+    const DTerm& d = s_term;
     const int tid = threadIdx.x, tx = tid % CG_NX, ty = tid / CG_NX;
+    if (tid == 0) s_term = terms[cc.term];
+    __syncthreads();
     const int nrows = min(BM, cc.nrows - it.row0);
     for (int j = tid; j < BN; j += NT) s_s[j] = j < cc.ncols ? cc.s[j] : cd{0.0, 0.0};
     for (int r = tid; r < BM; r += NT) {

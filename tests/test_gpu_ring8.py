@@ -48,7 +48,7 @@ def test_ring8_g_and_chi_zz(ring8):
     assert np.abs(G - ref).max() < 1e-10 * np.abs(ref).max()
     zb = L.bosonic(np.array(doc["chi_zz_m"]), 5.0)
     n = {i: g.quadratic(i, i) for i in (u, d)}
-    chi = {(x, y): g.susc(n[x], n[y], zb, pole_res=1e-8, coef_tol=0.0) for x in (u, d) for y in (u, d)}
+    chi = {(x, y): g.susc(n[x], n[y], zb, pole_res=1e-8, coef_tol=0.0)[0] for x in (u, d) for y in (u, d)}
     zz = 0.25 * (chi[(u, u)] - chi[(u, d)] - chi[(d, u)] + chi[(d, d)])
     ref = _c(doc["chi_zz"])
     assert np.abs(zz - ref).max() < 1e-10 * np.abs(ref).max()
