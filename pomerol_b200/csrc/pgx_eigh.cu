@@ -765,6 +765,10 @@ __global__ void __launch_bounds__(TRI_THREADS) vector_kernel(TriArgs g) {
 
 // Modified Gram-Schmidt, applied twice, of each chain member against the
 // earlier members closer than CHAIN_TOL ||T||; one thread per chain head.
+// The CTA's warp orthogonalises each chain whose head lies in its range:
+// modified Gram-Schmidt (two passes) of every member against its close
+// predecessors, the dot products and updates spread over the lanes (a chain
+// of a symmetry multiplet can hold dozens of vectors of thousands of states).
 __global__ void __launch_bounds__(TRI_THREADS) ortho_kernel(TriArgs g) {
     extern __shared__ double sh[];
     const TriItem it = g.items[blockIdx.x];
@@ -776,12 +780,13 @@ __global__ void __launch_bounds__(TRI_THREADS) ortho_kernel(TriArgs g) {
     const double tn = load_tri(g.tri, eo, n, d, e);
     for (int i = threadIdx.x; i < n; i += blockDim.x) lam[i] = g.lam[eo + i];
     __syncthreads();
+    const int lane = threadIdx.x;
     const double ortol = CHAIN_TOL * tn;
     const int* sa = g.sb + 2 * eo;
     const int* sbe = sa + n;
     const int* rank = g.rank + eo;
     double* Zb = g.Z + mo;
-    for (int j = it.j0 + threadIdx.x; j < it.j1; j += blockDim.x) {
+    for (int j = it.j0; j < it.j1; ++j) {
         const int a = sa[j], b = sbe[j];
         if (j > a && lam[j] - lam[j - 1] <= ortol) continue;  // not the head of a chain
         bool ok = true;
@@ -791,13 +796,23 @@ __global__ void __launch_bounds__(TRI_THREADS) ortho_kernel(TriArgs g) {
                 for (int pp = jj - 1; pp >= j && lam[jj] - lam[pp] <= ortol; --pp) {
                     const double* qv = Zb + (long)rank[pp] * n;
                     double dot = 0.0;
-                    for (int i = a; i <= b; ++i) dot = fma(qv[i], z[i], dot);
-                    for (int i = a; i <= b; ++i) z[i] = fma(-dot, qv[i], z[i]);
+                    for (int i = a + lane; i <= b; i += TRI_THREADS) dot = fma(qv[i], z[i], dot);
+                    dot = warp_sum(dot);
+                    for (int i = a + lane; i <= b; i += TRI_THREADS) z[i] = fma(-dot, qv[i], z[i]);
                 }
-                ok = normalize(z, a, b, 1);
+                double nn = 0.0;
+                for (int i = a + lane; i <= b; i += TRI_THREADS) nn = fma(z[i], z[i], nn);
+                nn = warp_sum(nn);
+                if (!(nn > 0.0) || !isfinite(nn)) {
+                    ok = false;
+                } else {
+                    const double inv = rsqrt(nn);
+                    for (int i = a + lane; i <= b; i += TRI_THREADS) z[i] *= inv;
+                }
             }
+            __syncwarp();
         }
-        if (!ok) atomicExch(g.status, PGX_ERR_NUMERIC);
+        if (!ok && lane == 0) atomicExch(g.status, PGX_ERR_NUMERIC);
     }
 }
 

@@ -99,6 +99,11 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
 constexpr uint32_t OZ_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(OZ_BN >> 3) << 17) |
                               ((uint32_t)(OZ_BM >> 4) << 24);
 
+// 2^e exactly: the bit pattern of a normal double, ldexp outside that range.
+__device__ __forceinline__ double pow2i(int e) {
+    return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -301,7 +306,7 @@ __global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_consta
                     for (int e = 0; e < 8; ++e) {
                         const int jc = (j0 + col_base) / 2 + 8 * q + e;
                         if (jc < p.N) {
-                            const double sc = ldexp(1.0, ei + fbi[jc] - 14 - 7 * s);
+                            const double sc = pow2i(ei + fbi[jc] - 14 - 7 * s);
                             const cd add{(double)(int)v[2 * e] * sc, (double)(int)v[2 * e + 1] * sc};
                             cd& dst = crow[(long)jc * p.sc_j];
                             dst = s == 0 ? add : cd{dst.x + add.x, dst.y + add.y};
@@ -546,7 +551,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(384, 1)
                     for (int e = 0; e < 8; ++e) {
                         const int jc = (j0 + col_base) / 2 + 8 * q + e;
                         if (jc < p.N) {
-                            const double sc = ldexp(1.0, ei + fbi[jc] - 14 - 7 * s);
+                            const double sc = pow2i(ei + fbi[jc] - 14 - 7 * s);
                             const cd add{(double)(int)v[2 * e] * sc, (double)(int)v[2 * e + 1] * sc};
                             cd& dst = crow[(long)jc * p.sc_j];
                             dst = s == 0 ? add : cd{dst.x + add.x, dst.y + add.y};
