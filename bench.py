@@ -156,41 +156,37 @@ def measured_peaks():
 
 # ------------------------------------------------------------------ CPU side
 def sample_spec(config, dims_of_parts):
-    """The bounded sample both CPU legs time: (part index, row step, col
-    step).  a5: the chain with the most quadruples, every 60th index1, every
-    index3.  ring8: the chain with the most (index1, index3) pairs among
-    those with d2*d4 <= 40000 quadruples per pair, index1 rows 0 and d1/2,
-    index3 row 0 (two pairs, every index2 and index4 chased)."""
+    """The bounded sample both CPU legs time: (part index, index1 step,
+    index3 step, index2/index4 step).  a5: the chain with the most
+    quadruples, every 60th index1, every index3, index2 and index4.  ring8:
+    the chain with the most quadruples (its blocks hold the thermally
+    dominant states), index1 rows 0 and d1/2 (the lowest state of the block
+    and one from its middle), index3 row 0, every 8th index2 and index4."""
+    k = int(np.argmax([np.prod(d, dtype=float) for d in dims_of_parts]))
     if config == "a5":
-        k = int(np.argmax([np.prod(d) for d in dims_of_parts]))
-        return k, 60, 1
-    best = None
-    for k, d in enumerate(dims_of_parts):
-        if d[1] * d[3] <= 40000 and (best is None or d[0] * d[2] > best[1]):
-            best = (k, d[0] * d[2])
-    k = best[0]
+        return k, 60, 1, 1
     d = dims_of_parts[k]
-    return k, max(1, d[0] // 2), d[2]
+    return k, max(1, d[0] // 2), d[2], 8
 
 
 def cpu_run(ed_like, parts, z, spec, threads):
     """One timed run of the reference algorithm on the sample."""
     from oracle import g2c
-    k, rs, cs = spec
+    k, rs, cs, ks = spec
     d1 = len(ed_like.E[parts[k]["b"][0]])
     t0 = time.perf_counter()
     _, nq, terms = g2c.evaluate(ed_like, parts, z, pole_res=POLE_RES, coef_tol=COEF_TOL, rule=True, nz_tol=NZ_TOL,
-                                rows=(k, 0, d1, rs, cs), nthreads=threads)
+                                rows=(k, 0, d1, rs, cs, ks), nthreads=threads)
     dt = time.perf_counter() - t0
     return nq * len(z) / dt, dt, nq, int(terms.sum())
 
 
 def describe_sample(config, parts, ed_like, spec, nq, terms, nz, dt, threads):
-    k, rs, cs = spec
+    k, rs, cs, ks = spec
     dims = [len(ed_like.E[b]) for b in parts[k]["b"]]
     return (f"reference algorithm restated (oracle/g2_oracle.cpp, rule=1): block chain {k} of {len(parts)} "
-            f"(blocks {dims}), index1 every {rs}-th, index3 every {min(cs, dims[2])}-th, {nq} quadruples, "
-            f"{terms} merged terms, {nz} triples, {dt:.2f} s on {threads} threads")
+            f"(blocks {dims}), index1 every {rs}-th, index3 every {min(cs, dims[2])}-th, index2 and index4 every "
+            f"{ks}-th, {nq} quadruples, {terms} merged terms, {nz} triples, {dt:.2f} s on {threads} threads")
 
 
 def oracle_problem(config):

@@ -122,16 +122,17 @@ long long g2o_count(int d1, int d2, int d3, int d4, const double* O1, const doub
 
 // Reference-rule (rule=1) or exact (rule=0) evaluation of one part.
 // z: nfreq triples (re,im)x3 BEFORE the part's permutation; out += values.
-// row_begin/row_end/row_step restrict index1 and col_step strides index3
-// (bounded samples: every quadruple of the sampled (index1, index3) pairs is
-// enumerated and evaluated as the reference does); returns the number of
+// row_begin/row_end/row_step restrict index1, col_step strides index3 and
+// chase_step strides index2 and index4 (bounded samples: every sampled
+// quadruple is filtered, split into sub-terms, merged and evaluated as the
+// reference does); returns the number of
 // quadruples enumerated; terms_out[0..1] = non-resonant / resonant terms kept.
 long long g2o_part(int d1, int d2, int d3, int d4, const double* O1, const double* O2, const double* O3,
                    const double* X4, const double* E1, const double* E2, const double* E3, const double* E4,
                    const double* w1, const double* w2, const double* w3, const double* w4, const int* perm, int sign,
                    double beta, double pole_res, double coef_tol, double nz_tol, int rule, int nfreq, const double* z,
-                   int row_begin, int row_end, int row_step, int col_step, double* out, long long* terms_out,
-                   int nthreads) {
+                   int row_begin, int row_end, int row_step, int col_step, int chase_step, double* out,
+                   long long* terms_out, int nthreads) {
     TermList NR{pole_res, coef_tol, {}}, RS{pole_res, coef_tol, {}};
     std::vector<Term> nr_plain, rs_plain;  // exact mode keeps every term
     std::vector<int> flags_nr, flags_rs;
@@ -141,11 +142,11 @@ long long g2o_part(int d1, int d2, int d3, int d4, const double* O1, const doubl
     for (int i1 = row_begin; i1 < row_end; i1 += std::max(row_step, 1)) {
         for (int i3 = 0; i3 < d3; i3 += std::max(col_step, 1)) {
             l4.clear();
-            for (int i4 = 0; i4 < d4; ++i4)
+            for (int i4 = 0; i4 < d4; i4 += std::max(chase_step, 1))
                 if (std::fabs(O3[(long)i3 * d4 + i4]) > nz_tol && std::fabs(X4[(long)i4 * d1 + i1]) > nz_tol)
                     l4.push_back(i4);
             if (l4.empty()) continue;
-            for (int i2 = 0; i2 < d2; ++i2) {
+            for (int i2 = 0; i2 < d2; i2 += std::max(chase_step, 1)) {
                 const double a12 = O1[(long)i1 * d2 + i2], a23 = O2[(long)i2 * d3 + i3];
                 if (!(std::fabs(a12) > nz_tol && std::fabs(a23) > nz_tol)) continue;
                 for (int i4 : l4) {

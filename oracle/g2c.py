@@ -21,7 +21,7 @@ def lib():
         L.g2o_count.restype = C.c_longlong
         L.g2o_count.argtypes = [I, I, I, I] + [P] * 8 + [D, D]
         L.g2o_part.restype = C.c_longlong
-        L.g2o_part.argtypes = [I, I, I, I] + [P] * 12 + [P, I, D, D, D, D, I, I, P, I, I, I, I, P, P, I]
+        L.g2o_part.argtypes = [I, I, I, I] + [P] * 12 + [P, I, D, D, D, D, I, I, P, I, I, I, I, I, P, P, I]
         _LIB = L
     return _LIB
 
@@ -49,8 +49,9 @@ def count(ed, parts, coef_tol=1e-16, nz_tol=NZ_TOL):
 
 def evaluate(ed, parts, freqs, pole_res=1e-8, coef_tol=1e-16, rule=True, nz_tol=NZ_TOL, rows=None, nthreads=0):
     """Sum over parts at triples `freqs` ((n,3) complex).  rows=(part_index,
-    begin, end[, row_step[, col_step]]) restricts to one part, a strided range
-    of index1 and every col_step-th index3 (bounded sample).
+    begin, end[, row_step[, col_step[, chase_step]]]) restricts to one part, a
+    strided range of index1, every col_step-th index3 and every chase_step-th
+    index2 and index4 (bounded sample).
     Returns (values, quadruples enumerated, [nr_terms, res_terms])."""
     z = np.ascontiguousarray(np.asarray(freqs, dtype=complex).reshape(-1, 3)).view(np.float64)
     out = np.zeros(2 * (len(z) // 6) if z.ndim == 1 else 2 * z.shape[0])
@@ -63,11 +64,12 @@ def evaluate(ed, parts, freqs, pole_res=1e-8, coef_tol=1e-16, rule=True, nz_tol=
         dims, mats, E, w = _part_arrays(ed, p)
         r0, r1, rs = (0, dims[0], 1) if rows is None else (rows[1], rows[2], rows[3] if len(rows) > 3 else 1)
         cs = 1 if rows is None or len(rows) < 5 else rows[4]
+        ks = 1 if rows is None or len(rows) < 6 else rows[5]
         perm = np.ascontiguousarray(p["perm"], dtype=np.int32)
         t = np.zeros(2, dtype=np.int64)
         nq += lib().g2o_part(*dims, *[m.ctypes.data for m in mats], *[x.ctypes.data for x in E],
                              *[x.ctypes.data for x in w], perm.ctypes.data, int(p["sign"]), ed.beta, pole_res,
-                             coef_tol, nz_tol, int(rule), out.size // 2, z.ctypes.data, r0, r1, rs, cs,
+                             coef_tol, nz_tol, int(rule), out.size // 2, z.ctypes.data, r0, r1, rs, cs, ks,
                              out.ctypes.data, t.ctypes.data, int(nthreads))
         terms += t
     return out.view(complex), nq, terms
