@@ -147,54 +147,122 @@ __global__ void __launch_bounds__(CT_THREADS) contract_kernel(ContractArgs g) {
     }
 }
 
+// Zero entries (|x| <= nz) of the four operator parts of a chain, as sorted
+// index lists: rows of O1 (over i2), columns of O2 (over i2), rows of O3 (over
+// i4), columns of CX4 (over i4).  off[i] .. off[i+1] delimits list i.
+struct ZeroLists {
+    const int *r1off, *r1idx;  // O1 row i1 -> zero i2
+    const int *c2off, *c2idx;  // O2 column i3 -> zero i2
+    const int *r3off, *r3idx;  // O3 row i3 -> zero i4
+    const int *c4off, *c4idx;  // CX4 column i1 -> zero i4
+};
+
+__device__ __forceinline__ bool in_sorted(const int* a, int n, int x) {
+    int lo = 0, hi = n;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (a[mid] < x) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo < n && a[lo] == x;
+}
+
+// Size of the union of two sorted index lists and its members with w <= tol.
+__device__ __forceinline__ void union_count(const int* a, int na, const int* b, int nb, const double* w, double tol,
+                                            long& n, long& ncold) {
+    int i = 0, j = 0;
+    n = 0;
+    ncold = 0;
+    while (i < na || j < nb) {
+        int x;
+        if (j >= nb || (i < na && a[i] < b[j])) x = a[i++];
+        else if (i >= na || b[j] < a[i]) x = b[j++];
+        else {
+            x = a[i++];
+            ++j;
+        }
+        ++n;
+        ncold += !(w[x] > tol);
+    }
+}
+
 // Number of state quadruples of one chain that the reference enumerates
 // (TwoParticleGFPart.cpp:210-250): all four rotated elements non-zero
 // (|x| > nz) and w1 + w2 + w3 + w4 > tol, summed in that order as the
-// reference does (:241).  One thread per (i1, i3).  When w1 + w3 > tol every
-// (i2, i4) of the pair counts (the rounded sum only grows when a non-negative
-// weight is added); otherwise a pair only fails when all four weights are
-// below tol, and the cold (i2, i4) pairs are enumerated only for i2 close
-// enough to the threshold to matter.
-template <typename T>
-__global__ void count_kernel(const T* O1, const T* O2, const T* O3, const T* X4, int d1, int d2, int d3, int d4,
-                             const double* w1, const double* w2, const double* w3, const double* w4, double tol,
-                             double nz, double cold_max4, unsigned long long* out) {
+// reference does (:241).  One thread per (i1, i3).  The zero elements are
+// few (rotated operators are dense), so the lists L2 = {i2 : O1[i1,i2] and
+// O2[i2,i3] non-zero} and L4 are handled through their complements Z2, Z4.
+// When w1 + w3 > tol every (i2, i4) of L2 x L4 counts (a rounded sum of
+// non-negative weights only grows as terms are added); otherwise only pairs
+// of cold states (w <= tol) can fail: of the cold pairs, those that pass are
+// found per cold i2 of the shell (sorted descending, c2 / c2i) by a binary
+// search over the sorted cold weights c4 of S4, minus the zero i4 among them.
+__global__ void count_kernel(ZeroLists z, int d1, int d2, int d3, int d4, const double* w1, const double* w2,
+                             const double* w3, const double* w4, const double* c2, const int* c2i, int n2c_all,
+                             const double* c4, int n4c_all, double tol, unsigned long long* out) {
     const long idx = blockIdx.x * (long)blockDim.x + threadIdx.x;
     unsigned long long cnt = 0;
     if (idx < (long)d1 * d3) {
         const int i1 = (int)(idx / d3), i3 = (int)(idx % d3);
+        const int* za = z.r1idx + z.r1off[i1];
+        const int nza = z.r1off[i1 + 1] - z.r1off[i1];
+        const int* zb = z.c2idx + z.c2off[i3];
+        const int nzb = z.c2off[i3 + 1] - z.c2off[i3];
+        const int* zc = z.r3idx + z.r3off[i3];
+        const int nzc = z.r3off[i3 + 1] - z.r3off[i3];
+        const int* zd = z.c4idx + z.c4off[i1];
+        const int nzd = z.c4off[i1 + 1] - z.c4off[i1];
+        long z2, z2c, z4, z4c;
+        union_count(za, nza, zb, nzb, w2, tol, z2, z2c);
+        union_count(zc, nzc, zd, nzd, w4, tol, z4, z4c);
+        const long n2 = d2 - z2, n4 = d4 - z4;
         const double x1 = w1[i1], x3 = w3[i3];
-        long n2 = 0, n4 = 0, n2c = 0, n4c = 0;
-        for (int i2 = 0; i2 < d2; ++i2) {
-            const bool v = sqrt(abs2(tocd(O1[(long)i1 * d2 + i2]))) > nz && sqrt(abs2(tocd(O2[(long)i2 * d3 + i3]))) > nz;
-            n2 += v;
-            n2c += v && !(w2[i2] > tol);
-        }
-        for (int i4 = 0; i4 < d4; ++i4) {
-            const bool v = sqrt(abs2(tocd(O3[(long)i3 * d4 + i4]))) > nz && sqrt(abs2(tocd(X4[(long)i4 * d1 + i1]))) > nz;
-            n4 += v;
-            n4c += v && !(w4[i4] > tol);
-        }
         if (x1 + x3 > tol) {
             cnt = (unsigned long long)(n2 * n4);
         } else {
-            cnt = (unsigned long long)(n2 * n4 - n2c * n4c);
-            for (int i2 = 0; i2 < d2; ++i2) {
-                if (w2[i2] > tol) continue;
-                const double s = (x1 + w2[i2]) + x3;
-                if (!(s + cold_max4 > tol)) continue;
-                if (!(sqrt(abs2(tocd(O1[(long)i1 * d2 + i2]))) > nz && sqrt(abs2(tocd(O2[(long)i2 * d3 + i3]))) > nz)) continue;
-                for (int i4 = 0; i4 < d4; ++i4) {
-                    if (w4[i4] > tol) continue;
-                    const bool v =
-                        sqrt(abs2(tocd(O3[(long)i3 * d4 + i4]))) > nz && sqrt(abs2(tocd(X4[(long)i4 * d1 + i1]))) > nz;
-                    cnt += v && (s + w4[i4] > tol);
+            const long n2c = n2c_all - z2c, n4c = n4c_all - z4c;
+            long pass = 0;
+            for (int q = 0; q < n2c_all; ++q) {
+                const double s = (x1 + c2[q]) + x3;
+                if (n4c_all == 0 || !(s + c4[0] > tol)) break;
+                const int i2 = c2i[q];
+                if (in_sorted(za, nza, i2) || in_sorted(zb, nzb, i2)) continue;
+                int lo = 1, hi = n4c_all;  // c4[0 .. lo) pass
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (s + c4[mid] > tol) lo = mid + 1;
+                    else hi = mid;
                 }
+                long drop = 0;  // zero i4 among the passing cold states
+                for (int t = 0; t < nzc; ++t) {
+                    const double v = w4[zc[t]];
+                    drop += !(v > tol) && (s + v > tol);
+                }
+                for (int t = 0; t < nzd; ++t) {
+                    const double v = w4[zd[t]];
+                    drop += !(v > tol) && (s + v > tol) && !in_sorted(zc, nzc, zd[t]);
+                }
+                pass += lo - drop;
             }
+            cnt = (unsigned long long)(n2 * n4 - n2c * n4c + pass);
         }
     }
     for (int o = 16; o > 0; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
     if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(out, cnt);
+}
+
+// (row, column) of every zero entry (|x| <= nz) of one operator part, in no
+// particular order; at most cap of them are written.
+template <typename T>
+__global__ void zero_list_kernel(const T* a, int rows, int cols, double nz, int2* out, unsigned long long* counter,
+                                 long cap) {
+    const long n = (long)rows * cols;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        if (!(sqrt(abs2(tocd(a[i]))) > nz)) {
+            const unsigned long long k = atomicAdd(counter, 1ull);
+            if ((long)k < cap) out[k] = make_int2((int)(i / cols), (int)(i % cols));
+        }
+    }
 }
 
 // Entries of one rotated operator part with |x| <= nz (absent from the
@@ -675,10 +743,86 @@ void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_
         std::sort(cold.begin() + cold_off[bl], cold.end(), [](double x, double y) { return x > y; });
     }
     cold_off[P.nblocks] = (long)cold.size();
+    // the block-local index of every cold weight, in the same order
+    std::vector<int> coldi(cold.size());
+    for (int bl = 0; bl < P.nblocks; ++bl) {
+        std::vector<int> ord;
+        for (int i = 0; i < P.dims[bl]; ++i)
+            if (!(w[P.eoff[bl] + i] > coef_tol)) ord.push_back(i);
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return w[P.eoff[bl] + x] > w[P.eoff[bl] + y]; });
+        std::copy(ord.begin(), ord.end(), coldi.begin() + cold_off[bl]);
+    }
     DevBuf& cb = c->scratch[11];
-    cb.reserve(std::max<size_t>(cold.size(), 1) * sizeof(double));
-    if (!cold.empty()) h2d(cb.p, cold.data(), cold.size() * sizeof(double), st);
+    const size_t cbytes = (std::max<size_t>(cold.size(), 1) * sizeof(double) + 255) & ~size_t(255);
+    cb.reserve(cbytes + std::max<size_t>(coldi.size(), 1) * sizeof(int));
+    if (!cold.empty()) {
+        h2d(cb.p, cold.data(), cold.size() * sizeof(double), st);
+        h2d(cb.as<char>() + cbytes, coldi.data(), coldi.size() * sizeof(int), st);
+    }
     const double* d_cold = cb.as<double>();
+    const int* d_coldi = reinterpret_cast<const int*>(cb.as<char>() + cbytes);
+    // zero lists of the operator parts of chains that have zero elements,
+    // built on first use: (row, column) pairs gathered on the device, sorted
+    // on the host into row and column lists
+    struct ZLists {
+        DevBuf buf;
+        const int *roff = nullptr, *ridx = nullptr, *coff = nullptr, *cidx = nullptr;
+    };
+    std::map<int, ZLists> zcache;
+    DevBuf pairs_b, ctr_b;
+    auto zl = [&](int opid, int left, int key) -> const ZLists& {
+        auto it = zcache.find(key);
+        if (it != zcache.end()) return it->second;
+        const Operator& o = P.ops[opid];
+        const OpPart& op = o.parts[o.by_left[left]];
+        const long nzero = (long)zeros[key];
+        ZLists& L = zcache[key];
+        std::vector<int2> pr(nzero);
+        if (nzero > 0) {
+            pairs_b.reserve(nzero * sizeof(int2));
+            ctr_b.reserve(sizeof(unsigned long long));
+            PGX_CUDA(cudaMemsetAsync(ctr_b.p, 0, sizeof(unsigned long long), st));
+            const long n = (long)op.dl * op.dr;
+            const int blocks = (int)std::max<long>(1, std::min<long>(ceil_div(n, 256), 148L * 8));
+            if (o.is_complex)
+                zero_list_kernel<cd><<<blocks, 256, 0, st>>>(o.mat.as<cd>() + op.off, op.dl, op.dr, nz_tol,
+                                                             pairs_b.as<int2>(), ctr_b.as<unsigned long long>(), nzero);
+            else
+                zero_list_kernel<double><<<blocks, 256, 0, st>>>(o.mat.as<double>() + op.off, op.dl, op.dr, nz_tol,
+                                                                 pairs_b.as<int2>(), ctr_b.as<unsigned long long>(),
+                                                                 nzero);
+            check_launch("zero_list_kernel");
+            PGX_CUDA(cudaMemcpyAsync(pr.data(), pairs_b.p, nzero * sizeof(int2), cudaMemcpyDeviceToHost, st));
+            PGX_CUDA(cudaStreamSynchronize(st));
+        }
+        std::vector<int> roff(op.dl + 1, 0), coff(op.dr + 1, 0), ridx(nzero), cidx(nzero);
+        std::sort(pr.begin(), pr.end(), [](int2 x, int2 y) { return x.x != y.x ? x.x < y.x : x.y < y.y; });
+        for (long k = 0; k < nzero; ++k) {
+            ++roff[pr[k].x + 1];
+            ridx[k] = pr[k].y;
+        }
+        std::sort(pr.begin(), pr.end(), [](int2 x, int2 y) { return x.y != y.y ? x.y < y.y : x.x < y.x; });
+        for (long k = 0; k < nzero; ++k) {
+            ++coff[pr[k].y + 1];
+            cidx[k] = pr[k].x;
+        }
+        for (int r = 0; r < op.dl; ++r) roff[r + 1] += roff[r];
+        for (int cc = 0; cc < op.dr; ++cc) coff[cc + 1] += coff[cc];
+        auto al = [](size_t x) { return (x * sizeof(int) + 255) & ~size_t(255); };
+        const size_t o1 = 0, o2 = o1 + al(roff.size()), o3 = o2 + al(std::max<long>(nzero, 1)),
+                     o4 = o3 + al(coff.size()), tot = o4 + al(std::max<long>(nzero, 1));
+        L.buf.reserve(tot);
+        char* base = L.buf.as<char>();
+        h2d(base + o1, roff.data(), roff.size() * sizeof(int), st);
+        if (nzero) h2d(base + o2, ridx.data(), nzero * sizeof(int), st);
+        h2d(base + o3, coff.data(), coff.size() * sizeof(int), st);
+        if (nzero) h2d(base + o4, cidx.data(), nzero * sizeof(int), st);
+        L.roff = reinterpret_cast<const int*>(base + o1);
+        L.ridx = reinterpret_cast<const int*>(base + o2);
+        L.coff = reinterpret_cast<const int*>(base + o3);
+        L.cidx = reinterpret_cast<const int*>(base + o4);
+        return L;
+    };
     unsigned long long dense_total = 0;  // closed-form chains: d1 d2 d3 d4 each
     for (int q = 0; q < nparts; ++q) {
         const pgx_g2_part& gp = parts[q];
@@ -701,25 +845,23 @@ void run_g2_count(pgx_ctx* c, int nparts, const pgx_g2_part* parts, double coef_
             }
             continue;
         }
-        double cold4 = 0.0;
-        for (int i = 0; i < d4; ++i) {
-            const double x = w[P.eoff[S4] + i];
-            if (!(x > coef_tol)) cold4 = std::max(cold4, x);
-        }
-        const Operator &o1 = P.ops[gp.op[0]], &o2 = P.ops[gp.op[1]], &o3 = P.ops[gp.op[2]], &o4 = P.ops[gp.op[3]];
+        // chains with zero elements: zero lists of the four parts, then one
+        // thread per (i1, i3)
+        const int keys[4] = {zslot.at({gp.op[0], P.ops[gp.op[0]].by_left[S1]}),
+                             zslot.at({gp.op[1], P.ops[gp.op[1]].by_left[S2]}),
+                             zslot.at({gp.op[2], P.ops[gp.op[2]].by_left[S3]}),
+                             zslot.at({gp.op[3], P.ops[gp.op[3]].by_left[S4]})};
+        const ZLists& L1 = zl(gp.op[0], S1, keys[0]);
+        const ZLists& L2 = zl(gp.op[1], S2, keys[1]);
+        const ZLists& L3 = zl(gp.op[2], S3, keys[2]);
+        const ZLists& L4 = zl(gp.op[3], S4, keys[3]);
+        ZeroLists zd{L1.roff, L1.ridx, L2.coff, L2.cidx, L3.roff, L3.ridx, L4.coff, L4.cidx};
         const long n = (long)d1 * d3;
         const double *w1 = P.d_w + P.eoff[S1], *w2 = P.d_w + P.eoff[S2], *w3 = P.d_w + P.eoff[S3], *w4 = P.d_w + P.eoff[S4];
-        if (P.is_complex) {
-            count_kernel<cd><<<ceil_div(n, 256), 256, 0, st>>>(
-                o1.mat.as<cd>() + o1.parts[o1.by_left[S1]].off, o2.mat.as<cd>() + o2.parts[o2.by_left[S2]].off,
-                o3.mat.as<cd>() + o3.parts[o3.by_left[S3]].off, o4.mat.as<cd>() + o4.parts[o4.by_left[S4]].off, d1, d2,
-                d3, d4, w1, w2, w3, w4, coef_tol, nz_tol, cold4, d_cnt);
-        } else {
-            count_kernel<double><<<ceil_div(n, 256), 256, 0, st>>>(
-                o1.mat.as<double>() + o1.parts[o1.by_left[S1]].off, o2.mat.as<double>() + o2.parts[o2.by_left[S2]].off,
-                o3.mat.as<double>() + o3.parts[o3.by_left[S3]].off, o4.mat.as<double>() + o4.parts[o4.by_left[S4]].off,
-                d1, d2, d3, d4, w1, w2, w3, w4, coef_tol, nz_tol, cold4, d_cnt);
-        }
+        const int n2c = (int)(cold_off[S2 + 1] - cold_off[S2]), n4c = (int)(cold_off[S4 + 1] - cold_off[S4]);
+        count_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(zd, d1, d2, d3, d4, w1, w2, w3, w4,
+                                                                 d_cold + cold_off[S2], d_coldi + cold_off[S2], n2c,
+                                                                 d_cold + cold_off[S4], n4c, coef_tol, d_cnt);
         check_launch("count_kernel");
     }
     unsigned long long h[2] = {0, 0};
