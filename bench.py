@@ -56,7 +56,7 @@ NZ_TOL = 1e-20   # the reference's sparseView(Tolerance=1e-8) keeps |x| > 1e-8 *
 COEF_TOL = 1e-16
 POLE_RES = 1e-8
 SETTINGS = {
-    "ring8": dict(beta=5.0, nfreq=24, dm_trunc=1e-12, site="S0", anchor_tol=1e-13, split=True, nbatch=20,
+    "ring8": dict(beta=5.0, nfreq=24, dm_trunc=1e-12, site="S0", anchor_tol=1e-13, split=True, slices=6, nbatch=20,
                   workload="hubbard_ring8_dim65536_chi_u0d0u0d0_24cube_beta5"),
     "a5": dict(beta=20.0, nfreq=16, dm_trunc=None, site="C", anchor_tol=1e-16, split=False, nbatch=1,
                workload="anderson_1+5_dim4096_chi_u0d0u0d0_16cube_beta20"),
@@ -272,7 +272,7 @@ def cpu_baseline_from_engine(config, run, z):
 
 
 # ------------------------------------------------------------------ GPU side
-def roofline_entry(top, steps, torch, config):
+def roofline_entry(top, steps, torch, config, slices=6):
     """Dominant kernel of the timed steps: algorithmic work per launch over its
     average event-timed duration, against the peak of the pipe it runs on."""
     if not top or top["ms"] <= 0:
@@ -287,11 +287,11 @@ def roofline_entry(top, steps, torch, config):
             traffic = json.loads(tf.read_text()).get(config, {}).get(name)
         except Exception:
             traffic = None
-    if name.startswith("oz_split_gemm"):
-        # int8 tensor-core split products: 84 int8 multiply-adds (21 slice
-        # products x 4 real products) per complex multiply-add; flops were
-        # recorded as 8 per complex multiply-add
-        int8_ops = top["flops"] / 8.0 * 84.0 * 2.0 / top["launches"]
+    if name.startswith("oz_gemm"):
+        # int8 tensor-core split products: 4 real products x S(S+1)/2 slice
+        # products of int8 multiply-adds per complex multiply-add (84 at six
+        # slices); flops were recorded as 8 per complex multiply-add
+        int8_ops = top["flops"] / 8.0 * (4.0 * slices * (slices + 1) / 2) * 2.0 / top["launches"]
         peak = 2.0 * peaks["bf16_tflops"] if peaks.get("bf16_tflops") else 2.0 * 1590.0
         achieved = int8_ops / per_launch_s / 1e12
         return {"kernel": name, "bound": "int8-tensor", "achieved": achieved, "peak": peak, "unit": "TOPS",
@@ -321,7 +321,7 @@ def run_ours_ring8(args, rank, world, local_rank):
     cfg = SETTINGS["ring8"]
     NB = cfg["nbatch"]
     prob = Problem("ring8", device=local_rank)
-    run = EngineRun(prob, device=local_rank, split=cfg["split"], anchor_tol=cfg["anchor_tol"])
+    run = EngineRun(prob, device=local_rank, split=cfg["split"], anchor_tol=cfg["anchor_tol"], slices=cfg["slices"])
     _, z = matsubara_cube(prob.beta, prob.nfreq)
     nfreq = len(z)
     eng = run.eng
@@ -428,7 +428,7 @@ def run_ours_ring8(args, rank, world, local_rank):
         triples = [tuple(x) for x in z]
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        v = prob.run_api(triples, split=cfg["split"], anchor_tol=cfg["anchor_tol"])
+        v = prob.run_api(triples, split=cfg["split"], anchor_tol=cfg["anchor_tol"], slices=cfg["slices"])
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - t0
         if world > 1:
@@ -446,7 +446,7 @@ def run_ours_ring8(args, rank, world, local_rank):
     if rank != 0:
         return
     top = kstats[0] if kstats else None
-    roof = roofline_entry(top, args.steps, torch, "ring8")
+    roof = roofline_entry(top, args.steps, torch, "ring8", cfg["slices"])
     if roof is not None:
         roof["kernels_ms_per_step"] = {k["name"]: round(k["ms"] / args.steps, 3) for k in kstats}
     cpu = None
@@ -466,7 +466,8 @@ def run_ours_ring8(args, rank, world, local_rank):
                    "step": "one batch of block chains over the whole 24^3 grid; 20 steps = one full G2",
                    "anchor_tol": cfg["anchor_tol"], "anchor_states": int(sum(anchors)),
                    "anchor_dropped_weight": dropped_w,
-                   "products": "int8 tensor-core split (Ozaki, 6 slices) for products >= 1e9 multiply-adds",
+                   "products": f"int8 tensor-core split (Ozaki, {cfg['slices']} slices) for products >= 1e9 "
+                               "multiply-adds",
                    "l2": "flushed (256 MB write) between timed steps; working set of a step is several GB",
                    "pole_resolution": POLE_RES, "nz_tol": NZ_TOL, "coef_tol": COEF_TOL},
         "stages": {"eigh_weights_rotation_ms": setup_ms, "g2_all_batches_ms": g2_ms, "full_g2_s": full_g2_s},

@@ -619,7 +619,6 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
                 rest.push_back(g);
                 continue;
             }
-            ProfRange pr("oz_split_gemm", st, 8.0 * macs, 0.0);
             oz_zgemm(g, split, c->oz, st);
         }
         launch_on(rest, region, st);

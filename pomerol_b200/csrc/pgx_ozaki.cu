@@ -767,6 +767,9 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
             }
             const int items = a_item ? cn : 1;
             dim3 grid((unsigned)ceil_div((long)M * 32, 256), (unsigned)items);
+            // minimum traffic: the source values once, the digits once
+            ProfRange pr("oz_prep_kernel", st, 0.0,
+                         (double)items * M * K * (is_cd<SA>::value ? 16.0 : 8.0) + (double)items * a_bytes);
             oz_prep_kernel<<<grid, 256, 0, st>>>(q, M, K, K2, S, 0, w.A.as<int8_t>(), a_bytes, w.ea.as<int>(), M);
             check_launch("oz_prep_kernel");
         }
@@ -787,6 +790,8 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
             }
             const int items = b_item ? cn : 1;
             dim3 grid((unsigned)ceil_div((long)N * 32, 256), (unsigned)items);
+            ProfRange pr("oz_prep_kernel", st, 0.0,
+                         (double)items * N * K * (is_cd<SB>::value ? 16.0 : 8.0) + (double)items * b_bytes);
             oz_prep_kernel<<<grid, 256, 0, st>>>(q, N, K, K2, S, 1, w.B.as<int8_t>(), b_bytes, w.fb.as<int>(), N);
             check_launch("oz_prep_kernel");
         }
@@ -809,11 +814,17 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
         a.sc_i = g.sc_i;
         a.sc_j = g.sc_j;
         a.err = w.err.as<int>();
+        // algorithmic work: 8 FP64-equivalent FLOP per complex multiply-add;
+        // minimum traffic: the digits of both operands once and C written once
+        const double fl = 8.0 * (double)M * N * K * cn;
+        const double by = (double)(a_item ? cn : 1) * a_bytes + (double)(b_item ? cn : 1) * b_bytes +
+                          16.0 * (double)M * N * cn;
         if (pair) {  // 256 x 256 tiles, one per CTA pair
             a.tiles_m = (int)ceil_div((long)M, 2L * OZ2_HALF);
             a.tiles_n = (int)ceil_div(2L * N, 2L * OZ2_HALF);
             PGX_CHECK((long)a.tiles_m * a.tiles_n < (1L << 30), PGX_ERR_ARG, "split product: too many tiles");
             dim3 grid((unsigned)(2L * a.tiles_m * a.tiles_n), 1u, (unsigned)cn);
+            ProfRange pr("oz_gemm_pair_kernel", st, fl, by);
             oz_gemm_pair_kernel<<<grid, 384, OZ2_SMEM, st>>>(tmA, tmB, a);
             check_launch("oz_gemm_pair_kernel");
         } else {
@@ -821,6 +832,7 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
             a.tiles_n = (int)ceil_div(2L * N, OZ_BN);
             PGX_CHECK((long)a.tiles_m * a.tiles_n < (1L << 31), PGX_ERR_ARG, "split product: too many tiles");
             dim3 grid((unsigned)((long)a.tiles_m * a.tiles_n), 1u, (unsigned)cn);
+            ProfRange pr("oz_gemm_tma_kernel", st, fl, by);
             oz_gemm_tma_kernel<<<grid, 384, OZ_SMEM, st>>>(tmA, tmB, a);
             check_launch("oz_gemm_tma_kernel");
         }

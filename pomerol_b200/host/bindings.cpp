@@ -282,6 +282,7 @@ PYBIND11_MODULE(_pomerol, m) {
         .def_readwrite("AnchorTolerance", &TwoParticleGF::AnchorTolerance)
         .def_readwrite("ExactSum", &TwoParticleGF::ExactSum)
         .def_readwrite("SplitProducts", &TwoParticleGF::SplitProducts)
+        .def_readwrite("SplitSlices", &TwoParticleGF::SplitSlices)
         .def("prepare", &TwoParticleGF::prepare)
         .def("compute",
              [](TwoParticleGF& g, bool clear, std::vector<std::tuple<C, C, C>> const& f, int) {
@@ -314,6 +315,7 @@ PYBIND11_MODULE(_pomerol, m) {
         .def_readwrite("CoefficientTolerance", &TwoParticleGFContainer::CoefficientTolerance)
         .def_readwrite("SplitProducts", &TwoParticleGFContainer::SplitProducts)
         .def_readwrite("AnchorTolerance", &TwoParticleGFContainer::AnchorTolerance)
+        .def_readwrite("SplitSlices", &TwoParticleGFContainer::SplitSlices)
         .def("prepareAll",
              [](TwoParticleGFContainer& g, std::vector<std::array<ParticleIndex, 4>> const& idx) {
                  std::set<IndexCombination4> s;

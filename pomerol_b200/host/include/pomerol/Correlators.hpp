@@ -158,6 +158,7 @@ public:
     // tensor cores (six 7-bit slices per operand, FP64 recombination; about
     // 1e-11 relative error of G2).  Ignored with ExactSum.
     bool SplitProducts = false;
+    int SplitSlices = 6;  // 7-bit digits per element of the split products (1..8)
 
     TwoParticleGF(StatesClassification const& S, Hamiltonian const& H, AnnihilationOperator const& C1,
                   AnnihilationOperator const& C2, CreationOperator const& CX3, CreationOperator const& CX4,
@@ -208,6 +209,7 @@ public:
     RealType CoefficientTolerance = 1e-16;
     bool SplitProducts = false;  // passed to every element (TwoParticleGF::SplitProducts)
     RealType AnchorTolerance = -1;  // passed to every element (TwoParticleGF::AnchorTolerance)
+    int SplitSlices = 6;            // passed to every element (TwoParticleGF::SplitSlices)
 
     TwoParticleGFContainer(IndexClassification const& IndexInfo, StatesClassification const& S, Hamiltonian const& H,
                            DensityMatrix const& DM, FieldOperatorContainer const& Ops);

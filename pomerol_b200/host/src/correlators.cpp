@@ -273,6 +273,7 @@ std::vector<ComplexType> TwoParticleGF::values(FreqVec3 const& freqs) const {
     // threshold are skipped (the same order as the coefficient filter);
     // ExactSum evaluates every state quadruple.
     const double anchor = AnchorTolerance < 0 ? CoefficientTolerance : AnchorTolerance;
+    if (SplitProducts && !ExactSum) dev.check(pgx_set_g2_split_slices(dev.ctx(), SplitSlices), "pgx_set_g2_split_slices");
     dev.check(pgx_g2(dev.ctx(), (int32_t)parts.size(), parts.data(), (int32_t)freqs.size(), z.data(), PoleResolution,
                      ExactSum ? 0.0 : anchor,
                      ExactSum ? PGX_G2_EXACT : (PGX_G2_ANCHORED | (SplitProducts ? PGX_G2_SPLIT_I8 : 0)),
@@ -375,6 +376,7 @@ void TwoParticleGFContainer::prepareAll(std::set<IndexCombination4> const& Indic
         g.CoefficientTolerance = CoefficientTolerance;
         g.SplitProducts = SplitProducts;
         g.AnchorTolerance = AnchorTolerance;
+        g.SplitSlices = SplitSlices;
         g.prepare();
     }
 }
@@ -387,6 +389,7 @@ std::map<IndexCombination4, std::vector<ComplexType>> TwoParticleGFContainer::co
     for (auto& kv : NonTrivialElements) {
         kv.second->SplitProducts = SplitProducts;
         kv.second->AnchorTolerance = AnchorTolerance;
+        kv.second->SplitSlices = SplitSlices;
     }
     if (split) {
         for (auto& kv : NonTrivialElements) out[kv.first] = kv.second->compute(clearTerms, freqs, comm);
@@ -404,6 +407,7 @@ ElementWithPermFreq<TwoParticleGF>& TwoParticleGFContainer::operator()(IndexComb
     e.element().CoefficientTolerance = CoefficientTolerance;
     e.element().SplitProducts = SplitProducts;
     e.element().AnchorTolerance = AnchorTolerance;
+    e.element().SplitSlices = SplitSlices;
     e.element().prepare();
     return e;
 }

@@ -105,7 +105,7 @@ class Problem:
         self.dims = [self.S.getBlockSize(b) for b in range(self.S.getNumberOfBlocks())]
         self.device = device
 
-    def run_api(self, freqs, split=False, anchor_tol=None):
+    def run_api(self, freqs, split=False, anchor_tol=None, slices=6):
         """Full drop-in sequence from the Hamiltonian expression: Hamiltonian
         (eigensolve), DensityMatrix, FieldOperatorContainer (rotation),
         TwoParticleGFContainer.computeAll on the triples (SplitProducts =
@@ -123,6 +123,7 @@ class Problem:
         ops.computeAll()
         chi = P.TwoParticleGFContainer(self.ii, self.S, H, rho, ops)
         chi.SplitProducts = bool(split)
+        chi.SplitSlices = int(slices)
         if anchor_tol is not None:
             chi.AnchorTolerance = float(anchor_tol)
         key = (self.u0, self.d0, self.u0, self.d0)
