@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <fstream>
+#include <memory>
 #include <set>
 #include <string>
 #include <tuple>
@@ -68,10 +69,16 @@ int main(int argc, char** argv) {
     Ops.computeAll();
 
     const IndexCombination4 uuuu(u0, u0, u0, u0), dddd(d0, d0, d0, d0);
-    TwoParticleGFContainer Chi(IndexInfo, S, H, rho, Ops);
-    Chi.PoleResolution = pole_res;
-    Chi.CoefficientTolerance = coef_tol;
-    Chi.prepareAll({uuuu, IndexCombination4(u0, d0, u0, d0), dddd});
+    // Each mode runs on a container of its own, as each SECTION of the
+    // reference test re-runs the setup: a computed element returns an empty
+    // list from a second compute() (TwoParticleGF.cpp:166-167).
+    auto make_chi = [&]() {
+        auto Chi = std::make_unique<TwoParticleGFContainer>(IndexInfo, S, H, rho, Ops);
+        Chi->PoleResolution = pole_res;
+        Chi->CoefficientTolerance = coef_tol;
+        Chi->prepareAll({uuuu, IndexCombination4(u0, d0, u0, d0), dddd});
+        return Chi;
+    };
 
     const ComplexType w0 = I * M_PI / beta, W1 = I * 2.0 * M_PI / beta;
     int bad = 0;
@@ -84,9 +91,10 @@ int main(int argc, char** argv) {
         }
     };
     // mode 1: computeAll without frequencies, then point evaluation
-    Chi.computeAll(false, {}, MPI_COMM_WORLD, true);
-    TwoParticleGF const& cu = Chi(uuuu);
-    TwoParticleGF const& cd = Chi(dddd);
+    auto Chi1 = make_chi();
+    Chi1->computeAll(false, {}, MPI_COMM_WORLD, true);
+    TwoParticleGF const& cu = (*Chi1)(uuuu);
+    TwoParticleGF const& cd = (*Chi1)(dddd);
     for (int k = 0; k < nval; ++k) {
         const ComplexType wp = I * (2.0 * k + 1.0) * M_PI / beta;
         check("point uuuu", k, cu(w0 + W1, wp, w0));
@@ -95,7 +103,13 @@ int main(int argc, char** argv) {
     // mode 2: computeAll on an explicit frequency list
     FreqVec3 freqs;
     for (int k = 0; k < nval; ++k) freqs.emplace_back(w0 + W1, I * (2.0 * k + 1.0) * M_PI / beta, w0);
-    auto data = Chi.computeAll(true, freqs, MPI_COMM_WORLD, true);
+    auto Chi2 = make_chi();
+    auto data = Chi2->computeAll(true, freqs, MPI_COMM_WORLD, true);
+    if ((int)data[uuuu].size() != nval || (int)data[dddd].size() != nval) {
+        std::fprintf(stderr, "computeAll returned %zu and %zu values, expected %d\n", data[uuuu].size(),
+                     data[dddd].size(), nval);
+        return 1;
+    }
     for (int k = 0; k < nval; ++k) {
         check("list uuuu", k, data[uuuu][k]);
         check("list dddd", k, data[dddd][k]);
