@@ -56,7 +56,7 @@ NZ_TOL = 1e-20   # the reference's sparseView(Tolerance=1e-8) keeps |x| > 1e-8 *
 COEF_TOL = 1e-16
 POLE_RES = 1e-8
 SETTINGS = {
-    "ring8": dict(beta=5.0, nfreq=24, dm_trunc=1e-12, site="S0", anchor_tol=1e-13, split=True, slices=6, nbatch=20,
+    "ring8": dict(beta=5.0, nfreq=24, dm_trunc=1e-12, site="S0", anchor_tol=1e-13, split=True, slices=5, nbatch=20,
                   workload="hubbard_ring8_dim65536_chi_u0d0u0d0_24cube_beta5"),
     "a5": dict(beta=20.0, nfreq=16, dm_trunc=None, site="C", anchor_tol=1e-16, split=False, nbatch=1,
                workload="anderson_1+5_dim4096_chi_u0d0u0d0_16cube_beta20"),
@@ -466,7 +466,7 @@ def run_ours_ring8(args, rank, world, local_rank):
                    "step": "one batch of block chains over the whole 24^3 grid; 20 steps = one full G2",
                    "anchor_tol": cfg["anchor_tol"], "anchor_states": int(sum(anchors)),
                    "anchor_dropped_weight": dropped_w,
-                   "products": f"int8 tensor-core split (Ozaki, {cfg['slices']} slices) for products >= 1e9 "
+                   "products": f"int8 tensor-core split (Ozaki, {cfg['slices']} balanced base-254 digits) for products >= 1e9 "
                                "multiply-adds",
                    "l2": "flushed (256 MB write) between timed steps; working set of a step is several GB",
                    "pole_resolution": POLE_RES, "nz_tol": NZ_TOL, "coef_tol": COEF_TOL},

@@ -34,9 +34,10 @@ extern "C" {
 #define PGX_G2_ANCHORED 2        /* weight-anchored sum: each sub-term is restricted to the
                                     states of its weighted index with w > coef_tol */
 #define PGX_G2_SPLIT_I8 4        /* with PGX_G2_ANCHORED: the stacked (z1, z3) products run on
-                                    the int8 tensor cores, operands split into six 7-bit
-                                    slices with power-of-two row/column scales (Ozaki scheme),
-                                    int32-exact partial products summed in FP64 */
+                                    the int8 tensor cores, operands split into balanced
+                                    base-254 digits (six by default) with power-of-two
+                                    row/column scales (Ozaki scheme), int32-exact partial
+                                    products summed in FP64 */
 
 typedef struct pgx_ctx pgx_ctx;
 
@@ -245,16 +246,19 @@ int pgx_set_g2_workspace(pgx_ctx* ctx, int64_t batch_bytes, int64_t chain_bytes)
  * 0 sends every stacked and anchored product to the tensor cores). */
 int pgx_set_g2_split_threshold(pgx_ctx* ctx, double min_macs);
 
-/* With PGX_G2_SPLIT_I8: digits (7-bit slices) per operand element, 1..8
- * (default 6).  The products keep the slice pairs a + b < slices; the error
- * left is below about slices * 2^(-7 slices) * K of |A|max |B|max per element
- * (no counterpart in the reference, which computes in FP64 only). */
+/* With PGX_G2_SPLIT_I8: digits per operand element, 1..8 (default 6), each a
+ * signed byte of a balanced base-254 expansion (7.99 bits).  The products keep
+ * the digit pairs a + b < slices; the error left is below about
+ * (slices + 1) * 254^(-slices) * K of |A|max |B|max per element (2^-37.4 K at
+ * 5 digits, 2^-45.1 K at 6), with no counterpart in the reference, which
+ * computes in FP64 only. */
 int pgx_set_g2_split_slices(pgx_ctx* ctx, int32_t slices);
 
 /* Tile shape of the int8 split products (no counterpart in the reference):
- * 1 (default) runs 256 x 256 tiles on pairs of CTAs (tcgen05 cta_group::2,
- * each SM loading half of the tile's operands), 0 runs 128 x 256 tiles on
- * single CTAs.  Results are identical. */
+ * 0 (default) runs 128 x 256 tiles on single CTAs, 1 runs 256 x 256 tiles on
+ * pairs of CTAs (tcgen05 cta_group::2, each SM loading half of the tile's
+ * operands).  Results are identical; on the 8-site ring's products the single
+ * CTAs measured 4-7% faster. */
 int pgx_set_split_cta_pair(pgx_ctx* ctx, int32_t cta_pair);
 
 /* Self-check of the int8 split product (no counterpart in the reference):

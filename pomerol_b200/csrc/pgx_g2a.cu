@@ -744,7 +744,7 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
         // over a range of anchors, about 2^22 complex multiply-adds
         std::vector<CClass> cls[CG_NBM][CG_NBN];
         std::vector<CItem> its[CG_NBM][CG_NBN];
-        double macs = 0.0;
+        double macs[CG_NBM][CG_NBN] = {};
         for (size_t q = 0; q < dt.size(); ++q) {
             const DTerm& d = dt[q];
             APlan& pl = plans[d.plan];
@@ -761,7 +761,7 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
                 const int hc = (int)std::max<long>(1, (1L << 22) / ((long)BM * BN * std::max(d.nk, 1)));
                 for (int r0 = 0; r0 < c.nrows; r0 += BM)
                     for (int h0 = 0; h0 < d.nh; h0 += hc) its[bm][bn].push_back(CItem{ci, r0, h0, std::min(d.nh, h0 + hc)});
-                macs += (double)c.nrows * c.ncols * d.nh * d.nk;
+                macs[bm][bn] += (double)c.nrows * c.ncols * d.nh * d.nk;
             }
         }
         size_t bytes = ((dt.size() * sizeof(DTerm) + 255) & ~size_t(255));
@@ -780,12 +780,24 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
             return d;
         };
         const DTerm* d_terms = reinterpret_cast<const DTerm*>(put(dt.data(), dt.size() * sizeof(DTerm)));
-        // 8 FP64 operations per complex multiply-add of (h, k, triple)
-        ProfRange pr("contract_gemm_kernel", st, 8.0 * macs, 0.0);
+        // profiler ranges per tile shape; 8 FP64 operations per complex
+        // multiply-add of (h, k, triple)
+        static const char* const kName[CG_NBM][CG_NBN] = {
+            {"contract_gemm_kernel<8,8>", "contract_gemm_kernel<8,16>", "contract_gemm_kernel<8,24>",
+             "contract_gemm_kernel<8,32>"},
+            {"contract_gemm_kernel<16,8>", "contract_gemm_kernel<16,16>", "contract_gemm_kernel<16,24>",
+             "contract_gemm_kernel<16,32>"},
+            {"contract_gemm_kernel<24,8>", "contract_gemm_kernel<24,16>", "contract_gemm_kernel<24,24>",
+             "contract_gemm_kernel<24,32>"},
+            {"contract_gemm_kernel<32,8>", "contract_gemm_kernel<32,16>", "contract_gemm_kernel<32,24>",
+             "contract_gemm_kernel<32,32>"},
+            {"contract_gemm_kernel<64,8>", "contract_gemm_kernel<64,16>", "contract_gemm_kernel<64,24>",
+             "contract_gemm_kernel<64,32>"}};
         const double tol2 = pole_res * pole_res;
         for (int a = 0; a < CG_NBM; ++a)
             for (int b = 0; b < CG_NBN; ++b) {
                 if (its[a][b].empty()) continue;
+                ProfRange pr(kName[a][b], st, 8.0 * macs[a][b], 0.0);
                 PGX_CHECK(its[a][b].size() < (1u << 31), PGX_ERR_ARG, "G2 contraction: too many work items");
                 const CClass* dc = reinterpret_cast<const CClass*>(put(cls[a][b].data(), cls[a][b].size() * sizeof(CClass)));
                 const CItem* di = reinterpret_cast<const CItem*>(put(its[a][b].data(), its[a][b].size() * sizeof(CItem)));

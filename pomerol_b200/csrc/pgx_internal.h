@@ -96,7 +96,7 @@ struct DevBuf {
 // Workspace of the int8 split products (digits, exponents, error flag).
 struct OzWork {
     DevBuf A, B, ea, fb, err;
-    int cta_pair = 1;  // 1: 256 x 256 tiles on CTA pairs (cta_group::2); 0: 128 x 256 tiles on single CTAs
+    int cta_pair = 0;  // 0: 128 x 256 tiles on single CTAs (measured faster); 1: 256 x 256 tiles on CTA pairs
 };
 
 // Times of the products measured since pgx_autotune_begin, per (operand-type

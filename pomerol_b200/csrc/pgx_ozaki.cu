@@ -3,13 +3,17 @@
 // (the stacked (z1, z3) products) when PGX_G2_SPLIT_I8 is set.
 //
 // Each row of A and each column of B is scaled by a power of two so that its
-// largest |Re| or |Im| is below 1, and cut into S signed 7-bit digits:
-//   x * 2^-e = sum_s d_s 2^(-7(s+1)),  d_s integer in [-127, 127]
-// (exact digit extraction in FP64; the truncation left after S digits is
-// below 2^(-7S) of the row's or column's largest element).  The product is
-//   C = diag(2^e) [ sum_{a+b<S} 2^(-7(a+b+2)) A_a B_b ] diag(2^f),
+// largest |Re| or |Im| is below 1, and cut into S balanced digits of base 254:
+//   127 x 2^-e = sum_s d_s 254^-s,  d_s integer in [-127, 127]
+// (d_0 = rint(127 x 2^-e), then each remainder, in [-1/2, 1/2], times 254 and
+// rounded to the nearest integer: every digit fits a signed byte and carries
+// log2(254) = 7.99 bits; the remainder left after S digits is below
+// 254^-(S-1) / 254 of the row's or column's largest element).  The product is
+//   C = diag(2^e) [ sum_{a+b<S} 254^-(a+b) / 127^2 A_a B_b ] diag(2^f),
 // each A_a B_b exact in int32, the diagonals a+b = s summed in FP64.  The
-// dropped diagonals (a+b >= S) are bounded by S 2^(-7S) K |A|max |B|max.
+// dropped diagonals (a+b >= S) are bounded by (S-1) 254^-S K |A|max |B|max,
+// the remainders by 2 254^-S K |A|max |B|max: in all about 2^-37.4 K of
+// |A|max |B|max at S = 5 and 2^-45.1 K at S = 6.
 // Complex operands become one real product of twice the depth:
 //   A' = [Re A, Im A] (M x 2K) and, per complex column j of B, two columns
 //   [Re B_j; -Im B_j] (the real part of C_j) and [Im B_j; Re B_j] (its imaginary
@@ -104,6 +108,15 @@ __device__ __forceinline__ double pow2i(int e) {
     return (e >= -1022 && e <= 1023) ? __longlong_as_double((long long)(e + 1023) << 52) : ldexp(1.0, e);
 }
 
+// Digit base of the split and the weight of diagonal s of the product:
+// 254^-s / 127^2 (127 scales the leading digit of each operand).
+constexpr double OZ_BASE = 254.0;
+__device__ __forceinline__ double diag_weight(int s) {
+    double w = 1.0 / (127.0 * 127.0);
+    for (int t = 0; t < s; ++t) w *= 1.0 / OZ_BASE;
+    return w;
+}
+
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -121,7 +134,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
 // issues the MMAs as soon as a stage is full and releases it with
 // tcgen05.commit; warps 0-7 (TMEM lanes 32 (w % 4) ..., 128 columns per warp
 // half) read each finished diagonal's accumulator with tcgen05.ld, add it,
-// scaled by 2^(e_i + f_j - 14 - 7s), into C (stored by the first diagonal,
+// scaled by 2^(e_i + f_j) 254^-s / 127^2, into C (stored by the first diagonal,
 // read and added by the others; the tile stays in L2) and release it.  Barriers: full and
 // empty per stage; per accumulator "finished" (commit) and "drained" (one
 // arrival per drain warp).
@@ -295,6 +308,7 @@ __global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_consta
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const double dw = diag_weight(s);
             const uint32_t base = tmem + ((uint32_t)lane_base << 16) + (uint32_t)((s & 1) * OZ_BN + col_base);
 #pragma unroll 1
             for (int q = 0; q < 8; ++q) {
@@ -302,14 +316,20 @@ __global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_consta
                 tmem_ld16(base + 16 * q, v);
                 asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
                 if (row_ok) {
+                    // the eight earlier partial sums are read before any store, so
+                    // their loads are in flight together
+                    const int jc0 = (j0 + col_base) / 2 + 8 * q;
+                    cd old[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        old[e] = (s > 0 && jc0 + e < p.N) ? crow[(long)(jc0 + e) * p.sc_j] : cd{0.0, 0.0};
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
-                        const int jc = (j0 + col_base) / 2 + 8 * q + e;
+                        const int jc = jc0 + e;
                         if (jc < p.N) {
-                            const double sc = pow2i(ei + fbi[jc] - 14 - 7 * s);
+                            const double sc = pow2i(ei + fbi[jc]) * dw;
                             const cd add{(double)(int)v[2 * e] * sc, (double)(int)v[2 * e + 1] * sc};
-                            cd& dst = crow[(long)jc * p.sc_j];
-                            dst = s == 0 ? add : cd{dst.x + add.x, dst.y + add.y};
+                            crow[(long)jc * p.sc_j] = s == 0 ? add : cd{old[e].x + add.x, old[e].y + add.y};
                         }
                     }
                 }
@@ -366,7 +386,7 @@ __global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_consta
 // wait is bounded as in oz_gemm_tma_kernel; both CTAs always reach the final
 // cluster barrier, so neither leaves while its partner may touch its memory.
 constexpr int OZ2_HALF = 128;                                  // rows of A' / B' per CTA
-constexpr int OZ2_STAGES = 6;
+constexpr int OZ2_STAGES = 7;  // 7 x 32 KiB + barriers: the most that fits the 227 KiB opt-in limit
 constexpr int OZ2_STAGE_BYTES = 2 * OZ2_HALF * OZ_BK;          // 32 KiB per CTA
 constexpr int OZ2_SMEM = OZ2_STAGES * OZ2_STAGE_BYTES + 1024 + 256;
 constexpr uint32_t OZ2_IDESC = (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
@@ -540,6 +560,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(384, 1)
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+            const double dw = diag_weight(s);
             const uint32_t base = tmem + ((uint32_t)lane_base << 16) + (uint32_t)((s & 1) * OZ_BN + col_base);
 #pragma unroll 1
             for (int q = 0; q < 8; ++q) {
@@ -547,14 +568,20 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(384, 1)
                 tmem_ld16(base + 16 * q, v);
                 asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
                 if (row_ok) {
+                    // the eight earlier partial sums are read before any store, so
+                    // their loads are in flight together
+                    const int jc0 = (j0 + col_base) / 2 + 8 * q;
+                    cd old[8];
+#pragma unroll
+                    for (int e = 0; e < 8; ++e)
+                        old[e] = (s > 0 && jc0 + e < p.N) ? crow[(long)(jc0 + e) * p.sc_j] : cd{0.0, 0.0};
 #pragma unroll
                     for (int e = 0; e < 8; ++e) {
-                        const int jc = (j0 + col_base) / 2 + 8 * q + e;
+                        const int jc = jc0 + e;
                         if (jc < p.N) {
-                            const double sc = pow2i(ei + fbi[jc] - 14 - 7 * s);
+                            const double sc = pow2i(ei + fbi[jc]) * dw;
                             const cd add{(double)(int)v[2 * e] * sc, (double)(int)v[2 * e + 1] * sc};
-                            cd& dst = crow[(long)jc * p.sc_j];
-                            dst = s == 0 ? add : cd{dst.x + add.x, dst.y + add.y};
+                            crow[(long)jc * p.sc_j] = s == 0 ? add : cd{old[e].x + add.x, old[e].y + add.y};
                         }
                     }
                 }
@@ -628,52 +655,161 @@ __device__ __forceinline__ cd oz_value(const OzSrc& q, int item, int r, int k) {
     return q.rk_order ? dress(x, q.Er[r], q.Ek[k], z) : dress(x, q.Ek[k], q.Er[r], z);
 }
 
-// One warp per output row r; is_b selects the B' layout (two rows per complex
-// column, slices in reverse order).
-__global__ void oz_prep_kernel(OzSrc q, int R, int K, int K2, int S, int is_b, int8_t* out, long out_item, int* ex,
-                               long ex_item) {
-    const int warp = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5), lane = threadIdx.x & 31;
-    const int item = blockIdx.y;
-    if (warp >= R) return;
-    const int r = warp;
-    double m = 0.0;
-    for (int k = lane; k < K; k += 32) {
-        const cd v = oz_value(q, item, r, k);
-        m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
-    }
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    int e = 0;
-    if (m > 0.0) frexp(m, &e);  // m = f 2^e, f in [0.5, 1): every |x| 2^-e < 1
-    if (lane == 0) ex[item * ex_item + r] = e;
-    const long row_bytes = (long)S * K2;
-    int8_t* o0 = out + item * out_item + (long)(is_b ? 2 * r : r) * row_bytes;
-    int8_t* o1 = o0 + row_bytes;  // B' only: the imaginary-part row
-    for (int k = lane; k < K2 / 2; k += 32) {
-        double vr = 0.0, vi = 0.0;
-        if (k < K) {
-            const cd v = oz_value(q, item, r, k);
-            vr = ldexp(v.x, -e);
-            vi = ldexp(v.y, -e);
+// Digits of an operand in two kernels.  oz_rowmax_kernel: the largest |Re|
+// or |Im| of each output row over a range of reduction indices, as the
+// exponent e with max < 2^e, merged into ex[] with atomicMax (ex starts below
+// every exponent; rows without a non-zero value keep the floor -1000).
+// oz_prep_kernel: one CTA per OP_ROWS rows x OP_KC reduction indices: the
+// values scaled by 127 2^-e go through a shared tile, then each thread turns
+// four consecutive k of one row into digits and stores each digit plane's four
+// bytes as one 32-bit word (a warp writes 64 contiguous bytes per row); is_b
+// selects the B' layout (two rows per complex column, digits in reverse
+// order).  Source reads are coalesced either way: lanes run along k when the
+// source is k-contiguous (s_k == 1), along the rows otherwise.
+constexpr int OP_ROWS = 32, OP_KC = 64, OP_THREADS = 256, OP_KSPAN = 512;
+constexpr int OP_EXP_FLOOR = -1000;  // rows below 2^-1000 keep a representable scale
+
+// Tile slot of (row r, chunk index k): rows 65 slots apart, the 16-byte slot
+// index XOR-swizzled so that row-wise, column-wise and 4-strided accesses of
+// eight lanes fall on distinct banks.
+__device__ __forceinline__ int op_slot(int r, int k) { return r * (OP_KC + 1) + (k ^ ((k >> 3) & 7)); }
+
+__global__ void __launch_bounds__(OP_THREADS) oz_rowmax_kernel(OzSrc q, int R, int K, int* ex, long ex_item) {
+    __shared__ double s_part[OP_THREADS / 32][OP_ROWS];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int item = blockIdx.z, r0 = blockIdx.x * OP_ROWS;
+    const int k0 = blockIdx.y * OP_KSPAN, k1 = min(K, k0 + OP_KSPAN);
+    double mrow = 0.0;  // thread t < OP_ROWS: the maximum of row r0 + t
+    if (q.s_k == 1) {   // warp w: rows w, w + 8, w + 16, w + 24; lanes along k
+        for (int rr = warp; rr < OP_ROWS; rr += OP_THREADS / 32) {
+            double m = 0.0;
+            if (r0 + rr < R)
+                for (int k = k0 + lane; k < k1; k += 32) {
+                    const cd v = oz_value(q, item, r0 + rr, k);
+                    m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+                }
+            for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+            if (lane == 0) s_part[0][rr] = m;
         }
-        for (int s = 0; s < S; ++s) {
-            vr *= 128.0;
-            vi *= 128.0;
-            const double dr = trunc(vr), di = trunc(vi);
-            vr -= dr;
-            vi -= di;
-            const long base = (long)(is_b ? S - 1 - s : s) * K2;
+        __syncthreads();
+        if (t < OP_ROWS) mrow = s_part[0][t];
+    } else {  // lane = row, warps along k
+        double m = 0.0;
+        if (r0 + lane < R)
+            for (int k = k0 + warp; k < k1; k += OP_THREADS / 32) {
+                const cd v = oz_value(q, item, r0 + lane, k);
+                m = fmax(m, fmax(fabs(v.x), fabs(v.y)));
+            }
+        s_part[warp][lane] = m;
+        __syncthreads();
+        if (t < OP_ROWS) {
+            mrow = s_part[0][t];
+            for (int w = 1; w < OP_THREADS / 32; ++w) mrow = fmax(mrow, s_part[w][t]);
+        }
+    }
+    if (t < OP_ROWS && r0 + t < R) {
+        int e = OP_EXP_FLOOR;
+        if (mrow > 0.0) {
+            frexp(mrow, &e);  // max = f 2^e, f in [0.5, 1): every |x| 2^-e < 1
+            e = max(e, OP_EXP_FLOOR);
+        }
+        atomicMax(ex + item * ex_item + r0 + t, e);
+    }
+}
+
+__global__ void __launch_bounds__(OP_THREADS) oz_prep_kernel(OzSrc q, int R, int K, int K2, int S, int is_b,
+                                                             int8_t* out, long out_item, const int* ex, long ex_item) {
+    __shared__ cd tile[OP_ROWS * (OP_KC + 1)];
+    __shared__ double s_scale[OP_ROWS];
+    const int t = threadIdx.x;
+    const int item = blockIdx.z, r0 = blockIdx.x * OP_ROWS, k0 = blockIdx.y * OP_KC;
+    const bool kcontig = q.s_k == 1;
+    // 127 2^-e exactly: |x| 127 2^-e < 127, so the leading digit fits a signed byte
+    if (t < OP_ROWS) s_scale[t] = r0 + t < R ? ldexp(127.0, -ex[item * ex_item + r0 + t]) : 0.0;
+    __syncthreads();
+    // scaled values of the chunk into the tile (zero past K and past R)
+#pragma unroll 4
+    for (int j = 0; j < OP_ROWS * OP_KC / OP_THREADS; ++j) {
+        const int idx = t + OP_THREADS * j;
+        const int rr = kcontig ? idx / OP_KC : idx % OP_ROWS;
+        const int kk = kcontig ? idx % OP_KC : idx / OP_ROWS;
+        cd v{0.0, 0.0};
+        if (r0 + rr < R && k0 + kk < K) {
+            v = oz_value(q, item, r0 + rr, k0 + kk);
+            v.x *= s_scale[rr];
+            v.y *= s_scale[rr];
+        }
+        tile[op_slot(rr, kk)] = v;
+    }
+    __syncthreads();
+    const long row_bytes = (long)S * K2;
+    const int half = K2 / 2;  // multiple of 64: K2 is a multiple of 128
+    // digits: thread -> (row, four consecutive k); 16 threads per row
+#pragma unroll
+    for (int j = 0; j < OP_ROWS * OP_KC / 4 / OP_THREADS; ++j) {
+        const int task = t + OP_THREADS * j;
+        const int rr = task / (OP_KC / 4), g = task % (OP_KC / 4);
+        uint32_t wr[8], wi[8];
+#pragma unroll
+        for (int d = 0; d < 8; ++d) wr[d] = wi[d] = 0u;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const cd v = tile[op_slot(rr, 4 * g + c)];
+            double vr = v.x, vi = v.y;
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                if (d >= S) break;
+                if (d > 0) {  // remainders in [-1/2, 1/2]: the next digit in [-127, 127]
+                    vr *= OZ_BASE;
+                    vi *= OZ_BASE;
+                }
+                const double dr = rint(vr), di = rint(vi);
+                vr -= dr;
+                vi -= di;
+                wr[d] |= ((uint32_t)(int)dr & 0xFFu) << (8 * c);
+                wi[d] |= ((uint32_t)(int)di & 0xFFu) << (8 * c);
+            }
+        }
+        if (r0 + rr >= R) continue;
+        const int r = r0 + rr, k = k0 + 4 * g;
+        int8_t* o0 = out + item * out_item + (long)(is_b ? 2 * r : r) * row_bytes;
+#pragma unroll
+        for (int d = 0; d < 8; ++d) {
+            if (d >= S) break;
+            const long base = (long)(is_b ? S - 1 - d : d) * K2;
             // the first K2/2 positions pair with Re of the other side, the rest with Im
-            if (!is_b) {
-                o0[base + k] = (int8_t)dr;               // A' = [Re A, Im A]
-                o0[base + K2 / 2 + k] = (int8_t)di;
+            if (!is_b) {  // A' = [Re A, Im A]
+                *reinterpret_cast<uint32_t*>(o0 + base + k) = wr[d];
+                *reinterpret_cast<uint32_t*>(o0 + base + half + k) = wi[d];
             } else {
-                o0[base + k] = (int8_t)dr;               // real-part column: [Re B; -Im B]
-                o0[base + K2 / 2 + k] = (int8_t)(-di);
-                o1[base + k] = (int8_t)di;               // imaginary-part column: [Im B; Re B]
-                o1[base + K2 / 2 + k] = (int8_t)dr;
+                // negated bytes: each byte is in [-127, 127], so per-byte negation never carries
+                uint32_t nwi = 0u;
+#pragma unroll
+                for (int c = 0; c < 4; ++c)
+                    nwi |= ((uint32_t)(-(int)(int8_t)((wi[d] >> (8 * c)) & 0xFFu)) & 0xFFu) << (8 * c);
+                int8_t* o1 = o0 + row_bytes;  // the imaginary-part column
+                *reinterpret_cast<uint32_t*>(o0 + base + k) = wr[d];  // [Re B; -Im B]
+                *reinterpret_cast<uint32_t*>(o0 + base + half + k) = nwi;
+                *reinterpret_cast<uint32_t*>(o1 + base + k) = wi[d];  // [Im B; Re B]
+                *reinterpret_cast<uint32_t*>(o1 + base + half + k) = wr[d];
             }
         }
     }
+}
+
+// Digits of one operand (rows R, reduction length K) for `items` items:
+// exponents into ex[item][R], digits into out[item].
+void oz_prepare(const OzSrc& q, int R, int K, int K2, int S, int is_b, int items, int8_t* out, long out_item, int* ex,
+                double min_bytes, cudaStream_t st) {
+    ProfRange pr("oz_prep_kernel", st, 0.0, min_bytes);
+    // below every exponent (0x80808080 = -2139062144): each row's first atomicMax sets it
+    PGX_CUDA(cudaMemsetAsync(ex, 0x80, (size_t)items * R * sizeof(int), st));
+    dim3 g1((unsigned)ceil_div((long)R, (long)OP_ROWS), (unsigned)ceil_div((long)K, (long)OP_KSPAN), (unsigned)items);
+    oz_rowmax_kernel<<<g1, OP_THREADS, 0, st>>>(q, R, K, ex, R);
+    check_launch("oz_rowmax_kernel");
+    dim3 g2((unsigned)ceil_div((long)R, (long)OP_ROWS), (unsigned)(K2 / 2 / OP_KC), (unsigned)items);
+    oz_prep_kernel<<<g2, OP_THREADS, 0, st>>>(q, R, K, K2, S, is_b, out, out_item, ex, R);
+    check_launch("oz_prep_kernel");
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point.
@@ -766,12 +902,9 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
                 q.zs = g.dzs + b0;
             }
             const int items = a_item ? cn : 1;
-            dim3 grid((unsigned)ceil_div((long)M * 32, 256), (unsigned)items);
-            // minimum traffic: the source values once, the digits once
-            ProfRange pr("oz_prep_kernel", st, 0.0,
-                         (double)items * M * K * (is_cd<SA>::value ? 16.0 : 8.0) + (double)items * a_bytes);
-            oz_prep_kernel<<<grid, 256, 0, st>>>(q, M, K, K2, S, 0, w.A.as<int8_t>(), a_bytes, w.ea.as<int>(), M);
-            check_launch("oz_prep_kernel");
+            // minimum traffic: the source values twice (maxima, digits), the digits once
+            oz_prepare(q, M, K, K2, S, 0, items, w.A.as<int8_t>(), a_bytes, w.ea.as<int>(),
+                       2.0 * items * M * K * (is_cd<SA>::value ? 16.0 : 8.0) + (double)items * a_bytes, st);
         }
         // B columns: B(k, j) = B[k sb_k + j sb_j]; dressed as dress(x, dEa[k], dEb[j], z)
         if (b_item || b0 == 0) {
@@ -789,11 +922,8 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
                 q.zs = g.dzs + b0;
             }
             const int items = b_item ? cn : 1;
-            dim3 grid((unsigned)ceil_div((long)N * 32, 256), (unsigned)items);
-            ProfRange pr("oz_prep_kernel", st, 0.0,
-                         (double)items * N * K * (is_cd<SB>::value ? 16.0 : 8.0) + (double)items * b_bytes);
-            oz_prep_kernel<<<grid, 256, 0, st>>>(q, N, K, K2, S, 1, w.B.as<int8_t>(), b_bytes, w.fb.as<int>(), N);
-            check_launch("oz_prep_kernel");
+            oz_prepare(q, N, K, K2, S, 1, items, w.B.as<int8_t>(), b_bytes, w.fb.as<int>(),
+                       2.0 * items * N * K * (is_cd<SB>::value ? 16.0 : 8.0) + (double)items * b_bytes, st);
         }
         const bool pair = w.cta_pair != 0;
         const CUtensorMap tmA = digit_map(w.A.p, row_bytes, M, a_item ? cn : 1, pair ? OZ2_HALF : OZ_BM);

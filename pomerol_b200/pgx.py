@@ -434,7 +434,7 @@ def _set_g2_split_threshold(self, min_macs=1e9):
 
 
 def _set_g2_split_slices(self, slices=6):
-    """7-bit digits per operand element of the int8 split products."""
+    """Balanced base-254 digits per operand element of the int8 split products."""
     self._ck(self.lib.pgx_set_g2_split_slices(self.h, int(slices)))
 
 

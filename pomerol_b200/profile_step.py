@@ -29,8 +29,10 @@ def main():
                     help="anchored G2 with its stacked products on the int8 tensor cores (PGX_G2_SPLIT_I8); "
                          "with --chain each cube also runs in FP64 for the error")
     ap.add_argument("--anchor-tol", type=float, default=1e-16, help="anchor weight threshold of the G2 sum")
-    ap.add_argument("--slices", type=int, default=6, help="7-bit digits per element of the split products")
+    ap.add_argument("--slices", type=int, default=6, help="base-254 digits per element of the split products")
     ap.add_argument("--fp64", action="store_true", help="with --split: also run the plain FP64 form (same sum)")
+    ap.add_argument("--cta-pair", type=int, default=0,
+                    help="split-product tiles: 0 for 128 x 256 on single CTAs (default), 1 for 256 x 256 on CTA pairs")
     ap.add_argument("--autotune", action="store_true",
                     help="measure the GEMM tile classes on one step (after one untimed step) before timing")
     a = ap.parse_args()
@@ -65,6 +67,7 @@ def main():
     else:
         _, z = matsubara_cube(prob.beta, prob.nfreq)
         run = EngineRun(prob, split=a.split, anchor_tol=a.anchor_tol, slices=a.slices)
+        run.eng.set_split_cta_pair(a.cta_pair)
     if a.autotune:
         autotune(run.eng, lambda: run.step(z))
     for s in range(a.steps):

@@ -56,8 +56,9 @@ def test_ring8_g_and_chi_zz(ring8):
 
 @pytest.mark.parametrize("split,tol,slices", [(False, 1e-16, 6), (True, 1e-16, 6), (True, 1e-13, 6), (True, 1e-13, 5)])
 def test_ring8_g2_sample(ring8, split, tol, slices):
-    """Five digits per element (the benchmark's setting for this model)
-    leave about 128 times the error of six; both stay below 1e-8."""
+    """Five base-254 digits per element (the benchmark's setting for this
+    model) leave about 250 times the product error of six; both stay far
+    below 1e-8."""
     from pomerol_b200.pgx import PGX_G2_ANCHORED, PGX_G2_SPLIT_I8
     g, m, doc = ring8
     u, d = m.info.getIndex("S0", 0, 1), m.info.getIndex("S0", 0, 0)
