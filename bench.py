@@ -280,22 +280,29 @@ def roofline_entry(top, steps, torch, config, slices=6):
     per_launch_s = top["ms"] / top["launches"] / 1e3
     name = top["name"]
     peaks = measured_peaks()
-    traffic = None
+    # DRAM bytes per unit of work of this kernel, from one ncu capture of a
+    # smaller case of the same kernel (profiles/roofline_traffic.json)
+    cap = {}
     tf = ROOT / "profiles" / "roofline_traffic.json"
     if tf.exists():
         try:
-            traffic = json.loads(tf.read_text()).get(config, {}).get(name)
+            cap = json.loads(tf.read_text()).get(config, {}).get(name) or {}
         except Exception:
-            traffic = None
+            cap = {}
+    algo_bytes = top.get("bytes", 0.0) / top["launches"]
     if name.startswith("oz_gemm"):
-        # int8 tensor-core split products: 4 real products x S(S+1)/2 slice
-        # products of int8 multiply-adds per complex multiply-add (84 at six
-        # slices); flops were recorded as 8 per complex multiply-add
+        # int8 tensor-core split products: 4 real products x S(S+1)/2 digit
+        # products of int8 multiply-adds per complex multiply-add (60 at five
+        # digits); flops were recorded as 8 per complex multiply-add
         int8_ops = top["flops"] / 8.0 * (4.0 * slices * (slices + 1) / 2) * 2.0 / top["launches"]
         peak = 2.0 * peaks["bf16_tflops"] if peaks.get("bf16_tflops") else 2.0 * 1590.0
         achieved = int8_ops / per_launch_s / 1e12
+        traffic = cap["dram_bytes_per_int8_mac"] * int8_ops / 2.0 if cap.get("dram_bytes_per_int8_mac") else None
         return {"kernel": name, "bound": "int8-tensor", "achieved": achieved, "peak": peak, "unit": "TOPS",
                 "frac": achieved / peak, "traffic": traffic,
+                "traffic_source": cap.get("source"),
+                "algorithmic_bytes_per_launch": algo_bytes,
+                "traffic_over_algorithmic": traffic / algo_bytes if traffic and algo_bytes else None,
                 "peak_source": ("2 x MEASURED_PEAKS.json bf16_tflops (dense int8 runs at twice the bf16 rate on "
                                 "the B200 tensor cores)" if peaks.get("bf16_tflops") else "2 x fallback bf16 1590"),
                 "fp64_equivalent_tflops": top["flops"] / top["launches"] / per_launch_s / 1e12,
@@ -303,8 +310,10 @@ def roofline_entry(top, steps, torch, config, slices=6):
                 "algorithmic_ops_per_launch": int8_ops}
     peak = fp64_peak_tflops(torch)
     achieved = top["flops"] / top["launches"] / per_launch_s / 1e12
+    traffic = cap["dram_bytes_per_flop"] * top["flops"] / top["launches"] if cap.get("dram_bytes_per_flop") else None
     return {"kernel": name, "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-            "frac": achieved / peak, "traffic": traffic,
+            "frac": achieved / peak, "traffic": traffic, "traffic_source": cap.get("source"),
+            "algorithmic_bytes_per_launch": algo_bytes,
             "peak_source": "measured live: cuBLAS FP64 DGEMM 8192^3 (torch.matmul float64); MEASURED_PEAKS.json "
                            "has no FP64 figure",
             "launches_per_step": top["launches"] / steps, "ms_per_launch": per_launch_s * 1e3,
