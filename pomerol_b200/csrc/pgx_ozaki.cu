@@ -22,7 +22,9 @@
 //   A row i: [digits of slice 0 | slice 1 | ... | slice S-1], each K2 = 2K
 //   rounded up to 128 bytes; B column j: [slice S-1 | ... | slice 0].
 // Then diagonal s is one product of depth (s+1) K2 with A from offset 0 and
-// B from offset (S-1-s) K2: both operands are plain strided views.
+// B from offset (S-1-s) K2: both operands are plain strided views.  Odd
+// diagonals sweep their depth from the end, so consecutive diagonals meet on
+// the planes and k-blocks read last (the int32 sums do not depend on order).
 //
 // The GEMM kernel: one CTA per 128 x 256 tile of C' (128 complex columns) and
 // batch item; tcgen05.mma with M = 128, N = 256 and K = 32 bytes per
@@ -233,8 +235,11 @@ __global__ void __launch_bounds__(384, 1) oz_gemm_tma_kernel(const __grid_consta
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(fb), "r"(OZ_STAGE_BYTES)
                          : "memory");
             const uint32_t dst = smem_u32(smem + st * OZ_STAGE_BYTES);
-            tma_load3(dst, &tmA, kb * OZ_BK, i0, p.a_items ? item : 0, fb);
-            tma_load3(dst + OZ_BM * OZ_BK, &tmB, (p.S - 1 - s) * p.K2 + kb * OZ_BK, j0, p.b_items ? item : 0, fb);
+            // odd diagonals run backwards, so each diagonal starts on the
+            // digit planes and k-blocks the previous one read last (still in L2)
+            const int kx = (s & 1) ? (s + 1) * kbd - 1 - kb : kb;
+            tma_load3(dst, &tmA, kx * OZ_BK, i0, p.a_items ? item : 0, fb);
+            tma_load3(dst + OZ_BM * OZ_BK, &tmB, (p.S - 1 - s) * p.K2 + kx * OZ_BK, j0, p.b_items ? item : 0, fb);
             issued = it + 1;
             if (++kb == (s + 1) * kbd) {
                 kb = 0;
@@ -499,8 +504,9 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(384, 1)
                              : "memory");
             const uint32_t fb = cluster_addr(fb_local, 0);
             const uint32_t dst = smem_u32(smem + st * OZ2_STAGE_BYTES);
-            tma_load3_pair(dst, &tmA, kb * OZ_BK, i0, p.a_items ? item : 0, fb);
-            tma_load3_pair(dst + OZ2_HALF * OZ_BK, &tmB, (p.S - 1 - s) * p.K2 + kb * OZ_BK, jb, p.b_items ? item : 0,
+            const int kx = (s & 1) ? (s + 1) * kbd - 1 - kb : kb;  // odd diagonals backwards, as above
+            tma_load3_pair(dst, &tmA, kx * OZ_BK, i0, p.a_items ? item : 0, fb);
+            tma_load3_pair(dst + OZ2_HALF * OZ_BK, &tmB, (p.S - 1 - s) * p.K2 + kx * OZ_BK, jb, p.b_items ? item : 0,
                            fb);
             issued = it + 1;
             if (++kb == (s + 1) * kbd) {
