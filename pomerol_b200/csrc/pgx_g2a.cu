@@ -137,37 +137,62 @@ __global__ void __launch_bounds__((BM / cg_tm(BM)) * CG_NX)
     const int nk = d.nk;
     const int ktiles = (nk + CG_BK - 1) / CG_BK;
     const long nsteps = (long)(it.h1 - it.h0) * ktiles;
-    cd ra[LA], rb[LB];
-    // operands of step q (anchor h0 + q / ktiles, k-tile q % ktiles) into registers
-    auto load = [&](long q) {
+    // Operands of step q (anchor h0 + q / ktiles, k-tile q % ktiles): fetch()
+    // issues the global loads of the raw values into registers before the
+    // current step's products; finish() forms VA VB and the Lehmann kernel from
+    // them and stores the tiles after the products, so the loads' latency is
+    // covered by the inner loop instead of stalling ahead of it.
+    cd rx[LA], ry[LA];
+    double rek[LB];
+    double r_eh = 0.0, r_w = 0.0;
+    auto fetch = [&](long q) {
         const int h = it.h0 + (int)(q / ktiles), k0 = (int)(q % ktiles) * CG_BK;
         const int hs = d.hot[h];
         const long oah = (long)(d.va_hstate ? hs : h) * d.ah, obh = (long)(d.vb_hstate ? hs : h) * d.bh;
 #pragma unroll
         for (int u = 0; u < LA; ++u) {
             const int l = tid + u * NT;
-            cd v{0.0, 0.0};
+            cd x{0.0, 0.0}, y{0.0, 0.0};
             if (l < BM * CG_BK) {
                 const int r = l / CG_BK, kk = l % CG_BK, k = k0 + kk;
                 if (r < nrows && k < nk) {
-                    const cd x = load_v(d.VA, d.va_cplx, s_oa[r] + oah + (long)k * d.ak);
-                    const cd y = load_v(d.VB, d.vb_cplx, s_ob[r] + obh + (long)k * d.bk);
-                    v = x * y;
+                    x = load_v(d.VA, d.va_cplx, s_oa[r] + oah + (long)k * d.ak);
+                    y = load_v(d.VB, d.vb_cplx, s_ob[r] + obh + (long)k * d.bk);
                 }
             }
-            ra[u] = v;
+            rx[u] = x;
+            ry[u] = y;
         }
-        const double eh = d.Eh[hs], w = d.wh[hs];
-        const double cw = d.cnum * w, cdl = d.cdelta * beta * w;
+        r_eh = d.Eh[hs];
+        r_w = d.wh[hs];
 #pragma unroll
         for (int u = 0; u < LB; ++u) {
             const int l = tid + u * NT;
-            cd v{0.0, 0.0};
+            double ek = 0.0;
+            if (l < BN * CG_BK) {
+                const int k = k0 + l / BN;
+                if (k < nk) ek = d.Ek[k];
+            }
+            rek[u] = ek;
+        }
+    };
+    auto finish = [&](long q, int buf) {
+        const int k0 = (int)(q % ktiles) * CG_BK;
+#pragma unroll
+        for (int u = 0; u < LA; ++u) {
+            const int l = tid + u * NT;
+            if (l < BM * CG_BK) As[buf][l % CG_BK][l / CG_BK] = rx[u] * ry[u];
+        }
+        const double cw = d.cnum * r_w, cdl = d.cdelta * beta * r_w;
+#pragma unroll
+        for (int u = 0; u < LB; ++u) {
+            const int l = tid + u * NT;
             if (l < BN * CG_BK) {
                 const int kk = l / BN, j = l % BN, k = k0 + kk;
+                cd v{0.0, 0.0};
                 if (k < nk && j < cc.ncols) {
                     const cd sv = s_s[j];
-                    const double dx = sv.x - d.sgn * (d.Ek[k] - eh);
+                    const double dx = sv.x - d.sgn * (rek[u] - r_eh);
                     const double m2 = fma(dx, dx, sv.y * sv.y);
                     if (d.use_delta && m2 <= tol2) {
                         v = cd{cdl, 0.0};
@@ -176,31 +201,19 @@ __global__ void __launch_bounds__((BM / cg_tm(BM)) * CG_NX)
                         v = cd{dx * rr, -sv.y * rr};
                     }
                 }
+                Bs[buf][kk][j] = v;
             }
-            rb[u] = v;
-        }
-    };
-    auto store = [&](int buf) {
-#pragma unroll
-        for (int u = 0; u < LA; ++u) {
-            const int l = tid + u * NT;
-            if (l < BM * CG_BK) As[buf][l % CG_BK][l / CG_BK] = ra[u];
-        }
-#pragma unroll
-        for (int u = 0; u < LB; ++u) {
-            const int l = tid + u * NT;
-            if (l < BN * CG_BK) Bs[buf][l / BN][l % BN] = rb[u];
         }
     };
     if (nsteps > 0) {
-        load(0);
-        store(0);
+        fetch(0);
+        finish(0, 0);
     }
     __syncthreads();
     int buf = 0;
     for (long q = 0; q < nsteps; ++q) {
         const bool more = q + 1 < nsteps;
-        if (more) load(q + 1);
+        if (more) fetch(q + 1);
 #pragma unroll
         for (int kk = 0; kk < CG_BK; ++kk) {
             cd a[CG_TM], b[TN];
@@ -218,7 +231,7 @@ __global__ void __launch_bounds__((BM / cg_tm(BM)) * CG_NX)
                     acc[qa][qb].y = fma(a[qa].y, b[qb].x, acc[qa][qb].y);
                 }
         }
-        if (more) store(buf ^ 1);
+        if (more) finish(q + 1, buf ^ 1);
         __syncthreads();
         buf ^= 1;
     }
