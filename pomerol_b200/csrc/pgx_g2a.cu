@@ -411,9 +411,74 @@ void build_classes(APlan& pl, int k, cudaStream_t st) {
         c.rows.push_back(g);
         for (auto& e : el) c.slots.push_back(std::get<2>(e));
     }
+    // Classes of few rows (such as the z1 + z3 classes of the T2 sub-terms
+    // near the grid's corners) make 8- or 16-row tiles that leave the FP64 pipe
+    // idle.  Consecutive ones, in the order of their sum lists, are merged while
+    // the union of their sums stays within CG_BN_MAX columns and their rows
+    // within 64; a merged row holds -1 in the columns that are not its own, so
+    // its tile computes those products and drops them.
+    std::vector<HC> merged;
+    {
+        using QK = std::pair<long long, long long>;
+        auto qk = [&](cd v) { return QK{std::llround(v.x / q), std::llround(v.y / q)}; };
+        std::vector<int> group;
+        std::map<QK, cd> uni;
+        int grow = 0;
+        auto flush = [&]() {
+            if (group.size() == 1) merged.push_back(std::move(hc[group[0]]));
+            if (group.size() > 1) {
+                HC m;
+                std::map<QK, int> col;
+                for (auto& e : uni) {
+                    col[e.first] = (int)m.s.size();
+                    m.s.push_back(e.second);
+                }
+                const int w = (int)m.s.size();
+                for (int ci : group) {
+                    const HC& c = hc[ci];
+                    const int nc = (int)c.s.size();
+                    for (size_t r = 0; r < c.rows.size(); ++r) {
+                        m.rows.push_back(c.rows[r]);
+                        const size_t base = m.slots.size();
+                        m.slots.resize(base + w, -1);
+                        for (int j = 0; j < nc; ++j) m.slots[base + col[qk(c.s[j])]] = c.slots[r * nc + j];
+                    }
+                }
+                merged.push_back(std::move(m));
+            }
+            group.clear();
+            uni.clear();
+            grow = 0;
+        };
+        for (auto& e : idx) {  // classes in the order of their sum lists
+            const int ci = e.second;
+            const HC& c = hc[ci];
+            std::map<QK, cd> own;
+            for (const cd& v : c.s) own.emplace(qk(v), v);
+            // large classes, and classes holding one sum twice (one column each
+            // in a merged class would collide), stay as they are
+            if (c.rows.size() > 16 || own.size() != c.s.size()) {
+                flush();
+                group.push_back(ci);
+                flush();
+                continue;
+            }
+            std::map<QK, cd> u2 = uni;
+            u2.insert(own.begin(), own.end());
+            if (!group.empty() && ((int)u2.size() > CG_BN_MAX || grow + (int)c.rows.size() > 64)) {
+                flush();
+                uni = std::move(own);
+            } else {
+                uni = std::move(u2);
+            }
+            group.push_back(ci);
+            grow += (int)c.rows.size();
+        }
+        flush();
+    }
     // column chunks, then one device buffer for every class of this sum
     std::vector<HC> fin;
-    for (HC& c : hc) {
+    for (HC& c : merged) {
         const int nc = (int)c.s.size(), nr = (int)c.rows.size();
         for (int j0 = 0; j0 < nc; j0 += CG_BN_MAX) {
             const int w = std::min(CG_BN_MAX, nc - j0);
