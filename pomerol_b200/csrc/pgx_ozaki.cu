@@ -51,7 +51,10 @@ namespace {
 
 constexpr int OZ_BM = 128, OZ_BN = 256, OZ_BK = 128;  // tile rows, tile columns, k-block bytes
 constexpr int OZ_STAGES = 4;
-constexpr int OZ_GROUP_M = 8;
+// tiles run in groups of 16 row tiles: a wave of 148 CTAs then holds about 16
+// row tiles x 9 column tiles, near the minimum of the A and B panel bytes it
+// reads per k-block (16 KiB per row tile, 32 KiB per column tile)
+constexpr int OZ_GROUP_M = 16;
 constexpr int OZ_STAGE_BYTES = (OZ_BM + OZ_BN) * OZ_BK;  // 48 KiB
 constexpr int OZ_SMEM = OZ_STAGES * OZ_STAGE_BYTES + 1024 + 256;
 constexpr int OZ_TMEM_COLS = 2 * OZ_BN;  // two accumulators: all 512 columns
