@@ -29,6 +29,7 @@
 
 #include <array>
 #include <map>
+#include <set>
 #include <tuple>
 
 #include "pgx_common.cuh"
@@ -421,60 +422,87 @@ void build_classes(APlan& pl, int k, cudaStream_t st) {
     {
         using QK = std::pair<long long, long long>;
         auto qk = [&](cd v) { return QK{std::llround(v.x / q), std::llround(v.y / q)}; };
-        std::vector<int> group;
-        std::map<QK, cd> uni;
-        int grow = 0;
-        auto flush = [&]() {
-            if (group.size() == 1) merged.push_back(std::move(hc[group[0]]));
-            if (group.size() > 1) {
-                HC m;
-                std::map<QK, int> col;
-                for (auto& e : uni) {
-                    col[e.first] = (int)m.s.size();
-                    m.s.push_back(e.second);
+        // groups of consecutive small classes under a row cap (sums within CG_BN_MAX)
+        auto split_run = [&](const std::vector<int>& run, int cap) {
+            std::vector<std::vector<int>> out;
+            std::set<QK> uni;
+            int rows = 0;
+            for (int ci : run) {
+                std::set<QK> u2 = uni;
+                for (const cd& v : hc[ci].s) u2.insert(qk(v));
+                const int r = (int)hc[ci].rows.size();
+                if (!out.empty() && !out.back().empty() && ((int)u2.size() > CG_BN_MAX || rows + r > cap)) {
+                    out.emplace_back();
+                    uni.clear();
+                    for (const cd& v : hc[ci].s) uni.insert(qk(v));
+                    rows = 0;
+                } else {
+                    if (out.empty()) out.emplace_back();
+                    uni = std::move(u2);
                 }
-                const int w = (int)m.s.size();
-                for (int ci : group) {
-                    const HC& c = hc[ci];
-                    const int nc = (int)c.s.size();
-                    for (size_t r = 0; r < c.rows.size(); ++r) {
-                        m.rows.push_back(c.rows[r]);
-                        const size_t base = m.slots.size();
-                        m.slots.resize(base + w, -1);
-                        for (int j = 0; j < nc; ++j) m.slots[base + col[qk(c.s[j])]] = c.slots[r * nc + j];
-                    }
-                }
-                merged.push_back(std::move(m));
+                out.back().push_back(ci);
+                rows += r;
             }
-            group.clear();
-            uni.clear();
-            grow = 0;
+            return out;
         };
+        auto emit = [&](const std::vector<int>& group) {
+            if (group.size() == 1) {
+                merged.push_back(std::move(hc[group[0]]));
+                return;
+            }
+            std::map<QK, int> col;
+            std::map<QK, cd> uni;
+            for (int ci : group)
+                for (const cd& v : hc[ci].s) uni.emplace(qk(v), v);
+            HC m;
+            for (auto& e : uni) {
+                col[e.first] = (int)m.s.size();
+                m.s.push_back(e.second);
+            }
+            const int w = (int)m.s.size();
+            for (int ci : group) {
+                const HC& c = hc[ci];
+                const int nc = (int)c.s.size();
+                for (size_t r = 0; r < c.rows.size(); ++r) {
+                    m.rows.push_back(c.rows[r]);
+                    const size_t base = m.slots.size();
+                    m.slots.resize(base + w, -1);
+                    for (int j = 0; j < nc; ++j) m.slots[base + col[qk(c.s[j])]] = c.slots[r * nc + j];
+                }
+            }
+            merged.push_back(std::move(m));
+        };
+        // a run of consecutive small classes is cut into as few groups as 64
+        // rows allow, then re-cut with the rows spread evenly over that many
+        // groups, so that no group is left with a few rows
+        auto flush_run = [&](std::vector<int>& run) {
+            if (run.empty()) return;
+            int total = 0, big = 0;
+            for (int ci : run) {
+                total += (int)hc[ci].rows.size();
+                big = std::max(big, (int)hc[ci].rows.size());
+            }
+            const int ng = (int)split_run(run, 64).size();
+            const int cap = std::max(big, (total + ng - 1) / ng);
+            for (const auto& g : split_run(run, cap)) emit(g);
+            run.clear();
+        };
+        std::vector<int> run;
         for (auto& e : idx) {  // classes in the order of their sum lists
             const int ci = e.second;
             const HC& c = hc[ci];
-            std::map<QK, cd> own;
-            for (const cd& v : c.s) own.emplace(qk(v), v);
+            std::set<QK> own;
+            for (const cd& v : c.s) own.insert(qk(v));
             // large classes, and classes holding one sum twice (one column each
             // in a merged class would collide), stay as they are
             if (c.rows.size() > 16 || own.size() != c.s.size()) {
-                flush();
-                group.push_back(ci);
-                flush();
+                flush_run(run);
+                emit({ci});
                 continue;
             }
-            std::map<QK, cd> u2 = uni;
-            u2.insert(own.begin(), own.end());
-            if (!group.empty() && ((int)u2.size() > CG_BN_MAX || grow + (int)c.rows.size() > 64)) {
-                flush();
-                uni = std::move(own);
-            } else {
-                uni = std::move(u2);
-            }
-            group.push_back(ci);
-            grow += (int)c.rows.size();
+            run.push_back(ci);
         }
-        flush();
+        flush_run(run);
     }
     // column chunks, then one device buffer for every class of this sum
     std::vector<HC> fin;
