@@ -116,6 +116,7 @@ __device__ __forceinline__ double pow2i(int e) {
 // Digit base of the split and the weight of diagonal s of the product:
 // 254^-s / 127^2 (127 scales the leading digit of each operand).
 constexpr double OZ_BASE = 254.0;
+constexpr double OZ_ROUND = 6755399441055744.0;  // 1.5 2^52
 __device__ __forceinline__ double diag_weight(int s) {
     double w = 1.0 / (127.0 * 127.0);
     for (int t = 0; t < s; ++t) w *= 1.0 / OZ_BASE;
@@ -772,11 +773,16 @@ __global__ void __launch_bounds__(OP_THREADS) oz_prep_kernel(OzSrc q, int R, int
                     vr *= OZ_BASE;
                     vi *= OZ_BASE;
                 }
-                const double dr = rint(vr), di = rint(vi);
-                vr -= dr;
-                vi -= di;
-                wr[d] |= ((uint32_t)(int)dr & 0xFFu) << (8 * c);
-                wi[d] |= ((uint32_t)(int)di & 0xFFu) << (8 * c);
+                // round to nearest (ties to even) by adding and removing
+                // 1.5 2^52: for |v| <= 128 the sum is exact up to that rounding,
+                // and its low word holds the digit in two's complement, so the
+                // digit costs FP64 additions instead of conversions
+                const double tr = __dadd_rn(vr, OZ_ROUND), ti = __dadd_rn(vi, OZ_ROUND);
+                const double dr = __dsub_rn(tr, OZ_ROUND), di = __dsub_rn(ti, OZ_ROUND);
+                vr = __dsub_rn(vr, dr);
+                vi = __dsub_rn(vi, di);
+                wr[d] |= ((uint32_t)__double2loint(tr) & 0xFFu) << (8 * c);
+                wi[d] |= ((uint32_t)__double2loint(ti) & 0xFFu) << (8 * c);
             }
         }
         if (r0 + rr >= R) continue;
