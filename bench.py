@@ -272,7 +272,7 @@ def cpu_baseline_from_engine(config, run, z):
 
 
 # ------------------------------------------------------------------ GPU side
-def roofline_entry(top, steps, torch, config, slices=6):
+def roofline_entry(top, steps, torch, config):
     """Dominant kernel of the timed steps: algorithmic work per launch over its
     average event-timed duration, against the peak of the pipe it runs on."""
     if not top or top["ms"] <= 0:
@@ -291,10 +291,10 @@ def roofline_entry(top, steps, torch, config, slices=6):
             cap = {}
     algo_bytes = top.get("bytes", 0.0) / top["launches"]
     if name.startswith("oz_gemm"):
-        # int8 tensor-core split products: 4 real products x S(S+1)/2 digit
-        # products of int8 multiply-adds per complex multiply-add (60 at five
-        # digits); flops were recorded as 8 per complex multiply-add
-        int8_ops = top["flops"] / 8.0 * (4.0 * slices * (slices + 1) / 2) * 2.0 / top["launches"]
+        # int8 tensor-core split products: the range records int8 operations
+        # (2 per multiply-add; 4 real multiply-adds in each of a product's
+        # S(S+1)/2 digit products per complex multiply-add, S per product)
+        int8_ops = top["flops"] / top["launches"]
         peak = 2.0 * peaks["bf16_tflops"] if peaks.get("bf16_tflops") else 2.0 * 1590.0
         achieved = int8_ops / per_launch_s / 1e12
         traffic = cap["dram_bytes_per_int8_mac"] * int8_ops / 2.0 if cap.get("dram_bytes_per_int8_mac") else None
@@ -305,7 +305,6 @@ def roofline_entry(top, steps, torch, config, slices=6):
                 "traffic_over_algorithmic": traffic / algo_bytes if traffic and algo_bytes else None,
                 "peak_source": ("2 x MEASURED_PEAKS.json bf16_tflops (dense int8 runs at twice the bf16 rate on "
                                 "the B200 tensor cores)" if peaks.get("bf16_tflops") else "2 x fallback bf16 1590"),
-                "fp64_equivalent_tflops": top["flops"] / top["launches"] / per_launch_s / 1e12,
                 "launches_per_step": top["launches"] / steps, "ms_per_launch": per_launch_s * 1e3,
                 "algorithmic_ops_per_launch": int8_ops}
     peak = fp64_peak_tflops(torch)
@@ -455,7 +454,7 @@ def run_ours_ring8(args, rank, world, local_rank):
     if rank != 0:
         return
     top = kstats[0] if kstats else None
-    roof = roofline_entry(top, args.steps, torch, "ring8", cfg["slices"])
+    roof = roofline_entry(top, args.steps, torch, "ring8")
     if roof is not None:
         roof["kernels_ms_per_step"] = {k["name"]: round(k["ms"] / args.steps, 3) for k in kstats}
     cpu = None
@@ -475,7 +474,8 @@ def run_ours_ring8(args, rank, world, local_rank):
                    "step": "one batch of block chains over the whole 24^3 grid; 20 steps = one full G2",
                    "anchor_tol": cfg["anchor_tol"], "anchor_states": int(sum(anchors)),
                    "anchor_dropped_weight": dropped_w,
-                   "products": f"int8 tensor-core split (Ozaki, {cfg['slices']} balanced base-254 digits) for products >= 1e9 "
+                   "products": f"int8 tensor-core split (Ozaki, {cfg['slices']} balanced base-254 digits, fewer for anchor blocks "
+                               "whose largest weight is far below the dominant one: weight budget 4) for products >= 1e9 "
                                "multiply-adds",
                    "l2": "flushed (256 MB write) between timed steps; working set of a step is several GB",
                    "pole_resolution": POLE_RES, "nz_tol": NZ_TOL, "coef_tol": COEF_TOL},

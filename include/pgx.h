@@ -254,6 +254,15 @@ int pgx_set_g2_split_threshold(pgx_ctx* ctx, double min_macs);
  * computes in FP64 only. */
 int pgx_set_g2_split_slices(pgx_ctx* ctx, int32_t slices);
 
+/* With PGX_G2_SPLIT_I8: digits per product from its anchor states' weights
+ * (no counterpart in the reference).  A product's error reaches G2 multiplied
+ * by the Boltzmann weights of its anchor block, so a block whose largest
+ * weight is below the overall largest by budget x 254^k or more runs its
+ * products with k fewer digits (at least 3): none then carries more than
+ * `budget` times the G2 error of a full-digit product of the dominant block.
+ * Default 4; budget <= 0 gives every product `slices` digits. */
+int pgx_set_g2_split_weight_budget(pgx_ctx* ctx, double budget);
+
 /* Tile shape of the int8 split products (no counterpart in the reference):
  * 0 (default) runs 128 x 256 tiles on single CTAs, 1 runs 256 x 256 tiles on
  * pairs of CTAs (tcgen05 cta_group::2, each SM loading half of the tile's

@@ -483,6 +483,13 @@ int pgx_set_g2_split_threshold(pgx_ctx* c, double min_macs) {
     });
 }
 
+int pgx_set_g2_split_weight_budget(pgx_ctx* c, double budget) {
+    return guarded(c, [&] {
+        PGX_CHECK(std::isfinite(budget), PGX_ERR_ARG, "budget must be finite");
+        c->g2_split_weight_budget = budget;
+    });
+}
+
 int pgx_set_split_cta_pair(pgx_ctx* c, int32_t cta_pair) {
     return guarded(c, [&] {
         PGX_CHECK(cta_pair == 0 || cta_pair == 1, PGX_ERR_ARG, "cta_pair must be 0 or 1");

@@ -639,7 +639,8 @@ template <typename T>
 static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector<int>& bplan,
                       const std::vector<ChainWs>& wsl, const pgx_g2_part* parts, std::vector<APlan>& plans,
                       const std::vector<std::array<int, 4>>& rs, cd* pool, const int* d_hot,
-                      const std::vector<long>& hot_off, double pole_res, int split, cd* d_out) {
+                      const std::vector<long>& hot_off, double pole_res, int split, const std::vector<int>& bdig,
+                      cd* d_out) {
     Problem& P = c->P;
     cudaStream_t st = c->stream;
     constexpr bool TC = is_cd<T>::value;
@@ -651,6 +652,12 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
     std::vector<GemmProblem<DT, T, cd>> pb;   // dressed x operator
     std::vector<GemmProblem<DT, cd, cd>> pc;  // dressed x stacked anchors (per z1 or z3)
     std::vector<GemmProblem<cd, DT, cd>> pd;  // stacked anchors x dressed
+    // digits of each split product: those of its anchor block (bdig)
+    std::vector<int> pa_d, pb_d, pc_d, pd_d;
+    auto push = [&](auto& list, std::vector<int>& digs, int anchor_block, const auto& prob) {
+        list.push_back(prob);
+        digs.push_back(bdig.empty() ? split : bdig[anchor_block]);
+    };
     for (size_t j = 0; j < idx.size(); ++j) {
         const int q = idx[j];
         const pgx_g2_part& g = parts[q];
@@ -672,30 +679,30 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
         const Dress C3{E3, E4, pl.dZ3};  // C3(z3) = O3 dressed with z3: d3 x d4, row-major
         // anchored products, one item per z1 (or z3)
         // outputs that the contractions read along k are stored k-contiguous
-        if (r2) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lc, 1, d4, r2, d1, nullptr, H2, A1, N1,
+        if (r2) push(pa, pa_d, S2, gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lc, 1, d4, r2, d1, nullptr, H2, A1, N1,
                                        (long)r2 * d4, d4));                               // Lc = X4 A1[:,H2]: [(i1,h)][k]
-        if (r4) pa.push_back(gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lr, d2, r4, d2, d1, H4, nullptr, A1, N1,
+        if (r4) push(pa, pa_d, S4, gp<T, DT>(X4, d1, 1, O1, d2, 1, pool + w.Lr, d2, r4, d2, d1, H4, nullptr, A1, N1,
                                        (long)r4 * d2));                                   // Lr = X4[H4,:] A1
-        if (r1) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pr, d3, r1, d3, d2, H1, nullptr, A1, N1,
+        if (r1) push(pb, pb_d, S1, gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pr, d3, r1, d3, d2, H1, nullptr, A1, N1,
                                        (long)r1 * d3));                                   // Pr = A1[H1,:] O2
-        if (r3) pb.push_back(gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pc, 1, d1, r3, d2, nullptr, H3, A1, N1,
+        if (r3) push(pb, pb_d, S3, gp<DT, T>(O1, d2, 1, O2, d3, 1, pool + w.Pc, 1, d1, r3, d2, nullptr, H3, A1, N1,
                                        (long)d1 * r3, d1));                               // Pc = A1 O2[:,H3]: [i1][h][k]
-        if (r3) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Rho, d1, r3, d1, d4, H3, nullptr, C3, N3,
+        if (r3) push(pb, pb_d, S3, gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Rho, d1, r3, d1, d4, H3, nullptr, C3, N3,
                                        (long)r3 * d1));                                   // rho = C3[H3,:] X4
-        if (r1) pb.push_back(gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Qc, 1, d3, r1, d4, nullptr, H1, C3, N3,
+        if (r1) push(pb, pb_d, S1, gp<DT, T>(O3, d4, 1, X4, d1, 1, pool + w.Qc, 1, d3, r1, d4, nullptr, H1, C3, N3,
                                        (long)d3 * r1, d3));                               // Qc = C3 X4[:,H1]: [i3][h][k]
-        if (r2) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rr, d4, r2, d4, d3, H2, nullptr, C3, N3,
+        if (r2) push(pa, pa_d, S2, gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rr, d4, r2, d4, d3, H2, nullptr, C3, N3,
                                        (long)r2 * d4));                                   // Rr = O2[H2,:] C3
-        if (r4) pa.push_back(gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rc, 1, d2, r4, d3, nullptr, H4, C3, N3,
+        if (r4) push(pa, pa_d, S4, gp<T, DT>(O2, d3, 1, O3, d4, 1, pool + w.Rc, 1, d2, r4, d3, nullptr, H4, C3, N3,
                                        (long)r4 * d2, d2));                               // Rc = O2 C3[:,H4]: [(i3,h)][k]
         // products over (z1, z3): anchors of all frequencies stacked as columns / rows
-        if (r2) pc.push_back(gp<DT, cd>(O3, d4, 1, pool + w.Lc, 1, d4, pool + w.V1a, 1, d3, N1 * r2, d4, nullptr,
+        if (r2) push(pc, pc_d, S2, gp<DT, cd>(O3, d4, 1, pool + w.Lc, 1, d4, pool + w.V1a, 1, d3, N1 * r2, d4, nullptr,
                                         nullptr, C3, N3, (long)d3 * N1 * r2, d3));  // V1a = C3 LcAll: [i3][(i1,h)][k]
-        if (r1) pd.push_back(gp<cd, DT>(pool + w.Pr, d3, 1, O3, d4, 1, pool + w.V2a, d4, N1 * r1, d4, d3, nullptr, nullptr,
+        if (r1) push(pd, pd_d, S1, gp<cd, DT>(pool + w.Pr, d3, 1, O3, d4, 1, pool + w.V2a, d4, N1 * r1, d4, d3, nullptr, nullptr,
                                         C3, N3, (long)N1 * r1 * d4));                         // V2a = PrAll C3
-        if (r3) pd.push_back(gp<cd, DT>(pool + w.Rho, d1, 1, O1, d2, 1, pool + w.V1b, d2, N3 * r3, d2, d1, nullptr, nullptr,
+        if (r3) push(pd, pd_d, S3, gp<cd, DT>(pool + w.Rho, d1, 1, O1, d2, 1, pool + w.V1b, d2, N3 * r3, d2, d1, nullptr, nullptr,
                                         A1, N1, (long)N3 * r3 * d2));                         // V1b = rhoAll A1
-        if (r4) pc.push_back(gp<DT, cd>(O1, d2, 1, pool + w.Rc, 1, d2, pool + w.V2b, 1, d1, N3 * r4, d2, nullptr,
+        if (r4) push(pc, pc_d, S4, gp<DT, cd>(O1, d2, 1, pool + w.Rc, 1, d2, pool + w.V2b, 1, d1, N3 * r4, d2, nullptr,
                                         nullptr, A1, N1, (long)d1 * N3 * r4, d1));  // V2b = A1 RcAll: [i1][(i3,h)][k]
     }
     // descriptor buffers: one region per product list, sized once for the
@@ -717,15 +724,16 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
     // ones, such as every product of a 400-state block, run faster on the FP64
     // tiles than their digit preparation and 128 x 256 tile padding allow.
     // Complex Hamiltonians keep the anchored products in FP64.
-    auto launch_split = [&](auto& probs, int region) {
+    auto launch_split = [&](auto& probs, const std::vector<int>& digs, int region) {
         std::remove_reference_t<decltype(probs)> rest;
-        for (const auto& g : probs) {
+        for (size_t i = 0; i < probs.size(); ++i) {
+            const auto& g = probs[i];
             const double macs = (double)g.M * g.N * g.K * std::max(g.nb, 1);
             if (macs < c->g2_split_min_macs) {
                 rest.push_back(g);
                 continue;
             }
-            oz_zgemm(g, split, c->oz, st);
+            oz_zgemm(g, digs[i], c->oz, st);
         }
         launch_on(rest, region, st);
     };
@@ -734,11 +742,11 @@ static void run_batch(pgx_ctx* c, const std::vector<int>& idx, const std::vector
             launch_on(pa, 0, st);
             launch_on(pb, 1, st);
         } else {
-            launch_split(pa, 0);
-            launch_split(pb, 1);
+            launch_split(pa, pa_d, 0);
+            launch_split(pb, pb_d, 1);
         }
-        launch_split(pc, 2);
-        launch_split(pd, 3);
+        launch_split(pc, pc_d, 2);
+        launch_split(pd, pd_d, 3);
     } else {
         // pa and pb are independent, and so are pc and pd (each needs both of
         // the first pair): each pair runs on two side streams at once
@@ -932,6 +940,27 @@ void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq
         nhot[b] = (int)(hot.size() - hot_off[b]);
     }
     hot_off[P.nblocks] = (long)hot.size();
+    // Digits of the split products per anchor block.  A product's error
+    // reaches G2 multiplied by the Boltzmann weights of its anchor states, so a
+    // block whose largest weight is a factor 254^k below the overall largest
+    // (with the budget F of pgx_set_g2_split_weight_budget as allowance) drops
+    // k digits, each of which multiplies the product's error by about 254: no
+    // product then carries more than F times the error of a product of the
+    // dominant block at the full digit count.  At least 3 digits are kept.
+    std::vector<int> bdig;
+    if (split > 0 && c->g2_split_weight_budget > 0.0) {
+        double wall = 0.0;
+        std::vector<double> wb(P.nblocks, 0.0);
+        for (int b = 0; b < P.nblocks; ++b)
+            for (int i = 0; i < P.dims[b]; ++i) wb[b] = std::max(wb[b], w[P.eoff[b] + i]);
+        for (double x : wb) wall = std::max(wall, x);
+        bdig.assign(P.nblocks, split);
+        for (int b = 0; b < P.nblocks; ++b) {
+            if (!(wb[b] > 0.0) || !(wall > 0.0)) continue;
+            const int k = (int)std::floor(std::log(c->g2_split_weight_budget * wall / wb[b]) / std::log(254.0));
+            bdig[b] = std::max(std::min(3, split), split - std::max(0, k));
+        }
+    }
     DevBuf& bh = c->scratch[11];
     bh.reserve(std::max<size_t>(hot.size(), 1) * sizeof(int));
     if (!hot.empty()) h2d(bh.p, hot.data(), hot.size() * sizeof(int), st);
@@ -1049,10 +1078,10 @@ void run_g2_anchored(pgx_ctx* c, int nparts, const pgx_g2_part* parts, int nfreq
         pool_b.reserve(std::max<long>(used, 1) * sizeof(cd));
         if (P.is_complex)
             run_batch<cd>(c, batch, bplan, bws, parts, plans, rs, pool_b.as<cd>(), bh.as<int>(), hot_off, pole_res,
-                          split, out_b.as<cd>());
+                          split, bdig, out_b.as<cd>());
         else
             run_batch<double>(c, batch, bplan, bws, parts, plans, rs, pool_b.as<cd>(), bh.as<int>(), hot_off, pole_res,
-                              split, out_b.as<cd>());
+                              split, bdig, out_b.as<cd>());
         batch.clear();
         bplan.clear();
         bws.clear();

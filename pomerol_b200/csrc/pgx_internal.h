@@ -309,6 +309,7 @@ struct pgx_ctx {
     cudaStream_t aux[4] = {nullptr, nullptr, nullptr, nullptr};
     long long g2_batch_bytes = 0, g2_chain_bytes = 0;  // pgx_set_g2_workspace (0: defaults)
     double g2_split_min_macs = 1e9;                     // pgx_set_g2_split_threshold
+    double g2_split_weight_budget = 4.0;                // pgx_set_g2_split_weight_budget (<= 0: every product at full digits)
     int g2_split_slices = 6;                            // pgx_set_g2_split_slices
     pgx::OzWork oz;                                     // int8 split products
     cudaEvent_t fork = nullptr, join[4] = {nullptr, nullptr, nullptr, nullptr};

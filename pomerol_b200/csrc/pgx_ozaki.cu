@@ -959,9 +959,10 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
         a.sc_i = g.sc_i;
         a.sc_j = g.sc_j;
         a.err = w.err.as<int>();
-        // algorithmic work: 8 FP64-equivalent FLOP per complex multiply-add;
+        // algorithmic work, as int8 operations (2 per multiply-add): per complex
+        // multiply-add 4 real ones in each of the S(S+1)/2 digit products;
         // minimum traffic: the digits of both operands once and C written once
-        const double fl = 8.0 * (double)M * N * K * cn;
+        const double fl = 2.0 * 4.0 * (S * (S + 1) / 2) * (double)M * N * K * cn;
         const double by = (double)(a_item ? cn : 1) * a_bytes + (double)(b_item ? cn : 1) * b_bytes +
                           16.0 * (double)M * N * cn;
         if (pair) {  // 256 x 256 tiles, one per CTA pair

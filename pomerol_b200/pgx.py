@@ -25,7 +25,7 @@ EXPORTS = [
     "pgx_launch_count", "pgx_eigh_noalloc", "pgx_profile_begin", "pgx_profile_end", "pgx_profile_kernel",
     "pgx_recip_check", "pgx_assemble_hamiltonian", "pgx_get_hamiltonian", "pgx_op_release",
     "pgx_gf_vjp", "pgx_susc_vjp", "pgx_chi3", "pgx_set_eigensystem", "pgx_autotune_begin", "pgx_autotune_end",
-    "pgx_set_g2_workspace", "pgx_set_g2_split_threshold", "pgx_set_g2_split_slices", "pgx_set_split_cta_pair", "pgx_split_gemm_check", "pgx_graph_begin", "pgx_graph_end",
+    "pgx_set_g2_workspace", "pgx_set_g2_split_threshold", "pgx_set_g2_split_slices", "pgx_set_g2_split_weight_budget", "pgx_set_split_cta_pair", "pgx_split_gemm_check", "pgx_graph_begin", "pgx_graph_end",
     "pgx_graph_replay", "pgx_graph_destroy", "pgx_set_models", "pgx_weights_models", "pgx_gf_models", "pgx_susc_models",
 ]
 
@@ -92,6 +92,7 @@ def load():
         lib.pgx_set_g2_split_threshold.argtypes = [P, C.c_double]
         lib.pgx_set_g2_split_slices.argtypes = [P, I32]
         lib.pgx_set_split_cta_pair.argtypes = [P, I32]
+        lib.pgx_set_g2_split_weight_budget.argtypes = [P, D]
         lib.pgx_split_gemm_check.argtypes = [P, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.c_uint64,
                                              P, P, P]
         lib.pgx_autotune_end.argtypes = [P, P]
@@ -438,6 +439,12 @@ def _set_g2_split_slices(self, slices=6):
     self._ck(self.lib.pgx_set_g2_split_slices(self.h, int(slices)))
 
 
+def _set_g2_split_weight_budget(self, budget=4.0):
+    """Digits of each split product from its anchor block's largest weight;
+    budget <= 0 gives every product the full digit count."""
+    self._ck(self.lib.pgx_set_g2_split_weight_budget(self.h, float(budget)))
+
+
 def _set_split_cta_pair(self, on=True):
     """256 x 256 split-product tiles on CTA pairs (True) or 128 x 256 tiles on
     single CTAs (False)."""
@@ -563,6 +570,7 @@ Engine.split_gemm_check = _split_gemm_check
 Engine.set_g2_split_threshold = _set_g2_split_threshold
 Engine.set_g2_split_slices = _set_g2_split_slices
 Engine.set_split_cta_pair = _set_split_cta_pair
+Engine.set_g2_split_weight_budget = _set_g2_split_weight_budget
 Engine.autotune_begin = _autotune_begin
 Engine.autotune_end = _autotune_end
 Engine.graph_end = _graph_end

@@ -54,11 +54,14 @@ def test_ring8_g_and_chi_zz(ring8):
     assert np.abs(zz - ref).max() < 1e-10 * np.abs(ref).max()
 
 
-@pytest.mark.parametrize("split,tol,slices", [(False, 1e-16, 6), (True, 1e-16, 6), (True, 1e-13, 6), (True, 1e-13, 5)])
-def test_ring8_g2_sample(ring8, split, tol, slices):
-    """Five base-254 digits per element (the benchmark's setting for this
-    model) leave about 250 times the product error of six; both stay far
-    below 1e-8."""
+@pytest.mark.parametrize("split,tol,slices,budget", [(False, 1e-16, 6, 0.0), (True, 1e-16, 6, 0.0), (True, 1e-13, 6, 0.0),
+                                                     (True, 1e-13, 5, 0.0), (True, 1e-13, 5, 4.0)])
+def test_ring8_g2_sample(ring8, split, tol, slices, budget):
+    """Five base-254 digits per element leave about 250 times the product
+    error of six; both stay far below 1e-8.  With the weight budget (the
+    benchmark's setting: five digits, budget 4), products of anchor blocks
+    whose largest Boltzmann weight is far below the dominant one run with
+    fewer digits; the error stays within a few times that of five digits."""
     from pomerol_b200.pgx import PGX_G2_ANCHORED, PGX_G2_SPLIT_I8
     g, m, doc = ring8
     u, d = m.info.getIndex("S0", 0, 1), m.info.getIndex("S0", 0, 0)
@@ -69,14 +72,16 @@ def test_ring8_g2_sample(ring8, split, tol, slices):
     if split:
         g.eng.set_g2_split_threshold(0.0)  # every stacked and anchored product on the tensor cores
         g.eng.set_g2_split_slices(slices)
+        g.eng.set_g2_split_weight_budget(budget)
     try:
         v = g.eng.g2(parts, fz, pole_res=1e-8, coef_tol=tol, flags=flags)
     finally:
         g.eng.set_g2_split_threshold(1e9)
         g.eng.set_g2_split_slices(6)
+        g.eng.set_g2_split_weight_budget(4.0)
     ref = _c(doc["g2"])
     err = np.abs(v - ref).max() / np.abs(ref).max()
-    print(f"ring8 G2 split={split} anchor_tol={tol:g} slices={slices}: max|diff|/max|G2| = {err:.2e}")
+    print(f"ring8 G2 split={split} anchor_tol={tol:g} slices={slices} budget={budget:g}: max|diff|/max|G2| = {err:.2e}")
     assert err < 1e-8
     if not split:
         assert err < 1e-11  # FP64 products with the oracle's own anchor threshold
