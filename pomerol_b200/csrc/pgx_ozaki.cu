@@ -891,11 +891,15 @@ void oz_zgemm(const GemmProblem<TA, TB, cd>& g, int S, OzWork& w, cudaStream_t s
         w.err.reserve(sizeof(int));
         PGX_CUDA(cudaMemsetAsync(w.err.p, 0, sizeof(int), st));
     }
-    static bool attr = false;
-    if (!attr) {
+    // the shared-memory opt-in is a property of each device's context: set it
+    // once per device (every time for device numbers beyond the table)
+    static bool attr[64] = {};
+    int dev = 0;
+    PGX_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64 || !attr[dev]) {
         PGX_CUDA(cudaFuncSetAttribute(oz_gemm_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ_SMEM));
         PGX_CUDA(cudaFuncSetAttribute(oz_gemm_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, OZ2_SMEM));
-        attr = true;
+        if (dev >= 0 && dev < 64) attr[dev] = true;
     }
     using SA = typename src_t<TA>::type;
     using SB = typename src_t<TB>::type;
