@@ -16,6 +16,11 @@ import time
 import numpy as np
 
 
+def _unit(name):
+    """The split-product ranges record int8 operations, the others FP64 ones."""
+    return "TOPS(i8)" if name.startswith("oz_gemm") else "TFLOP/s "
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--config", default="a5")
@@ -81,7 +86,8 @@ def main():
         if last:
             for k in run.eng.profile_end():
                 print(f"  {k['name']:40s} x{k['launches']:<3d} {k['ms']:9.3f} ms  "
-                      f"{k['flops'] / max(k['ms'], 1e-9) / 1e9:9.3f} TFLOP/s  {k['bytes'] / max(k['ms'], 1e-9) / 1e6:9.2f} GB/s")
+                      f"{k['flops'] / max(k['ms'], 1e-9) / 1e9:9.3f} {_unit(k['name'])}  "
+                      f"{k['bytes'] / max(k['ms'], 1e-9) / 1e6:9.2f} GB/s")
         extra = "" if a.chi3 else f"g2 {run.eng.g2_timing()}, "
         print(f"step {s}: device {ms:.1f} ms, wall {1e3 * (time.perf_counter() - t0):.1f} ms, "
               f"{extra}|v|max {np.abs(v).max():.4e}", flush=True)
